@@ -1,0 +1,383 @@
+// C ABI of the B200 Cowling GRMHD stage library (include/grace_b200.h).
+//
+// Host orchestration only: validates arguments, owns the scratch arrays
+// (the reference keeps them in the variable_list singleton,
+// src/data_structures/variables.cpp:100-211), and launches the kernels of
+// stage_kernels.cuh / fused_kernels.cuh on the caller's stream.  No call
+// here synchronises the stream except grb_get_status and grb_reserve.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "grace_b200.h"
+#include "stage_kernels.cuh"
+
+using namespace grb;
+
+struct grb_handle {
+  grb_params p;
+  DevParams dp;
+  Geo geo;
+  bool reserved = false;
+  int64_t cap_f = 0, cap_c = 0;  // capacities (elements) of face-grid / cell scratch
+  StageBufs B{};
+  uint32_t* d_flags = nullptr;
+  unsigned long long* d_counters = nullptr;
+  int last_error = GRB_OK;
+};
+
+namespace {
+
+int fail(grb_handle* h, int code) {
+  if (h) h->last_error = code;
+  return code;
+}
+#define CK(call)                                       \
+  do {                                                 \
+    cudaError_t e_ = (call);                           \
+    if (e_ != cudaSuccess) return fail(h, GRB_ERR_CUDA); \
+  } while (0)
+
+DevParams to_dev(const grb_params& p) {
+  DevParams d{};
+  DevEos& e = d.eos;
+  e.kind = p.eos.kind;
+  e.eps_max = p.eos.eps_max;
+  if (p.eos.kind == GRB_EOS_IDEAL_GAS) {
+    // ideal_gas_eos.hh:56-86
+    e.rhomax = 1e100; e.rhomin = 1e-100; e.tempmax = 1e100; e.yemax = 1e100;
+    e.h_min = 1. + 1e-15;
+    e.gm1 = p.eos.gamma - 1.;
+    e.g = e.gm1 + 1.;
+    e.ggm1 = e.g * e.gm1;
+    e.ent_min = (p.eos.temp_atm > 0.0) ? (p.eos.temp_atm / e.gm1) : 1e-100;
+    e.n = 1;
+  } else {
+    // hybrid_eos.hh:62-75 with the polytrope bounds of eos_storage.cpp:143-150
+    e.rhomax = 1e10; e.rhomin = 1e-100; e.tempmax = 1e99; e.yemax = 1e99;
+    e.h_min = 1. + 1e-10;
+    e.gthm1 = p.eos.gamma_th - 1.;
+    e.entropy_min = p.eos.entropy_min;
+    e.n = p.eos.n_pieces;
+    for (int i = 0; i < GRB_MAX_PIECES; ++i) {
+      e.K[i] = p.eos.pw_kappa[i]; e.G[i] = p.eos.pw_gamma[i];
+      e.R[i] = p.eos.pw_rho[i]; e.E[i] = p.eos.pw_eps[i];
+    }
+  }
+  d.rho_fl = p.rho_fl; d.ye_fl = p.ye_fl; d.temp_fl = p.temp_fl; d.atmo_tol = p.atmo_tol;
+  d.excise_by_radius = p.excise_by_radius; d.r_ex = p.r_ex; d.alp_ex = p.alp_ex;
+  d.tol = p.c2p_tol; d.max_w = p.max_w; d.max_sigma = p.max_sigma;
+  d.beta_fallback = p.beta_fallback; d.alp_bh_thresh = p.alp_bh_thresh;
+  d.use_ent_backup = p.use_ent_backup;
+  d.rusanov_c_limit = p.rusanov_use_c_limit;
+  d.fofc = p.fofc_enable; d.dmp_enable = p.dmp_enable; d.dmp_M = p.dmp_M;
+  d.recon = p.recon; d.riemann = p.riemann; d.emf = p.emf;
+  return d;
+}
+
+bool valid_params(const grb_params* p) {
+  if (!p) return false;
+  if (p->eos.kind != GRB_EOS_IDEAL_GAS && p->eos.kind != GRB_EOS_HYBRID_PWPOLY) return false;
+  if (p->eos.kind == GRB_EOS_HYBRID_PWPOLY && (p->eos.n_pieces < 1 || p->eos.n_pieces > GRB_MAX_PIECES)) return false;
+  if (p->recon < GRB_RECON_WENOZ || p->recon > GRB_RECON_DONOR) return false;
+  if (p->riemann != GRB_RIEMANN_HLL && p->riemann != GRB_RIEMANN_LLF) return false;
+  if (p->emf != GRB_EMF_GS && p->emf != GRB_EMF_UCT) return false;
+  // flag_fofc_cells asserts on UCT (evolve.cpp:479-481)
+  if (p->fofc_enable && p->emf == GRB_EMF_UCT) return false;
+  return true;
+}
+
+bool same_geo(const Geo& a, const grb_grid* g) {
+  return a.nx == g->nx && a.ny == g->ny && a.nz == g->nz && a.g == g->ngz && a.nq == g->nq;
+}
+
+int check_grid(grb_handle* h, const grb_grid* g) {
+  if (!g || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->nq < 1 || !g->idx) return GRB_ERR_INVALID;
+  if (g->ngz < 4) return GRB_ERR_INVALID;  // WENO-Z + FOFC need ngz >= 4 (evolve.cpp:476-478)
+  if (!h->reserved) return GRB_ERR_NOT_RESERVED;
+  const Geo t = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  if (t.fcells * t.nq > h->cap_f || t.cells * t.nq > h->cap_c) return GRB_ERR_NOT_RESERVED;
+  if (h->p.excise_by_radius && !g->coords) return GRB_ERR_INVALID;
+  return GRB_OK;
+}
+
+inline Box box(int l0, int l1, int l2, int n0, int n1, int n2, int64_t nq) {
+  Box b;
+  b.lo[0] = l0; b.lo[1] = l1; b.lo[2] = l2;
+  b.n[0] = n0; b.n[1] = n1; b.n[2] = n2;
+  b.nq = nq;
+  return b;
+}
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+extern "C" {
+
+void grb_params_defaults(grb_params* p, int32_t eos_kind) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->eos.kind = eos_kind;
+  p->eos.n_pieces = 1;
+  p->eos.gamma = 5.0 / 3.0;
+  p->eos.gamma_th = 1.8;
+  p->eos.eps_max = 1.0e5;
+  p->eos.entropy_min = 1.0e-13;
+  p->eos.temp_atm = 0.0;
+  p->rho_fl = 1.0e-14; p->ye_fl = 0.0; p->temp_fl = 0.0; p->atmo_tol = 1.0e-3;
+  p->excise_by_radius = 0; p->r_ex = 1.0; p->alp_ex = 0.05; p->rho_ex = 1.0e-14;
+  p->temp_ex = 0.0; p->ye_ex = 0.0;
+  p->c2p_tol = 1.0e-10; p->max_w = 50.0; p->max_sigma = 100.0; p->beta_fallback = 1.0e-2;
+  p->alp_bh_thresh = 0.2; p->use_ent_backup = 1;
+  p->rusanov_use_c_limit = 0.0;
+  p->fofc_enable = 1; p->dmp_enable = 1; p->dmp_M = 1.2;
+  p->recon = GRB_RECON_WENOZ; p->riemann = GRB_RIEMANN_HLL; p->emf = GRB_EMF_GS;
+}
+
+int grb_eos_setup_pwpoly(grb_eos_params* e, int32_t n, double kappa_0, const double* gammas,
+                         const double* rhos) {
+  if (!e || n < 1 || n > GRB_MAX_PIECES || !gammas || (n > 1 && !rhos)) return GRB_ERR_INVALID;
+  double r[GRB_MAX_PIECES] = {0.0};
+  for (int i = 1; i < n; ++i) r[i] = rhos[i - 1];
+  for (int i = 0; i + 1 < n; ++i)
+    if (!(r[i + 1] > r[i])) return GRB_ERR_INVALID;
+  double k[GRB_MAX_PIECES] = {0}, ep[GRB_MAX_PIECES] = {0}, pr[GRB_MAX_PIECES] = {0};
+  k[0] = kappa_0;
+  for (int i = 1; i < n; ++i) {
+    k[i] = k[i - 1] * std::pow(r[i], gammas[i - 1] - gammas[i]);
+    ep[i] = ep[i - 1] + k[i - 1] * std::pow(r[i], gammas[i - 1] - 1.) / (gammas[i - 1] - 1.) -
+            k[i] * std::pow(r[i], gammas[i] - 1.) / (gammas[i] - 1.);
+    pr[i] = k[i] * std::pow(r[i], gammas[i]);
+  }
+  e->n_pieces = n;
+  for (int i = 0; i < GRB_MAX_PIECES; ++i) {
+    e->pw_kappa[i] = i < n ? k[i] : 0.0;
+    e->pw_gamma[i] = i < n ? gammas[i] : 0.0;
+    e->pw_rho[i] = i < n ? r[i] : 0.0;
+    e->pw_eps[i] = i < n ? ep[i] : 0.0;
+    e->pw_press[i] = i < n ? pr[i] : 0.0;
+  }
+  return GRB_OK;
+}
+
+int grb_create(grb_handle** out, const grb_params* p) {
+  if (!out) return GRB_ERR_INVALID;
+  *out = nullptr;
+  if (!valid_params(p)) return GRB_ERR_INVALID;
+  grb_handle* h = new (std::nothrow) grb_handle();
+  if (!h) return GRB_ERR_NOMEM;
+  h->p = *p;
+  h->dp = to_dev(*p);
+  if (cudaMalloc(&h->d_flags, sizeof(uint32_t)) != cudaSuccess ||
+      cudaMalloc(&h->d_counters, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+    cudaFree(h->d_flags);
+    delete h;
+    return GRB_ERR_CUDA;
+  }
+  cudaMemset(h->d_flags, 0, sizeof(uint32_t));
+  cudaMemset(h->d_counters, 0, 2 * sizeof(unsigned long long));
+  *out = h;
+  return GRB_OK;
+}
+
+static void free_scratch(grb_handle* h) {
+  cudaFree(h->B.flux); cudaFree(h->B.eface); cudaFree(h->B.vbar); cudaFree(h->B.ecenter);
+  cudaFree(h->B.emf); cudaFree(h->B.ftag); cudaFree(h->B.etag);
+  h->B.flux = h->B.eface = h->B.vbar = h->B.ecenter = h->B.emf = nullptr;
+  h->B.ftag = h->B.etag = nullptr;
+  h->reserved = false;
+  h->cap_f = h->cap_c = 0;
+}
+
+int grb_destroy(grb_handle* h) {
+  if (!h) return GRB_ERR_INVALID;
+  free_scratch(h);
+  cudaFree(h->d_flags);
+  cudaFree(h->d_counters);
+  delete h;
+  return GRB_OK;
+}
+
+int grb_reserve(grb_handle* h, const grb_grid* g) {
+  if (!h || !g || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->nq < 1 || g->ngz < 4) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  if (h->reserved && same_geo(h->geo, g)) return GRB_OK;
+  free_scratch(h);
+  const int64_t nf = G.fcells * G.nq, nc = G.cells * G.nq;
+  auto al = [&](void** p, size_t bytes) { return cudaMalloc(p, bytes) == cudaSuccess; };
+  bool ok = al((void**)&h->B.flux, sizeof(double) * nf * 7 * 3) &&
+            al((void**)&h->B.emf, sizeof(double) * nf * 3) &&
+            al((void**)&h->B.ftag, (size_t)nf * 3) && al((void**)&h->B.etag, (size_t)nf * 3);
+  if (ok && h->p.emf == GRB_EMF_GS)
+    ok = al((void**)&h->B.eface, sizeof(double) * nf * 2 * 3) &&
+         al((void**)&h->B.ecenter, sizeof(double) * nc * 3);
+  if (ok && h->p.emf == GRB_EMF_UCT) ok = al((void**)&h->B.vbar, sizeof(double) * nf * 4 * 3);
+  if (!ok) {
+    free_scratch(h);
+    cudaGetLastError();
+    return fail(h, GRB_ERR_NOMEM);
+  }
+  // Edge EMFs outside the computed range stay zero for the lifetime of the
+  // scratch, as the zero-initialised reference view does; the FOFC
+  // tentative CT update of ghost-layer cells reads them.
+  CK(cudaMemset(h->B.emf, 0, sizeof(double) * nf * 3));
+  CK(cudaMemset(h->B.flux, 0, sizeof(double) * nf * 7 * 3));
+  if (h->B.eface) CK(cudaMemset(h->B.eface, 0, sizeof(double) * nf * 2 * 3));
+  if (h->B.ecenter) CK(cudaMemset(h->B.ecenter, 0, sizeof(double) * nc * 3));
+  if (h->B.vbar) CK(cudaMemset(h->B.vbar, 0, sizeof(double) * nf * 4 * 3));
+  CK(cudaDeviceSynchronize());
+  h->geo = G;
+  h->cap_f = nf;
+  h->cap_c = nc;
+  h->reserved = true;
+  h->B.counters = h->d_counters;
+  h->B.flags = h->d_flags;
+  return GRB_OK;
+}
+
+int grb_get_status(grb_handle* h, grb_status* st) {
+  if (!h || !st) return GRB_ERR_INVALID;
+  uint32_t f = 0;
+  unsigned long long c[2] = {0, 0};
+  CK(cudaMemcpy(&f, h->d_flags, sizeof(f), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(c, h->d_counters, sizeof(c), cudaMemcpyDeviceToHost));
+  st->device_flags = f;
+  st->last_error = h->last_error;
+  st->fofc_faces = (int64_t)c[0];
+  st->fofc_edges = (int64_t)c[1];
+  return GRB_OK;
+}
+
+int grb_clear_status(grb_handle* h) {
+  if (!h) return GRB_ERR_INVALID;
+  CK(cudaMemset(h->d_flags, 0, sizeof(uint32_t)));
+  h->last_error = GRB_OK;
+  return GRB_OK;
+}
+
+int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt, double dtfact,
+                        const grb_fields* nw, const grb_fields* old, const double* aux,
+                        void* stream) {
+  (void)t;
+  if (!h) return GRB_ERR_INVALID;
+  int rc = check_grid(h, g);
+  if (rc) return fail(h, rc);
+  if (!nw || !old || !aux || !nw->state || !old->state || !nw->bx || !old->bx) return fail(h, GRB_ERR_INVALID);
+  cudaStream_t s = (cudaStream_t)stream;
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  const DevParams& P = h->dp;
+  const int gz = G.g, T = 128;
+  StageBufs B = h->B;
+  // compute_fluxes: reference ranges (evolve.cpp:908-922)
+  const double* bf[3] = {old->bx, old->by, old->bz};
+  for (int dir = 0; dir < 3; ++dir) {
+    int lo[3] = {0, 0, 0}, n[3] = {G.NX, G.NY, G.NZ};
+    lo[dir] = gz - 1;
+    n[dir] = (dir == 0 ? G.nx : dir == 1 ? G.ny : G.nz) + 3;
+    const Box b = box(lo[0], lo[1], lo[2], n[0], n[1], n[2], G.nq);
+    if (dir == 0) k_flux<0><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, old->state, aux, bf[0], B);
+    if (dir == 1) k_flux<1><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, old->state, aux, bf[1], B);
+    if (dir == 2) k_flux<2><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, old->state, aux, bf[2], B);
+  }
+  const Box eb = box(gz, gz, gz, G.nx + 1, G.ny + 1, G.nz + 1, G.nq);
+  if (P.emf == GRB_EMF_GS)
+    k_emf_gs<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, B);
+  else
+    k_emf_uct<<<nblk(eb.count(), T), T, 0, s>>>(P, G, eb, old->bx, old->by, old->bz, B);
+  if (P.fofc && P.emf == GRB_EMF_GS) {
+    const int64_t nf = G.fcells * G.nq * 3;
+    CK(cudaMemsetAsync(B.ftag, 0, (size_t)nf, s));
+    CK(cudaMemsetAsync(B.etag, 0, (size_t)nf, s));
+    CK(cudaMemsetAsync(B.counters, 0, 2 * sizeof(unsigned long long), s));
+    const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, G.nq);
+    k_fofc_flag<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, dt, dtfact, nw->state, old->state, old->bx,
+                                                   old->by, old->bz, g->idx, g->coords, B);
+    k_fofc_faces<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by, old->bz, B);
+    k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B);
+  }
+  const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, G.nq);
+  k_update<<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, nw->state, old->state, aux, g->idx, B);
+  k_ct<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, dt, dtfact, nw->bx, nw->by, nw->bz, g->idx, B);
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g, const grb_fields* st,
+                                     double* aux, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  int rc = check_grid(h, g);
+  if (rc) return fail(h, rc);
+  if (!st || !st->state || !st->bx || !st->by || !st->bz || !aux) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  const Box b = box(0, 0, 0, G.NX, G.NY, G.NZ, G.nq);
+  k_aux<<<nblk(b.count(), 128), 128, 0, (cudaStream_t)stream>>>(h->dp, G, b, st->state, st->bx, st->by,
+                                                                  st->bz, aux, g->idx, g->coords, h->B);
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_reset_c2p_diagnostics(grb_handle* h, const grb_grid* g, double* aux, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  int rc = check_grid(h, g);
+  if (rc) return fail(h, rc);
+  if (!aux) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  k_reset_diag<<<1184, 256, 0, (cudaStream_t)stream>>>(G, aux);
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A, const grb_fields* Bf,
+                    const grb_fields* Cf, double b, double c, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!g || g->nq < 1) return fail(h, GRB_ERR_INVALID);
+  if (!A || !Bf || !A->state || !Bf->state) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t n[4] = {G.cells * GRB_N_EVOL_VARS * G.nq, (int64_t)(G.NX + 1) * G.NY * G.NZ * G.nq,
+                        (int64_t)G.NX * (G.NY + 1) * G.NZ * G.nq, (int64_t)G.NX * G.NY * (G.NZ + 1) * G.nq};
+  double* a[4] = {A->state, A->bx, A->by, A->bz};
+  const double* x[4] = {Bf->state, Bf->bx, Bf->by, Bf->bz};
+  const double* y[4] = {Cf ? Cf->state : nullptr, Cf ? Cf->bx : nullptr, Cf ? Cf->by : nullptr, Cf ? Cf->bz : nullptr};
+  for (int v = 0; v < 4; ++v) k_linop<<<148 * 16, 256, 0, s>>>(n[v], a[v], x[v], y[v], b, c);
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons, const double* metric, double* prims,
+                  double* cons_out, uint32_t* err, int32_t use_learned, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (n < 0 || (n > 0 && (!cons || !prims))) return fail(h, GRB_ERR_INVALID);
+  if (use_learned) return fail(h, GRB_ERR_INVALID);  // model loading is separate
+  if (n == 0) return GRB_OK;
+  k_c2p_batch<<<nblk(n, 128), 128, 0, (cudaStream_t)stream>>>(h->dp, n, cons, metric, prims, cons_out, err,
+                                                               nullptr, h->d_flags);
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+
+int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
+                          int32_t nby, int32_t nbz, const int32_t* periodic, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!g || !f || !f->state || !f->bx || !f->by || !f->bz || !periodic || g->ngz < 1 ||
+      nbx < 1 || nby < 1 || nbz < 1 || (int64_t)nbx * nby * nbz != g->nq)
+    return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  Brick br;
+  br.nbx = nbx; br.nby = nby; br.nbz = nbz;
+  for (int a = 0; a < 3; ++a) br.periodic[a] = periodic[a] != 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  double* bf[3] = {f->bx, f->by, f->bz};
+  for (int ax = 0; ax < 3; ++ax) {
+    k_ghost_cells<<<148 * 8, 256, 0, s>>>(G, br, ax, f->state);
+    for (int fd = 0; fd < 3; ++fd) k_ghost_faces<<<148 * 4, 256, 0, s>>>(G, br, ax, fd, bf[fd]);
+  }
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+}  // extern "C"

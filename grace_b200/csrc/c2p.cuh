@@ -1,0 +1,496 @@
+// Device conservative-to-primitive recovery (FP64), following
+// src/physics/eos/c2p.cpp:40-455, include/grace/physics/eos/c2p.hh:124-316,
+// include/grace/physics/eos/kastaun_c2p.hh:44-402 and
+// include/grace/physics/eos/ent_based_c2p.hh:44-260.  Root solves are
+// Brent's method (Brent 1973, "zero") and the safeguarded Newton of
+// include/grace/utils/rootfinding.hh:73-306.  Every loop is bounded: Brent
+// by an iteration cap far above its convergence bound for the 1e-15
+// abscissa tolerance, Newton by its 30-step limit.
+#pragma once
+#include "physics.cuh"
+
+namespace grb {
+
+// fatal conditions (the reference calls Kokkos::abort there) -> status bits
+enum : uint32_t {
+  FAT_C2P_RHO_HIGH = GRB_FLAG_C2P_RHO_TOO_HIGH, FAT_EOS_RHO_HIGH = GRB_FLAG_EOS_RHO_TOO_HIGH,
+  FAT_EOS_EPS_HIGH = GRB_FLAG_EOS_EPS_TOO_HIGH, FAT_EOS_TEMP_HIGH = GRB_FLAG_EOS_TEMP_TOO_HIGH,
+  FAT_EOS_PRESS_HIGH = GRB_FLAG_EOS_PRESS_TOO_HIGH
+};
+constexpr int kBrentMaxIter = 200;
+
+// Brent's zero finder on [a,b] with tol = 2 eps |b| + t.  F: double(double).
+template <class F>
+GRB_HD double brent(F& f, double a, double b, double t, int& iters) {
+  double sa = a, sb = b;
+  double fa = f(sa), fb = f(sb);
+  double c = sa, fc = fa, e = sb - sa, d = e;
+  const double macheps = 2.220446049250313e-16;
+  for (int it = 0; it < kBrentMaxIter; ++it) {
+    if (fabs(fc) < fabs(fb)) {
+      sa = sb; sb = c; c = sa;
+      fa = fb; fb = fc; fc = fa;
+    }
+    const double tol = 2.0 * macheps * fabs(sb) + t;
+    const double m = 0.5 * (c - sb);
+    if (fabs(m) <= tol || fb == 0.0) break;
+    if (fabs(e) < tol || fabs(fa) <= fabs(fb)) {
+      e = m; d = e;
+    } else {
+      double s = fb / fa, p, q;
+      if (sa == c) {
+        p = 2.0 * m * s;
+        q = 1.0 - s;
+      } else {
+        q = fa / fc;
+        const double r = fb / fc;
+        p = s * (2.0 * m * q * (q - r) - (sb - sa) * (r - 1.0));
+        q = (q - 1.0) * (r - 1.0) * (s - 1.0);
+      }
+      if (0.0 < p) q = -q; else p = -p;
+      s = e; e = d;
+      if (2.0 * p < 3.0 * m * q - fabs(tol * q) && p < fabs(0.5 * s * q)) d = p / q;
+      else { e = m; d = e; }
+    }
+    sa = sb; fa = fb;
+    if (tol < fabs(d)) sb = sb + d;
+    else if (0.0 < m) sb = sb + tol;
+    else sb = sb - tol;
+    fb = f(sb);
+    ++iters;
+    if ((0.0 < fb && 0.0 < fc) || (fb <= 0.0 && fc <= 0.0)) {
+      c = sa; fc = fa; e = sb - sa; d = e;
+    }
+  }
+  return sb;
+}
+
+// Kastaun auxiliary function mu sqrt(h0^2 + rbar^2(mu)) - 1 (kastaun_c2p.hh:44-117)
+struct KBr {
+  double rsqr, bsqr, rbsqr, h0sqr;
+  GRB_HD double xmu(double mu) const { return 1. / (1. + mu * bsqr); }
+  GRB_HD double rb2(double mu, double x) const { return x * (rsqr * x + mu * (x + 1.0) * rbsqr); }
+  GRB_HD double operator()(double mu) const {
+    const double x = xmu(mu);
+    return mu * sqrt(h0sqr + rb2(mu, x)) - 1.;
+  }
+  GRB_HD void fdf(double mu, double& f, double& df) const {
+    const double x = xmu(mu), x2 = x * x;
+    const double hw = sqrt(h0sqr + rb2(mu, x));
+    const double b = x * (x2 * rsqr + mu * (1 + x + x2) * rbsqr);
+    f = mu * hw - 1.;
+    df = (h0sqr + b) / hw;
+  }
+};
+GRB_HD double newton_br(double sa, double sb, const KBr& g, int maxiter, double tol, int& err) {
+  const double macheps = 2.220446049250313e-16;
+  double a = sa, b = sb, fa, fb, dum;
+  g.fdf(a, fa, dum);
+  g.fdf(b, fb, dum);
+  if (fa == 0) { err = 0; return a; }
+  if (fb == 0) { err = 0; return b; }
+  if (fa * fb > 0) { err = 1; return 0; }
+  double x = (fb * a - fa * b) / (fb - fa);
+  for (int it = 0; it < maxiter; ++it) {
+    const double xold = x;
+    double fx, dfx;
+    g.fdf(x, fx, dfx);
+    if (fx * fb > 0) { fb = fx; b = x; }
+    else if (fx * fa > 0) { fa = fx; a = x; }
+    x -= fx / dfx;
+    const double tt = 2. * macheps * fabs(x) + tol;
+    if (fabs(x - xold) < tt || fx == 0) { err = 0; return x; }
+    if (x > b || x < a) x = 0.5 * (b + a);
+  }
+  err = 1;
+  return 0;
+}
+
+// Kastaun scalars (kastaun_c2p.hh:306-337)
+struct KSc {
+  double D, q, s, ye, r2, Bt2, rBt, rBt2, h0;
+  double rup[3], Bt[3], B[3];
+};
+GRB_HD KSc kscalars(const DevEos& e, const Met& m, double c[10]) {
+  KSc k;
+  k.h0 = e.h_min;
+  c[0] = fmax(0., c[0]);
+  k.D = c[0];
+  const double iD = 1.0 / k.D;
+  k.q = c[4] * iD;
+  k.s = c[6] * iD;
+  const double r[3] = {c[1] * iD, c[2] * iD, c[3] * iD};
+  const double isD = 1.0 / sqrt(k.D);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) { k.B[i] = c[7 + i]; k.Bt[i] = c[7 + i] * isD; }
+  k.r2 = sqs(m.gi, r);
+  k.Bt2 = sqs(m.g, k.Bt);
+  k.rBt = r[0] * k.Bt[0] + r[1] * k.Bt[1] + r[2] * k.Bt[2];
+  k.rBt2 = k.rBt * k.rBt;
+  mvs(m.gi, r, k.rup);
+  k.ye = c[5] * iD;
+  return k;
+}
+
+// Kastaun master function (kastaun_c2p.hh:122-295)
+struct KRt {
+  const DevEos* e;
+  double d, qtot, rsqr, bsqr, rbsqr, brosqr, vsqrmax, wmax;
+  GRB_HD KRt(const DevEos& eos, const KSc& k) : e(&eos) {
+    d = k.D; qtot = k.q; rsqr = k.r2; bsqr = k.Bt2; rbsqr = k.rBt2;
+    brosqr = rsqr * bsqr - rbsqr;
+    const double zs = rsqr / (k.h0 * k.h0);
+    const double ws = 1 + zs;
+    wmax = sqrt(ws);
+    vsqrmax = zs / ws;
+  }
+  GRB_HD double eval(double mu, bool full, uint32_t& sig, double& x, double& w, double& rho,
+                     double& press, double& eps, double& temp, double& ent) const {
+    x = 1. / (1. + mu * bsqr);
+    const double rf = x * (rsqr * x + mu * (x + 1.0) * rbsqr);
+    const double mx = mu * x;
+    const double qf = qtot - 0.5 * (bsqr + mx * mx * brosqr);
+    const double vsqr = rf * mu * mu;
+    if (vsqr > vsqrmax) { w = wmax; if (full) sig |= SIG_VEL_HIGH; }
+    else w = 1 / sqrt(1 - vsqr);
+    rho = d / w;
+    if (full) {
+      if (rho >= e->rhomax) { sig |= SIG_RHO_HIGH; rho = e->rhomax; }
+      else if (rho <= e->rhomin) { sig |= SIG_RHO_LOW; rho = e->rhomin; }
+    } else {
+      rho = fmin(e->rhomax, fmax(e->rhomin, rho));
+    }
+    eps = w * (qf - mu * rf * (1.0 - mu * w / (1 + w)));
+    double lo, hi;
+    eos_eps_range(*e, lo, hi, rho);
+    uint32_t qe = 0;
+    if (full) {
+      hi = fmin(hi, e->eps_max);
+      if (eps >= hi) { sig |= SIG_EPS_HIGH; eps = hi * 0.999; }
+      else if (eps < lo) { sig |= SIG_EPS_LOW; eps = lo; }
+      press = eos_Peps_full(*e, temp, ent, eps, rho, qe);
+    } else {
+      eps = fmin(hi, fmax(lo, eps));
+      press = eos_Peps(*e, eps, rho, qe);
+    }
+    const double a = press / (rho * (1 + eps));
+    const double h = (1 + eps) * (1 + a);
+    const double hbw = fmax((1 + a) * (1 + qf - mu * rf), h / w);
+    return mu - 1. / (hbw + rf * mu);
+  }
+  GRB_HD double operator()(double mu) const {
+    uint32_t s = 0;
+    double x, w, rho, p, eps, t, en;
+    return eval(mu, false, s, x, w, rho, p, eps, t, en);
+  }
+};
+
+// Entropy master function (ent_based_c2p.hh:44-170); s persists clamped.
+struct ERt {
+  const DevEos* e;
+  double d, s, rsqr, bsqr, rbsqr, vsqrmax, wmax;
+  GRB_HD ERt(const DevEos& eos, const KSc& k) : e(&eos) {
+    d = k.D; s = k.s; rsqr = k.r2; bsqr = k.Bt2; rbsqr = k.rBt2;
+    const double zs = rsqr / (k.h0 * k.h0);
+    const double ws = 1 + zs;
+    wmax = sqrt(ws);
+    vsqrmax = zs / ws;
+  }
+  GRB_HD double eval(double mu, double& ent, bool full, uint32_t& sig, double& x, double& w,
+                     double& rho, double& press, double& eps, double& temp) {
+    x = 1. / (1. + mu * bsqr);
+    const double rf = x * (rsqr * x + mu * (x + 1.0) * rbsqr);
+    const double vsqr = rf * mu * mu;
+    w = 1 / sqrt(1 - vsqr);
+    if (vsqr > vsqrmax) { w = wmax; if (full) sig |= SIG_VEL_HIGH; }
+    rho = d / w;
+    if (full) {
+      if (rho >= e->rhomax) { sig |= SIG_RHO_HIGH; rho = e->rhomax; }
+      else if (rho <= e->rhomin) { sig |= SIG_RHO_LOW; rho = e->rhomin; }
+    } else {
+      rho = fmin(e->rhomax, fmax(e->rhomin, rho));
+    }
+    uint32_t qe = 0;
+    press = eos_Pent(*e, temp, eps, ent, rho, qe);
+    if (full) {
+      if (qe & EOS_ENT_LOW) sig |= SIG_ENT_LOW;
+      if (qe & EOS_ENT_HIGH) sig |= SIG_ENT_HIGH;
+    }
+    const double a = press / (rho * (1 + eps));
+    const double h = (1 + eps) * (1 + a);
+    return mu - 1. / (h / w + rf * mu);
+  }
+  GRB_HD double operator()(double mu) {
+    uint32_t sg = 0;
+    double x, w, rho, p, eps, t;
+    return eval(mu, s, false, sg, x, w, rho, p, eps, t);
+  }
+};
+
+GRB_HD double kastaun_mu0(const KSc& k) {
+  double mu0 = 1 / k.h0;
+  if (k.r2 >= k.h0 * k.h0) {
+    KBr g{k.r2, k.Bt2, k.rBt2, k.h0 * k.h0};
+    double lo = 1. / (g.h0sqr + g.rsqr);
+    const double m0 = 1. / sqrt(g.h0sqr);
+    double hi = 1.0 / sqrt(g.h0sqr + g.rb2(m0, g.xmu(m0)));
+    lo *= (1 - 1e-10);
+    hi *= (1 + 1e-10);
+    if (hi <= lo) { lo = 0; hi = m0 * (1.0 + 1e-10); }
+    int err;
+    mu0 = newton_br(lo, hi, g, 30, 1e-10, err);
+    if (err == 0) mu0 *= 1 + 1e-10;
+    else mu0 = 1.0 / k.h0;
+  }
+  return mu0;
+}
+
+// Optional learned bracket for the Kastaun solve.
+struct Guess {
+  bool valid;
+  double lo, hi;
+};
+
+GRB_HD double kastaun_invert(const DevEos& e, const Met& m, double c[10], double pr[13],
+                             uint32_t& sig, int& iters, const Guess& gs, bool& guess_used) {
+  const KSc k = kscalars(e, m, c);
+  const KRt f(e, k);
+  double mu;
+  guess_used = false;
+  if (gs.valid) {
+    const double flo = f(gs.lo), fhi = f(gs.hi);
+    if (flo * fhi < 0) {
+      mu = brent(f, gs.lo, gs.hi, 1e-15, iters);
+      guess_used = true;
+    }
+  }
+  if (!guess_used) {
+    const double mu0 = kastaun_mu0(k);
+    mu = brent(f, 0, mu0, 1e-15, iters);
+  }
+  double x, w, rho, press, eps, temp, ent;
+  const double res = f.eval(mu, true, sig, x, w, rho, press, eps, temp, ent);
+  pr[GRB_P_EPS] = eps; pr[GRB_P_RHO] = rho; pr[GRB_P_PRESS] = press;
+  pr[GRB_P_TEMP] = temp; pr[GRB_P_ENT] = ent;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    pr[GRB_P_BX + i] = k.B[i];
+    pr[GRB_P_ZX + i] = w * mu * x * (k.rup[i] + mu * k.rBt * k.Bt[i]);
+  }
+  return fabs(res);
+}
+
+GRB_HD double entropy_invert(const DevEos& e, const Met& m, double c[10], double pr[13],
+                             uint32_t& sig) {
+  const KSc k = kscalars(e, m, c);
+  double mu0 = 1 / k.h0;
+  int it = 0;
+  if (k.r2 >= k.h0 * k.h0) {
+    KBr g{k.r2, k.Bt2, k.rBt2, k.h0 * k.h0};
+    int rerr;
+    mu0 = newton_br(0, 1. / k.h0, g, 30, 1e-10, rerr);
+    if (rerr == 0) mu0 *= 1 + 1e-10;
+    else mu0 = brent(g, 0, 1. / k.h0, 1e-10, it) * (1 + 1e-10);
+  }
+  ERt f(e, k);
+  const double mu = brent(f, 0, mu0, 1e-15, it);
+  double x, w, rho, press, eps, temp;
+  double ent = f.s;
+  const double res = f.eval(mu, ent, true, sig, x, w, rho, press, eps, temp);
+  pr[GRB_P_EPS] = eps; pr[GRB_P_RHO] = rho; pr[GRB_P_PRESS] = press;
+  pr[GRB_P_TEMP] = temp; pr[GRB_P_ENT] = ent;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    pr[GRB_P_BX + i] = k.B[i];
+    pr[GRB_P_ZX + i] = w * mu * x * (k.rup[i] + mu * k.rBt * k.Bt[i]);
+  }
+  return fabs(res);
+}
+
+// prims -> densitized cons (c2p.cpp:416-455)
+GRB_HD void prims_to_cons(const double pr[13], double c[10], const Met& m) {
+  const double W = lorentz(m.g, pr + GRB_P_ZX);
+  double b[4], b2;
+  comoving_b(m.alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, W, b, b2);
+  const double rhoh = pr[GRB_P_RHO] * (1. + pr[GRB_P_EPS]) + pr[GRB_P_PRESS] + b2;
+  const double pstar = pr[GRB_P_PRESS] + 0.5 * b2;
+  double bl[3], betal[3], zl[3];
+  mvs(m.g, b + 1, bl);
+  mvs(m.g, m.beta, betal);
+  mvs(m.g, pr + GRB_P_ZX, zl);
+  const double D = pr[GRB_P_RHO] * W;
+  const double tau = rhoh * W * W - pstar - m.alp * m.alp * b[0] * b[0] - D;
+  c[0] = m.sqrtg * D;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) c[1 + i] = m.sqrtg * (rhoh * W * zl[i] - m.alp * b[0] * (bl[i] + betal[i] * b[0]));
+  c[4] = m.sqrtg * tau;
+  c[6] = m.sqrtg * (pr[GRB_P_ENT] * D);
+  c[5] = c[0] * pr[GRB_P_YE];
+}
+
+GRB_HD void handle_sig(uint32_t sig, bool lenient, uint32_t& err, uint32_t& fatal) {
+  if (sig & SIG_RHO_HIGH) {
+    err |= ERR_SIG_RHO_HIGH | ERR_ALL_RESETS;
+    if (!lenient) fatal |= FAT_C2P_RHO_HIGH;
+  }
+  if (sig & SIG_RHO_LOW)
+    err |= ERR_RESET_DENS | ERR_RESET_TAU | ERR_RESET_STILDE | ERR_RESET_ENTROPY | ERR_SIG_RHO_LOW;
+  if (sig & SIG_ENT_LOW) err |= ERR_RESET_ENTROPY | ERR_SIG_ENT_LOW;
+  if (sig & SIG_ENT_HIGH) err |= ERR_RESET_ENTROPY | ERR_SIG_ENT_HIGH;
+  if (sig & SIG_EPS_HIGH) err |= ERR_RESET_STILDE | ERR_RESET_TAU | ERR_SIG_EPS_HIGH;
+  if (sig & SIG_EPS_LOW) err |= ERR_RESET_STILDE | ERR_RESET_TAU | ERR_SIG_EPS_LOW;
+  if (sig & SIG_VEL_HIGH)
+    err |= ERR_RESET_DENS | ERR_RESET_TAU | ERR_RESET_STILDE | ERR_RESET_ENTROPY | ERR_SIG_VEL_HIGH;
+  if (sig & SIG_SIGMA_HIGH)
+    err |= ERR_RESET_DENS | ERR_RESET_TAU | ERR_RESET_STILDE | ERR_RESET_ENTROPY | ERR_SIG_SIGMA_HIGH;
+}
+GRB_HD void handle_eos_sig(uint32_t q, bool lenient, uint32_t& err, uint32_t& fatal) {
+  if (q & EOS_RHO_HIGH) { err |= ERR_SIG_RHO_HIGH; fatal |= FAT_EOS_RHO_HIGH; }
+  if (q & EOS_RHO_LOW)
+    err |= ERR_RESET_DENS | ERR_RESET_TAU | ERR_RESET_STILDE | ERR_RESET_ENTROPY | ERR_SIG_RHO_LOW;
+  if (q & EOS_ENT_HIGH) err |= ERR_RESET_ENTROPY | ERR_SIG_ENT_HIGH;
+  if (q & EOS_ENT_LOW) err |= ERR_RESET_ENTROPY | ERR_SIG_ENT_LOW;
+  if (q & EOS_EPS_HIGH) { err |= ERR_SIG_EPS_HIGH | ERR_RESET_STILDE | ERR_RESET_TAU; if (!lenient) fatal |= FAT_EOS_EPS_HIGH; }
+  if (q & EOS_EPS_LOW) err |= ERR_RESET_STILDE | ERR_RESET_TAU | ERR_SIG_EPS_LOW;
+  if (q & EOS_TEMP_HIGH) { err |= ERR_SIG_TEMP_HIGH | ERR_RESET_STILDE | ERR_RESET_TAU; if (!lenient) fatal |= FAT_EOS_TEMP_HIGH; }
+  if (q & EOS_TEMP_LOW) err |= ERR_RESET_STILDE | ERR_RESET_TAU | ERR_SIG_TEMP_LOW;
+  if (q & EOS_PRESS_HIGH) { err |= ERR_SIG_PRESS_HIGH | ERR_RESET_STILDE | ERR_RESET_TAU; if (!lenient) fatal |= FAT_EOS_PRESS_HIGH; }
+  if (q & EOS_PRESS_LOW) err |= ERR_RESET_STILDE | ERR_RESET_TAU | ERR_SIG_PRESS_LOW;
+}
+
+GRB_HD void reset_atmo(double c[10], double pr[13], const Met& m, const DevParams& P,
+                       uint32_t& err) {
+  pr[GRB_P_RHO] = P.rho_fl;
+  pr[GRB_P_YE] = P.ye_fl;
+  pr[GRB_P_TEMP] = P.temp_fl;
+  pr[GRB_P_ZX] = pr[GRB_P_ZY] = pr[GRB_P_ZZ] = 0.;
+  double cs2;
+  uint32_t q = 0;
+  pr[GRB_P_PRESS] = eos_PT(P.eos, pr[GRB_P_EPS], cs2, &pr[GRB_P_ENT], pr[GRB_P_TEMP], pr[GRB_P_RHO], q);
+  prims_to_cons(pr, c, m);
+  err |= ERR_ALL_RESETS | ERR_ATMO;
+}
+
+struct C2POut {
+  uint32_t err;
+  uint32_t fatal;
+  int iters;
+  bool floored;
+  bool guess_used;
+};
+
+// conservs_to_prims (c2p.cpp:188-414).  c: densitized cons with densitized
+// cell-centred B (in), re-densitized consistent cons (out).
+GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P, double r_sph,
+                  bool dry_run, double alp_bh_thresh, const Guess& gs) {
+  C2POut o{0u, 0u, 0, false, false};
+  const DevEos& e = P.eos;
+  bool failed = false;
+  uint32_t ret = 0;
+  o.err = ERR_RESET_ENTROPY;
+  const double isg = 1.0 / m.sqrtg;
+#pragma unroll
+  for (int v = 0; v < 10; ++v) c[v] = c[v] / m.sqrtg;
+  (void)isg;
+  pr[GRB_P_BX] = c[7]; pr[GRB_P_BY] = c[8]; pr[GRB_P_BZ] = c[9];
+  if (c[0] < 0) {
+    reset_atmo(c, pr, m, P, o.err);
+    o.floored = true;
+    return o;
+  }
+  pr[GRB_P_YE] = c[5] / c[0];
+  if (pr[GRB_P_YE] > e.yemax) { pr[GRB_P_YE] = e.yemax; o.err |= ERR_RESET_YE; }
+  if (pr[GRB_P_YE] < 0.0) { pr[GRB_P_YE] = 0.0; o.err |= ERR_RESET_YE; }
+  const bool lenient = m.alp < alp_bh_thresh;
+  {  // limit_conservatives (c2p.cpp:117-157)
+    double lo, hi;
+    eos_eps_range(e, lo, hi, c[0]);
+    const double B2 = sqs(m.g, c + 7);
+    if (c[4] / c[0] - 0.5 * B2 / c[0] < fmin(0.0, lo)) {
+      c[4] = lo * c[0] + 0.5 * B2;
+      o.err |= ERR_RESET_TAU;
+      o.floored = true;
+    }
+    const double qd = c[4] / c[0] + 1;
+    const double st2 = sqs(m.gi, c + 1) / (c[0] * c[0]);
+    if (st2 > qd * qd) {
+      const double f = sqrt(qd * qd / st2);
+      c[1] *= f; c[2] *= f; c[3] *= f;
+      o.err |= ERR_RESET_STILDE;
+      o.floored = true;
+    }
+  }
+  if (o.floored && dry_run) return o;
+  if (c[0] >= P.rho_fl * (1 + P.atmo_tol)) {
+    const double res = kastaun_invert(e, m, c, pr, ret, o.iters, gs, o.guess_used);
+    failed = (fabs(res) > P.tol) || (ret & SIG_RHO_HIGH) || (ret & SIG_EPS_HIGH) || !isfinite(res);
+    double beta;
+    {
+      const double W = lorentz(m.g, pr + GRB_P_ZX);
+      double b[4], b2;
+      comoving_b(m.alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, W, b, b2);
+      beta = 2.0 * pr[GRB_P_PRESS] / fmax(b2, 1e-50);
+    }
+    const bool distrust = failed || (ret & SIG_EPS_LOW) || (beta <= P.beta_fallback);
+    if (distrust && P.use_ent_backup && !dry_run) {
+      double save[13];
+#pragma unroll
+      for (int v = 0; v < 13; ++v) save[v] = pr[v];
+      uint32_t bret = 0;
+      const double rb = entropy_invert(e, m, c, pr, bret);
+      const bool ok = (fabs(rb) <= P.tol) && isfinite(rb) && (pr[GRB_P_EPS] < e.eps_max);
+      if (ok) {
+        ret = bret;
+        failed = false;
+        o.err |= ERR_ENT_BACKUP;
+      } else if (!failed) {
+#pragma unroll
+        for (int v = 0; v < 13; ++v) pr[v] = save[v];
+      }
+    }
+    if (ret & (SIG_EPS_HIGH | SIG_RHO_LOW | SIG_RHO_HIGH | SIG_VEL_HIGH)) o.floored = true;
+    if (e.kind == GRB_EOS_IDEAL_GAS && (ret & SIG_EPS_LOW)) o.floored = true;
+    handle_sig(ret, lenient, o.err, o.fatal);
+  } else {
+    failed = true;
+  }
+  const bool excise = P.excise_by_radius ? (r_sph <= P.r_ex) : (m.alp <= P.alp_ex);
+  if (failed || excise || pr[GRB_P_RHO] < (1. + P.atmo_tol) * P.rho_fl) {
+    reset_atmo(c, pr, m, P, o.err);
+    o.floored = true;
+  } else if (pr[GRB_P_TEMP] < P.temp_fl) {
+    pr[GRB_P_TEMP] = P.temp_fl;
+    double cs2;
+    uint32_t q = 0;
+    pr[GRB_P_PRESS] = eos_PT(e, pr[GRB_P_EPS], cs2, &pr[GRB_P_ENT], pr[GRB_P_TEMP], pr[GRB_P_RHO], q);
+    handle_eos_sig(q, lenient, o.err, o.fatal);
+    o.err |= ERR_RESET_TAU | ERR_RESET_STILDE | ERR_RESET_ENTROPY | ERR_T_FLOORED;
+    if (e.kind == GRB_EOS_IDEAL_GAS) o.floored = true;
+  } else {  // limit_primitives (c2p.cpp:63-115)
+    uint32_t s2 = 0;
+    const double z2max = P.max_w * P.max_w - 1.;
+    const double z2 = sqs(m.g, pr + GRB_P_ZX);
+    if (z2 >= z2max) {
+      const double zn = 0.99 * sqrt(z2max / z2);
+      pr[GRB_P_ZX] *= zn; pr[GRB_P_ZY] *= zn; pr[GRB_P_ZZ] *= zn;
+      s2 |= SIG_VEL_HIGH;
+    }
+    const double W = lorentz(m.g, pr + GRB_P_ZX);
+    double b[4], b2;
+    comoving_b(m.alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, W, b, b2);
+    const double sigma = b2 / pr[GRB_P_RHO];
+    if (sigma >= P.max_sigma) {
+      pr[GRB_P_RHO] *= 1.001 * sigma / P.max_sigma;
+      double cs2;
+      uint32_t q = 0;
+      pr[GRB_P_PRESS] = eos_PT(e, pr[GRB_P_EPS], cs2, &pr[GRB_P_ENT], pr[GRB_P_TEMP], pr[GRB_P_RHO], q);
+      s2 |= SIG_SIGMA_HIGH;
+    }
+    handle_sig(s2, lenient, o.err, o.fatal);
+    if (s2 & (SIG_VEL_HIGH | SIG_SIGMA_HIGH)) o.floored = true;
+  }
+  prims_to_cons(pr, c, m);
+  return o;
+}
+
+}  // namespace grb

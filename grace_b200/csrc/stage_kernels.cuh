@@ -1,0 +1,722 @@
+// Per-item kernels of the Cowling GRMHD stage (one thread per face, edge or
+// cell).  Launch ranges and evaluation order follow the reference drivers:
+//   compute_fluxes          src/evolution/evolve.cpp:813-1068, grmhd.hh:551-970
+//   compute_emfs (GS / UCT) src/evolution/evolve.cpp:1069-1340, grmhd_helpers.hh:492-627
+//   flag / apply FOFC       src/evolution/evolve.cpp:456-811
+//   fluxes + sources        src/evolution/evolve.cpp:1342-1404, grmhd.hh:190-297
+//   update_CT               src/evolution/evolve.cpp:1406-1479
+//   aux (c2p, BDIV, E_c)    src/evolution/auxiliaries.cpp:81-162, grmhd.hh:306-434
+//   linop_apply             include/grace/utils/tstep_utils.hh:54-229
+#pragma once
+#include "c2p.cuh"
+#include "layout.cuh"
+
+namespace grb {
+
+struct StageBufs {
+  double* flux;     // fluxes(i,j,k,v,dir,q)
+  double* eface;    // GS face EMFs
+  double* vbar;     // UCT face velocities and speeds
+  double* ecenter;  // GS cell-centred E
+  double* emf;      // edge EMFs
+  int8_t* ftag;     // FOFC face tags
+  int8_t* etag;     // FOFC edge tags
+  unsigned long long* counters;  // [0] faces, [1] edges recomputed by FOFC
+  uint32_t* flags;  // device status word
+};
+
+// ---- the Riemann problem at one face (grmhd.hh:774-970) -------------------
+template <int dir>
+__device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
+                                           double* pl, double* pr, const Met& m, double f[7],
+                                           double vb[4]) {
+  const double alp = m.alp, sqrtg = m.sqrtg;
+  const double wl = lorentz(m.g, pl + GRB_P_ZX), wr = lorentz(m.g, pr + GRB_P_ZX);
+  double bl[4], br[4], b2l, b2r, vtl[3], vtr[3];
+  comoving_b(alp, m.beta, m.g, pl + GRB_P_BX, pl + GRB_P_ZX, wl, bl, b2l);
+  comoving_b(alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, wr, br, b2r);
+  vtilde(alp, m.beta, pl + GRB_P_ZX, wl, vtl);
+  vtilde(alp, m.beta, pr + GRB_P_ZX, wr, vtr);
+  const double gdd = dir == 0 ? m.gi[0] : dir == 1 ? m.gi[3] : m.gi[5];
+  double cml, cpl, cmr, cpr, cmin, cmax;
+  char_speeds(alp, m.beta[dir], pl[GRB_P_RHO], pl[GRB_P_PRESS], pl[GRB_P_EPS], pl[GRB_P_CS2], wl,
+              b2l, vtl[dir], gdd, cml, cpl);
+  char_speeds(alp, m.beta[dir], pr[GRB_P_RHO], pr[GRB_P_PRESS], pr[GRB_P_EPS], pr[GRB_P_CS2], wr,
+              b2r, vtr[dir], gdd, cmr, cpr);
+  if (rusanov) {
+    cmax = fmax(fmax(fabs(cml), fabs(cmr)), fmax(fabs(cpl), fabs(cpr)));
+    if (fmin(pl[GRB_P_RHO], pr[GRB_P_RHO]) < P.rusanov_c_limit)
+      cmax = fmax(cmax, alp * sqrt(gdd) + fabs(m.beta[dir]));
+    cmin = cmax;
+  } else {
+    cmin = -fmin(0., fmin(cml, cmr));
+    cmax = fmax(0., fmax(cpl, cpr));
+  }
+  if (cmin < 1e-12 && cmax < 1e-12) { cmin = 1; cmax = 1; }
+  if (P.emf == GRB_EMF_UCT) {
+    const int a0 = dir == 0 ? 1 : 0, a1 = dir == 2 ? 1 : 2;
+    vb[0] = hll(vtl[a0], vtr[a0], 0, 0, cmin, cmax);
+    vb[1] = hll(vtl[a1], vtr[a1], 0, 0, cmin, cmax);
+    vb[2] = cmin;
+    vb[3] = cmax;
+  }
+  const ConsFlux L = cons_flux(alp, m.beta, m.g, pl[GRB_P_RHO], pl[GRB_P_PRESS], pl[GRB_P_EPS],
+                               pl + GRB_P_ZX, pl[GRB_P_ENT], wl, b2l, bl, vtl, dir);
+  const ConsFlux R = cons_flux(alp, m.beta, m.g, pr[GRB_P_RHO], pr[GRB_P_PRESS], pr[GRB_P_EPS],
+                               pr + GRB_P_ZX, pr[GRB_P_ENT], wr, b2r, br, vtr, dir);
+  f[GRB_DENS] = sqrtg * hll(L.fD, R.fD, L.D, R.D, cmin, cmax);
+  f[GRB_ENTROPYSTAR] = sqrtg * hll(L.fent, R.fent, L.ents, R.ents, cmin, cmax);
+  f[GRB_TAU] = sqrtg * hll(L.ftau, R.ftau, L.tau, R.tau, cmin, cmax);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) f[GRB_SX + c] = sqrtg * hll(L.fS[c], R.fS[c], L.S[c], R.S[c], cmin, cmax);
+  const double yl = pl[GRB_P_YE], yr = pr[GRB_P_YE];
+  f[GRB_YESTAR] = sqrtg * hll(yl * L.fD, yr * R.fD, yl * L.D, yr * R.D, cmin, cmax);
+  if (P.emf == GRB_EMF_GS) {
+    const double* Bl = pl + GRB_P_BX;
+    const double* Br = pr + GRB_P_BX;
+    if (dir == 0) {
+      vb[0] = sqrtg * hll(-Bl[0] * vtl[2] + Bl[2] * vtl[0], -Br[0] * vtr[2] + Br[2] * vtr[0], Bl[2], Br[2], cmin, cmax);
+      vb[1] = -sqrtg * hll(-Bl[0] * vtl[1] + Bl[1] * vtl[0], -Br[0] * vtr[1] + Br[1] * vtr[0], Bl[1], Br[1], cmin, cmax);
+    } else if (dir == 1) {
+      vb[0] = -sqrtg * hll(-Bl[1] * vtl[2] + Bl[2] * vtl[1], -Br[1] * vtr[2] + Br[2] * vtr[1], Bl[2], Br[2], cmin, cmax);
+      vb[1] = sqrtg * hll(Bl[0] * vtl[1] - Bl[1] * vtl[0], Br[0] * vtr[1] - Br[1] * vtr[0], Bl[0], Br[0], cmin, cmax);
+    } else {
+      vb[0] = sqrtg * hll(Bl[1] * vtl[2] - Bl[2] * vtl[1], Br[1] * vtr[2] - Br[2] * vtr[1], Bl[1], Br[1], cmin, cmax);
+      vb[1] = -sqrtg * hll(Bl[0] * vtl[2] - Bl[2] * vtl[0], Br[0] * vtr[2] - Br[2] * vtr[0], Bl[0], Br[0], cmin, cmax);
+    }
+  }
+}
+
+// getflux<idir> (grmhd.hh:551-773) reading GRACE arrays through the cache.
+template <int dir>
+__device__ __forceinline__ void getflux(const DevParams& P, const Geo& G, int i, int j,
+                                        int k, int64_t q, int recon, bool rusanov,
+                                        const double* __restrict__ st,
+                                        const double* __restrict__ aux,
+                                        const double* __restrict__ bface, double f[7],
+                                        double vb[4]) {
+  const int64_t s = dir == 0 ? 1 : dir == 1 ? (int64_t)G.NX : (int64_t)G.NX * G.NY;
+  const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
+  const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
+  const double alpl = __ldg(st + c0 - s + G.cells * GRB_ALP);
+  const double alpr = __ldg(st + c0 + G.cells * GRB_ALP);
+  double gm[10];
+#pragma unroll
+  for (int a = 0; a < 10; ++a) {
+    const double* p = st + c0 + G.cells * (GRB_GXX + a);
+    gm[a] = face4(__ldg(p - 2 * s), __ldg(p - s), __ldg(p), __ldg(p + s));
+  }
+  const Met m = make_met(gm, gm + 7, gm[6]);
+  const int av[10] = {GRB_RHO, GRB_ZVECX, GRB_ZVECY, GRB_ZVECZ, GRB_YE, GRB_TEMP, GRB_ENTROPY, GRB_BX, GRB_BY, GRB_BZ};
+  const int pv[10] = {GRB_P_RHO, GRB_P_ZX, GRB_P_ZY, GRB_P_ZZ, GRB_P_YE, GRB_P_TEMP, GRB_P_ENT, GRB_P_BX, GRB_P_BY, GRB_P_BZ};
+  double pl[13], pr[13];
+  const bool donor = (alpl <= P.alp_ex || alpr <= P.alp_ex);
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const double* p = aux + a0 + G.cells * av[r];
+    if (donor) {
+      pl[pv[r]] = __ldg(p - s);
+      pr[pv[r]] = __ldg(p);
+    } else {
+      double u[6];
+#pragma unroll
+      for (int o = 0; o < 6; ++o) u[o] = __ldg(p + (o - 3) * s);
+      recon6(recon, u, pl[pv[r]], pr[pv[r]]);
+    }
+  }
+  const int64_t bi = dir == 0 ? bxi(G, i, j, k, q) : dir == 1 ? byi(G, i, j, k, q) : bzi(G, i, j, k, q);
+  const double bn = __ldg(bface + bi) / m.sqrtg;
+  pl[GRB_P_BX + dir] = bn;
+  pr[GRB_P_BX + dir] = bn;
+  uint32_t q0 = 0;
+  pl[GRB_P_PRESS] = eos_PT(P.eos, pl[GRB_P_EPS], pl[GRB_P_CS2], nullptr, pl[GRB_P_TEMP], pl[GRB_P_RHO], q0);
+  pr[GRB_P_PRESS] = eos_PT(P.eos, pr[GRB_P_EPS], pr[GRB_P_CS2], nullptr, pr[GRB_P_TEMP], pr[GRB_P_RHO], q0);
+  mhd_fluxes<dir>(P, rusanov, pl, pr, m, f, vb);
+}
+
+__device__ __forceinline__ void store_face(const Geo& G, const StageBufs& B, int emf_kind, int dir,
+                                           int i, int j, int k, int64_t q, const double f[7],
+                                           const double vb[4]) {
+#pragma unroll
+  for (int v = 0; v < 7; ++v) B.flux[flx(G, i, j, k, v, dir, q)] = f[v];
+  if (emf_kind == GRB_EMF_GS) {
+    B.eface[efi(G, i, j, k, 0, dir, q)] = vb[0];
+    B.eface[efi(G, i, j, k, 1, dir, q)] = vb[1];
+  } else {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) B.vbar[vbi(G, i, j, k, c, dir, q)] = vb[c];
+  }
+}
+
+// Box of items: [lo, hi) per axis, decoded from a linear thread index.
+struct Box {
+  int lo[3], n[3];
+  int64_t nq;
+  __host__ __device__ int64_t count() const { return (int64_t)n[0] * n[1] * n[2] * nq; }
+};
+__device__ __forceinline__ bool decode(const Box& b, int64_t t, int& i, int& j, int& k, int64_t& q) {
+  if (t >= b.count()) return false;
+  i = b.lo[0] + (int)(t % b.n[0]); t /= b.n[0];
+  j = b.lo[1] + (int)(t % b.n[1]); t /= b.n[1];
+  k = b.lo[2] + (int)(t % b.n[2]); t /= b.n[2];
+  q = t;
+  return true;
+}
+
+template <int dir>
+__global__ void __launch_bounds__(128) k_flux(DevParams P, Geo G, Box box,
+                                               const double* __restrict__ st,
+                                               const double* __restrict__ aux,
+                                               const double* __restrict__ bface, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  double f[7], vb[4];
+  getflux<dir>(P, G, i, j, k, q, P.recon, P.riemann == GRB_RIEMANN_LLF, st, aux, bface, f, vb);
+  store_face(G, B, P.emf, dir, i, j, k, q, f, vb);
+}
+
+// ---- Gardiner-Stone edge EMF (grmhd_helpers.hh:492-627) -------------------
+__device__ __forceinline__ double gs_edge(const Geo& G, const StageBufs& B, int dir, int i, int j,
+                                          int k, int64_t q) {
+  // (a, b): the two face directions feeding this edge; da/db: their
+  // transverse neighbour offsets; component slots in Eface.
+  const double* EF = B.eface;
+  const double* EC = B.ecenter;
+  const double* FL = B.flux;
+  auto sg = [](double x) { return copysign(1., x); };
+  if (dir == 0) {
+    const double Ezf = EF[efi(G, i, j, k, 0, 2, q)], Ezfm = EF[efi(G, i, j - 1, k, 0, 2, q)];
+    const double Eyf = EF[efi(G, i, j, k, 0, 1, q)], Eyfm = EF[efi(G, i, j, k - 1, 0, 1, q)];
+    const double NE = EC[eci(G, i, j, k, 0, q)], NW = EC[eci(G, i, j - 1, k, 0, q)];
+    const double SE = EC[eci(G, i, j, k - 1, 0, q)], SW = EC[eci(G, i, j - 1, k - 1, 0, q)];
+    const double a = sg(FL[flx(G, i, j, k, GRB_DENS, 1, q)]), am = sg(FL[flx(G, i, j, k - 1, GRB_DENS, 1, q)]);
+    const double b = sg(FL[flx(G, i, j, k, GRB_DENS, 2, q)]), bm = sg(FL[flx(G, i, j - 1, k, GRB_DENS, 2, q)]);
+    const double avg = 0.25 * (Ezf + Ezfm + Eyf + Eyfm);
+    const double dN = (1. - a) * (NE - Ezf) + (1. + a) * (NW - Ezfm);
+    const double dS = (1. - am) * (Ezf - SE) + (1. + am) * (Ezfm - SW);
+    const double dE = (1. - b) * (NE - Eyf) + (1. + b) * (SE - Eyfm);
+    const double dW = (1. - bm) * (Eyf - NW) + (1. + bm) * (Eyfm - SW);
+    return avg + (1. / 8.) * (dS - dN) + (1. / 8.) * (dW - dE);
+  } else if (dir == 1) {
+    const double Ezf = EF[efi(G, i, j, k, 1, 2, q)], Ezfm = EF[efi(G, i - 1, j, k, 1, 2, q)];
+    const double Exf = EF[efi(G, i, j, k, 0, 0, q)], Exfm = EF[efi(G, i, j, k - 1, 0, 0, q)];
+    const double NE = EC[eci(G, i, j, k, 1, q)], NW = EC[eci(G, i - 1, j, k, 1, q)];
+    const double SE = EC[eci(G, i, j, k - 1, 1, q)], SW = EC[eci(G, i - 1, j, k - 1, 1, q)];
+    const double a = sg(FL[flx(G, i, j, k, GRB_DENS, 0, q)]), am = sg(FL[flx(G, i, j, k - 1, GRB_DENS, 0, q)]);
+    const double b = sg(FL[flx(G, i, j, k, GRB_DENS, 2, q)]), bm = sg(FL[flx(G, i - 1, j, k, GRB_DENS, 2, q)]);
+    const double avg = 0.25 * (Ezf + Ezfm + Exf + Exfm);
+    const double dN = (1. - a) * (NE - Ezf) + (1. + a) * (NW - Ezfm);
+    const double dS = (1. - am) * (Ezf - SE) + (1. + am) * (Ezfm - SW);
+    const double dE = (1. - b) * (NE - Exf) + (1. + b) * (SE - Exfm);
+    const double dW = (1. - bm) * (Exf - NW) + (1. + bm) * (Exfm - SW);
+    return avg + (1. / 8.) * (dS - dN) + (1. / 8.) * (dW - dE);
+  } else {
+    const double Eyf = EF[efi(G, i, j, k, 1, 1, q)], Eyfm = EF[efi(G, i - 1, j, k, 1, 1, q)];
+    const double Exf = EF[efi(G, i, j, k, 1, 0, q)], Exfm = EF[efi(G, i, j - 1, k, 1, 0, q)];
+    const double NE = EC[eci(G, i, j, k, 2, q)], NW = EC[eci(G, i - 1, j, k, 2, q)];
+    const double SE = EC[eci(G, i, j - 1, k, 2, q)], SW = EC[eci(G, i - 1, j - 1, k, 2, q)];
+    const double a = sg(FL[flx(G, i, j, k, GRB_DENS, 0, q)]), am = sg(FL[flx(G, i, j - 1, k, GRB_DENS, 0, q)]);
+    const double b = sg(FL[flx(G, i, j, k, GRB_DENS, 1, q)]), bm = sg(FL[flx(G, i - 1, j, k, GRB_DENS, 1, q)]);
+    const double avg = 0.25 * (Eyf + Eyfm + Exf + Exfm);
+    const double dN = (1. - a) * (NE - Eyf) + (1. + a) * (NW - Eyfm);
+    const double dS = (1. - am) * (Eyf - SE) + (1. + am) * (Eyfm - SW);
+    const double dE = (1. - b) * (NE - Exf) + (1. + b) * (SE - Exfm);
+    const double dW = (1. - bm) * (Exf - NW) + (1. + bm) * (Exfm - SW);
+    return avg + (1. / 8.) * (dS - dN) + (1. / 8.) * (dW - dE);
+  }
+}
+
+// edge range of compute_emfs: [g, n+g] per axis, minus the top along the
+// edge's own direction (evolve.cpp:1089-1103)
+__global__ void __launch_bounds__(128) k_emf_gs(Geo G, Box box, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  if (i < G.nx + G.g) B.emf[emi(G, i, j, k, 0, q)] = gs_edge(G, B, 0, i, j, k, q);
+  if (j < G.ny + G.g) B.emf[emi(G, i, j, k, 1, q)] = gs_edge(G, B, 1, i, j, k, q);
+  if (k < G.nz + G.g) B.emf[emi(G, i, j, k, 2, q)] = gs_edge(G, B, 2, i, j, k, q);
+}
+
+// ---- UCT edge EMF (evolve.cpp:1131-1340) ----------------------------------
+__device__ __forceinline__ void recon_line(int recon, const double* p, int64_t s, double& L, double& R) {
+  double u[6];
+#pragma unroll
+  for (int o = 0; o < 6; ++o) u[o] = __ldg(p + (o - 3) * s);
+  recon6(recon, u, L, R);
+}
+__global__ void __launch_bounds__(128) k_emf_uct(DevParams P, Geo G, Box box,
+                                                  const double* __restrict__ bx,
+                                                  const double* __restrict__ by,
+                                                  const double* __restrict__ bz, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  const int rk = P.recon;
+  const double* VB = B.vbar;
+  // strides of the three face arrays along x, y, z
+  const int64_t sxx = 1, sxy = G.NX + 1, sxz = (int64_t)(G.NX + 1) * G.NY;
+  const int64_t syx = 1, syy = G.NX, syz = (int64_t)G.NX * (G.NY + 1);
+  const int64_t szx = 1, szy = G.NX, szz = (int64_t)G.NX * G.NY;
+  const int64_t vs[3] = {1, G.FX, (int64_t)G.FX * G.FY};
+  if (i < G.nx + G.g) {  // E^x at (i, j-1/2, k-1/2)
+    double ByL, ByR, vzL, vzR, BzL, BzR, vyL, vyR;
+    recon_line(rk, by + byi(G, i, j, k, q), syz, ByL, ByR);
+    recon_line(rk, VB + vbi(G, i, j, k, 1, 1, q), vs[2], vzL, vzR);
+    recon_line(rk, bz + bzi(G, i, j, k, q), szy, BzL, BzR);
+    recon_line(rk, VB + vbi(G, i, j, k, 1, 2, q), vs[1], vyL, vyR);
+    const double cmin_y = fmax(VB[vbi(G, i, j, k, 2, 1, q)], VB[vbi(G, i, j, k - 1, 2, 1, q)]);
+    const double cmax_y = fmax(VB[vbi(G, i, j, k, 3, 1, q)], VB[vbi(G, i, j, k - 1, 3, 1, q)]);
+    const double cmin_z = fmax(VB[vbi(G, i, j, k, 2, 2, q)], VB[vbi(G, i, j - 1, k, 2, 2, q)]);
+    const double cmax_z = fmax(VB[vbi(G, i, j, k, 3, 2, q)], VB[vbi(G, i, j - 1, k, 3, 2, q)]);
+    B.emf[emi(G, i, j, k, 0, q)] = hll(vzL * ByL, vzR * ByR, ByL, ByR, cmin_z, cmax_z) -
+                                   hll(vyL * BzL, vyR * BzR, BzL, BzR, cmin_y, cmax_y);
+  }
+  if (j < G.ny + G.g) {  // E^y at (i-1/2, j, k-1/2)
+    double BzL, BzR, vxL, vxR, BxL, BxR, vzL, vzR;
+    recon_line(rk, bz + bzi(G, i, j, k, q), szx, BzL, BzR);
+    recon_line(rk, VB + vbi(G, i, j, k, 0, 2, q), vs[0], vxL, vxR);
+    recon_line(rk, bx + bxi(G, i, j, k, q), sxz, BxL, BxR);
+    recon_line(rk, VB + vbi(G, i, j, k, 1, 0, q), vs[2], vzL, vzR);
+    const double cmin_z = fmax(VB[vbi(G, i, j, k, 2, 2, q)], VB[vbi(G, i - 1, j, k, 2, 2, q)]);
+    const double cmax_z = fmax(VB[vbi(G, i, j, k, 3, 2, q)], VB[vbi(G, i - 1, j, k, 3, 2, q)]);
+    const double cmin_x = fmax(VB[vbi(G, i, j, k, 2, 0, q)], VB[vbi(G, i, j, k - 1, 2, 0, q)]);
+    const double cmax_x = fmax(VB[vbi(G, i, j, k, 3, 0, q)], VB[vbi(G, i, j, k - 1, 3, 0, q)]);
+    B.emf[emi(G, i, j, k, 1, q)] = hll(vxL * BzL, vxR * BzR, BzL, BzR, cmin_x, cmax_x) -
+                                   hll(vzL * BxL, vzR * BxR, BxL, BxR, cmin_z, cmax_z);
+  }
+  if (k < G.nz + G.g) {  // E^z at (i-1/2, j-1/2, k)
+    double BxL, BxR, vyL, vyR, ByL, ByR, vxL, vxR;
+    recon_line(rk, bx + bxi(G, i, j, k, q), sxy, BxL, BxR);
+    recon_line(rk, VB + vbi(G, i, j, k, 0, 0, q), vs[1], vyL, vyR);
+    recon_line(rk, by + byi(G, i, j, k, q), syx, ByL, ByR);
+    recon_line(rk, VB + vbi(G, i, j, k, 0, 1, q), vs[0], vxL, vxR);
+    const double cmin_x = fmax(VB[vbi(G, i, j, k, 2, 0, q)], VB[vbi(G, i, j - 1, k, 2, 0, q)]);
+    const double cmax_x = fmax(VB[vbi(G, i, j, k, 3, 0, q)], VB[vbi(G, i, j - 1, k, 3, 0, q)]);
+    const double cmin_y = fmax(VB[vbi(G, i, j, k, 2, 1, q)], VB[vbi(G, i - 1, j, k, 2, 1, q)]);
+    const double cmax_y = fmax(VB[vbi(G, i, j, k, 3, 1, q)], VB[vbi(G, i - 1, j, k, 3, 1, q)]);
+    B.emf[emi(G, i, j, k, 2, q)] = hll(vyL * BxL, vyR * BxR, BxL, BxR, cmin_y, cmax_y) -
+                                   hll(vxL * ByL, vxR * ByR, ByL, ByR, cmin_x, cmax_x);
+  }
+  (void)sxx; (void)syx; (void)szx; (void)szz; (void)syy;
+}
+
+// ---- FOFC ------------------------------------------------------------------
+__device__ __forceinline__ double ct_bx(const Geo& G, const double* bx, const double* E, const double* ix,
+                                        int i, int j, int k, int64_t q, double dte) {
+  return bx[bxi(G, i, j, k, q)] + dte * ((E[emi(G, i, j, k + 1, 1, q)] - E[emi(G, i, j, k, 1, q)]) * ix[2] +
+                                         (E[emi(G, i, j, k, 2, q)] - E[emi(G, i, j + 1, k, 2, q)]) * ix[1]);
+}
+__device__ __forceinline__ double ct_by(const Geo& G, const double* by, const double* E, const double* ix,
+                                        int i, int j, int k, int64_t q, double dte) {
+  return by[byi(G, i, j, k, q)] + dte * ((E[emi(G, i + 1, j, k, 2, q)] - E[emi(G, i, j, k, 2, q)]) * ix[0] +
+                                         (E[emi(G, i, j, k, 0, q)] - E[emi(G, i, j, k + 1, 0, q)]) * ix[2]);
+}
+__device__ __forceinline__ double ct_bz(const Geo& G, const double* bz, const double* E, const double* ix,
+                                        int i, int j, int k, int64_t q, double dte) {
+  return bz[bzi(G, i, j, k, q)] + dte * ((E[emi(G, i, j + 1, k, 0, q)] - E[emi(G, i, j, k, 0, q)]) * ix[1] +
+                                         (E[emi(G, i, j, k, 1, q)] - E[emi(G, i + 1, j, k, 1, q)]) * ix[0]);
+}
+
+__device__ __forceinline__ Met cell_met(const Geo& G, const double* st, int i, int j, int k, int64_t q) {
+  const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
+  double g[6], b[3];
+#pragma unroll
+  for (int a = 0; a < 6; ++a) g[a] = st[c0 + G.cells * (GRB_GXX + a)];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) b[a] = st[c0 + G.cells * (GRB_BETAX + a)];
+  return make_met(g, b, st[c0 + G.cells * GRB_ALP]);
+}
+__device__ __forceinline__ double cell_r(const Geo& G, const double* coords, const double* ix, int i,
+                                         int j, int k, int64_t q) {
+  if (!coords) return 0.0;
+  const double x = coords[3 * q] + i / ix[0], y = coords[3 * q + 1] + j / ix[1], z = coords[3 * q + 2] + k / ix[2];
+  return sqrt(x * x + y * y + z * z);
+}
+
+// flag_fofc_cells (evolve.cpp:456-635) over cells [g-1, n+g]^3
+__global__ void __launch_bounds__(128) k_fofc_flag(DevParams P, Geo G, Box box, double dt,
+                                                    double dtfact, const double* __restrict__ ns,
+                                                    const double* __restrict__ os,
+                                                    const double* __restrict__ obx,
+                                                    const double* __restrict__ oby,
+                                                    const double* __restrict__ obz,
+                                                    const double* __restrict__ idx,
+                                                    const double* __restrict__ coords, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
+  double c[10];
+  const double* F = B.flux;
+#pragma unroll
+  for (int v = 0; v < 7; ++v)
+    c[v] = ns[cvar(G, i, j, k, v, GRB_N_EVOL_VARS, q)] +
+           dt * dtfact *
+               ((F[flx(G, i, j, k, v, 0, q)] - F[flx(G, i + 1, j, k, v, 0, q)]) * ix[0] +
+                (F[flx(G, i, j, k, v, 1, q)] - F[flx(G, i, j + 1, k, v, 1, q)]) * ix[1] +
+                (F[flx(G, i, j, k, v, 2, q)] - F[flx(G, i, j, k + 1, v, 2, q)]) * ix[2]);
+  const double dte = dt * dtfact;
+  c[7] = 0.5 * (ct_bx(G, obx, B.emf, ix, i, j, k, q, dte) + ct_bx(G, obx, B.emf, ix, i + 1, j, k, q, dte));
+  c[8] = 0.5 * (ct_by(G, oby, B.emf, ix, i, j, k, q, dte) + ct_by(G, oby, B.emf, ix, i, j + 1, k, q, dte));
+  c[9] = 0.5 * (ct_bz(G, obz, B.emf, ix, i, j, k, q, dte) + ct_bz(G, obz, B.emf, ix, i, j, k + 1, q, dte));
+  bool dmp = false;
+  if (P.dmp_enable) {
+    const double invM = 1.0 / P.dmp_M;
+    const int lv[2] = {GRB_DENS, GRB_TAU};
+    for (int n = 0; n < 2 && !dmp; ++n) {
+      double vmax = -1.7976931348623157e308, vmin = 1.7976931348623157e308;
+      for (int kt = -1; kt <= 1; ++kt)
+        for (int jt = -1; jt <= 1; ++jt)
+          for (int it = -1; it <= 1; ++it) {
+            const double v = ns[cvar(G, i + it, j + jt, k + kt, lv[n], GRB_N_EVOL_VARS, q)];
+            vmax = fmax(vmax, v);
+            vmin = fmin(vmin, v);
+          }
+      const double t = c[lv[n]];
+      if (t > P.dmp_M * vmax || t < vmin * invM) dmp = true;
+    }
+  }
+  bool floored = false;
+  if (!dmp) {  // the c2p dry run only matters when the DMP test passed
+    const Met m = cell_met(G, os, i, j, k, q);
+    double pr[13];
+    const Guess none{false, 0., 0.};
+    floored = c2p(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), true, 1e30, none).floored;
+  }
+  if (floored || dmp) {
+    int8_t* T = B.ftag;
+    T[emi(G, i, j, k, 0, q)] = 1; T[emi(G, i + 1, j, k, 0, q)] = 1;
+    T[emi(G, i, j, k, 1, q)] = 1; T[emi(G, i, j + 1, k, 1, q)] = 1;
+    T[emi(G, i, j, k, 2, q)] = 1; T[emi(G, i, j, k + 1, 2, q)] = 1;
+    int8_t* E = B.etag;
+    E[emi(G, i, j, k, 0, q)] = 1; E[emi(G, i, j + 1, k, 0, q)] = 1; E[emi(G, i, j, k + 1, 0, q)] = 1; E[emi(G, i, j + 1, k + 1, 0, q)] = 1;
+    E[emi(G, i, j, k, 1, q)] = 1; E[emi(G, i + 1, j, k, 1, q)] = 1; E[emi(G, i, j, k + 1, 1, q)] = 1; E[emi(G, i + 1, j, k + 1, 1, q)] = 1;
+    E[emi(G, i, j, k, 2, q)] = 1; E[emi(G, i + 1, j, k, 2, q)] = 1; E[emi(G, i, j + 1, k, 2, q)] = 1; E[emi(G, i + 1, j + 1, k, 2, q)] = 1;
+  }
+}
+
+// correct_{x,y,z}_fluxes_fofc: donor + LLF on tagged faces.  The box is the
+// compaction range [g-1, n+g]^3; a face of direction d needs index_d >= g.
+__global__ void __launch_bounds__(128) k_fofc_faces(DevParams P, Geo G, Box box,
+                                                     const double* __restrict__ st,
+                                                     const double* __restrict__ aux,
+                                                     const double* __restrict__ bx,
+                                                     const double* __restrict__ by,
+                                                     const double* __restrict__ bz, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  unsigned cnt = 0;
+  double f[7], vb[4];
+  if (i >= G.g && B.ftag[emi(G, i, j, k, 0, q)]) {
+    getflux<0>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bx, f, vb);
+    store_face(G, B, P.emf, 0, i, j, k, q, f, vb);
+    ++cnt;
+  }
+  if (j >= G.g && B.ftag[emi(G, i, j, k, 1, q)]) {
+    getflux<1>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, by, f, vb);
+    store_face(G, B, P.emf, 1, i, j, k, q, f, vb);
+    ++cnt;
+  }
+  if (k >= G.g && B.ftag[emi(G, i, j, k, 2, q)]) {
+    getflux<2>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bz, f, vb);
+    store_face(G, B, P.emf, 2, i, j, k, q, f, vb);
+    ++cnt;
+  }
+  if (cnt) atomicAdd(&B.counters[0], (unsigned long long)cnt);
+}
+__global__ void __launch_bounds__(128) k_fofc_edges(Geo G, Box box, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  if (i < G.g || j < G.g || k < G.g) return;
+  unsigned cnt = 0;
+  if (i < G.nx + G.g && B.etag[emi(G, i, j, k, 0, q)]) { B.emf[emi(G, i, j, k, 0, q)] = gs_edge(G, B, 0, i, j, k, q); ++cnt; }
+  if (j < G.ny + G.g && B.etag[emi(G, i, j, k, 1, q)]) { B.emf[emi(G, i, j, k, 1, q)] = gs_edge(G, B, 1, i, j, k, q); ++cnt; }
+  if (k < G.nz + G.g && B.etag[emi(G, i, j, k, 2, q)]) { B.emf[emi(G, i, j, k, 2, q)] = gs_edge(G, B, 2, i, j, k, q); ++cnt; }
+  if (cnt) atomicAdd(&B.counters[1], (unsigned long long)cnt);
+}
+
+// ---- flux divergence + geometric sources on interior cells -----------------
+__global__ void __launch_bounds__(128) k_update(DevParams P, Geo G, Box box, double dt, double dtfact,
+                                                 double* __restrict__ ns, const double* __restrict__ os,
+                                                 const double* __restrict__ aux,
+                                                 const double* __restrict__ idx, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
+  const Met m = cell_met(G, os, i, j, k, q);
+  const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
+  const double z[3] = {aux[a0 + G.cells * GRB_ZVECX], aux[a0 + G.cells * GRB_ZVECY], aux[a0 + G.cells * GRB_ZVECZ]};
+  const double Bv[3] = {aux[a0 + G.cells * GRB_BX], aux[a0 + G.cells * GRB_BY], aux[a0 + G.cells * GRB_BZ]};
+  const double W = lorentz(m.g, z);
+  const double h = ix[0];  // one spacing for all axes, as in grmhd.hh:232-235
+  const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
+  const int64_t sy = G.NX, sz = (int64_t)G.NX * G.NY;
+  auto der = [&](int v, double o[3]) {
+    const double* p = os + c0 + G.cells * v;
+    o[0] = fd6(p[-3], p[-2], p[-1], p[1], p[2], p[3], h);
+    o[1] = fd6(p[-3 * sy], p[-2 * sy], p[-sy], p[sy], p[2 * sy], p[3 * sy], h);
+    o[2] = fd6(p[-3 * sz], p[-2 * sz], p[-sz], p[sz], p[2 * sz], p[3 * sz], h);
+  };
+  double dalp[3], db[9], dg[18], t3[3];
+  der(GRB_ALP, dalp);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    der(GRB_BETAX + c, t3);
+    db[c] = t3[0]; db[3 + c] = t3[1]; db[6 + c] = t3[2];
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    der(GRB_GXX + c, t3);
+    dg[c] = t3[0]; dg[6 + c] = t3[1]; dg[12 + c] = t3[2];
+  }
+  double K[6];
+#pragma unroll
+  for (int c = 0; c < 6; ++c) K[c] = os[c0 + G.cells * (GRB_KXX + c)];
+  double stau, sS[3];
+  geom_sources(m, K, dalp, dg, db, aux[a0 + G.cells * GRB_RHO], aux[a0 + G.cells * GRB_PRESS],
+               aux[a0 + G.cells * GRB_EPS], Bv, z, W, stau, sS);
+  const double* F = B.flux;
+  const double sd = m.sqrtg * dt * dtfact;
+  double src[7] = {0., sd * sS[0], sd * sS[1], sd * sS[2], sd * stau, 0., 0.};
+#pragma unroll
+  for (int v = 0; v < GRB_N_HRSC; ++v) {
+    double* p = ns + c0 + G.cells * v;
+    double u = *p;
+    if (v >= 1 && v <= 4) u += src[v];
+    const double dFx = (F[flx(G, i, j, k, v, 0, q)] - F[flx(G, i + 1, j, k, v, 0, q)]) * ix[0];
+    const double dFy = (F[flx(G, i, j, k, v, 1, q)] - F[flx(G, i, j + 1, k, v, 1, q)]) * ix[1];
+    const double dFz = (F[flx(G, i, j, k, v, 2, q)] - F[flx(G, i, j, k + 1, v, 2, q)]) * ix[2];
+    *p = u + dt * dtfact * ((dFx + dFy) + dFz);
+  }
+}
+
+// update_CT on faces [g, n+g] (+1 on the face's own axis)
+__global__ void __launch_bounds__(128) k_ct(Geo G, Box box, double dt, double dtfact,
+                                             double* __restrict__ bx, double* __restrict__ by,
+                                             double* __restrict__ bz, const double* __restrict__ idx,
+                                             StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
+  const double* E = B.emf;
+  const double dd = dt * dtfact;
+  if (j < G.ny + G.g && k < G.nz + G.g)
+    bx[bxi(G, i, j, k, q)] += dd * ((E[emi(G, i, j, k + 1, 1, q)] - E[emi(G, i, j, k, 1, q)]) * ix[2] +
+                                    (E[emi(G, i, j, k, 2, q)] - E[emi(G, i, j + 1, k, 2, q)]) * ix[1]);
+  if (i < G.nx + G.g && k < G.nz + G.g)
+    by[byi(G, i, j, k, q)] += dd * ((E[emi(G, i + 1, j, k, 2, q)] - E[emi(G, i, j, k, 2, q)]) * ix[0] +
+                                    (E[emi(G, i, j, k, 0, q)] - E[emi(G, i, j, k + 1, 0, q)]) * ix[2]);
+  if (i < G.nx + G.g && j < G.ny + G.g)
+    bz[bzi(G, i, j, k, q)] += dd * ((E[emi(G, i, j + 1, k, 0, q)] - E[emi(G, i, j, k, 0, q)]) * ix[1] +
+                                    (E[emi(G, i, j, k, 1, q)] - E[emi(G, i + 1, j, k, 1, q)]) * ix[0]);
+}
+
+// ---- aux: c2p on every cell + resets + C2P_ERR + BDIV + cell-centred E -----
+__global__ void __launch_bounds__(128) k_aux(DevParams P, Geo G, Box box, double* __restrict__ st,
+                                              const double* __restrict__ bx,
+                                              const double* __restrict__ by,
+                                              const double* __restrict__ bz,
+                                              double* __restrict__ aux,
+                                              const double* __restrict__ idx,
+                                              const double* __restrict__ coords, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
+  const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
+  const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
+  const double bx0 = bx[bxi(G, i, j, k, q)], bx1 = bx[bxi(G, i + 1, j, k, q)];
+  const double by0 = by[byi(G, i, j, k, q)], by1 = by[byi(G, i, j + 1, k, q)];
+  const double bz0 = bz[bzi(G, i, j, k, q)], bz1 = bz[bzi(G, i, j, k + 1, q)];
+  double c[10], orig[7];
+#pragma unroll
+  for (int v = 0; v < 7; ++v) { c[v] = st[c0 + G.cells * v]; orig[v] = c[v]; }
+  c[7] = 0.5 * (bx0 + bx1);
+  c[8] = 0.5 * (by0 + by1);
+  c[9] = 0.5 * (bz0 + bz1);
+  const Met m = cell_met(G, st, i, j, k, q);
+  aux[a0 + G.cells * GRB_BX] = c[7] / m.sqrtg;
+  aux[a0 + G.cells * GRB_BY] = c[8] / m.sqrtg;
+  aux[a0 + G.cells * GRB_BZ] = c[9] / m.sqrtg;
+  const double cbx = c[7], cby = c[8], cbz = c[9];
+  double pr[13];
+  const Guess none{false, 0., 0.};
+  const C2POut o = c2p(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), false, P.alp_bh_thresh, none);
+  if (o.fatal) atomicOr(B.flags, o.fatal);
+  aux[a0 + G.cells * GRB_RHO] = pr[GRB_P_RHO];
+  aux[a0 + G.cells * GRB_EPS] = pr[GRB_P_EPS];
+  aux[a0 + G.cells * GRB_PRESS] = pr[GRB_P_PRESS];
+  aux[a0 + G.cells * GRB_TEMP] = pr[GRB_P_TEMP];
+  aux[a0 + G.cells * GRB_ENTROPY] = pr[GRB_P_ENT];
+  aux[a0 + G.cells * GRB_YE] = pr[GRB_P_YE];
+  aux[a0 + G.cells * GRB_ZVECX] = pr[GRB_P_ZX];
+  aux[a0 + G.cells * GRB_ZVECY] = pr[GRB_P_ZY];
+  aux[a0 + G.cells * GRB_ZVECZ] = pr[GRB_P_ZZ];
+  if (o.err & ERR_RESET_DENS) {
+    aux[a0 + G.cells * GRB_C2P_DENS_ERR] += orig[GRB_DENS] - c[0];
+    st[c0] = c[0];
+  }
+  if (o.err & ERR_RESET_STILDE)
+    for (int v = 1; v <= 3; ++v) st[c0 + G.cells * v] = c[v];
+  if (o.err & ERR_RESET_TAU) st[c0 + G.cells * GRB_TAU] = c[4];
+  if (o.err & ERR_RESET_ENTROPY) st[c0 + G.cells * GRB_ENTROPYSTAR] = c[6];
+  if (o.err & ERR_RESET_YE) st[c0 + G.cells * GRB_YESTAR] = c[5];
+  {
+    const uint64_t prev = (uint64_t)aux[a0 + G.cells * GRB_C2P_ERR];
+    aux[a0 + G.cells * GRB_C2P_ERR] = (double)(prev | (uint64_t)o.err);
+  }
+  aux[a0 + G.cells * GRB_BDIV] = ((bx1 - bx0) * ix[0] + (by1 - by0) * ix[1] + (bz1 - bz0) * ix[2]) / m.sqrtg;
+  if (P.emf == GRB_EMF_GS) {
+    const double W = sqrt(1. + sqs(m.g, pr + GRB_P_ZX));
+    double vt[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) vt[a] = m.alp * pr[GRB_P_ZX + a] / W - m.beta[a];
+    B.ecenter[eci(G, i, j, k, 0, q)] = cby * vt[2] - cbz * vt[1];
+    B.ecenter[eci(G, i, j, k, 1, q)] = -cbx * vt[2] + cbz * vt[0];
+    B.ecenter[eci(G, i, j, k, 2, q)] = cbx * vt[1] - cby * vt[0];
+  }
+}
+
+// reset_c2p_diagnostics (evolve.cpp:154-161)
+__global__ void k_reset_diag(Geo G, double* __restrict__ aux) {
+  const int64_t n = G.cells * G.nq;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = t / G.cells, c = t % G.cells;
+    aux[c + G.cells * (GRB_C2P_DENS_ERR + (int64_t)GRB_N_AUX_VARS * q)] = 0.0;
+    aux[c + G.cells * (GRB_C2P_ERR + (int64_t)GRB_N_AUX_VARS * q)] = 0.0;
+  }
+}
+
+// linop_apply: a = b*x (+ c*y) elementwise, 2 doubles per thread
+__global__ void k_linop(int64_t n, double* __restrict__ a, const double* __restrict__ x,
+                        const double* __restrict__ y, double b, double c) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    a[t] = y ? b * x[t] + c * y[t] : b * x[t];
+}
+
+
+// ---- ghost fill for a brick of same-level blocks ---------------------------
+// One sweep along axis `ax` over the full extent of the other two axes, so
+// three sweeps (x, y, z) also fill edges and corners.  Periodic axes copy
+// from the neighbouring block (wrapping), others copy the nearest interior
+// cell or face (zero-gradient outflow).  Only the 7 evolved HRSC variables
+// and the three face-B arrays are exchanged; the Cowling metric is static.
+struct Brick {
+  int nbx, nby, nbz;
+  int periodic[3];
+};
+__global__ void k_ghost_cells(Geo G, Brick br, int ax, double* __restrict__ st) {
+  const int n[3] = {G.NX, G.NY, G.NZ};
+  const int nin[3] = {G.nx, G.ny, G.nz};
+  const int ng = 2 * G.g;  // ghost layers along ax
+  const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+  const int64_t per_q = (int64_t)ng * n[o1] * n[o2] * GRB_N_HRSC;
+  const int64_t total = per_q * G.nq;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int gi = (int)(r % ng); r /= ng;
+    const int a = (int)(r % n[o1]); r /= n[o1];
+    const int b = (int)(r % n[o2]); r /= n[o2];
+    const int v = (int)(r % GRB_N_HRSC); r /= GRB_N_HRSC;
+    const int64_t q = r;
+    const int qc[3] = {(int)(q % br.nbx), (int)((q / br.nbx) % br.nby), (int)(q / ((int64_t)br.nbx * br.nby))};
+    const int nb[3] = {br.nbx, br.nby, br.nbz};
+    const bool lo = gi < G.g;
+    const int ig = lo ? gi : nin[ax] + gi;  // ghost index along ax
+    int src = lo ? ig + nin[ax] : ig - nin[ax];
+    int qs[3] = {qc[0], qc[1], qc[2]};
+    const bool edge = lo ? (qc[ax] == 0) : (qc[ax] == nb[ax] - 1);
+    if (edge && !br.periodic[ax]) {
+      src = lo ? G.g : nin[ax] + G.g - 1;
+    } else {
+      qs[ax] = (qc[ax] + (lo ? nb[ax] - 1 : 1)) % nb[ax];
+    }
+    const int64_t qsrc = qs[0] + (int64_t)br.nbx * (qs[1] + (int64_t)br.nby * qs[2]);
+    int d[3], sidx[3];
+    d[ax] = ig; d[o1] = a; d[o2] = b;
+    sidx[ax] = src; sidx[o1] = a; sidx[o2] = b;
+    st[cvar(G, d[0], d[1], d[2], v, GRB_N_EVOL_VARS, q)] = st[cvar(G, sidx[0], sidx[1], sidx[2], v, GRB_N_EVOL_VARS, qsrc)];
+  }
+}
+// face arrays: `fd` is the staggered axis of the array (0: bx, 1: by, 2: bz)
+__global__ void k_ghost_faces(Geo G, Brick br, int ax, int fd, double* __restrict__ bf) {
+  int n[3] = {G.NX, G.NY, G.NZ};
+  n[fd] += 1;
+  const int nin[3] = {G.nx, G.ny, G.nz};
+  const bool stag = (fd == ax);
+  const int nlo = G.g, nhi = stag ? G.g : G.g;  // ghost faces below / above
+  const int ng = nlo + nhi;
+  const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
+  const int64_t per_q = (int64_t)ng * n[o1] * n[o2];
+  const int64_t total = per_q * G.nq;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = t;
+    const int gi = (int)(r % ng); r /= ng;
+    const int a = (int)(r % n[o1]); r /= n[o1];
+    const int b = (int)(r % n[o2]); r /= n[o2];
+    const int64_t q = r;
+    const int qc[3] = {(int)(q % br.nbx), (int)((q / br.nbx) % br.nby), (int)(q / ((int64_t)br.nbx * br.nby))};
+    const int nb[3] = {br.nbx, br.nby, br.nbz};
+    const bool lo = gi < nlo;
+    // staggered axis: ghost faces are [0,g) and [n+g+1, n+2g]; the faces
+    // g and n+g belong to the block.  Unstaggered: like cells.
+    const int ig = lo ? gi : (stag ? nin[ax] + G.g + 1 + (gi - nlo) : nin[ax] + gi);
+    int src = lo ? ig + nin[ax] : ig - nin[ax];
+    int qs[3] = {qc[0], qc[1], qc[2]};
+    const bool edge = lo ? (qc[ax] == 0) : (qc[ax] == nb[ax] - 1);
+    if (edge && !br.periodic[ax]) {
+      src = lo ? G.g : (stag ? nin[ax] + G.g : nin[ax] + G.g - 1);
+    } else {
+      qs[ax] = (qc[ax] + (lo ? nb[ax] - 1 : 1)) % nb[ax];
+    }
+    const int64_t qsrc = qs[0] + (int64_t)br.nbx * (qs[1] + (int64_t)br.nby * qs[2]);
+    int d[3], si[3];
+    d[ax] = ig; d[o1] = a; d[o2] = b;
+    si[ax] = src; si[o1] = a; si[o2] = b;
+    auto lin = [&](const int* c, int64_t qq) {
+      return (int64_t)c[0] + (int64_t)n[0] * (c[1] + (int64_t)n[1] * (c[2] + (int64_t)n[2] * qq));
+    };
+    bf[lin(d, q)] = bf[lin(si, qsrc)];
+  }
+}
+
+// batched c2p on SoA arrays
+__global__ void __launch_bounds__(128) k_c2p_batch(DevParams P, int64_t n, const double* __restrict__ cons,
+                                                    const double* __restrict__ metric,
+                                                    double* __restrict__ prims, double* __restrict__ cons_out,
+                                                    uint32_t* __restrict__ err, int32_t* __restrict__ iters,
+                                                    uint32_t* flags) {
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  double g[6] = {1, 0, 0, 1, 0, 1}, b[3] = {0, 0, 0}, alp = 1.0;
+  if (metric) {
+#pragma unroll
+    for (int a = 0; a < 6; ++a) g[a] = metric[a * n + t];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) b[a] = metric[(6 + a) * n + t];
+    alp = metric[9 * n + t];
+  }
+  const Met m = make_met(g, b, alp);
+  double c[10], pr[13];
+#pragma unroll
+  for (int v = 0; v < 10; ++v) c[v] = cons[v * n + t];
+  const Guess none{false, 0., 0.};
+  const C2POut o = c2p(c, pr, m, P, 0.0, false, P.alp_bh_thresh, none);
+  if (o.fatal) atomicOr(flags, o.fatal);
+  pr[GRB_P_CS2] = 0.0;
+#pragma unroll
+  for (int v = 0; v < 13; ++v) prims[v * n + t] = pr[v];
+  if (cons_out) {
+#pragma unroll
+    for (int v = 0; v < 10; ++v) cons_out[v * n + t] = c[v];
+  }
+  if (err) err[t] = o.err;
+  if (iters) iters[t] = o.iters;
+}
+
+}  // namespace grb

@@ -1,0 +1,187 @@
+"""Host-side mirror of GRACE's Cowling GRMHD evolution interface.
+
+The names and argument meanings follow the reference's free functions:
+  advance_substep(t, dt, dtfact, new_state, old_state, new_stag, old_stag)
+      src/evolution/evolve.cpp:1671-1717
+  compute_auxiliary_quantities(state, sstate, aux)
+      src/evolution/auxiliaries.cpp:81-180
+  linop_apply(A, B, C, AS, BS, CS, b, c)
+      include/grace/utils/tstep_utils.hh:54-229
+  evolve_impl<eos_t>() RK3 branch
+      src/evolution/evolve.cpp:190-225
+Every call goes through the C ABI of libgrace_b200.so on torch CUDA tensors
+(device memory and streams only; all arithmetic is in the CUDA library).
+Errors surface as RuntimeError with the library's status code, as GRACE's
+ERROR() macro would abort the run.
+"""
+import ctypes
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib, abi
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return ctypes.c_void_p(stream.cuda_stream)
+
+
+@dataclass
+class Fields:
+    """One evolved state: GRACE's var_array_t + staggered_variable_arrays_t.
+
+    state: (nq, 23, NZ, NY, NX) float64, bx: (nq, NZ, NY, NX+1),
+    by: (nq, NZ, NY+1, NX), bz: (nq, NZ+1, NY, NX) — C order, which is
+    GRACE's LayoutLeft (i fastest, block index slowest).
+    """
+    state: torch.Tensor
+    bx: torch.Tensor
+    by: torch.Tensor
+    bz: torch.Tensor
+
+    def c(self):
+        return abi.Fields(self.state.data_ptr(), self.bx.data_ptr(), self.by.data_ptr(),
+                          self.bz.data_ptr())
+
+    def copy_(self, other):
+        self.state.copy_(other.state)
+        self.bx.copy_(other.bx)
+        self.by.copy_(other.by)
+        self.bz.copy_(other.bz)
+        return self
+
+    def clone(self):
+        return Fields(self.state.clone(), self.bx.clone(), self.by.clone(), self.bz.clone())
+
+    def to(self, device):
+        return Fields(self.state.to(device), self.bx.to(device), self.by.to(device),
+                      self.bz.to(device))
+
+
+class Blocks:
+    """Block geometry: nq blocks of nx*ny*nz interior cells with ngz ghosts."""
+
+    def __init__(self, nx, ny, nz, ngz, nq, idx, coords=None, device="cuda"):
+        self.nx, self.ny, self.nz, self.ngz, self.nq = nx, ny, nz, ngz, nq
+        self.NX, self.NY, self.NZ = nx + 2 * ngz, ny + 2 * ngz, nz + 2 * ngz
+        self.idx = torch.as_tensor(idx, dtype=torch.float64, device=device).reshape(nq, 3).contiguous()
+        self.coords = (None if coords is None else
+                       torch.as_tensor(coords, dtype=torch.float64, device=device).reshape(nq, 3).contiguous())
+        self.device = device
+
+    def c(self):
+        return abi.Grid(self.nx, self.ny, self.nz, self.ngz, self.nq, self.idx.data_ptr(),
+                        self.coords.data_ptr() if self.coords is not None else None)
+
+    def new_fields(self):
+        z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=self.device)
+        return Fields(z(self.nq, abi.N_EVOL_VARS, self.NZ, self.NY, self.NX),
+                      z(self.nq, self.NZ, self.NY, self.NX + 1),
+                      z(self.nq, self.NZ, self.NY + 1, self.NX),
+                      z(self.nq, self.NZ + 1, self.NY, self.NX))
+
+    def new_aux(self):
+        return torch.zeros(self.nq, abi.N_AUX_VARS, self.NZ, self.NY, self.NX,
+                           dtype=torch.float64, device=self.device)
+
+
+class GRMHDEquationsSystem:
+    """grmhd_equations_system_t<eos_t> + the evolve.cpp drivers, on the GPU."""
+
+    def __init__(self, params):
+        self.lib = _lib.load()
+        self.params = params
+        h = ctypes.c_void_p()
+        _lib.check(self.lib.grb_create(ctypes.byref(h), ctypes.byref(params)), "grb_create")
+        self.h = h
+        self._grid = None
+
+    def close(self):
+        if self.h:
+            self.lib.grb_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reserve(self, blocks):
+        self._grid = blocks.c()
+        _lib.check(self.lib.grb_reserve(self.h, ctypes.byref(self._grid)), "grb_reserve")
+        self.blocks = blocks
+
+    def advance_substep(self, t, dt, dtfact, new_state, old_state, aux, stream=None):
+        g = self.blocks.c()
+        nf, of = new_state.c(), old_state.c()
+        _lib.check(self.lib.grb_advance_substep(self.h, ctypes.byref(g), t, dt, dtfact,
+                                                ctypes.byref(nf), ctypes.byref(of), _ptr(aux),
+                                                _stream_ptr(stream)), "grb_advance_substep")
+
+    def compute_auxiliary_quantities(self, state, aux, stream=None):
+        g = self.blocks.c()
+        f = state.c()
+        _lib.check(self.lib.grb_compute_auxiliary_quantities(self.h, ctypes.byref(g), ctypes.byref(f),
+                                                             _ptr(aux), _stream_ptr(stream)),
+                   "grb_compute_auxiliary_quantities")
+
+    def reset_c2p_diagnostics(self, aux, stream=None):
+        g = self.blocks.c()
+        _lib.check(self.lib.grb_reset_c2p_diagnostics(self.h, ctypes.byref(g), _ptr(aux),
+                                                      _stream_ptr(stream)), "grb_reset_c2p_diagnostics")
+
+    def linop_apply(self, A, B, C, b, c=0.0, stream=None):
+        g = self.blocks.c()
+        fa, fb = A.c(), B.c()
+        fc = C.c() if C is not None else None
+        _lib.check(self.lib.grb_linop_apply(self.h, ctypes.byref(g), ctypes.byref(fa), ctypes.byref(fb),
+                                            ctypes.byref(fc) if fc is not None else None, b, c,
+                                            _stream_ptr(stream)), "grb_linop_apply")
+
+    def fill_ghosts_brick(self, fields, nb, periodic, stream=None):
+        g = self.blocks.c()
+        f = fields.c()
+        per = (ctypes.c_int32 * 3)(*[int(bool(x)) for x in periodic])
+        _lib.check(self.lib.grb_fill_ghosts_brick(self.h, ctypes.byref(g), ctypes.byref(f), nb[0], nb[1],
+                                                  nb[2], per, _stream_ptr(stream)), "grb_fill_ghosts_brick")
+
+    def conservs_to_prims(self, cons, metric=None, cons_out=None, err=None, use_learned=False,
+                          stream=None):
+        """Batched c2p: cons (10, n) float64 -> prims (13, n)."""
+        n = cons.shape[1]
+        prims = torch.empty(abi.P_CS2 + 1, n, dtype=torch.float64, device=cons.device)
+        _lib.check(self.lib.grb_c2p_batch(self.h, n, _ptr(cons), _ptr(metric), _ptr(prims), _ptr(cons_out),
+                                          _ptr(err), 1 if use_learned else 0, _stream_ptr(stream)),
+                   "grb_c2p_batch")
+        return prims
+
+    def status(self):
+        st = abi.Status()
+        _lib.check(self.lib.grb_get_status(self.h, ctypes.byref(st)), "grb_get_status")
+        return st
+
+    # --- evolve_impl<eos_t>() RK3 branch (evolve.cpp:147-225, 427-428) -----
+    def rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, stream=None):
+        """One SSP-RK3 step.  `bc(fields)` applies the boundary conditions
+        (GRACE's amr::apply_boundary_conditions); on entry aux holds the
+        primitives of `state` and state_p equals state."""
+        self.reset_c2p_diagnostics(aux, stream)
+        self.advance_substep(t, dt, 1.0, state_p, state, aux, stream)
+        bc(state_p)
+        self.compute_auxiliary_quantities(state_p, aux, stream)
+        self.linop_apply(state_pp, state, state_p, 0.75, 0.25, stream)
+        self.advance_substep(t, dt, 0.25, state_pp, state_p, aux, stream)
+        bc(state_pp)
+        self.compute_auxiliary_quantities(state_pp, aux, stream)
+        self.linop_apply(state, state, state_pp, 1.0 / 3, 2.0 / 3.0, stream)
+        self.advance_substep(t, dt, 2.0 / 3.0, state, state_pp, aux, stream)
+        bc(state)
+        self.compute_auxiliary_quantities(state, aux, stream)
+        self.linop_apply(state_p, state, None, 1.0, 0.0, stream)

@@ -1,0 +1,221 @@
+"""Seeded synthetic inputs of the benchmark configurations (numpy, host).
+
+None of these is a public benchmark suite; they are initial data written
+directly from the configuration text (the reference's own initial-data
+routines for these setups are absent or differ, see the design notes):
+  * Balsara-1 shock tube (ideal gas Gamma=2), 1024x16x16 cells in 16^3 blocks
+  * 3-D blast wave (ideal gas Gamma=4/3), 256^3 cells in 4096 blocks of 16^3
+  * c2p micro-benchmark states (hybrid EOS K=100, Gamma=2, Gamma_th=1.8)
+Initial data follow GRACE's convention (src/physics/grmhd.cpp:380-530):
+primitives into aux, the metric into state, face B = B * sqrt(gamma), then
+conserved variables from the primitives (set_conservs_from_prims,
+src/physics/grmhd.cpp:676-759) — here on the flat metric.
+"""
+import numpy as np
+
+from . import abi
+
+SEED = 0x6A5CE
+
+
+def flat_prims_to_cons(rho, press, eps, z, B, s, ye=None):
+    """Conserved variables on the flat metric (sqrt(gamma)=1, alpha=1, beta=0).
+
+    rho, press, eps, s: (...); z, B: (3, ...).  Returns (7, ...) in the order
+    DENS, SX, SY, SZ, TAU, YESTAR, ENTROPYSTAR."""
+    W = np.sqrt(1.0 + np.sum(z * z, axis=0))
+    Bz = np.sum(B * z, axis=0)
+    b = (B + Bz[None] * z) / W[None]
+    b2 = (np.sum(B * B, axis=0) + Bz * Bz) / (W * W)
+    rhoh = rho * (1.0 + eps) + press + b2
+    D = rho * W
+    tau = rhoh * W * W - press - 0.5 * b2 - Bz * Bz - D
+    S = rhoh[None] * W[None] * z - Bz[None] * b
+    out = np.zeros((7,) + rho.shape)
+    out[0] = D
+    out[1:4] = S
+    out[4] = tau
+    out[5] = D * (0.0 if ye is None else ye)
+    out[6] = s * D
+    return out
+
+
+class BrickSetup:
+    """A brick of nbx*nby*nbz blocks of n^3 cells on [lo, hi]^3 (flat metric)."""
+
+    def __init__(self, nb, n, lo, hi, ngz=4, periodic=(False, False, False)):
+        self.nb = tuple(nb)
+        self.n = tuple(n)
+        self.ngz = ngz
+        self.lo = np.asarray(lo, float)
+        self.hi = np.asarray(hi, float)
+        self.periodic = tuple(periodic)
+        self.nq = nb[0] * nb[1] * nb[2]
+        self.dx = (self.hi - self.lo) / (np.asarray(nb) * np.asarray(n))
+        self.N = tuple(ni + 2 * ngz for ni in n)
+
+    def idx(self):
+        return np.tile(1.0 / self.dx, (self.nq, 1))
+
+    def block_origin(self, q):
+        qc = (q % self.nb[0], (q // self.nb[0]) % self.nb[1], q // (self.nb[0] * self.nb[1]))
+        return np.array([self.lo[a] + qc[a] * self.n[a] * self.dx[a] for a in range(3)])
+
+    def coords(self):
+        """Centre of cell (0,0,0) (a ghost cell) of each block."""
+        return np.stack([self.block_origin(q) + (0.5 - self.ngz) * self.dx for q in range(self.nq)])
+
+    def cell_centres(self):
+        """(nq, 3, NZ, NY, NX) physical cell centres, ghosts included."""
+        NX, NY, NZ = self.N
+        i = np.arange(NX)
+        j = np.arange(NY)
+        k = np.arange(NZ)
+        out = np.empty((self.nq, 3, NZ, NY, NX))
+        for q in range(self.nq):
+            o = self.block_origin(q)
+            out[q, 0] = o[0] + (i[None, None, :] - self.ngz + 0.5) * self.dx[0]
+            out[q, 1] = o[1] + (j[None, :, None] - self.ngz + 0.5) * self.dx[1]
+            out[q, 2] = o[2] + (k[:, None, None] - self.ngz + 0.5) * self.dx[2]
+        return out
+
+    def global_cell_index(self):
+        """(nq, NZ, NY, NX) global (unwrapped) integer cell coordinates."""
+        NX, NY, NZ = self.N
+        gi = np.empty((self.nq, 3, NZ, NY, NX), dtype=np.int64)
+        for q in range(self.nq):
+            qc = (q % self.nb[0], (q // self.nb[0]) % self.nb[1], q // (self.nb[0] * self.nb[1]))
+            gi[q, 0] = qc[0] * self.n[0] + np.arange(NX)[None, None, :] - self.ngz
+            gi[q, 1] = qc[1] * self.n[1] + np.arange(NY)[None, :, None] - self.ngz
+            gi[q, 2] = qc[2] * self.n[2] + np.arange(NZ)[:, None, None] - self.ngz
+        return gi
+
+    def empty(self):
+        NX, NY, NZ = self.N
+        nq = self.nq
+        state = np.zeros((nq, abi.N_EVOL_VARS, NZ, NY, NX))
+        bx = np.zeros((nq, NZ, NY, NX + 1))
+        by = np.zeros((nq, NZ, NY + 1, NX))
+        bz = np.zeros((nq, NZ + 1, NY, NX))
+        aux = np.zeros((nq, abi.N_AUX_VARS, NZ, NY, NX))
+        # flat Cowling metric: g = 1, alpha = 1, beta = K = 0
+        state[:, abi.GXX] = state[:, abi.GYY] = state[:, abi.GZZ] = 1.0
+        state[:, abi.ALP] = 1.0
+        return state, bx, by, bz, aux
+
+
+def _counter_uniform(gid, seed, nx_glob):
+    """U(-1,1) from a counter hash of the global cell index (block-order free)."""
+    key = (gid[:, 0].astype(np.uint64) + np.uint64(nx_glob[0]) *
+           (gid[:, 1].astype(np.uint64) + np.uint64(nx_glob[1]) * gid[:, 2].astype(np.uint64)))
+    x = key * np.uint64(0x9E3779B97F4A7C15) + np.uint64(seed)
+    x ^= x >> np.uint64(30)
+    x *= np.uint64(0xBF58476D1CE4E5B9)
+    x ^= x >> np.uint64(27)
+    x *= np.uint64(0x94D049BB133111EB)
+    x ^= x >> np.uint64(31)
+    return (x >> np.uint64(11)).astype(np.float64) / float(1 << 53) * 2.0 - 1.0
+
+
+def _fill(setup, gamma, rho, press, B_cell, Bface_fn):
+    """Write primitives / conserved / face B for an ideal gas on the flat metric."""
+    state, bx, by, bz, aux = setup.empty()
+    eps = press / ((gamma - 1.0) * rho)
+    T = eps * (gamma - 1.0)
+    s = np.log(eps) / (gamma - 1.0) - np.log(rho)
+    z = np.zeros((3,) + rho.shape)
+    Bx, By, Bz = Bface_fn(bx.shape, by.shape, bz.shape)
+    bx[:], by[:], bz[:] = Bx, By, Bz
+    Bc = np.stack([0.5 * (bx[..., :-1] + bx[..., 1:]),
+                   0.5 * (by[:, :, :-1, :] + by[:, :, 1:, :]),
+                   0.5 * (bz[:, :-1] + bz[:, 1:])])
+    cons = flat_prims_to_cons(rho, press, eps, z, Bc, s)
+    state[:, 0:7] = np.moveaxis(cons, 0, 1)
+    aux[:, abi.RHO] = rho
+    aux[:, abi.PRESS] = press
+    aux[:, abi.EPS] = eps
+    aux[:, abi.TEMP] = T
+    aux[:, abi.ENTROPY] = s
+    aux[:, abi.BX:abi.BZ + 1] = np.moveaxis(Bc, 0, 1)
+    return state, bx, by, bz, aux
+
+
+def blast(nb=(16, 16, 16), n=(16, 16, 16), ngz=4, seed=SEED):
+    """3-D blast wave: Gamma=4/3, rho=1e-4 / p=5e-4 outside, rho=1e-2 / p=1
+    inside r<0.8, Bx=0.1, domain [-6,6]^3, pressure x (1 + 1e-3 U(-1,1))
+    seeded per global cell.  Outflow boundaries."""
+    su = BrickSetup(nb, n, (-6, -6, -6), (6, 6, 6), ngz, (False, False, False))
+    X = su.cell_centres()
+    r = np.sqrt(np.sum(X * X, axis=1))
+    inside = r < 0.8
+    rho = np.where(inside, 1e-2, 1e-4)
+    press = np.where(inside, 1.0, 5e-4)
+    gid = su.global_cell_index()
+    ng = np.asarray(nb) * np.asarray(n) + 2 * ngz
+    u = _counter_uniform(np.moveaxis(gid, 1, -1).reshape(-1, 3) + ngz, seed, ng).reshape(rho.shape)
+    press = press * (1.0 + 1e-3 * u)
+
+    def faces(sx, sy, sz):
+        return np.full(sx, 0.1), np.zeros(sy), np.zeros(sz)
+
+    return su, _fill(su, 4.0 / 3.0, rho, press, None, faces)
+
+
+def balsara1(nb=(64, 1, 1), n=(16, 16, 16), ngz=4):
+    """Balsara-1 shock tube: Gamma=2; left rho=1,p=1,B=(0.5,1,0); right
+    rho=0.125,p=0.1,B=(0.5,-1,0); x in [-0.5,0.5], y,z in [-1/128,1/128]
+    (1024x16x16 cells at the default size); periodic y,z, outflow x."""
+    su = BrickSetup(nb, n, (-0.5, -1 / 128, -1 / 128), (0.5, 1 / 128, 1 / 128), ngz,
+                    (False, True, True))
+    X = su.cell_centres()
+    left = X[:, 0] < 0.0
+    rho = np.where(left, 1.0, 0.125)
+    press = np.where(left, 1.0, 0.1)
+    NX, NY, NZ = su.N
+
+    def faces(sx, sy, sz):
+        Bx = np.full(sx, 0.5)
+        # By lives on y-faces at cell-centred x
+        xl = X[:, 0][:, :, :1, :]  # (nq, NZ, 1, NX)
+        By = np.broadcast_to(np.where(xl < 0.0, 1.0, -1.0), sy).copy()
+        return Bx, By, np.zeros(sz)
+
+    return su, _fill(su, 2.0, rho, press, None, faces)
+
+
+def c2p_states(n, seed=SEED, kappa=100.0, gamma=2.0, gamma_th=1.8):
+    """c2p micro-benchmark states on the flat metric with the hybrid EOS:
+    rho log-U[1e-12,1e-3], eps_th log-U[1e-6,10] above the cold curve,
+    W U[1,50), sigma=b^2/rho log-U[1e-4,1e3], isotropic directions for the
+    velocity and the field.  Returns (cons (10,n), prims (13,n))."""
+    rng = np.random.default_rng(seed)
+    rho = 10 ** rng.uniform(-12, -3, n)
+    eth = 10 ** rng.uniform(-6, 1, n)
+    W = rng.uniform(1.0, 50.0, n)
+    sig = 10 ** rng.uniform(-4, 3, n)
+
+    def unit():
+        v = rng.standard_normal((3, n))
+        return v / np.linalg.norm(v, axis=0)[None]
+
+    z = np.sqrt(W * W - 1.0)[None] * unit()
+    ec = kappa * rho ** (gamma - 1.0) / (gamma - 1.0)
+    eps = ec + eth
+    gm = gamma_th - 1.0
+    press = kappa * rho ** gamma + gm * rho * eth
+    T = eth * gm
+    s = np.log(np.maximum(eth, 1e-13) * rho ** (-gm)) / gm
+    Bd = unit()
+    Bzd = np.sum(Bd * z, axis=0)
+    b2_unit = (1.0 + Bzd * Bzd) / (W * W)
+    B = np.sqrt(sig * rho / b2_unit)[None] * Bd
+    cons7 = flat_prims_to_cons(rho, press, eps, z, B, s)
+    cons = np.zeros((10, n))
+    cons[0:7] = cons7
+    cons[7:10] = B
+    prims = np.zeros((13, n))
+    prims[abi.P_RHO], prims[abi.P_PRESS], prims[abi.P_EPS] = rho, press, eps
+    prims[abi.P_ZX:abi.P_ZZ + 1] = z
+    prims[abi.P_TEMP], prims[abi.P_ENT] = T, s
+    prims[abi.P_BX:abi.P_BZ + 1] = B
+    return cons, prims

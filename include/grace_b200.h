@@ -1,0 +1,228 @@
+/*
+ * grace_b200.h — C ABI of the B200-native Cowling GRMHD stage library.
+ *
+ * The library replaces GRACE's Cowling-metric GRMHD right-hand-side-and-
+ * update path on one GPU.  GRACE's host side (p4est forest, ghost exchange,
+ * regrid, I/O) keeps ownership of its Kokkos views and passes their raw
+ * device pointers (view.data()) through this interface; the library borrows
+ * them for the duration of a call and owns only its own scratch.
+ *
+ * Array layout contract (GRACE LayoutLeft, i fastest):
+ *   state  (nx+2g, ny+2g, nz+2g, GRB_N_EVOL_VARS, nq)    var_array_t
+ *   aux    (nx+2g, ny+2g, nz+2g, GRB_N_AUX_VARS,  nq)    var_array_t
+ *   bx     (nx+2g+1, ny+2g, nz+2g, 1, nq)                face_staggered_fields_x
+ *   by     (nx+2g, ny+2g+1, nz+2g, 1, nq)                face_staggered_fields_y
+ *   bz     (nx+2g, ny+2g, nz+2g+1, 1, nq)                face_staggered_fields_z
+ *   idx    (3, nq)  inverse cell spacings, idx[d + 3*q]   getinvspacings()
+ * Variable indices follow include/grace/data_structures/variable_indices.hh
+ * (Cowling build): evolved DENS..ENTROPYSTAR (0-6), GXX..GZZ (7-12), ALP (13),
+ * BETAX..BETAZ (14-16), KXX..KZZ (17-22); aux RHO, ZVEC(3), B(3), YE, TEMP,
+ * ENTROPY, EPS, PRESS, BDIV, C2P_DENS_ERR, C2P_ERR (0-14).
+ *
+ * All calls are ordered on the CUDA stream passed in (a cudaStream_t given
+ * as void*, NULL = legacy default stream); the caller synchronises.  Every
+ * entry point returns GRB_OK (0) or a negative GRB_ERR_* code; device-side
+ * fatal conditions (the reference's Kokkos::abort sites) are recorded in a
+ * device status word read back by grb_get_status(), never by a trap.
+ */
+#ifndef GRACE_B200_H
+#define GRACE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- variable counts and indices (variable_indices.hh:162-287) ---------- */
+#define GRB_N_HRSC 7
+#define GRB_N_EVOL_VARS 23
+#define GRB_N_AUX_VARS 15
+enum grb_evol_index {
+  GRB_DENS = 0, GRB_SX, GRB_SY, GRB_SZ, GRB_TAU, GRB_YESTAR, GRB_ENTROPYSTAR,
+  GRB_GXX, GRB_GXY, GRB_GXZ, GRB_GYY, GRB_GYZ, GRB_GZZ, GRB_ALP,
+  GRB_BETAX, GRB_BETAY, GRB_BETAZ,
+  GRB_KXX, GRB_KXY, GRB_KXZ, GRB_KYY, GRB_KYZ, GRB_KZZ
+};
+enum grb_aux_index {
+  GRB_RHO = 0, GRB_ZVECX, GRB_ZVECY, GRB_ZVECZ, GRB_BX, GRB_BY, GRB_BZ,
+  GRB_YE, GRB_TEMP, GRB_ENTROPY, GRB_EPS, GRB_PRESS, GRB_BDIV,
+  GRB_C2P_DENS_ERR, GRB_C2P_ERR
+};
+/* local cons / prims orderings of one cell (grmhd_helpers.hh:105-149) */
+enum grb_cons_local { GRB_C_DENS = 0, GRB_C_STX, GRB_C_STY, GRB_C_STZ, GRB_C_TAU,
+                      GRB_C_YES, GRB_C_ENTS, GRB_C_BSX, GRB_C_BSY, GRB_C_BSZ,
+                      GRB_NUM_CONS };
+enum grb_prims_local { GRB_P_RHO = 0, GRB_P_PRESS, GRB_P_ZX, GRB_P_ZY, GRB_P_ZZ,
+                       GRB_P_YE, GRB_P_TEMP, GRB_P_EPS, GRB_P_ENT, GRB_P_BX,
+                       GRB_P_BY, GRB_P_BZ, GRB_P_CS2, GRB_NUM_PRIMS };
+
+/* ---- status codes -------------------------------------------------------- */
+enum grb_status_code {
+  GRB_OK = 0,
+  GRB_ERR_INVALID = -1,     /* bad argument / unsupported option */
+  GRB_ERR_CUDA = -2,        /* a CUDA runtime call failed */
+  GRB_ERR_NOMEM = -3,       /* scratch allocation failed */
+  GRB_ERR_NOT_RESERVED = -4 /* grb_reserve was not called for this grid */
+};
+/* bits of grb_status.device_flags: device-side conditions the reference
+ * turns into Kokkos::abort (c2p.hh:167-316); the kernels record and go on
+ * with the lenient branch instead. */
+enum grb_device_flag {
+  GRB_FLAG_C2P_RHO_TOO_HIGH = 1u << 0,
+  GRB_FLAG_EOS_RHO_TOO_HIGH = 1u << 1,
+  GRB_FLAG_EOS_EPS_TOO_HIGH = 1u << 2,
+  GRB_FLAG_EOS_TEMP_TOO_HIGH = 1u << 3,
+  GRB_FLAG_EOS_PRESS_TOO_HIGH = 1u << 4,
+  GRB_FLAG_BAD_LEARNED_BRACKET = 1u << 8 /* informational: fallback taken */
+};
+
+/* ---- scheme selectors (runtime; the reference picks them in CMake) ------- */
+enum grb_eos_kind { GRB_EOS_IDEAL_GAS = 0, GRB_EOS_HYBRID_PWPOLY = 1 };
+enum grb_recon_kind { GRB_RECON_WENOZ = 0, GRB_RECON_MC2 = 1,
+                      GRB_RECON_MINMOD = 2, GRB_RECON_DONOR = 3 };
+enum grb_riemann_kind { GRB_RIEMANN_HLL = 0, GRB_RIEMANN_LLF = 1 };
+enum grb_emf_kind { GRB_EMF_GS = 0, GRB_EMF_UCT = 1 };
+
+#define GRB_MAX_PIECES 8
+
+/* EOS description (eos_storage.cpp:160-190, piecewise_polytropic_eos.hh,
+ * hybrid_eos.hh, ideal_gas_eos.hh).  grb_eos_setup_pwpoly() fills the
+ * derived pw_* tables from kappa_0 / gammas / rhos exactly as GRACE's
+ * setup_cold_polytrope does. */
+typedef struct grb_eos_params {
+  int32_t kind;          /* grb_eos_kind */
+  int32_t n_pieces;      /* hybrid: number of polytropic pieces (<= 8) */
+  double gamma;          /* ideal gas adiabatic index */
+  double pw_kappa[GRB_MAX_PIECES];
+  double pw_gamma[GRB_MAX_PIECES];
+  double pw_rho[GRB_MAX_PIECES];   /* segment lower densities, pw_rho[0] = 0 */
+  double pw_eps[GRB_MAX_PIECES];
+  double pw_press[GRB_MAX_PIECES];
+  double gamma_th;       /* hybrid thermal index */
+  double eps_max;        /* eos.eps_maximum (c2p eps ceiling) */
+  double entropy_min;    /* eos.entropy_minimum */
+  double temp_atm;       /* EOS atmosphere temperature = grmhd.atmosphere.temp_fl */
+} grb_eos_params;
+
+/* Runtime parameters of the path (grmhd_helpers.hh:41-96 POD structs). */
+typedef struct grb_params {
+  grb_eos_params eos;
+  /* atmosphere: grmhd.atmosphere.* */
+  double rho_fl, ye_fl, temp_fl, atmo_tol;
+  /* excision: grmhd.excision.* */
+  int32_t excise_by_radius;
+  double r_ex, alp_ex, rho_ex, temp_ex, ye_ex;
+  /* c2p: grmhd.c2p.* */
+  double c2p_tol, max_w, max_sigma, beta_fallback, alp_bh_thresh;
+  int32_t use_ent_backup;
+  /* Riemann: grmhd.riemann.rusanov_use_c_limit */
+  double rusanov_use_c_limit;
+  /* FOFC: GRACE_ENABLE_FOFC + grmhd.fofc.* */
+  int32_t fofc_enable, dmp_enable;
+  double dmp_M;
+  /* scheme selection */
+  int32_t recon, riemann, emf;
+} grb_params;
+
+/* Block geometry shared by all blocks of a call. */
+typedef struct grb_grid {
+  int32_t nx, ny, nz, ngz;  /* interior cells per block, ghost width (>= 4) */
+  int64_t nq;               /* number of blocks (quadrants) */
+  const double* idx;        /* device (3, nq): inverse spacings */
+  const double* coords;     /* device (3, nq) or NULL: Cartesian centre of
+                               cell (0,0,0) of each block (ghosts included);
+                               required only for radius-based excision */
+} grb_grid;
+
+/* One evolved state: cell-centred vars + the three face-staggered B arrays. */
+typedef struct grb_fields {
+  double* state;
+  double* bx;
+  double* by;
+  double* bz;
+} grb_fields;
+
+typedef struct grb_status {
+  uint32_t device_flags;    /* OR of grb_device_flag since the last clear */
+  int32_t last_error;       /* last grb_status_code returned */
+  int64_t fofc_faces;       /* faces recomputed by FOFC in the last stage */
+  int64_t fofc_edges;       /* edges recomputed by FOFC in the last stage */
+} grb_status;
+
+typedef struct grb_handle grb_handle;
+
+/* ---- parameter helpers (host only) --------------------------------------- */
+/* Fill p with GRACE's schema defaults (parameters/grmhd.yaml, eos.yaml) for
+ * an EOS of the given kind; EOS-specific numbers still have to be set. */
+void grb_params_defaults(grb_params* p, int32_t eos_kind);
+/* Derive pw_kappa/pw_eps/pw_press from kappa_0, gammas[n], rhos[n-1]
+ * (eos_storage.cpp:53-100, setup_cold_polytrope). */
+int grb_eos_setup_pwpoly(grb_eos_params* e, int32_t n_pieces, double kappa_0,
+                         const double* gammas, const double* rhos);
+
+/* ---- lifetime ------------------------------------------------------------ */
+/* Replaces eos_storage_t construction + the get_*_params() lookups
+ * (grmhd_helpers.hh:163-292): validates p and uploads it. */
+int grb_create(grb_handle** out, const grb_params* p);
+int grb_destroy(grb_handle* h);
+/* Size library-owned scratch (fluxes, face/edge EMFs, FOFC tags) for grid g;
+ * mirrors resize_aux_staging_and_flux_buffers (variables.cpp:227-). */
+int grb_reserve(grb_handle* h, const grb_grid* g);
+int grb_get_status(grb_handle* h, grb_status* st);
+int grb_clear_status(grb_handle* h);
+
+/* ---- the hot path -------------------------------------------------------- */
+/* = grace::advance_substep<eos_t>(t, dt, dtfact, new_state, old_state,
+ *   new_stag, old_stag) (src/evolution/evolve.cpp:1671-1717): fluxes, EMFs,
+ *   FOFC flag + correction, flux divergence + geometric sources, CT update.
+ *   aux must hold the primitives of old_state. */
+int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt,
+                        double dtfact, const grb_fields* new_state,
+                        const grb_fields* old_state, const double* aux,
+                        void* stream);
+/* = grace::compute_auxiliary_quantities<eos_t>(state, sstate, aux)
+ *   (src/evolution/auxiliaries.cpp:81-180): c2p on every cell including
+ *   ghosts, conservative rewrites, C2P_ERR sticky-OR, BDIV, and (GS) the
+ *   cell-centred E used by the next stage's EMF. */
+int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g,
+                                     const grb_fields* state, double* aux,
+                                     void* stream);
+/* = the reset_c2p_diagnostics kernel at the top of evolve_impl
+ *   (evolve.cpp:154-161). */
+int grb_reset_c2p_diagnostics(grb_handle* h, const grb_grid* g, double* aux,
+                              void* stream);
+/* = grace::linop_apply (include/grace/utils/tstep_utils.hh:54-229):
+ *   A = b*B (C == NULL) or A = b*B + c*C on cells and faces, all 23 vars. */
+int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A,
+                    const grb_fields* B, const grb_fields* C, double b,
+                    double c, void* stream);
+/* Batched c2p on n independent states (the unit of the c2p micro-benchmark):
+ *   cons   [GRB_NUM_CONS][n] densitized conserved incl. cell-centred B*sqrtg
+ *   metric [10][n] gxx,gxy,gxz,gyy,gyz,gzz,betax,betay,betaz,alp, or NULL
+ *          for the flat metric
+ *   prims  [GRB_NUM_PRIMS][n] out; cons_out [GRB_NUM_CONS][n] out or NULL
+ *   err    [n] out: c2p_err bits (c2p.hh:98-121); NULL allowed
+ *   use_learned: 1 = seed the root bracket with the learned model loaded by
+ *          grb_load_c2p_model (falls back per state when it misses). */
+int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons,
+                  const double* metric, double* prims, double* cons_out,
+                  uint32_t* err, int32_t use_learned, void* stream);
+
+
+/* ---- harness-side helper (outside the reference's hot path) -------------- */
+/* Ghost fill for a brick of nbx*nby*nbz same-level blocks (block q at
+ * (q % nbx, (q / nbx) % nby, q / (nbx*nby))): periodic axes copy from the
+ * neighbouring block, the others copy the nearest interior cell / face
+ * (zero-gradient outflow, extrap_bc_t<0> of
+ * include/grace/amr/ghostzone_kernels/phys_bc_kernels.hh:169).  Stands in for
+ * GRACE's amr::apply_boundary_conditions on a unigrid brick; exchanges the
+ * 7 evolved HRSC variables and the three face-B arrays. */
+int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
+                          int32_t nby, int32_t nbz, const int32_t* periodic, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRACE_B200_H */

@@ -1,0 +1,216 @@
+// Pinning build — test infrastructure only.  Compiled (with the shim headers
+// in oracle/ref/shim) against the GRACE sources where they lie, together
+// with GRACE's src/physics/eos/c2p.cpp, into oracle/_ref/libgrace_ref.so.
+// It binds the reference's OWN per-cell numerics (SymPy kernels, WENO-Z /
+// slope-limited reconstruction, HLLE, EOS classes, conservs_to_prims,
+// Gardiner-Stone edge EMF, 4-point face interpolation, 6th-order
+// derivatives) to the shared loop drivers of stage_driver.hpp and exports
+// them with the ref_ prefix.  Tests compare the oracle (orc_) against it.
+#include <grace_config.h>
+
+#include <grace/physics/grmhd_subexpressions.hh>
+#include <grace/physics/fd_subexpressions.hh>
+#include <grace/physics/eos/c2p.hh>
+#include <grace/physics/grmhd_helpers.hh>
+#include <grace/utils/reconstruction.hh>
+#include <grace/utils/weno_reconstruction.hh>
+#include <grace/utils/riemann_solvers.hh>
+
+#include "stage_driver.hpp"
+
+namespace refglue {
+
+using hyb_t = grace::hybrid_eos_t<grace::piecewise_polytropic_eos_t>;
+using ideal_t = grace::ideal_gas_eos_t;
+
+struct Eos {
+  int kind = 0;
+  ideal_t ideal;
+  hyb_t hyb;
+};
+
+// 1-D stencil adapter: u(i,j,k) over a short array, with the stencil along i.
+struct Line {
+  const double* v;
+  int base;
+  double operator()(int i, int, int) const { return v[i - base]; }
+};
+// 5-index adapter for face_interp_4: view(i,j,k,ivar,q)
+struct Line5 {
+  const double* v;
+  int base;
+  double operator()(int i, int, int, int, int) const { return v[i - base]; }
+};
+
+template <class St>
+struct EfaceV {
+  St* s;
+  double operator()(int i, int j, int k, int c, int dir, int q) const { return s->EF(i, j, k, c, dir, q); }
+};
+template <class St>
+struct EcV {
+  St* s;
+  double operator()(int i, int j, int k, int c, int q) const { return s->EC(i, j, k, c, q); }
+};
+template <class St>
+struct FluxV {
+  St* s;
+  double operator()(int i, int j, int k, int v, int dir, int q) const { return s->F(i, j, k, v, dir, q); }
+};
+
+struct RefNumerics {
+  using Eos = refglue::Eos;
+  static Eos make_eos(const grb_eos_params& p) {
+    Eos e;
+    e.kind = p.kind;
+    if (p.kind == GRB_EOS_IDEAL_GAS) {
+      grace::shim_param_table()["eos.ideal_gas_eos.gamma"] = p.gamma;
+      grace::shim_param_table()["eos.ideal_gas_eos.kappa_id"] = 0.0;
+      e.ideal = ideal_t(p.temp_atm, p.eps_max);
+    } else {
+      using V = Kokkos::View<double[grace::piecewise_polytropic_eos_t::max_n_pieces], grace::default_space>;
+      V k, g, r, ep, pr;
+      for (int i = 0; i < GRB_MAX_PIECES; ++i) {
+        k(i) = p.pw_kappa[i]; g(i) = p.pw_gamma[i]; r(i) = p.pw_rho[i];
+        ep(i) = p.pw_eps[i]; pr(i) = p.pw_press[i];
+      }
+      grace::piecewise_polytropic_eos_t cold(k, g, r, ep, pr, p.n_pieces, 1e+10, 1e-100);
+      e.hyb = hyb_t(cold, p.gamma_th - 1., p.entropy_min, 1. + 1e-10, 1, p.eps_max, p.temp_atm);
+    }
+    return e;
+  }
+  static grace::metric_array_t gm(const double g[6], const double b[3], double alp) {
+    return grace::metric_array_t({g[0], g[1], g[2], g[3], g[4], g[5]}, {b[0], b[1], b[2]}, alp);
+  }
+  static orc::Metric metric(const double g[6], const double b[3], double alp) {
+    const auto m = gm(g, b, alp);
+    orc::Metric o;
+    for (int a = 0; a < 6; ++a) { o.g[a] = m._g[a]; o.ginv[a] = m._ginv[a]; }
+    for (int a = 0; a < 3; ++a) o.beta[a] = m._beta[a];
+    o.alp = m._alp;
+    o.sqrtg = m._sqrtg;
+    return o;
+  }
+  static void recon(int kind, const double u[6], double& L, double& R) {
+    Line v{u, 0};
+    if (kind == GRB_RECON_WENOZ) { grace::weno_reconstructor_t<5> r; r(v, 3, 0, 0, L, R, 0); }
+    else if (kind == GRB_RECON_MC2) { grace::slope_limited_reconstructor_t<grace::MCbeta> r; r(v, 3, 0, 0, L, R, 0); }
+    else if (kind == GRB_RECON_MINMOD) { grace::slope_limited_reconstructor_t<grace::minmod> r; r(v, 3, 0, 0, L, R, 0); }
+    else { grace::donor_cell_reconstructor_t r; r(v, 3, 0, 0, L, R, 0); }
+  }
+  static double face_interp4(double a, double b, double c, double d) {
+    const double v[4] = {a, b, c, d};
+    Line5 w{v, 0};
+    return grace::face_interp_4(w, 2, 0, 0, 0, 0, 0);
+  }
+  static double fd6(double m3, double m2, double m1, double p1, double p2, double p3, double h) {
+    const double v[7] = {m3, m2, m1, 0.0, p1, p2, p3};
+    Line w{v, 0};
+    double du;
+    fd_der_x<6>(w, 3, 0, 0, h, &du);
+    return du;
+  }
+  static double press_eps_csnd2__temp_rho(const Eos& e, double& eps, double& cs2, double& t, double& r) {
+    grace::eos_err_t err;
+    double ye = 0.0;
+    if (e.kind == GRB_EOS_IDEAL_GAS) return e.ideal.press_eps_csnd2__temp_rho_ye(eps, cs2, t, r, ye, err);
+    return e.hyb.press_eps_csnd2__temp_rho_ye(eps, cs2, t, r, ye, err);
+  }
+  static double lorentz(const double g[6], const double z[3]) {
+    double W;
+    grmhd_get_W(g, z, &W);
+    return W;
+  }
+  static void comoving_b(double alp, const double* beta, const double* g, const double* B,
+                         const double* z, double W, double b[4], double& b2) {
+    double bb[4];
+    grmhd_get_smallbu_smallb2(alp, beta, g, B, z, W, &bb, &b2);
+    for (int i = 0; i < 4; ++i) b[i] = bb[i];
+  }
+  static void vtilde(double alp, const double* beta, const double* z, double W, double vt[3]) {
+    double v[3];
+    grmhd_get_vtildeu(alp, beta, z, W, &v);
+    for (int i = 0; i < 3; ++i) vt[i] = v[i];
+  }
+  static void char_speeds(double alp, const double* beta, double rho, double p, double eps,
+                          double cs2, double W, double b2, const double* vt, double guu, int d,
+                          double& cm, double& cp) {
+    grmhd_get_cm_cp(alp, beta, rho, p, eps, cs2, W, b2, vt, guu, d, &cm, &cp);
+  }
+  static void cons_and_flux(double alp, const double* beta, const double* g, double rho, double p,
+                            double eps, const double* z, double s, double W, double b2,
+                            const double* b, const double* vt, int d, double& D, double& tau,
+                            double S[3], double& ents, double& fD, double& ft, double fS[3],
+                            double& fe) {
+    double st[3], fst[3];
+    grmhd_get_fluxes(alp, beta, g, rho, p, eps, z, s, W, b2, b, vt, d, &D, &tau, &st, &ents, &fD,
+                     &ft, &fst, &fe);
+    for (int i = 0; i < 3; ++i) { S[i] = st[i]; fS[i] = fst[i]; }
+  }
+  static void geom_sources(double alp, const double* beta, const double* g, const double* guu,
+                           const double* K, const double* dalp, const double* dg, const double* db,
+                           double rho, double p, double eps, const double* B, const double* z,
+                           double W, double& st, double sS[3]) {
+    double s3[3];
+    grmhd_get_geom_sources(alp, beta, g, guu, K, dalp, dg, db, rho, p, eps, B, z, W, &st, &s3);
+    for (int i = 0; i < 3; ++i) sS[i] = s3[i];
+  }
+  static double hll(double fL, double fR, double uL, double uR, double cmin, double cmax) {
+    grace::hll_riemann_solver_t s;
+    return s(fL, fR, uL, uR, cmin, cmax);
+  }
+  static void prims_to_conservs(const double pr[13], double c[10], const orc::Metric& m) {
+    grace::grmhd_prims_array_t p;
+    grace::grmhd_cons_array_t cc{};
+    for (int v = 0; v < 13; ++v) p[v] = pr[v];
+    grace::prims_to_conservs(p, cc, gm(m.g, m.beta, m.alp));
+    for (int v = 0; v < 10; ++v) c[v] = cc[v];
+  }
+  static bool c2p_counted(double cons[10], double pr[13], const orc::Metric& m, const Eos& e,
+                          const grb_params& P, double r, uint32_t& err, bool dry, int& fatal,
+                          double alp_bh_override, int* iters) {
+    atmo_params_t atmo{P.ye_fl, P.rho_fl, P.temp_fl, 0.0, 0.0, P.atmo_tol};
+    excision_params_t ex{P.rho_ex, P.temp_ex, P.ye_ex, P.r_ex, P.alp_ex, P.excise_by_radius != 0};
+    c2p_params_t cp{P.c2p_tol, P.max_w, P.max_sigma, P.beta_fallback, P.use_ent_backup != 0,
+                    alp_bh_override > 0 ? alp_bh_override : P.alp_bh_thresh};
+    grace::grmhd_cons_array_t c;
+    grace::grmhd_prims_array_t p{};
+    for (int v = 0; v < 10; ++v) c[v] = cons[v];
+    grace::c2p_err_t ce;
+    double rtp[3] = {r, 0.0, 0.0};
+    bool fl = false;
+    try {
+      if (e.kind == GRB_EOS_IDEAL_GAS)
+        fl = grace::conservs_to_prims<ideal_t>(c, p, gm(m.g, m.beta, m.alp), e.ideal, atmo, ex, cp, rtp, ce, dry);
+      else
+        fl = grace::conservs_to_prims<hyb_t>(c, p, gm(m.g, m.beta, m.alp), e.hyb, atmo, ex, cp, rtp, ce, dry);
+    } catch (...) {
+      fatal |= 1 << 30;  // the reference aborted here
+    }
+    for (int v = 0; v < 10; ++v) cons[v] = c[v];
+    for (int v = 0; v < 13; ++v) pr[v] = p[v];
+    err = (uint32_t)ce.words[0];
+    if (iters) *iters = 0;
+    return fl;
+  }
+  static bool c2p(double cons[10], double pr[13], const orc::Metric& m, const Eos& e,
+                  const grb_params& P, double r, uint32_t& err, bool dry, int& fatal,
+                  double alp_bh_override) {
+    return c2p_counted(cons, pr, m, e, P, r, err, dry, fatal, alp_bh_override, nullptr);
+  }
+  template <class St>
+  static double gs_edge(St& s, int dir, int i, int j, int k, int64_t q) {
+    EfaceV<St> ef{&s};
+    EcV<St> ec{&s};
+    FluxV<St> fl{&s};
+    if (dir == 0) return grace::gs_edge_emf_x(ef, ec, fl, i, j, k, (int)q);
+    if (dir == 1) return grace::gs_edge_emf_y(ef, ec, fl, i, j, k, (int)q);
+    return grace::gs_edge_emf_z(ef, ec, fl, i, j, k, (int)q);
+  }
+};
+
+}  // namespace refglue
+
+#define NUMERICS refglue::RefNumerics
+#define API(name) ref_##name
+#include "api_impl.hpp"

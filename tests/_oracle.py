@@ -1,0 +1,155 @@
+"""ctypes access to the CPU oracle (oracle/liboracle.so) and, when it was
+built in this checkout, the reference-numerics pinning build
+(oracle/_ref/libgrace_ref.so).  Test infrastructure only."""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from grace_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+ORACLE = os.path.join(ROOT, "oracle", "liboracle.so")
+REF = os.path.join(ROOT, "oracle", "_ref", "libgrace_ref.so")
+
+VP = C.c_void_p
+
+
+def _bind(lib, pre):
+    P = C.POINTER
+    sig = {
+        "create": (VP, [P(abi.Params), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int64]),
+        "destroy": (None, [VP]),
+        "advance_substep": (C.c_int, [VP, VP, VP, C.c_double, C.c_double] + [VP] * 9),
+        "compute_aux": (C.c_int, [VP, VP, VP] + [VP] * 5),
+        "reset_diag": (None, [VP, VP]),
+        "linop": (None, [VP] + [VP] * 12 + [C.c_double, C.c_double]),
+        "scratch": (C.c_int64, [VP, C.c_int, VP]),
+        "fofc_counts": (None, [VP, P(C.c_int64), P(C.c_int64)]),
+        "c2p_batch": (C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP, VP, VP, VP, C.c_int32, VP]),
+        "prims_to_conservs": (C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP]),
+        "eos_press_eps_csnd2_temp_rho": (C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP, VP, VP]),
+        "recon": (None, [C.c_int, C.c_int64, VP, VP, VP]),
+        "kernels": (None, [C.c_int64, VP, C.c_int, VP]),
+        "geom_sources": (None, [C.c_int64, VP, VP]),
+        "fill_ghosts_brick": (None, [C.c_int] * 7 + [VP, VP, VP, VP, VP]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, pre + name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def build_oracle():
+    """Build liboracle.so (and the pinning build when the GRACE sources are
+    present) with oracle/Makefile."""
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
+    if os.path.isdir("/root/reference/src"):
+        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+
+
+_cache = {}
+
+
+def lib(which="orc"):
+    if which in _cache:
+        return _cache[which]
+    path = ORACLE if which == "orc" else REF
+    if not os.path.exists(path):
+        if which == "orc":
+            build_oracle()
+        if not os.path.exists(path):
+            return None
+    L = _bind(C.CDLL(path), which + "_")
+    _cache[which] = L
+    return L
+
+
+def p(a):
+    return a.ctypes.data_as(VP) if a is not None else None
+
+
+class Stage:
+    """Oracle stage driver on host numpy arrays (GRACE LayoutLeft shapes)."""
+
+    def __init__(self, params, nx, ny, nz, g, nq, which="orc"):
+        self.L = lib(which)
+        self.pre = which + "_"
+        self.params = params
+        self.h = getattr(self.L, self.pre + "create")(C.byref(params), nx, ny, nz, g, nq)
+
+    def __del__(self):
+        try:
+            getattr(self.L, self.pre + "destroy")(self.h)
+        except Exception:
+            pass
+
+    def advance_substep(self, idx, dt, dtfact, new, old, aux, coords=None):
+        return getattr(self.L, self.pre + "advance_substep")(
+            self.h, p(idx), p(coords), dt, dtfact, p(new[0]), p(new[1]), p(new[2]), p(new[3]),
+            p(old[0]), p(old[1]), p(old[2]), p(old[3]), p(aux))
+
+    def compute_aux(self, idx, st, aux, coords=None):
+        return getattr(self.L, self.pre + "compute_aux")(self.h, p(idx), p(coords), p(st[0]), p(st[1]),
+                                                         p(st[2]), p(st[3]), p(aux))
+
+    def reset_diag(self, aux):
+        getattr(self.L, self.pre + "reset_diag")(self.h, p(aux))
+
+    def linop(self, A, B, Cf, b, c):
+        Cp = [p(x) for x in Cf] if Cf is not None else [None] * 4
+        getattr(self.L, self.pre + "linop")(self.h, *[p(x) for x in A], *[p(x) for x in B], *Cp, b, c)
+
+    def fofc_counts(self):
+        f, e = C.c_int64(), C.c_int64()
+        getattr(self.L, self.pre + "fofc_counts")(self.h, C.byref(f), C.byref(e))
+        return f.value, e.value
+
+    def scratch(self, which):
+        n = getattr(self.L, self.pre + "scratch")(self.h, which, None)
+        out = np.empty(n)
+        getattr(self.L, self.pre + "scratch")(self.h, which, p(out))
+        return out
+
+
+def fill_ghosts(which, setup, fields):
+    L = lib(which)
+    per = np.asarray([int(x) for x in setup.periodic], dtype=np.int32)
+    getattr(L, which + "_fill_ghosts_brick")(setup.n[0], setup.n[1], setup.n[2], setup.ngz,
+                                             setup.nb[0], setup.nb[1], setup.nb[2], p(per),
+                                             p(fields[0]), p(fields[1]), p(fields[2]), p(fields[3]))
+
+
+def rk3_step(st, setup, dt, state, state_p, state_pp, aux, which="orc"):
+    """One SSP-RK3 step of evolve_impl (evolve.cpp:147-225) on host arrays."""
+    idx = setup.idx().copy()
+    bc = lambda f: fill_ghosts(which, setup, f)
+    st.reset_diag(aux)
+    st.advance_substep(idx, dt, 1.0, state_p, state, aux)
+    bc(state_p)
+    st.compute_aux(idx, state_p, aux)
+    st.linop(state_pp, state, state_p, 0.75, 0.25)
+    st.advance_substep(idx, dt, 0.25, state_pp, state_p, aux)
+    bc(state_pp)
+    st.compute_aux(idx, state_pp, aux)
+    st.linop(state, state, state_pp, 1.0 / 3, 2.0 / 3.0)
+    st.advance_substep(idx, dt, 2.0 / 3.0, state, state_pp, aux)
+    bc(state)
+    st.compute_aux(idx, state, aux)
+    st.linop(state_p, state, None, 1.0, 0.0)
+
+
+def c2p_batch(params, cons, metric=None, which="orc", dry_run=False):
+    L = lib(which)
+    n = cons.shape[1]
+    cons = np.ascontiguousarray(cons)
+    pr = np.zeros((13, n))
+    co = np.zeros((10, n))
+    err = np.zeros(n, np.uint32)
+    fl = np.zeros(n, np.int32)
+    it = np.zeros(n, np.int32)
+    rc = getattr(L, which + "_c2p_batch")(C.byref(params), n, p(cons), p(metric), p(pr), p(co), p(err),
+                                          p(fl), 1 if dry_run else 0, p(it))
+    return pr, co, err, fl, it, rc

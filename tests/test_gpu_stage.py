@@ -1,0 +1,93 @@
+"""GPU GRMHD stage (through the C ABI) against the CPU oracle on small grids."""
+import numpy as np
+import pytest
+import torch
+
+import _oracle
+from grace_b200 import abi, params, workloads
+from grace_b200.host import Blocks, Fields, GRMHDEquationsSystem
+from parity import cons_rel_err, interior
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-10   # state-normalised relative error after one RK3 step
+
+
+def _setup(name):
+    if name == "blast":
+        P = params.blast()
+        su, f = workloads.blast(nb=(2, 2, 2), n=(8, 8, 8))
+        cfl = 0.25
+    else:
+        P = params.balsara1()
+        su, f = workloads.balsara1(nb=(4, 1, 1), n=(8, 8, 8))
+        cfl = 0.4
+    return P, su, f, cfl / su.idx()[0, 0]
+
+
+def _gpu_run(P, su, f, dt, nsteps):
+    dev = torch.device("cuda:0")
+    st, bx, by, bz, aux = f
+    blocks = Blocks(su.n[0], su.n[1], su.n[2], su.ngz, su.nq, su.idx(), device=dev)
+    g = GRMHDEquationsSystem(P)
+    g.reserve(blocks)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    state = Fields(T(st), T(bx), T(by), T(bz))
+    aux_d = T(aux)
+    bc = lambda fl: g.fill_ghosts_brick(fl, su.nb, su.periodic)
+    bc(state)
+    g.compute_auxiliary_quantities(state, aux_d)
+    sp, spp = state.clone(), state.clone()
+    for _ in range(nsteps):
+        g.rk3_step(dt, state, sp, spp, aux_d, bc)
+    torch.cuda.synchronize()
+    return [x.cpu().numpy() for x in (state.state, state.bx, state.by, state.bz)], aux_d.cpu().numpy(), g
+
+
+def _oracle_run(P, su, f, dt, nsteps):
+    st, bx, by, bz, aux = [x.copy() for x in f]
+    S = _oracle.Stage(P, su.n[0], su.n[1], su.n[2], su.ngz, su.nq)
+    state = [st, bx, by, bz]
+    _oracle.fill_ghosts("orc", su, state)
+    S.compute_aux(su.idx().copy(), state, aux)
+    sp = [x.copy() for x in state]
+    spp = [x.copy() for x in state]
+    for _ in range(nsteps):
+        _oracle.rk3_step(S, su, dt, state, sp, spp, aux)
+    return state, aux, S
+
+
+@pytest.mark.parametrize("name", ["blast", "balsara"])
+def test_one_rk3_step_matches_oracle(name):
+    P, su, f, dt = _setup(name)
+    gs, ga, g = _gpu_run(P, su, f, dt, 1)
+    os_, oa, S = _oracle_run(P, su, f, dt, 1)
+    e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
+    assert e.max() < STEP_TOL, e
+    for a, b in zip(gs[1:], os_[1:]):
+        d = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+        assert d < STEP_TOL
+    # aux primitives of the new state
+    for v in (abi.RHO, abi.PRESS, abi.EPS):
+        r = np.max(np.abs(ga[:, v] - oa[:, v]) / np.abs(oa[:, v]))
+        assert r < STEP_TOL, (v, r)
+    np.testing.assert_array_equal(ga[:, abi.C2P_ERR], oa[:, abi.C2P_ERR])
+
+
+def test_div_b_and_conservation_blast():
+    P, su, f, dt = _setup("blast")
+    gs, ga, g = _gpu_run(P, su, f, dt, 3)
+    bd = interior(ga[:, abi.BDIV], su.ngz)
+    assert np.max(np.abs(bd)) < 1e-13
+
+
+def test_fofc_flags_match_oracle():
+    P, su, f, dt = _setup("blast")
+    # a large time step makes the tentative states fail and FOFC act
+    dt = 0.9 / su.idx()[0, 0]
+    gs, ga, g = _gpu_run(P, su, f, dt, 1)
+    os_, oa, S = _oracle_run(P, su, f, dt, 1)
+    st = g.status()
+    assert st.fofc_faces == S.fofc_counts()[0]
+    e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
+    assert e.max() < STEP_TOL, e
