@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark: GRMHD zone-updates/s per RK stage on the 3-D blast wave.
+
+Workload: 256^3 cells in 4096 blocks of 16^3 (4 ghost layers), ideal gas
+Gamma=4/3, WENO-Z + HLLE + Gardiner-Stone CT + FOFC, SSP-RK3, flat Cowling
+metric, seeded synthetic initial data.  One step = one full RK3 step (three
+stages, each advance_substep + ghost fill + c2p/aux), so
+value = interior cells x 3 x steps / time.  Inputs (the block arrays, ~60 GB
+with scratch) are far larger than L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N>1: one process per GPU (torchrun), each rank advances its own copy of the
+workload (weak scaling, no collective in the data path); time = max over
+ranks of the device-timed region.  `--impl reference` times the CPU
+reference numerics (oracle/_ref: GRACE's own per-cell functions compiled in
+place, driven by the restated loop drivers) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+# algorithmic FP64 bytes per item of each kernel kind (unique array
+# footprint the kernel must touch; see the design notes for the accounting)
+ALGO_BYTES = {
+    # per face: 10 reconstructed aux vars + 10 metric comps + face B read
+    # per cell crossed, 7 fluxes + 2 face EMFs written
+    "flux": 8 * (10 + 10 + 1 + 9),
+    # per cell incl. ghosts: 7 cons + 3 face B + 10 metric + C2P_ERR read;
+    # 12 aux + C2P_ERR + 3 E_centre + ENTROPYSTAR written
+    "aux": 8 * (7 + 3 + 10 + 1 + 12 + 1 + 3 + 1),
+    # per interior cell: 21 face fluxes, 9 aux, 16 metric/curvature, 7 cons RMW
+    "update": 8 * (21 + 9 + 16 + 14),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--nb", type=int, default=16, help="blocks per axis")
+    ap.add_argument("--n", type=int, default=16, help="cells per block per axis")
+    ap.add_argument("--cfl", type=float, default=0.25)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-c2p", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.idx)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[0]) for r in self.rows if len(r) >= 8 and r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if len(r) >= 8 and r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 8 for k in range(4)
+                          if r[4 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_run(nb_side, n, cfl, min_s=10.0, which="ref"):
+    """Time RK3 steps of the blast wave on the CPU with the reference numerics
+    (or the oracle port if the pinning build is absent).  Bounded sample:
+    the central nb_side^3 blocks of the full grid (same cell size).
+    Returns (zone-updates/s, cores, kind, sample description)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import _oracle
+    from grace_b200 import params, workloads
+    lib = _oracle.lib(which)
+    kind = "reference"
+    if lib is None:
+        which, kind = "orc", "port"
+    half = 6.0 * nb_side / 16.0 * (n / 16.0) * 16.0 / n
+    su, f = workloads.blast(nb=(nb_side,) * 3, n=(n, n, n), lo=(-half,) * 3, hi=(half,) * 3)
+    P = params.blast()
+    st, bx, by, bz, aux = [x.copy() for x in f]
+    S = _oracle.Stage(P, n, n, n, su.ngz, su.nq, which)
+    state = [st, bx, by, bz]
+    _oracle.fill_ghosts(which, su, state)
+    S.compute_aux(su.idx().copy(), state, aux)
+    sp = [x.copy() for x in state]
+    spp = [x.copy() for x in state]
+    dt = cfl / su.idx()[0, 0]
+    done = 0
+    t0 = time.perf_counter()
+    while done < 1 or time.perf_counter() - t0 < min_s:
+        _oracle.rk3_step(S, su, dt, state, sp, spp, aux, which)
+        done += 1
+    el = time.perf_counter() - t0
+    zu = su.nq * n ** 3 * 3 * done
+    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+    sample = (f"{done} RK3 step(s) of the blast wave on the central {nb_side}^3 blocks of "
+              f"{n}^3 cells (same cell size), {kind} numerics, OpenMP over blocks")
+    return zu / el, cores, kind, sample
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    nb_side = 4
+    vals = []
+    cpu = None
+    for _ in range(args.warmup):
+        cpu_reference_run(nb_side, args.n, args.cfl, min_s=0.0)
+    for _ in range(args.steps):
+        v, cores, kind, sample = cpu_reference_run(nb_side, args.n, args.cfl, min_s=10.0)
+        vals.append(v)
+        cpu = (cores, kind, sample)
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference", "metric": "GRMHD zone-updates/s per RK stage", "value": value,
+        "unit": "zone-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "blast wave 256^3 (4096 blocks of 16^3), sampled: central 4^3 blocks",
+                   "cells_per_block": args.n, "ngz": 4},
+        "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": cpu[0], "kind": cpu[1],
+                         "sample": cpu[2]},
+        "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def build_blast_on_device(blocks, su, nb, n, dev, torch, fields_cls, chunk=256):
+    from grace_b200 import workloads
+    st = blocks.new_fields()
+    aux = blocks.new_aux()
+    for q0 in range(0, su.nq, chunk):
+        q1 = min(su.nq, q0 + chunk)
+        _, (s, bx, by, bz, a) = workloads.blast(nb=(nb,) * 3, n=(n,) * 3, qr=(q0, q1))
+        st.state[q0:q1].copy_(torch.from_numpy(s))
+        st.bx[q0:q1].copy_(torch.from_numpy(bx))
+        st.by[q0:q1].copy_(torch.from_numpy(by))
+        st.bz[q0:q1].copy_(torch.from_numpy(bz))
+        aux[q0:q1].copy_(torch.from_numpy(a))
+    return st, aux
+
+
+def ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from grace_b200 import abi, params, workloads
+    from grace_b200.host import Blocks, Fields, GRMHDEquationsSystem
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    nb, n = args.nb, args.n
+    su = workloads.BrickSetup((nb,) * 3, (n,) * 3, (-6,) * 3, (6,) * 3, 4, (False,) * 3)
+    blocks = Blocks(n, n, n, 4, su.nq, su.idx(), device=dev)
+    P = params.blast()
+    g = GRMHDEquationsSystem(P)
+    g.reserve(blocks)
+    state, aux = build_blast_on_device(blocks, su, nb, n, dev, torch, Fields)
+    bc = lambda f: g.fill_ghosts_brick(f, su.nb, su.periodic)
+    bc(state)
+    g.compute_auxiliary_quantities(state, aux)
+    sp, spp = state.clone(), state.clone()
+    dt = args.cfl / su.idx()[0, 0]
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        g.rk3_step(dt, state, sp, spp, aux, bc)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    g.set_kernel_timing(True)
+    st0 = g.status()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        g.rk3_step(dt, state, sp, spp, aux, bc)
+    e1.record()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    kt = g.kernel_times()
+    g.set_kernel_timing(False)
+    st1 = g.status()
+    launches = st1.launches - st0.launches
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    zu_rank = su.nq * n ** 3 * 3 * args.steps
+    value = zu_rank * world / (ms * 1e-3)
+
+    # --- end to end: evolved variables from / to pinned host memory each step
+    e2e = None
+    if not args.no_e2e:
+        hs = torch.empty((su.nq, abi.N_HRSC) + tuple(state.state.shape[2:]), dtype=torch.float64,
+                         pin_memory=True)
+        hb = [torch.empty(x.shape, dtype=torch.float64, pin_memory=True) for x in (state.bx, state.by, state.bz)]
+        hs.copy_(state.state[:, :abi.N_HRSC])
+        for h, d in zip(hb, (state.bx, state.by, state.bz)):
+            h.copy_(d)
+        ksteps = max(1, min(args.steps, 3))
+        torch.cuda.synchronize()
+        barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record()
+        for _ in range(ksteps):
+            state.state[:, :abi.N_HRSC].copy_(hs, non_blocking=True)
+            for h, d in zip(hb, (state.bx, state.by, state.bz)):
+                d.copy_(h, non_blocking=True)
+            g.compute_auxiliary_quantities(state, aux)
+            sp.copy_(state)
+            g.rk3_step(dt, state, sp, spp, aux, bc)
+            hs.copy_(state.state[:, :abi.N_HRSC], non_blocking=True)
+            for h, d in zip(hb, (state.bx, state.by, state.bz)):
+                h.copy_(d, non_blocking=True)
+        f1.record()
+        torch.cuda.synchronize()
+        ems = f0.elapsed_time(f1)
+        if world > 1:
+            t = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        nbytes = hs.numel() * 8 + sum(h.numel() * 8 for h in hb)
+        e2e = {"value": su.nq * n ** 3 * 3 * ksteps * world / (ems * 1e-3), "unit": "zone-updates/s",
+               "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ksteps,
+               "note": "evolved variables (7 HRSC + face B) copied host->device and back every step; "
+                       "each step recomputes the primitives of the uploaded state first"}
+
+    # --- dominant kernel roofline (HBM), measured over the timed region
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    top = max(kt.items(), key=lambda kv: kv[1][0])
+    name, (kms, kcnt) = top
+    items = {
+        "flux": 3 * su.nq * (n + 3) * (n + 8) ** 2 / 3.0,
+        "aux": su.nq * (n + 8) ** 3,
+        "update": su.nq * n ** 3,
+    }
+    roof = None
+    if name in ALGO_BYTES and kcnt:
+        bytes_per_launch = ALGO_BYTES[name] * items[name]
+        per_launch_ms = kms / kcnt
+        ach = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+        roof = {"bound": "hbm", "kernel": name, "achieved": ach, "peak": hbm, "unit": "GB/s",
+                "frac": ach / hbm, "peak_source": peak_src, "traffic": None,
+                "launch_ms": per_launch_ms,
+                "note": "FP64 arithmetic, not HBM, binds this kernel (see profiles/)"}
+
+    # --- c2p micro-benchmark (2^24 states, plain)
+    c2p = None
+    if not args.no_c2p and rank == 0:
+        cons, _ = workloads.c2p_states(1 << 24, seed=5)
+        gc = GRMHDEquationsSystem(params.c2p_bench())
+        c_d = torch.from_numpy(cons).to(dev)
+        del cons
+        for _ in range(2):
+            gc.conservs_to_prims(c_d)
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(5):
+            gc.conservs_to_prims(c_d)
+        a1.record()
+        torch.cuda.synchronize()
+        c2p = {"plain_solves_per_s": (1 << 24) * 5 / (a0.elapsed_time(a1) * 1e-3), "states": 1 << 24,
+               "tolerance": 1e-12}
+        gc.close()
+
+    cpu = None
+    if rank == 0 and not args.no_cpu and world == 1:
+        v, cores, kind, sample = cpu_reference_run(4, n, args.cfl, min_s=10.0)
+        cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": kind, "sample": sample}
+
+    if rank == 0:
+        line = {
+            "metric": "GRMHD zone-updates/s per RK stage", "value": value, "unit": "zone-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded blast-wave initial data)",
+            "config": {"workload": f"blast wave {nb * n}^3 ({su.nq} blocks of {n}^3), Gamma=4/3, "
+                                   "WENO-Z+HLLE+GS CT+FOFC, SSP-RK3",
+                       "blocks": su.nq, "cells_per_block": n ** 3, "ngz": 4,
+                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}"},
+            "clocks": clk, "gpu_launches": launches,
+            "kernel_ms": {k: round(v[0], 3) for k, v in kt.items() if v[1]},
+            "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "c2p": c2p,
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ours(args, rank, world, local_rank)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -28,6 +28,8 @@ RIEMANN_HLL, RIEMANN_LLF = 0, 1
 EMF_GS, EMF_UCT = 0, 1
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_RESERVED = 0, -1, -2, -3, -4
+KIND_NAMES = ["flux", "emf", "fofc_flag", "fofc_fix", "update", "ct", "aux", "linop", "ghost",
+              "c2p", "other"]
 
 
 class EosParams(C.Structure):
@@ -81,7 +83,8 @@ class Fields(C.Structure):
 
 class Status(C.Structure):
     _fields_ = [("device_flags", C.c_uint32), ("last_error", C.c_int32),
-                ("fofc_faces", C.c_int64), ("fofc_edges", C.c_int64)]
+                ("fofc_faces", C.c_int64), ("fofc_edges", C.c_int64),
+                ("launches", C.c_int64)]
 
 
 # Every extern "C" symbol declared in include/grace_b200.h, with its
@@ -108,6 +111,9 @@ PROTOTYPES = {
                                   C.c_double, C.c_void_p]),
     "grb_c2p_batch": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "grb_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "grb_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
+                                   C.c_int32]),
     "grb_fill_ghosts_brick": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields),
                                         C.c_int32, C.c_int32, C.c_int32,
                                         C.POINTER(C.c_int32), C.c_void_p]),

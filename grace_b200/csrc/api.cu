@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "grace_b200.h"
 #include "stage_kernels.cuh"
@@ -27,6 +28,14 @@ struct grb_handle {
   uint32_t* d_flags = nullptr;
   unsigned long long* d_counters = nullptr;
   int last_error = GRB_OK;
+  int64_t launches = 0;  // kernels launched through this handle
+  // optional per-kernel-kind timing with events on the launching stream
+  bool timing = false;
+  struct Mark { int kind; cudaEvent_t a, b; };
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> pool;
+  double kind_ms[GRB_KIND_COUNT] = {0};
+  int64_t kind_n[GRB_KIND_COUNT] = {0};
 };
 
 namespace {
@@ -113,6 +122,35 @@ inline Box box(int l0, int l1, int l2, int n0, int n1, int n2, int64_t nq) {
 }
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+cudaEvent_t take_event(grb_handle* h) {
+  if (!h->pool.empty()) {
+    cudaEvent_t e = h->pool.back();
+    h->pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+// Brackets the launches between begin() and end() with a pair of events
+// when timing is on; a no-op otherwise.
+struct KScope {
+  grb_handle* h;
+  cudaStream_t s;
+  int kind;
+  cudaEvent_t a = nullptr;
+  KScope(grb_handle* h_, cudaStream_t s_, int k) : h(h_), s(s_), kind(k) {
+    if (h->timing) { a = take_event(h); cudaEventRecord(a, s); }
+  }
+  ~KScope() {
+    if (h->timing) {
+      cudaEvent_t b = take_event(h);
+      cudaEventRecord(b, s);
+      h->marks.push_back({kind, a, b});
+    }
+  }
+};
+
 }  // namespace
 
 extern "C" {
@@ -194,6 +232,8 @@ static void free_scratch(grb_handle* h) {
 
 int grb_destroy(grb_handle* h) {
   if (!h) return GRB_ERR_INVALID;
+  for (auto& m : h->marks) { cudaEventDestroy(m.a); cudaEventDestroy(m.b); }
+  for (auto e : h->pool) cudaEventDestroy(e);
   free_scratch(h);
   cudaFree(h->d_flags);
   cudaFree(h->d_counters);
@@ -248,6 +288,7 @@ int grb_get_status(grb_handle* h, grb_status* st) {
   st->last_error = h->last_error;
   st->fofc_faces = (int64_t)c[0];
   st->fofc_edges = (int64_t)c[1];
+  st->launches = h->launches;
   return GRB_OK;
 }
 
@@ -278,29 +319,47 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt, d
     lo[dir] = gz - 1;
     n[dir] = (dir == 0 ? G.nx : dir == 1 ? G.ny : G.nz) + 3;
     const Box b = box(lo[0], lo[1], lo[2], n[0], n[1], n[2], G.nq);
+    KScope ks(h, s, GRB_KIND_FLUX);
     if (dir == 0) k_flux<0><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, old->state, aux, bf[0], B);
     if (dir == 1) k_flux<1><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, old->state, aux, bf[1], B);
     if (dir == 2) k_flux<2><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, old->state, aux, bf[2], B);
+    ++h->launches;
   }
   const Box eb = box(gz, gz, gz, G.nx + 1, G.ny + 1, G.nz + 1, G.nq);
+  {
+  KScope ks(h, s, GRB_KIND_EMF);
   if (P.emf == GRB_EMF_GS)
     k_emf_gs<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, B);
   else
     k_emf_uct<<<nblk(eb.count(), T), T, 0, s>>>(P, G, eb, old->bx, old->by, old->bz, B);
+  ++h->launches;
+  }
   if (P.fofc && P.emf == GRB_EMF_GS) {
     const int64_t nf = G.fcells * G.nq * 3;
     CK(cudaMemsetAsync(B.ftag, 0, (size_t)nf, s));
     CK(cudaMemsetAsync(B.etag, 0, (size_t)nf, s));
     CK(cudaMemsetAsync(B.counters, 0, 2 * sizeof(unsigned long long), s));
     const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, G.nq);
+    {
+    KScope ks(h, s, GRB_KIND_FOFC_FLAG);
     k_fofc_flag<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, dt, dtfact, nw->state, old->state, old->bx,
-                                                   old->by, old->bz, g->idx, g->coords, B);
-    k_fofc_faces<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by, old->bz, B);
-    k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B);
+                                                   old->by, old->bz, g->idx, g->coords, B); ++h->launches;
+    }
+    {
+    KScope ks(h, s, GRB_KIND_FOFC_FIX);
+    k_fofc_faces<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by, old->bz, B); ++h->launches;
+    k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B); ++h->launches;
+    }
   }
   const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, G.nq);
-  k_update<<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, nw->state, old->state, aux, g->idx, B);
-  k_ct<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, dt, dtfact, nw->bx, nw->by, nw->bz, g->idx, B);
+  {
+  KScope ks(h, s, GRB_KIND_UPDATE);
+  k_update<<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, nw->state, old->state, aux, g->idx, B); ++h->launches;
+  }
+  {
+  KScope ks(h, s, GRB_KIND_CT);
+  k_ct<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, dt, dtfact, nw->bx, nw->by, nw->bz, g->idx, B); ++h->launches;
+  }
   CK(cudaGetLastError());
   return GRB_OK;
 }
@@ -313,8 +372,9 @@ int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g, const grb
   if (!st || !st->state || !st->bx || !st->by || !st->bz || !aux) return fail(h, GRB_ERR_INVALID);
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   const Box b = box(0, 0, 0, G.NX, G.NY, G.NZ, G.nq);
+  KScope ks(h, (cudaStream_t)stream, GRB_KIND_AUX);
   k_aux<<<nblk(b.count(), 128), 128, 0, (cudaStream_t)stream>>>(h->dp, G, b, st->state, st->bx, st->by,
-                                                                  st->bz, aux, g->idx, g->coords, h->B);
+                                                                  st->bz, aux, g->idx, g->coords, h->B); ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;
 }
@@ -325,7 +385,8 @@ int grb_reset_c2p_diagnostics(grb_handle* h, const grb_grid* g, double* aux, voi
   if (rc) return fail(h, rc);
   if (!aux) return fail(h, GRB_ERR_INVALID);
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
-  k_reset_diag<<<1184, 256, 0, (cudaStream_t)stream>>>(G, aux);
+  KScope ks(h, (cudaStream_t)stream, GRB_KIND_OTHER);
+  k_reset_diag<<<1184, 256, 0, (cudaStream_t)stream>>>(G, aux); ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;
 }
@@ -342,7 +403,11 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A, const
   double* a[4] = {A->state, A->bx, A->by, A->bz};
   const double* x[4] = {Bf->state, Bf->bx, Bf->by, Bf->bz};
   const double* y[4] = {Cf ? Cf->state : nullptr, Cf ? Cf->bx : nullptr, Cf ? Cf->by : nullptr, Cf ? Cf->bz : nullptr};
-  for (int v = 0; v < 4; ++v) k_linop<<<148 * 16, 256, 0, s>>>(n[v], a[v], x[v], y[v], b, c);
+  KScope ks(h, s, GRB_KIND_LINOP);
+  for (int v = 0; v < 4; ++v) {
+    k_linop<<<148 * 16, 256, 0, s>>>(n[v], a[v], x[v], y[v], b, c);
+    ++h->launches;
+  }
   CK(cudaGetLastError());
   return GRB_OK;
 }
@@ -353,8 +418,9 @@ int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons, const double* me
   if (n < 0 || (n > 0 && (!cons || !prims))) return fail(h, GRB_ERR_INVALID);
   if (use_learned) return fail(h, GRB_ERR_INVALID);  // model loading is separate
   if (n == 0) return GRB_OK;
+  KScope ks(h, (cudaStream_t)stream, GRB_KIND_C2P);
   k_c2p_batch<<<nblk(n, 128), 128, 0, (cudaStream_t)stream>>>(h->dp, n, cons, metric, prims, cons_out, err,
-                                                               nullptr, h->d_flags);
+                                                               nullptr, h->d_flags); ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;
 }
@@ -372,11 +438,45 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
   for (int a = 0; a < 3; ++a) br.periodic[a] = periodic[a] != 0;
   cudaStream_t s = (cudaStream_t)stream;
   double* bf[3] = {f->bx, f->by, f->bz};
+  KScope ks(h, s, GRB_KIND_GHOST);
   for (int ax = 0; ax < 3; ++ax) {
-    k_ghost_cells<<<148 * 8, 256, 0, s>>>(G, br, ax, f->state);
-    for (int fd = 0; fd < 3; ++fd) k_ghost_faces<<<148 * 4, 256, 0, s>>>(G, br, ax, fd, bf[fd]);
+    k_ghost_cells<<<148 * 8, 256, 0, s>>>(G, br, ax, f->state); ++h->launches;
+    for (int fd = 0; fd < 3; ++fd) {
+      k_ghost_faces<<<148 * 4, 256, 0, s>>>(G, br, ax, fd, bf[fd]);
+      ++h->launches;
+    }
   }
   CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+
+int grb_set_kernel_timing(grb_handle* h, int32_t enable) {
+  if (!h) return GRB_ERR_INVALID;
+  h->timing = enable != 0;
+  return GRB_OK;
+}
+
+int grb_kernel_times(grb_handle* h, double* ms, int64_t* counts, int32_t nkinds) {
+  if (!h || nkinds < GRB_KIND_COUNT) return GRB_ERR_INVALID;
+  if (!h->marks.empty()) {
+    CK(cudaEventSynchronize(h->marks.back().b));
+    for (auto& m : h->marks) {
+      float t = 0.f;
+      CK(cudaEventElapsedTime(&t, m.a, m.b));
+      h->kind_ms[m.kind] += t;
+      h->kind_n[m.kind] += 1;
+      h->pool.push_back(m.a);
+      h->pool.push_back(m.b);
+    }
+    h->marks.clear();
+  }
+  for (int k = 0; k < GRB_KIND_COUNT; ++k) {
+    if (ms) ms[k] = h->kind_ms[k];
+    if (counts) counts[k] = h->kind_n[k];
+    h->kind_ms[k] = 0;
+    h->kind_n[k] = 0;
+  }
   return GRB_OK;
 }
 

@@ -162,6 +162,17 @@ class GRMHDEquationsSystem:
                    "grb_c2p_batch")
         return prims
 
+    def set_kernel_timing(self, on):
+        _lib.check(self.lib.grb_set_kernel_timing(self.h, 1 if on else 0), "grb_set_kernel_timing")
+
+    def kernel_times(self):
+        """{kind: (ms, launch groups)} accumulated since the last call."""
+        n = len(abi.KIND_NAMES)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int64 * n)()
+        _lib.check(self.lib.grb_kernel_times(self.h, ms, cnt, n), "grb_kernel_times")
+        return {abi.KIND_NAMES[k]: (ms[k], cnt[k]) for k in range(n)}
+
     def status(self):
         st = abi.Status()
         _lib.check(self.lib.grb_get_status(self.h, ctypes.byref(st)), "grb_get_status")

@@ -65,34 +65,39 @@ class BrickSetup:
         """Centre of cell (0,0,0) (a ghost cell) of each block."""
         return np.stack([self.block_origin(q) + (0.5 - self.ngz) * self.dx for q in range(self.nq)])
 
-    def cell_centres(self):
+    def blocks(self, qr=None):
+        return range(self.nq) if qr is None else range(*qr)
+
+    def cell_centres(self, qr=None):
         """(nq, 3, NZ, NY, NX) physical cell centres, ghosts included."""
         NX, NY, NZ = self.N
         i = np.arange(NX)
         j = np.arange(NY)
         k = np.arange(NZ)
-        out = np.empty((self.nq, 3, NZ, NY, NX))
-        for q in range(self.nq):
+        qs = self.blocks(qr)
+        out = np.empty((len(qs), 3, NZ, NY, NX))
+        for t, q in enumerate(qs):
             o = self.block_origin(q)
-            out[q, 0] = o[0] + (i[None, None, :] - self.ngz + 0.5) * self.dx[0]
-            out[q, 1] = o[1] + (j[None, :, None] - self.ngz + 0.5) * self.dx[1]
-            out[q, 2] = o[2] + (k[:, None, None] - self.ngz + 0.5) * self.dx[2]
+            out[t, 0] = o[0] + (i[None, None, :] - self.ngz + 0.5) * self.dx[0]
+            out[t, 1] = o[1] + (j[None, :, None] - self.ngz + 0.5) * self.dx[1]
+            out[t, 2] = o[2] + (k[:, None, None] - self.ngz + 0.5) * self.dx[2]
         return out
 
-    def global_cell_index(self):
-        """(nq, NZ, NY, NX) global (unwrapped) integer cell coordinates."""
+    def global_cell_index(self, qr=None):
+        """(nq, 3, NZ, NY, NX) global (unwrapped) integer cell coordinates."""
         NX, NY, NZ = self.N
-        gi = np.empty((self.nq, 3, NZ, NY, NX), dtype=np.int64)
-        for q in range(self.nq):
+        qs = self.blocks(qr)
+        gi = np.empty((len(qs), 3, NZ, NY, NX), dtype=np.int64)
+        for t, q in enumerate(qs):
             qc = (q % self.nb[0], (q // self.nb[0]) % self.nb[1], q // (self.nb[0] * self.nb[1]))
-            gi[q, 0] = qc[0] * self.n[0] + np.arange(NX)[None, None, :] - self.ngz
-            gi[q, 1] = qc[1] * self.n[1] + np.arange(NY)[None, :, None] - self.ngz
-            gi[q, 2] = qc[2] * self.n[2] + np.arange(NZ)[:, None, None] - self.ngz
+            gi[t, 0] = qc[0] * self.n[0] + np.arange(NX)[None, None, :] - self.ngz
+            gi[t, 1] = qc[1] * self.n[1] + np.arange(NY)[None, :, None] - self.ngz
+            gi[t, 2] = qc[2] * self.n[2] + np.arange(NZ)[:, None, None] - self.ngz
         return gi
 
-    def empty(self):
+    def empty(self, qr=None):
         NX, NY, NZ = self.N
-        nq = self.nq
+        nq = len(self.blocks(qr))
         state = np.zeros((nq, abi.N_EVOL_VARS, NZ, NY, NX))
         bx = np.zeros((nq, NZ, NY, NX + 1))
         by = np.zeros((nq, NZ, NY + 1, NX))
@@ -117,9 +122,9 @@ def _counter_uniform(gid, seed, nx_glob):
     return (x >> np.uint64(11)).astype(np.float64) / float(1 << 53) * 2.0 - 1.0
 
 
-def _fill(setup, gamma, rho, press, B_cell, Bface_fn):
+def _fill(setup, gamma, rho, press, B_cell, Bface_fn, qr=None):
     """Write primitives / conserved / face B for an ideal gas on the flat metric."""
-    state, bx, by, bz, aux = setup.empty()
+    state, bx, by, bz, aux = setup.empty(qr)
     eps = press / ((gamma - 1.0) * rho)
     T = eps * (gamma - 1.0)
     s = np.log(eps) / (gamma - 1.0) - np.log(rho)
@@ -140,17 +145,21 @@ def _fill(setup, gamma, rho, press, B_cell, Bface_fn):
     return state, bx, by, bz, aux
 
 
-def blast(nb=(16, 16, 16), n=(16, 16, 16), ngz=4, seed=SEED):
+def blast(nb=(16, 16, 16), n=(16, 16, 16), ngz=4, seed=SEED, qr=None, lo=(-6, -6, -6),
+          hi=(6, 6, 6)):
     """3-D blast wave: Gamma=4/3, rho=1e-4 / p=5e-4 outside, rho=1e-2 / p=1
     inside r<0.8, Bx=0.1, domain [-6,6]^3, pressure x (1 + 1e-3 U(-1,1))
-    seeded per global cell.  Outflow boundaries."""
-    su = BrickSetup(nb, n, (-6, -6, -6), (6, 6, 6), ngz, (False, False, False))
-    X = su.cell_centres()
+    seeded per global cell.  Outflow boundaries.  qr=(q0, q1) restricts the
+    arrays to blocks q0..q1-1 (the values do not depend on the chunking);
+    lo/hi select a sub-box of the domain (same cell size for a proportional
+    block count)."""
+    su = BrickSetup(nb, n, lo, hi, ngz, (False, False, False))
+    X = su.cell_centres(qr)
     r = np.sqrt(np.sum(X * X, axis=1))
     inside = r < 0.8
     rho = np.where(inside, 1e-2, 1e-4)
     press = np.where(inside, 1.0, 5e-4)
-    gid = su.global_cell_index()
+    gid = su.global_cell_index(qr)
     ng = np.asarray(nb) * np.asarray(n) + 2 * ngz
     u = _counter_uniform(np.moveaxis(gid, 1, -1).reshape(-1, 3) + ngz, seed, ng).reshape(rho.shape)
     press = press * (1.0 + 1e-3 * u)
@@ -158,7 +167,7 @@ def blast(nb=(16, 16, 16), n=(16, 16, 16), ngz=4, seed=SEED):
     def faces(sx, sy, sz):
         return np.full(sx, 0.1), np.zeros(sy), np.zeros(sz)
 
-    return su, _fill(su, 4.0 / 3.0, rho, press, None, faces)
+    return su, _fill(su, 4.0 / 3.0, rho, press, None, faces, qr)
 
 
 def balsara1(nb=(64, 1, 1), n=(16, 16, 16), ngz=4):

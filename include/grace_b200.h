@@ -149,6 +149,7 @@ typedef struct grb_status {
   int32_t last_error;       /* last grb_status_code returned */
   int64_t fofc_faces;       /* faces recomputed by FOFC in the last stage */
   int64_t fofc_edges;       /* edges recomputed by FOFC in the last stage */
+  int64_t launches;         /* kernels launched by this handle since creation */
 } grb_status;
 
 typedef struct grb_handle grb_handle;
@@ -210,6 +211,20 @@ int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons,
                   const double* metric, double* prims, double* cons_out,
                   uint32_t* err, int32_t use_learned, void* stream);
 
+
+/* ---- measurement helpers -------------------------------------------------- */
+/* Kernel kinds for grb_kernel_times. */
+enum grb_kernel_kind {
+  GRB_KIND_FLUX = 0, GRB_KIND_EMF, GRB_KIND_FOFC_FLAG, GRB_KIND_FOFC_FIX, GRB_KIND_UPDATE,
+  GRB_KIND_CT, GRB_KIND_AUX, GRB_KIND_LINOP, GRB_KIND_GHOST, GRB_KIND_C2P, GRB_KIND_OTHER,
+  GRB_KIND_COUNT
+};
+/* When enabled, every launch group is bracketed by CUDA events recorded on
+ * the caller's stream.  grb_kernel_times synchronises on the last event,
+ * returns the summed milliseconds and launch-group counts per kind
+ * (arrays of GRB_KIND_COUNT) and resets the accumulators. */
+int grb_set_kernel_timing(grb_handle* h, int32_t enable);
+int grb_kernel_times(grb_handle* h, double* ms, int64_t* counts, int32_t nkinds);
 
 /* ---- harness-side helper (outside the reference's hot path) -------------- */
 /* Ghost fill for a brick of nbx*nby*nbz same-level blocks (block q at

@@ -83,11 +83,14 @@ def test_div_b_and_conservation_blast():
 
 def test_fofc_flags_match_oracle():
     P, su, f, dt = _setup("blast")
-    # a large time step makes the tentative states fail and FOFC act
-    dt = 0.9 / su.idx()[0, 0]
+    # With the schema-default magnetisation ceiling (max_sigma = 100) the
+    # blast background sits on the clamp, the dry-run c2p reports "floored"
+    # and FOFC recomputes several hundred faces per stage.
+    P.max_sigma = 100.0
     gs, ga, g = _gpu_run(P, su, f, dt, 1)
     os_, oa, S = _oracle_run(P, su, f, dt, 1)
     st = g.status()
-    assert st.fofc_faces == S.fofc_counts()[0]
+    assert st.fofc_faces > 0
+    assert (st.fofc_faces, st.fofc_edges) == S.fofc_counts()
     e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
     assert e.max() < STEP_TOL, e
