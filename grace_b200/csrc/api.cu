@@ -440,9 +440,13 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
   double* bf[3] = {f->bx, f->by, f->bz};
   KScope ks(h, s, GRB_KIND_GHOST);
   for (int ax = 0; ax < 3; ++ax) {
-    k_ghost_cells<<<148 * 8, 256, 0, s>>>(G, br, ax, f->state); ++h->launches;
-    for (int fd = 0; fd < 3; ++fd) {
-      k_ghost_faces<<<148 * 4, 256, 0, s>>>(G, br, ax, fd, bf[fd]);
+    for (int fd = -1; fd < 3; ++fd) {
+      int n[3] = {G.NX, G.NY, G.NZ};
+      if (fd >= 0) n[fd] += 1;
+      n[ax] = 2 * G.g;
+      const int total = n[0] * n[1] * n[2];
+      const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq);
+      k_ghost<<<grid, 256, 0, s>>>(G, br, ax, fd, fd < 0 ? f->state : bf[fd]);
       ++h->launches;
     }
   }

@@ -606,82 +606,47 @@ __global__ void k_linop(int64_t n, double* __restrict__ a, const double* __restr
 // from the neighbouring block (wrapping), others copy the nearest interior
 // cell or face (zero-gradient outflow).  Only the 7 evolved HRSC variables
 // and the three face-B arrays are exchanged; the Cowling metric is static.
+// Threads run x-fastest over the ghost slab of one block (blockIdx.y = q),
+// so the y and z sweeps read and write whole contiguous rows.
 struct Brick {
   int nbx, nby, nbz;
   int periodic[3];
 };
-__global__ void k_ghost_cells(Geo G, Brick br, int ax, double* __restrict__ st) {
-  const int n[3] = {G.NX, G.NY, G.NZ};
-  const int nin[3] = {G.nx, G.ny, G.nz};
-  const int ng = 2 * G.g;  // ghost layers along ax
-  const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
-  const int64_t per_q = (int64_t)ng * n[o1] * n[o2] * GRB_N_HRSC;
-  const int64_t total = per_q * G.nq;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = t;
-    const int gi = (int)(r % ng); r /= ng;
-    const int a = (int)(r % n[o1]); r /= n[o1];
-    const int b = (int)(r % n[o2]); r /= n[o2];
-    const int v = (int)(r % GRB_N_HRSC); r /= GRB_N_HRSC;
-    const int64_t q = r;
-    const int qc[3] = {(int)(q % br.nbx), (int)((q / br.nbx) % br.nby), (int)(q / ((int64_t)br.nbx * br.nby))};
-    const int nb[3] = {br.nbx, br.nby, br.nbz};
-    const bool lo = gi < G.g;
-    const int ig = lo ? gi : nin[ax] + gi;  // ghost index along ax
-    int src = lo ? ig + nin[ax] : ig - nin[ax];
-    int qs[3] = {qc[0], qc[1], qc[2]};
-    const bool edge = lo ? (qc[ax] == 0) : (qc[ax] == nb[ax] - 1);
-    if (edge && !br.periodic[ax]) {
-      src = lo ? G.g : nin[ax] + G.g - 1;
-    } else {
-      qs[ax] = (qc[ax] + (lo ? nb[ax] - 1 : 1)) % nb[ax];
-    }
-    const int64_t qsrc = qs[0] + (int64_t)br.nbx * (qs[1] + (int64_t)br.nby * qs[2]);
-    int d[3], sidx[3];
-    d[ax] = ig; d[o1] = a; d[o2] = b;
-    sidx[ax] = src; sidx[o1] = a; sidx[o2] = b;
-    st[cvar(G, d[0], d[1], d[2], v, GRB_N_EVOL_VARS, q)] = st[cvar(G, sidx[0], sidx[1], sidx[2], v, GRB_N_EVOL_VARS, qsrc)];
-  }
-}
-// face arrays: `fd` is the staggered axis of the array (0: bx, 1: by, 2: bz)
-__global__ void k_ghost_faces(Geo G, Brick br, int ax, int fd, double* __restrict__ bf) {
+// `fd` = -1: cell-centred HRSC vars of `a`; 0..2: face array staggered along fd.
+__global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, int ax, int fd, double* __restrict__ a) {
+  const int64_t q = blockIdx.y;
   int n[3] = {G.NX, G.NY, G.NZ};
-  n[fd] += 1;
+  if (fd >= 0) n[fd] += 1;
   const int nin[3] = {G.nx, G.ny, G.nz};
   const bool stag = (fd == ax);
-  const int nlo = G.g, nhi = stag ? G.g : G.g;  // ghost faces below / above
-  const int ng = nlo + nhi;
-  const int o1 = (ax + 1) % 3, o2 = (ax + 2) % 3;
-  const int64_t per_q = (int64_t)ng * n[o1] * n[o2];
-  const int64_t total = per_q * G.nq;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
-    int64_t r = t;
-    const int gi = (int)(r % ng); r /= ng;
-    const int a = (int)(r % n[o1]); r /= n[o1];
-    const int b = (int)(r % n[o2]); r /= n[o2];
-    const int64_t q = r;
-    const int qc[3] = {(int)(q % br.nbx), (int)((q / br.nbx) % br.nby), (int)(q / ((int64_t)br.nbx * br.nby))};
-    const int nb[3] = {br.nbx, br.nby, br.nbz};
-    const bool lo = gi < nlo;
-    // staggered axis: ghost faces are [0,g) and [n+g+1, n+2g]; the faces
-    // g and n+g belong to the block.  Unstaggered: like cells.
-    const int ig = lo ? gi : (stag ? nin[ax] + G.g + 1 + (gi - nlo) : nin[ax] + gi);
+  int box[3] = {n[0], n[1], n[2]};
+  box[ax] = 2 * G.g;
+  const int total = box[0] * box[1] * box[2];
+  const int nb[3] = {br.nbx, br.nby, br.nbz};
+  const int qc[3] = {(int)(q % br.nbx), (int)((q / br.nbx) % br.nby), (int)(q / ((int64_t)br.nbx * br.nby))};
+  const int64_t nv = fd < 0 ? GRB_N_HRSC : 1;
+  const int64_t vstride = (int64_t)n[0] * n[1] * n[2];
+  const int64_t qstride = vstride * (fd < 0 ? GRB_N_EVOL_VARS : 1);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    int c[3];
+    c[0] = t % box[0];
+    c[1] = (t / box[0]) % box[1];
+    c[2] = t / (box[0] * box[1]);
+    const int gi = c[ax];
+    const bool lo = gi < G.g;
+    const int ig = lo ? gi : (stag ? nin[ax] + G.g + 1 + (gi - G.g) : nin[ax] + gi);
     int src = lo ? ig + nin[ax] : ig - nin[ax];
     int qs[3] = {qc[0], qc[1], qc[2]};
     const bool edge = lo ? (qc[ax] == 0) : (qc[ax] == nb[ax] - 1);
-    if (edge && !br.periodic[ax]) {
-      src = lo ? G.g : (stag ? nin[ax] + G.g : nin[ax] + G.g - 1);
-    } else {
-      qs[ax] = (qc[ax] + (lo ? nb[ax] - 1 : 1)) % nb[ax];
-    }
+    if (edge && !br.periodic[ax]) src = lo ? G.g : (stag ? nin[ax] + G.g : nin[ax] + G.g - 1);
+    else qs[ax] = (qc[ax] + (lo ? nb[ax] - 1 : 1)) % nb[ax];
     const int64_t qsrc = qs[0] + (int64_t)br.nbx * (qs[1] + (int64_t)br.nby * qs[2]);
-    int d[3], si[3];
-    d[ax] = ig; d[o1] = a; d[o2] = b;
-    si[ax] = src; si[o1] = a; si[o2] = b;
-    auto lin = [&](const int* c, int64_t qq) {
-      return (int64_t)c[0] + (int64_t)n[0] * (c[1] + (int64_t)n[1] * (c[2] + (int64_t)n[2] * qq));
-    };
-    bf[lin(d, q)] = bf[lin(si, qsrc)];
+    int d[3] = {c[0], c[1], c[2]}, sidx[3] = {c[0], c[1], c[2]};
+    d[ax] = ig;
+    sidx[ax] = src;
+    const int64_t ld = d[0] + (int64_t)n[0] * (d[1] + (int64_t)n[1] * d[2]) + q * qstride;
+    const int64_t ls = sidx[0] + (int64_t)n[0] * (sidx[1] + (int64_t)n[1] * sidx[2]) + qsrc * qstride;
+    for (int v = 0; v < nv; ++v) a[ld + v * vstride] = a[ls + v * vstride];
   }
 }
 
