@@ -28,6 +28,7 @@ RIEMANN_HLL, RIEMANN_LLF = 0, 1
 EMF_GS, EMF_UCT = 0, 1
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_RESERVED = 0, -1, -2, -3, -4
+STATIC_SCRATCH_BYTES = 64 << 20
 KIND_NAMES = ["flux", "emf", "fofc_flag", "fofc_fix", "update", "ct", "aux", "linop", "ghost",
               "c2p", "other"]
 
@@ -114,6 +115,9 @@ PROTOTYPES = {
     "grb_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "grb_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                    C.c_int32]),
+    "grb_advance_substep_static": (C.c_int, [C.POINTER(Params), C.POINTER(Grid), C.c_double,
+                                             C.c_double, C.c_double, C.POINTER(Fields),
+                                             C.POINTER(Fields), C.c_void_p, C.c_void_p]),
     "grb_fill_ghosts_brick": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields),
                                         C.c_int32, C.c_int32, C.c_int32,
                                         C.POINTER(C.c_int32), C.c_void_p]),

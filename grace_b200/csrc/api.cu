@@ -10,6 +10,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -485,3 +486,169 @@ int grb_kernel_times(grb_handle* h, double* ms, int64_t* counts, int32_t nkinds)
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Scratch-free stage: grb_advance_substep_static.
+//
+// For callers that cannot call cudaMalloc: host codes whose device memory is
+// entirely reserved up front by a pooling allocator (a Kokkos or RMM arena
+// that owns the GPU), and plugin hosts that forbid a library from allocating
+// device memory once the run has started.  The face/edge scratch of the
+// stage lives in this file-scope device array instead of handle-owned
+// memory.  Its size is fixed at GRB_STATIC_SCRATCH_BYTES; the stage runs
+// over the blocks in chunks that fit, so the limit is per block: one block's
+// scratch (about 30 doubles per face-grid point plus 3 per cell, ~4.2 MB for
+// 16^3 blocks with 4 ghosts) must fit in the array.  Every GPU that loads the
+// library holds the array until the process exits.
+// ---------------------------------------------------------------------------
+namespace {
+static __device__ __align__(256) unsigned char g_static_scratch[GRB_STATIC_SCRATCH_BYTES];
+std::mutex g_static_mu;
+void* g_static_addr[256] = {};  // device address of g_static_scratch, per device ordinal
+
+// cell-centred E = -vtilde x B with B including sqrt(gamma)
+// (auxiliaries.cpp:131-162), for the blocks of one chunk
+__global__ void __launch_bounds__(128) k_ecenter_static(Geo G, Box box, const double* __restrict__ st,
+                                                         const double* __restrict__ bx,
+                                                         const double* __restrict__ by,
+                                                         const double* __restrict__ bz,
+                                                         const double* __restrict__ aux, double* __restrict__ ec) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  const Met m = cell_met(G, st, i, j, k, q);
+  const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
+  const double cbx = 0.5 * (bx[bxi(G, i, j, k, q)] + bx[bxi(G, i + 1, j, k, q)]);
+  const double cby = 0.5 * (by[byi(G, i, j, k, q)] + by[byi(G, i, j + 1, k, q)]);
+  const double cbz = 0.5 * (bz[bzi(G, i, j, k, q)] + bz[bzi(G, i, j, k + 1, q)]);
+  const double z[3] = {aux[a0 + G.cells * GRB_ZVECX], aux[a0 + G.cells * GRB_ZVECY], aux[a0 + G.cells * GRB_ZVECZ]};
+  const double W = sqrt(1. + sqs(m.g, z));
+  double vt[3];
+  for (int a = 0; a < 3; ++a) vt[a] = m.alp * z[a] / W - m.beta[a];
+  ec[eci(G, i, j, k, 0, q)] = cby * vt[2] - cbz * vt[1];
+  ec[eci(G, i, j, k, 1, q)] = -cbx * vt[2] + cbz * vt[0];
+  ec[eci(G, i, j, k, 2, q)] = cbx * vt[1] - cby * vt[0];
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct StaticLayout {
+  size_t flux, eface, vbar, ecenter, emf, ftag, etag, per_block;
+};
+StaticLayout static_layout(const Geo& G1, int emf_kind) {
+  StaticLayout L{};
+  L.flux = align256(sizeof(double) * G1.fcells * 7 * 3);
+  L.eface = emf_kind == GRB_EMF_GS ? align256(sizeof(double) * G1.fcells * 2 * 3) : 0;
+  L.vbar = emf_kind == GRB_EMF_UCT ? align256(sizeof(double) * G1.fcells * 4 * 3) : 0;
+  L.ecenter = emf_kind == GRB_EMF_GS ? align256(sizeof(double) * G1.cells * 3) : 0;
+  L.emf = align256(sizeof(double) * G1.fcells * 3);
+  L.ftag = align256((size_t)G1.fcells * 3);
+  L.etag = align256((size_t)G1.fcells * 3);
+  L.per_block = L.flux + L.eface + L.vbar + L.ecenter + L.emf + L.ftag + L.etag;
+  return L;
+}
+}  // namespace
+
+extern "C" int grb_advance_substep_static(const grb_params* p, const grb_grid* g, double t,
+                                          double dt, double dtfact, const grb_fields* nw,
+                                          const grb_fields* old, const double* aux,
+                                          void* stream) {
+  (void)t;
+  if (!valid_params(p)) return GRB_ERR_INVALID;
+  if (!g || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->nq < 1 || g->ngz < 4 || !g->idx) return GRB_ERR_INVALID;
+  if (p->excise_by_radius && !g->coords) return GRB_ERR_INVALID;
+  if (!nw || !old || !aux || !nw->state || !nw->bx || !nw->by || !nw->bz || !old->state || !old->bx ||
+      !old->by || !old->bz)
+    return GRB_ERR_INVALID;
+  const size_t header = 256;  // [0,16): FOFC counters, [16,20): status flags
+  const Geo G1 = make_geo(g->nx, g->ny, g->nz, g->ngz, 1);
+  const StaticLayout L = static_layout(G1, p->emf);
+  if (L.per_block + header > (size_t)GRB_STATIC_SCRATCH_BYTES) {
+    std::fprintf(stderr,
+                 "grb_advance_substep_static: one %dx%dx%d block with %d ghosts needs %zu bytes of "
+                 "scratch, above the static maximum of %zu bytes\n",
+                 g->nx, g->ny, g->nz, g->ngz, L.per_block, (size_t)GRB_STATIC_SCRATCH_BYTES - header);
+    return GRB_ERR_INVALID;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return GRB_ERR_CUDA;
+  unsigned char* base = nullptr;
+  {
+    // Set-up, once per device with that device current: the host-side name
+    // g_static_scratch is only a stand-in, the kernels need its device address.
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    if (!g_static_addr[dev]) {
+      void* ptr = nullptr;
+      if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || !ptr) return GRB_ERR_CUDA;
+      g_static_addr[dev] = ptr;
+    }
+    base = static_cast<unsigned char*>(g_static_addr[dev]);
+  }
+  const DevParams P = to_dev(*p);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t chunk = (int64_t)((GRB_STATIC_SCRATCH_BYTES - header) / L.per_block);
+  const int gz = G1.g, T = 128;
+  StageBufs B{};
+  B.counters = reinterpret_cast<unsigned long long*>(base);
+  B.flags = reinterpret_cast<uint32_t*>(base + 16);
+  if (cudaMemsetAsync(base, 0, header, s) != cudaSuccess) return GRB_ERR_CUDA;
+  const int64_t cst = G1.cells, bxs = (int64_t)(G1.NX + 1) * G1.NY * G1.NZ,
+                bys = (int64_t)G1.NX * (G1.NY + 1) * G1.NZ, bzs = (int64_t)G1.NX * G1.NY * (G1.NZ + 1);
+  for (int64_t q0 = 0; q0 < g->nq; q0 += chunk) {
+    const int64_t nq = (g->nq - q0 < chunk) ? g->nq - q0 : chunk;
+    const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, nq);
+    unsigned char* c = base + header;
+    B.flux = reinterpret_cast<double*>(c); c += L.flux * nq;
+    B.eface = L.eface ? reinterpret_cast<double*>(c) : nullptr; c += L.eface * nq;
+    B.vbar = L.vbar ? reinterpret_cast<double*>(c) : nullptr; c += L.vbar * nq;
+    B.ecenter = L.ecenter ? reinterpret_cast<double*>(c) : nullptr; c += L.ecenter * nq;
+    B.emf = reinterpret_cast<double*>(c); c += L.emf * nq;
+    B.ftag = reinterpret_cast<int8_t*>(c); c += L.ftag * nq;
+    B.etag = reinterpret_cast<int8_t*>(c); c += L.etag * nq;
+    // edge EMFs outside the computed range must read as zero (see grb_reserve)
+    if (cudaMemsetAsync(B.emf, 0, L.emf * nq, s) != cudaSuccess) return GRB_ERR_CUDA;
+    double* ns = nw->state + q0 * cst * GRB_N_EVOL_VARS;
+    double* nbx = nw->bx + q0 * bxs;
+    double* nby = nw->by + q0 * bys;
+    double* nbz = nw->bz + q0 * bzs;
+    const double* os = old->state + q0 * cst * GRB_N_EVOL_VARS;
+    const double* obx = old->bx + q0 * bxs;
+    const double* oby = old->by + q0 * bys;
+    const double* obz = old->bz + q0 * bzs;
+    const double* ax = aux + q0 * cst * GRB_N_AUX_VARS;
+    const double* idx = g->idx + 3 * q0;
+    const double* crd = g->coords ? g->coords + 3 * q0 : nullptr;
+    if (P.emf == GRB_EMF_GS) {
+      const Box cb = box(0, 0, 0, G.NX, G.NY, G.NZ, nq);
+      k_ecenter_static<<<nblk(cb.count(), T), T, 0, s>>>(G, cb, os, obx, oby, obz, ax, B.ecenter);
+    }
+    const double* bf[3] = {obx, oby, obz};
+    for (int dir = 0; dir < 3; ++dir) {
+      int lo[3] = {0, 0, 0}, n[3] = {G.NX, G.NY, G.NZ};
+      lo[dir] = gz - 1;
+      n[dir] = (dir == 0 ? G.nx : dir == 1 ? G.ny : G.nz) + 3;
+      const Box b = box(lo[0], lo[1], lo[2], n[0], n[1], n[2], nq);
+      if (dir == 0) k_flux<0><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, os, ax, bf[0], B);
+      if (dir == 1) k_flux<1><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, os, ax, bf[1], B);
+      if (dir == 2) k_flux<2><<<nblk(b.count(), T), T, 0, s>>>(P, G, b, os, ax, bf[2], B);
+    }
+    const Box eb = box(gz, gz, gz, G.nx + 1, G.ny + 1, G.nz + 1, nq);
+    if (P.emf == GRB_EMF_GS)
+      k_emf_gs<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, B);
+    else
+      k_emf_uct<<<nblk(eb.count(), T), T, 0, s>>>(P, G, eb, obx, oby, obz, B);
+    if (P.fofc && P.emf == GRB_EMF_GS) {
+      if (cudaMemsetAsync(B.ftag, 0, L.ftag * nq, s) != cudaSuccess) return GRB_ERR_CUDA;
+      if (cudaMemsetAsync(B.etag, 0, L.etag * nq, s) != cudaSuccess) return GRB_ERR_CUDA;
+      const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, nq);
+      k_fofc_flag<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, dt, dtfact, ns, os, obx, oby, obz, idx, crd, B);
+      k_fofc_faces<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, os, ax, obx, oby, obz, B);
+      k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B);
+    }
+    const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, nq);
+    k_update<<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, ns, os, ax, idx, B);
+    k_ct<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, dt, dtfact, nbx, nby, nbz, idx, B);
+    if (cudaGetLastError() != cudaSuccess) return GRB_ERR_CUDA;
+  }
+  return GRB_OK;
+}

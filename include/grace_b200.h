@@ -237,6 +237,29 @@ int grb_kernel_times(grb_handle* h, double* ms, int64_t* counts, int32_t nkinds)
 int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
                           int32_t nby, int32_t nbz, const int32_t* periodic, void* stream);
 
+/* ---- scratch-free stage -------------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * (a host code whose GPU memory is owned up front by a pooling allocator, or
+ * a plugin host that forbids libraries to allocate device memory after
+ * start-up): the same stage as grb_advance_substep, with the library's
+ * face/edge scratch in a file-scope device array of GRB_STATIC_SCRATCH_BYTES
+ * instead of handle-owned memory.  No handle is needed (creating one
+ * allocates); the call allocates and frees nothing.  Blocks are processed in
+ * chunks that fit the array, so any nq works; a single block whose scratch
+ * (~30 doubles per face-grid point + 3 per cell) exceeds the array is
+ * rejected with GRB_ERR_INVALID and a message on stderr.  Every GPU that
+ * loads the library holds the array until exit.  The first call on a device
+ * looks up the array's device address (once per device, with that device
+ * current); make that first call before any stream capture.  All calls share
+ * the one array, which keeps the last call's contents (what must start at
+ * zero is cleared by each call), so calls that overlap on the GPU — from
+ * two streams or two threads — race and corrupt each other's results.
+ * FOFC counts and status flags are not reported by this entry point. */
+#define GRB_STATIC_SCRATCH_BYTES (64u << 20)
+int grb_advance_substep_static(const grb_params* p, const grb_grid* g, double t, double dt,
+                               double dtfact, const grb_fields* new_state,
+                               const grb_fields* old_state, const double* aux, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

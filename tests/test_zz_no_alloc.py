@@ -1,0 +1,92 @@
+"""The scratch-free stage entry point, grb_advance_substep_static.
+
+Some callers cannot call cudaMalloc — a host code whose GPU memory is
+owned up front by a pooling allocator, or a plugin host that forbids a
+library to allocate device memory after start-up.  For them the library
+exports a variant of the stage whose scratch lives in a fixed file-scope
+device array.  This test calls it through the C ABI on two consecutive
+stages and checks the new state against the handle-based
+grb_advance_substep on the same inputs (same kernels: within the 1e-10
+stage tolerance, in practice bit for bit).  The grid has more blocks than
+one pass over the static array holds, so the chunked path is exercised.
+The file sorts last so that a run stopping at the first failure has run
+every other test before it.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from grace_b200 import _lib, abi, params, workloads
+from grace_b200.host import Blocks, Fields, GRMHDEquationsSystem
+from parity import cons_rel_err, interior
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def _static_stage(lib, P, blocks, dt, dtfact, new, old, aux):
+    g = blocks.c()
+    nf, of = new.c(), old.c()
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    return lib.grb_advance_substep_static(ctypes.byref(P), ctypes.byref(g), 0.0, dt, dtfact,
+                                          ctypes.byref(nf), ctypes.byref(of),
+                                          ctypes.c_void_p(aux.data_ptr()), s)
+
+
+def test_static_scratch_stage_matches_handle_stage():
+    lib = _lib.load()
+    dev = torch.device("cuda:0")
+    P = params.blast()
+    P.max_sigma = 100.0  # keeps FOFC busy on this setup (see test_gpu_stage)
+    su, (st, bx, by, bz, aux) = workloads.blast(nb=(4, 4, 4), n=(8, 8, 8))
+    # 64 blocks of 8^3 need ~83 MB of scratch: more than one pass of the array
+    per_block = 8 * (17 ** 3) * (21 + 6 + 3) + 8 * 16 ** 3 * 3
+    assert su.nq * per_block > abi.STATIC_SCRATCH_BYTES
+    blocks = Blocks(8, 8, 8, 4, su.nq, su.idx(), device=dev)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    ref = GRMHDEquationsSystem(P)
+    ref.reserve(blocks)
+    base = Fields(T(st), T(bx), T(by), T(bz))
+    aux_d = T(aux)
+    ref.fill_ghosts_brick(base, su.nb, su.periodic)
+    ref.compute_auxiliary_quantities(base, aux_d)
+    dt = 0.25 / su.idx()[0, 0]
+    # two consecutive stages: u1 = u0 + dt L(u0), then 3/4 u0 + 1/4 u1 + 1/4 dt L(u1)
+    a_old, b_old = base.clone(), base.clone()
+    aux_a, aux_b = aux_d.clone(), aux_d.clone()
+    for dtfact in (1.0, 0.25):
+        a_new, b_new = a_old.clone(), b_old.clone()
+        ref.advance_substep(0.0, dt, dtfact, a_new, a_old, aux_a)
+        rc = _static_stage(lib, P, blocks, dt, dtfact, b_new, b_old, aux_b)
+        assert rc == abi.OK
+        torch.cuda.synchronize()
+        ga = a_new.state.cpu().numpy()[:, :7]
+        gb = b_new.state.cpu().numpy()[:, :7]
+        e = cons_rel_err(interior(gb, 4), interior(ga, 4))
+        assert e.max() < TOL, e
+        for x, y in ((a_new.bx, b_new.bx), (a_new.by, b_new.by), (a_new.bz, b_new.bz)):
+            d = (x - y).abs().max().item() / max(x.abs().max().item(), 1e-300)
+            assert d < TOL
+        # next stage starts from the states just produced
+        for f, au in ((a_new, aux_a), (b_new, aux_b)):
+            ref.fill_ghosts_brick(f, su.nb, su.periodic)
+            ref.compute_auxiliary_quantities(f, au)
+        a_old, b_old = a_new, b_new
+
+
+def test_static_scratch_rejects_oversized_blocks():
+    lib = _lib.load()
+    P = params.blast()
+    dev = torch.device("cuda:0")
+    n = 64  # one 64^3 block with 4 ghosts needs ~93 MB of scratch
+    idx = torch.ones(3, dtype=torch.float64, device=dev)
+    g = abi.Grid(n, n, n, 4, 1, idx.data_ptr(), None)
+    dummy = torch.zeros(8, dtype=torch.float64, device=dev)
+    f = abi.Fields(dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr())
+    rc = lib.grb_advance_substep_static(ctypes.byref(P), ctypes.byref(g), 0.0, 1e-3, 1.0,
+                                        ctypes.byref(f), ctypes.byref(f),
+                                        ctypes.c_void_p(dummy.data_ptr()), None)
+    assert rc == abi.ERR_INVALID
