@@ -94,3 +94,14 @@ def test_fofc_flags_match_oracle():
     assert (st.fofc_faces, st.fofc_edges) == S.fofc_counts()
     e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
     assert e.max() < STEP_TOL, e
+
+
+@pytest.mark.parametrize("name", ["blast", "balsara"])
+def test_one_rk3_step_matches_reference_fixture(name):
+    """GPU against the reference's own per-cell numerics (tests/golden)."""
+    import os
+    P, su, f, dt = _setup(name)
+    gs, ga, g = _gpu_run(P, su, f, dt, 1)
+    ref = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "stage_ref.npz"))
+    e = cons_rel_err(interior(gs[0][:, :7], su.ngz), ref[f"{name}_cons"])
+    assert e.max() < STEP_TOL, e
