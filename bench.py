@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c2p", action="store_true")
+    ap.add_argument("--mode", default="tuned", choices=["tuned", "plain"])
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
     return ap.parse_args()
 
 
@@ -203,6 +205,10 @@ def ours(args, rank, world, local_rank):
     g.compute_auxiliary_quantities(state, aux)
     sp, spp = state.clone(), state.clone()
     dt = args.cfl / su.idx()[0, 0]
+    tuning = None
+    if args.mode == "tuned":
+        g.set_mode(abi.MODE_TUNED)
+        tuning = g.autotune(sp, state, aux)
 
     def barrier():
         if world > 1:
@@ -238,6 +244,24 @@ def ours(args, rank, world, local_rank):
         ms = float(t.item())
     zu_rank = su.nq * n ** 3 * 3 * args.steps
     value = zu_rank * world / (ms * 1e-3)
+
+    # --- the plain per-item form on the same state, for the speed-up ratio
+    plain = None
+    if args.mode == "tuned" and not args.no_plain:
+        g.set_mode(abi.MODE_PLAIN)
+        g.rk3_step(dt, state, sp, spp, aux, bc)
+        torch.cuda.synchronize()
+        p0 = torch.cuda.Event(enable_timing=True)
+        p1 = torch.cuda.Event(enable_timing=True)
+        psteps = max(1, min(args.steps, 2))
+        p0.record()
+        for _ in range(psteps):
+            g.rk3_step(dt, state, sp, spp, aux, bc)
+        p1.record()
+        torch.cuda.synchronize()
+        pv = su.nq * n ** 3 * 3 * psteps / (p0.elapsed_time(p1) * 1e-3)
+        plain = {"value": pv, "steps": psteps, "speedup_tuned_over_plain": (value / world) / pv}
+        g.set_mode(abi.MODE_TUNED)
 
     # --- end to end: evolved variables from / to pinned host memory each step
     e2e = None
@@ -341,6 +365,7 @@ def ours(args, rank, world, local_rank):
             "clocks": clk, "gpu_launches": launches,
             "kernel_ms": {k: round(v[0], 3) for k, v in kt.items() if v[1]},
             "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "c2p": c2p,
+            "mode": args.mode, "plain_form": plain, "tuning": tuning,
         }
         print(json.dumps(line), flush=True)
     g.close()

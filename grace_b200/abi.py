@@ -29,6 +29,7 @@ EMF_GS, EMF_UCT = 0, 1
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_RESERVED = 0, -1, -2, -3, -4
 STATIC_SCRATCH_BYTES = 64 << 20
+MODE_PLAIN, MODE_TUNED = 0, 1
 KIND_NAMES = ["flux", "emf", "fofc_flag", "fofc_fix", "update", "ct", "aux", "linop", "ghost",
               "c2p", "other"]
 
@@ -112,6 +113,10 @@ PROTOTYPES = {
                                   C.c_double, C.c_void_p]),
     "grb_c2p_batch": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "grb_set_mode": (C.c_int, [C.c_void_p, C.c_int32]),
+    "grb_autotune": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Fields),
+                               C.c_void_p, C.c_void_p]),
+    "grb_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "grb_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "grb_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                    C.c_int32]),

@@ -30,6 +30,11 @@ struct grb_handle {
   unsigned long long* d_counters = nullptr;
   int last_error = GRB_OK;
   int64_t launches = 0;  // kernels launched through this handle
+  int mode = GRB_MODE_PLAIN;
+  // tuned mode: register-cap variant per kernel family (index into kMinB)
+  int var_flux = 0, var_flag = 0, var_update = 0, var_aux = 0;
+  bool autotuned = false;
+  float tune_ms[4][3] = {};
   // optional per-kernel-kind timing with events on the launching stream
   bool timing = false;
   struct Mark { int kind; cudaEvent_t a, b; };
@@ -151,6 +156,121 @@ struct KScope {
     }
   }
 };
+
+
+// ---- tuned-mode variant dispatch (launch-bounds register caps) -------------
+// kMinB[v]: minimum resident CTAs of 128 threads per SM requested from the
+// compiler; 1 leaves the register count free, 4 caps it at 128, 5 at 102.
+constexpr int kMinB[3] = {1, 4, 5};
+constexpr int kNumVar = 3;
+
+template <int dir>
+void launch_flux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
+                       const double* st, const double* aux, const double* bf, const StageBufs& B) {
+  if (v == 1) k_flux<dir, true, 4><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
+  else if (v == 2) k_flux<dir, true, 5><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
+  else k_flux<dir, true, 1><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
+}
+void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
+                       double dt, double dtfact, const double* ns, const double* os, const double* bx,
+                       const double* by, const double* bz, const double* idx, const double* crd,
+                       const StageBufs& B) {
+  if (v == 1) k_fofc_flag<4><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
+  else if (v == 2) k_fofc_flag<5><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
+  else k_fofc_flag<1><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
+}
+void launch_update_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
+                         double dt, double dtfact, double* ns, const double* os, const double* aux,
+                         const double* idx, const StageBufs& B) {
+  if (v == 1) k_update<4><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B);
+  else if (v == 2) k_update<5><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B);
+  else k_update<1><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B);
+}
+void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
+                      double* st, const double* bx, const double* by, const double* bz, double* aux,
+                      const double* idx, const double* crd, const StageBufs& B) {
+  if (v == 1) k_aux<4><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
+  else if (v == 2) k_aux<5><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
+  else k_aux<1><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
+}
+
+// linop on the evolved HRSC variables and the face arrays only
+__global__ void k_linop_hrsc(Geo G, double* __restrict__ a, const double* __restrict__ x,
+                             const double* __restrict__ y, double b, double c) {
+  const int64_t per = G.cells * GRB_N_HRSC;
+  const int64_t n = per * G.nq;
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = t / per, r = t - q * per;
+    const int64_t o = q * G.cells * GRB_N_EVOL_VARS + r;
+    a[o] = y ? b * x[o] + c * y[o] : b * x[o];
+  }
+}
+
+// The stage in tuned mode: only the faces the stage reads, FAST flux math,
+// tuned register caps.  Returns the number of kernels launched.
+int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, double dtfact,
+                const grb_fields* nw, const grb_fields* old, const double* aux, cudaStream_t s,
+                StageBufs B, bool count_fofc) {
+  const DevParams& P = h->dp;
+  const int gz = G.g, T = 128;
+  int launches = 0;
+  const double* bf[3] = {old->bx, old->by, old->bz};
+  const int nn[3] = {G.nx, G.ny, G.nz};
+  for (int dir = 0; dir < 3; ++dir) {
+    KScope ks(h, s, GRB_KIND_FLUX);
+    int lo[3], n[3];
+    for (int a = 0; a < 3; ++a) {
+      if (a == dir) { lo[a] = gz - 1; n[a] = nn[a] + 3; }
+      else if (P.emf == GRB_EMF_GS) { lo[a] = gz - 1; n[a] = nn[a] + 2; }
+      else { lo[a] = gz - 3; n[a] = nn[a] + 6; }  // UCT reconstructs face data across
+    }
+    const Box b = box(lo[0], lo[1], lo[2], n[0], n[1], n[2], G.nq);
+    const unsigned nb = nblk(b.count(), T);
+    if (dir == 0) launch_flux_tuned<0>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[0], B);
+    if (dir == 1) launch_flux_tuned<1>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[1], B);
+    if (dir == 2) launch_flux_tuned<2>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[2], B);
+    ++launches;
+  }
+  const Box eb = box(gz, gz, gz, G.nx + 1, G.ny + 1, G.nz + 1, G.nq);
+  {
+    KScope ks(h, s, GRB_KIND_EMF);
+    if (P.emf == GRB_EMF_GS) k_emf_gs<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, B);
+    else k_emf_uct<<<nblk(eb.count(), T), T, 0, s>>>(P, G, eb, old->bx, old->by, old->bz, B);
+    ++launches;
+  }
+  if (P.fofc && P.emf == GRB_EMF_GS) {
+    const int64_t nf = G.fcells * G.nq * 3;
+    cudaMemsetAsync(B.ftag, 0, (size_t)nf, s);
+    cudaMemsetAsync(B.etag, 0, (size_t)nf, s);
+    if (count_fofc) cudaMemsetAsync(B.counters, 0, 2 * sizeof(unsigned long long), s);
+    const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, G.nq);
+    {
+      KScope ks(h, s, GRB_KIND_FOFC_FLAG);
+      launch_flag_tuned(h->var_flag, nblk(fb.count(), T), s, P, G, fb, dt, dtfact, nw->state, old->state,
+                        old->bx, old->by, old->bz, g->idx, g->coords, B);
+      ++launches;
+    }
+    {
+      KScope ks(h, s, GRB_KIND_FOFC_FIX);
+      k_fofc_faces<true><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by, old->bz, B);
+      k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B);
+      launches += 2;
+    }
+  }
+  const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, G.nq);
+  {
+    KScope ks(h, s, GRB_KIND_UPDATE);
+    launch_update_tuned(h->var_update, nblk(ub.count(), T), s, P, G, ub, dt, dtfact, nw->state, old->state,
+                        aux, g->idx, B);
+    ++launches;
+  }
+  {
+    KScope ks(h, s, GRB_KIND_CT);
+    k_ct<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, dt, dtfact, nw->bx, nw->by, nw->bz, g->idx, B);
+    ++launches;
+  }
+  return launches;
+}
 
 }  // namespace
 
@@ -313,6 +433,11 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt, d
   const DevParams& P = h->dp;
   const int gz = G.g, T = 128;
   StageBufs B = h->B;
+  if (h->mode == GRB_MODE_TUNED) {
+    h->launches += stage_tuned(h, G, g, dt, dtfact, nw, old, aux, s, B, true);
+    CK(cudaGetLastError());
+    return GRB_OK;
+  }
   // compute_fluxes: reference ranges (evolve.cpp:908-922)
   const double* bf[3] = {old->bx, old->by, old->bz};
   for (int dir = 0; dir < 3; ++dir) {
@@ -343,19 +468,19 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt, d
     const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, G.nq);
     {
     KScope ks(h, s, GRB_KIND_FOFC_FLAG);
-    k_fofc_flag<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, dt, dtfact, nw->state, old->state, old->bx,
+    k_fofc_flag<1><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, dt, dtfact, nw->state, old->state, old->bx,
                                                    old->by, old->bz, g->idx, g->coords, B); ++h->launches;
     }
     {
     KScope ks(h, s, GRB_KIND_FOFC_FIX);
-    k_fofc_faces<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by, old->bz, B); ++h->launches;
+    k_fofc_faces<false><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by, old->bz, B); ++h->launches;
     k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B); ++h->launches;
     }
   }
   const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, G.nq);
   {
   KScope ks(h, s, GRB_KIND_UPDATE);
-  k_update<<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, nw->state, old->state, aux, g->idx, B); ++h->launches;
+  k_update<1><<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, nw->state, old->state, aux, g->idx, B); ++h->launches;
   }
   {
   KScope ks(h, s, GRB_KIND_CT);
@@ -374,7 +499,14 @@ int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g, const grb
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   const Box b = box(0, 0, 0, G.NX, G.NY, G.NZ, G.nq);
   KScope ks(h, (cudaStream_t)stream, GRB_KIND_AUX);
-  k_aux<<<nblk(b.count(), 128), 128, 0, (cudaStream_t)stream>>>(h->dp, G, b, st->state, st->bx, st->by,
+  if (h->mode == GRB_MODE_TUNED) {
+    launch_aux_tuned(h->var_aux, nblk(b.count(), 128), (cudaStream_t)stream, h->dp, G, b, st->state, st->bx,
+                     st->by, st->bz, aux, g->idx, g->coords, h->B);
+    ++h->launches;
+    CK(cudaGetLastError());
+    return GRB_OK;
+  }
+  k_aux<1><<<nblk(b.count(), 128), 128, 0, (cudaStream_t)stream>>>(h->dp, G, b, st->state, st->bx, st->by,
                                                                   st->bz, aux, g->idx, g->coords, h->B); ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;
@@ -405,6 +537,18 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A, const
   const double* x[4] = {Bf->state, Bf->bx, Bf->by, Bf->bz};
   const double* y[4] = {Cf ? Cf->state : nullptr, Cf ? Cf->bx : nullptr, Cf ? Cf->by : nullptr, Cf ? Cf->bz : nullptr};
   KScope ks(h, s, GRB_KIND_LINOP);
+  if (h->mode == GRB_MODE_TUNED) {
+    // The Cowling metric and curvature are static: combine only the
+    // evolved HRSC variables (and the face arrays below).
+    k_linop_hrsc<<<148 * 16, 256, 0, s>>>(G, a[0], x[0], y[0], b, c);
+    ++h->launches;
+    for (int v = 1; v < 4; ++v) {
+      k_linop<<<148 * 16, 256, 0, s>>>(n[v], a[v], x[v], y[v], b, c);
+      ++h->launches;
+    }
+    CK(cudaGetLastError());
+    return GRB_OK;
+  }
   for (int v = 0; v < 4; ++v) {
     k_linop<<<148 * 16, 256, 0, s>>>(n[v], a[v], x[v], y[v], b, c);
     ++h->launches;
@@ -455,6 +599,122 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
   return GRB_OK;
 }
 
+
+int grb_set_mode(grb_handle* h, int32_t mode) {
+  if (!h || (mode != GRB_MODE_PLAIN && mode != GRB_MODE_TUNED)) return GRB_ERR_INVALID;
+  h->mode = mode;
+  return GRB_OK;
+}
+
+// Time the register-cap variants of the heavy kernels on device copies of
+// the first blocks of the grid (live arrays are only read) and keep the
+// fastest per kernel family for the tuned mode.
+int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const grb_fields* old,
+                 const double* aux, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  int rc = check_grid(h, g);
+  if (rc) return fail(h, rc);
+  if (!nw || !old || !aux) return fail(h, GRB_ERR_INVALID);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t nt = g->nq < 96 ? g->nq : 96;
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, nt);
+  const size_t cs = sizeof(double) * G.cells * nt;
+  const size_t fx = sizeof(double) * (size_t)(G.NX + 1) * G.NY * G.NZ * nt;
+  const size_t fy = sizeof(double) * (size_t)G.NX * (G.NY + 1) * G.NZ * nt;
+  const size_t fz = sizeof(double) * (size_t)G.NX * G.NY * (G.NZ + 1) * nt;
+  double *ns = nullptr, *os = nullptr, *ax = nullptr, *b3[6] = {nullptr};
+  bool ok = cudaMalloc(&ns, cs * GRB_N_EVOL_VARS) == cudaSuccess &&
+            cudaMalloc(&os, cs * GRB_N_EVOL_VARS) == cudaSuccess &&
+            cudaMalloc(&ax, cs * GRB_N_AUX_VARS) == cudaSuccess;
+  const size_t fsz[3] = {fx, fy, fz};
+  for (int a = 0; a < 6 && ok; ++a) ok = cudaMalloc(&b3[a], fsz[a % 3]) == cudaSuccess;
+  auto cleanup = [&]() {
+    cudaFree(ns); cudaFree(os); cudaFree(ax);
+    for (int a = 0; a < 6; ++a) cudaFree(b3[a]);
+  };
+  if (!ok) { cleanup(); cudaGetLastError(); return fail(h, GRB_ERR_NOMEM); }
+  cudaMemcpyAsync(ns, nw->state, cs * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(os, old->state, cs * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(ax, aux, cs * GRB_N_AUX_VARS, cudaMemcpyDeviceToDevice, s);
+  const double* srcb[6] = {nw->bx, nw->by, nw->bz, old->bx, old->by, old->bz};
+  for (int a = 0; a < 6; ++a) cudaMemcpyAsync(b3[a], srcb[a], fsz[a % 3], cudaMemcpyDeviceToDevice, s);
+  grb_fields fn{ns, b3[0], b3[1], b3[2]}, fo{os, b3[3], b3[4], b3[5]};
+  grb_grid gs = *g;
+  gs.nq = nt;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  const bool timing = h->timing;
+  h->timing = false;
+  const DevParams& P = h->dp;
+  StageBufs B = h->B;
+  auto time_it = [&](auto&& fn_launch) {
+    fn_launch();  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < 3; ++r) {
+      cudaEventRecord(e0, s);
+      fn_launch();
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      best = t < best ? t : best;
+    }
+    return best;
+  };
+  const int gz = G.g;
+  // face fluxes along x with the tuned range
+  int lo[3] = {gz - 1, gz - 1, gz - 1}, n[3] = {G.nx + 3, G.ny + 2, G.nz + 2};
+  if (P.emf == GRB_EMF_UCT) { lo[1] = lo[2] = gz - 3; n[1] = G.ny + 6; n[2] = G.nz + 6; }
+  const Box fbx = box(lo[0], lo[1], lo[2], n[0], n[1], n[2], nt);
+  const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, nt);
+  const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, nt);
+  const Box ab = box(0, 0, 0, G.NX, G.NY, G.NZ, nt);
+  int best[4] = {0, 0, 0, 0};
+  for (int fam = 0; fam < 4; ++fam) {
+    float bt = 1e30f;
+    for (int v = 0; v < kNumVar; ++v) {
+      float t = 0.f;
+      if (fam == 0)
+        t = time_it([&] { launch_flux_tuned<0>(v, nblk(fbx.count(), 128), s, P, G, fbx, os, ax, fo.bx, B); });
+      else if (fam == 1)
+        t = time_it([&] { launch_flag_tuned(v, nblk(fb.count(), 128), s, P, G, fb, 1e-3, 1.0, ns, os, fo.bx,
+                                            fo.by, fo.bz, gs.idx, gs.coords, B); });
+      else if (fam == 2)
+        t = time_it([&] { launch_update_tuned(v, nblk(ub.count(), 128), s, P, G, ub, 1e-12, 1.0, ns, os, ax,
+                                              gs.idx, B); });
+      else
+        t = time_it([&] { launch_aux_tuned(v, nblk(ab.count(), 128), s, P, G, ab, ns, fn.bx, fn.by, fn.bz,
+                                           ax, gs.idx, gs.coords, B); });
+      h->tune_ms[fam][v] = t;
+      if (t < bt) { bt = t; best[fam] = v; }
+    }
+  }
+  h->var_flux = best[0];
+  h->var_flag = best[1];
+  h->var_update = best[2];
+  h->var_aux = best[3];
+  h->autotuned = true;
+  h->timing = timing;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaStreamSynchronize(s);
+  cleanup();
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
+  if (!h || !variant) return GRB_ERR_INVALID;
+  variant[0] = kMinB[h->var_flux];
+  variant[1] = kMinB[h->var_flag];
+  variant[2] = kMinB[h->var_update];
+  variant[3] = kMinB[h->var_aux];
+  if (ms)
+    for (int f = 0; f < 4; ++f)
+      for (int v = 0; v < kNumVar; ++v) ms[f * kNumVar + v] = h->tune_ms[f][v];
+  return GRB_OK;
+}
 
 int grb_set_kernel_timing(grb_handle* h, int32_t enable) {
   if (!h) return GRB_ERR_INVALID;
@@ -641,12 +901,12 @@ extern "C" int grb_advance_substep_static(const grb_params* p, const grb_grid* g
       if (cudaMemsetAsync(B.ftag, 0, L.ftag * nq, s) != cudaSuccess) return GRB_ERR_CUDA;
       if (cudaMemsetAsync(B.etag, 0, L.etag * nq, s) != cudaSuccess) return GRB_ERR_CUDA;
       const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, nq);
-      k_fofc_flag<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, dt, dtfact, ns, os, obx, oby, obz, idx, crd, B);
-      k_fofc_faces<<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, os, ax, obx, oby, obz, B);
+      k_fofc_flag<1><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, dt, dtfact, ns, os, obx, oby, obz, idx, crd, B);
+      k_fofc_faces<false><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, os, ax, obx, oby, obz, B);
       k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B);
     }
     const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, nq);
-    k_update<<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, ns, os, ax, idx, B);
+    k_update<1><<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, ns, os, ax, idx, B);
     k_ct<<<nblk(eb.count(), T), T, 0, s>>>(G, eb, dt, dtfact, nbx, nby, nbz, idx, B);
     if (cudaGetLastError() != cudaSuccess) return GRB_ERR_CUDA;
   }

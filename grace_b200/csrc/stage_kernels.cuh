@@ -26,7 +26,7 @@ struct StageBufs {
 };
 
 // ---- the Riemann problem at one face (grmhd.hh:774-970) -------------------
-template <int dir>
+template <int dir, bool FAST = false>
 __device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
                                            double* pl, double* pr, const Met& m, double f[7],
                                            double vb[4]) {
@@ -53,6 +53,11 @@ __device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
     cmax = fmax(0., fmax(cpl, cpr));
   }
   if (cmin < 1e-12 && cmax < 1e-12) { cmin = 1; cmax = 1; }
+  // FAST: one reciprocal for all HLL fluxes of the face
+  const double isum = FAST ? 1.0 / (cmax + cmin) : 0.0;
+  auto hll = [&](double fL, double fR, double uL, double uR, double cn, double cx) {
+    return FAST ? hll_r(fL, fR, uL, uR, cn, cx, isum) : grb::hll(fL, fR, uL, uR, cn, cx);
+  };
   if (P.emf == GRB_EMF_UCT) {
     const int a0 = dir == 0 ? 1 : 0, a1 = dir == 2 ? 1 : 2;
     vb[0] = hll(vtl[a0], vtr[a0], 0, 0, cmin, cmax);
@@ -88,7 +93,7 @@ __device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
 }
 
 // getflux<idir> (grmhd.hh:551-773) reading GRACE arrays through the cache.
-template <int dir>
+template <int dir, bool FAST = false>
 __device__ __forceinline__ void getflux(const DevParams& P, const Geo& G, int i, int j,
                                         int k, int64_t q, int recon, bool rusanov,
                                         const double* __restrict__ st,
@@ -121,7 +126,8 @@ __device__ __forceinline__ void getflux(const DevParams& P, const Geo& G, int i,
       double u[6];
 #pragma unroll
       for (int o = 0; o < 6; ++o) u[o] = __ldg(p + (o - 3) * s);
-      recon6(recon, u, pl[pv[r]], pr[pv[r]]);
+      if (FAST) recon6_fast(recon, u, pl[pv[r]], pr[pv[r]]);
+      else recon6(recon, u, pl[pv[r]], pr[pv[r]]);
     }
   }
   const int64_t bi = dir == 0 ? bxi(G, i, j, k, q) : dir == 1 ? byi(G, i, j, k, q) : bzi(G, i, j, k, q);
@@ -131,7 +137,7 @@ __device__ __forceinline__ void getflux(const DevParams& P, const Geo& G, int i,
   uint32_t q0 = 0;
   pl[GRB_P_PRESS] = eos_PT(P.eos, pl[GRB_P_EPS], pl[GRB_P_CS2], nullptr, pl[GRB_P_TEMP], pl[GRB_P_RHO], q0);
   pr[GRB_P_PRESS] = eos_PT(P.eos, pr[GRB_P_EPS], pr[GRB_P_CS2], nullptr, pr[GRB_P_TEMP], pr[GRB_P_RHO], q0);
-  mhd_fluxes<dir>(P, rusanov, pl, pr, m, f, vb);
+  mhd_fluxes<dir, FAST>(P, rusanov, pl, pr, m, f, vb);
 }
 
 __device__ __forceinline__ void store_face(const Geo& G, const StageBufs& B, int emf_kind, int dir,
@@ -163,8 +169,8 @@ __device__ __forceinline__ bool decode(const Box& b, int64_t t, int& i, int& j, 
   return true;
 }
 
-template <int dir>
-__global__ void __launch_bounds__(128) k_flux(DevParams P, Geo G, Box box,
+template <int dir, bool FAST = false, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) k_flux(DevParams P, Geo G, Box box,
                                                const double* __restrict__ st,
                                                const double* __restrict__ aux,
                                                const double* __restrict__ bface, StageBufs B) {
@@ -172,7 +178,7 @@ __global__ void __launch_bounds__(128) k_flux(DevParams P, Geo G, Box box,
   int64_t q;
   if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
   double f[7], vb[4];
-  getflux<dir>(P, G, i, j, k, q, P.recon, P.riemann == GRB_RIEMANN_LLF, st, aux, bface, f, vb);
+  getflux<dir, FAST>(P, G, i, j, k, q, P.recon, P.riemann == GRB_RIEMANN_LLF, st, aux, bface, f, vb);
   store_face(G, B, P.emf, dir, i, j, k, q, f, vb);
 }
 
@@ -335,7 +341,8 @@ __device__ __forceinline__ double cell_r(const Geo& G, const double* coords, con
 }
 
 // flag_fofc_cells (evolve.cpp:456-635) over cells [g-1, n+g]^3
-__global__ void __launch_bounds__(128) k_fofc_flag(DevParams P, Geo G, Box box, double dt,
+template <int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box box, double dt,
                                                     double dtfact, const double* __restrict__ ns,
                                                     const double* __restrict__ os,
                                                     const double* __restrict__ obx,
@@ -398,6 +405,7 @@ __global__ void __launch_bounds__(128) k_fofc_flag(DevParams P, Geo G, Box box, 
 
 // correct_{x,y,z}_fluxes_fofc: donor + LLF on tagged faces.  The box is the
 // compaction range [g-1, n+g]^3; a face of direction d needs index_d >= g.
+template <bool FAST = false>
 __global__ void __launch_bounds__(128) k_fofc_faces(DevParams P, Geo G, Box box,
                                                      const double* __restrict__ st,
                                                      const double* __restrict__ aux,
@@ -410,17 +418,17 @@ __global__ void __launch_bounds__(128) k_fofc_faces(DevParams P, Geo G, Box box,
   unsigned cnt = 0;
   double f[7], vb[4];
   if (i >= G.g && B.ftag[emi(G, i, j, k, 0, q)]) {
-    getflux<0>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bx, f, vb);
+    getflux<0, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bx, f, vb);
     store_face(G, B, P.emf, 0, i, j, k, q, f, vb);
     ++cnt;
   }
   if (j >= G.g && B.ftag[emi(G, i, j, k, 1, q)]) {
-    getflux<1>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, by, f, vb);
+    getflux<1, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, by, f, vb);
     store_face(G, B, P.emf, 1, i, j, k, q, f, vb);
     ++cnt;
   }
   if (k >= G.g && B.ftag[emi(G, i, j, k, 2, q)]) {
-    getflux<2>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bz, f, vb);
+    getflux<2, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bz, f, vb);
     store_face(G, B, P.emf, 2, i, j, k, q, f, vb);
     ++cnt;
   }
@@ -439,7 +447,8 @@ __global__ void __launch_bounds__(128) k_fofc_edges(Geo G, Box box, StageBufs B)
 }
 
 // ---- flux divergence + geometric sources on interior cells -----------------
-__global__ void __launch_bounds__(128) k_update(DevParams P, Geo G, Box box, double dt, double dtfact,
+template <int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) k_update(DevParams P, Geo G, Box box, double dt, double dtfact,
                                                  double* __restrict__ ns, const double* __restrict__ os,
                                                  const double* __restrict__ aux,
                                                  const double* __restrict__ idx, StageBufs B) {
@@ -517,7 +526,8 @@ __global__ void __launch_bounds__(128) k_ct(Geo G, Box box, double dt, double dt
 }
 
 // ---- aux: c2p on every cell + resets + C2P_ERR + BDIV + cell-centred E -----
-__global__ void __launch_bounds__(128) k_aux(DevParams P, Geo G, Box box, double* __restrict__ st,
+template <int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, double* __restrict__ st,
                                               const double* __restrict__ bx,
                                               const double* __restrict__ by,
                                               const double* __restrict__ bz,

@@ -162,6 +162,26 @@ class GRMHDEquationsSystem:
                    "grb_c2p_batch")
         return prims
 
+    def set_mode(self, mode):
+        """abi.MODE_PLAIN (reference launch ranges, one thread per item) or
+        abi.MODE_TUNED (needed faces only, faster math, tuned variants)."""
+        _lib.check(self.lib.grb_set_mode(self.h, mode), "grb_set_mode")
+
+    def autotune(self, new_state, old_state, aux, stream=None):
+        g = self.blocks.c()
+        nf, of = new_state.c(), old_state.c()
+        _lib.check(self.lib.grb_autotune(self.h, ctypes.byref(g), ctypes.byref(nf), ctypes.byref(of),
+                                         _ptr(aux), _stream_ptr(stream)), "grb_autotune")
+        return self.tuning()
+
+    def tuning(self):
+        v = (ctypes.c_int32 * 4)()
+        ms = (ctypes.c_float * 12)()
+        _lib.check(self.lib.grb_get_tuning(self.h, v, ms), "grb_get_tuning")
+        fam = ["flux", "fofc_flag", "update", "aux"]
+        return {f: {"min_ctas_per_sm": v[i], "ms": [round(ms[3 * i + k], 4) for k in range(3)]}
+                for i, f in enumerate(fam)}
+
     def set_kernel_timing(self, on):
         _lib.check(self.lib.grb_set_kernel_timing(self.h, 1 if on else 0), "grb_set_kernel_timing")
 

@@ -212,6 +212,27 @@ int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons,
                   uint32_t* err, int32_t use_learned, void* stream);
 
 
+/* ---- execution mode and autotuning --------------------------------------- */
+/* GRB_MODE_PLAIN: one thread per face / edge / cell over the reference's own
+ * launch ranges (compute_fluxes computes faces over the full transverse
+ * ghost range, evolve.cpp:908-922; linop_apply combines all 23 variables).
+ * GRB_MODE_TUNED: only the faces the stage reads, one reciprocal per face
+ * for the HLL fluxes, division-free WENO-Z weights, the register-cap
+ * variant picked by grb_autotune, and linop on the evolved variables only
+ * (the Cowling metric is static).  Results agree with the plain mode to
+ * rounding. */
+enum grb_mode { GRB_MODE_PLAIN = 0, GRB_MODE_TUNED = 1 };
+int grb_set_mode(grb_handle* h, int32_t mode);
+/* Times the register-cap variants of the flux, FOFC-flag, update and aux
+ * kernels on device copies of the first blocks of the grid (the arrays
+ * passed in are only read) and keeps the fastest for the tuned mode.
+ * Allocates and frees temporary copies; synchronises the stream. */
+int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* new_state,
+                 const grb_fields* old_state, const double* aux, void* stream);
+/* variant[4]: chosen minimum-CTAs-per-SM of flux, flag, update, aux;
+ * ms[12] (or NULL): timed milliseconds of the 3 candidates per family. */
+int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms);
+
 /* ---- measurement helpers -------------------------------------------------- */
 /* Kernel kinds for grb_kernel_times. */
 enum grb_kernel_kind {

@@ -25,12 +25,13 @@ def _setup(name):
     return P, su, f, cfl / su.idx()[0, 0]
 
 
-def _gpu_run(P, su, f, dt, nsteps):
+def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN):
     dev = torch.device("cuda:0")
     st, bx, by, bz, aux = f
     blocks = Blocks(su.n[0], su.n[1], su.n[2], su.ngz, su.nq, su.idx(), device=dev)
     g = GRMHDEquationsSystem(P)
     g.reserve(blocks)
+    g.set_mode(mode)
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     state = Fields(T(st), T(bx), T(by), T(bz))
     aux_d = T(aux)
@@ -38,6 +39,8 @@ def _gpu_run(P, su, f, dt, nsteps):
     bc(state)
     g.compute_auxiliary_quantities(state, aux_d)
     sp, spp = state.clone(), state.clone()
+    if mode == abi.MODE_TUNED:
+        g.autotune(sp, state, aux_d)
     for _ in range(nsteps):
         g.rk3_step(dt, state, sp, spp, aux_d, bc)
     torch.cuda.synchronize()
@@ -57,10 +60,11 @@ def _oracle_run(P, su, f, dt, nsteps):
     return state, aux, S
 
 
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
 @pytest.mark.parametrize("name", ["blast", "balsara"])
-def test_one_rk3_step_matches_oracle(name):
+def test_one_rk3_step_matches_oracle(name, mode):
     P, su, f, dt = _setup(name)
-    gs, ga, g = _gpu_run(P, su, f, dt, 1)
+    gs, ga, g = _gpu_run(P, su, f, dt, 1, mode)
     os_, oa, S = _oracle_run(P, su, f, dt, 1)
     e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
     assert e.max() < STEP_TOL, e
@@ -74,20 +78,22 @@ def test_one_rk3_step_matches_oracle(name):
     np.testing.assert_array_equal(ga[:, abi.C2P_ERR], oa[:, abi.C2P_ERR])
 
 
-def test_div_b_and_conservation_blast():
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_div_b_and_conservation_blast(mode):
     P, su, f, dt = _setup("blast")
-    gs, ga, g = _gpu_run(P, su, f, dt, 3)
+    gs, ga, g = _gpu_run(P, su, f, dt, 3, mode)
     bd = interior(ga[:, abi.BDIV], su.ngz)
     assert np.max(np.abs(bd)) < 1e-13
 
 
-def test_fofc_flags_match_oracle():
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_fofc_flags_match_oracle(mode):
     P, su, f, dt = _setup("blast")
     # With the schema-default magnetisation ceiling (max_sigma = 100) the
     # blast background sits on the clamp, the dry-run c2p reports "floored"
     # and FOFC recomputes several hundred faces per stage.
     P.max_sigma = 100.0
-    gs, ga, g = _gpu_run(P, su, f, dt, 1)
+    gs, ga, g = _gpu_run(P, su, f, dt, 1, mode)
     os_, oa, S = _oracle_run(P, su, f, dt, 1)
     st = g.status()
     assert st.fofc_faces > 0
