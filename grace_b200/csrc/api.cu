@@ -648,10 +648,19 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
   h->timing = false;
   const DevParams& P = h->dp;
   StageBufs B = h->B;
+  // restore the copies before every launch so that each candidate sees the
+  // same input (the update and aux kernels modify their arrays)
+  auto restore = [&]() {
+    cudaMemcpyAsync(ns, nw->state, cs * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(ax, aux, cs * GRB_N_AUX_VARS, cudaMemcpyDeviceToDevice, s);
+    for (int a = 0; a < 3; ++a) cudaMemcpyAsync(b3[a], srcb[a], fsz[a], cudaMemcpyDeviceToDevice, s);
+  };
   auto time_it = [&](auto&& fn_launch) {
+    restore();
     fn_launch();  // warm-up
     float best = 1e30f;
     for (int r = 0; r < 3; ++r) {
+      restore();
       cudaEventRecord(e0, s);
       fn_launch();
       cudaEventRecord(e1, s);
