@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-c2p", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="c2p leg: plain bracket only")
     ap.add_argument("--mode", default="tuned", choices=["tuned", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
     return ap.parse_args()
@@ -326,26 +327,11 @@ def ours(args, rank, world, local_rank):
                 "launch_ms": per_launch_ms,
                 "note": "FP64 arithmetic, not HBM, binds this kernel (see profiles/)"}
 
-    # --- c2p micro-benchmark (2^24 states, plain)
+    # --- c2p micro-benchmark (2^24 states): plain, then with the learned
+    # bracket trained on the GPU from 2^20 other seeded states
     c2p = None
     if not args.no_c2p and rank == 0:
-        cons, _ = workloads.c2p_states(1 << 24, seed=5)
-        gc = GRMHDEquationsSystem(params.c2p_bench())
-        c_d = torch.from_numpy(cons).to(dev)
-        del cons
-        for _ in range(2):
-            gc.conservs_to_prims(c_d)
-        torch.cuda.synchronize()
-        a0 = torch.cuda.Event(enable_timing=True)
-        a1 = torch.cuda.Event(enable_timing=True)
-        a0.record()
-        for _ in range(5):
-            gc.conservs_to_prims(c_d)
-        a1.record()
-        torch.cuda.synchronize()
-        c2p = {"plain_solves_per_s": (1 << 24) * 5 / (a0.elapsed_time(a1) * 1e-3), "states": 1 << 24,
-               "tolerance": 1e-12}
-        gc.close()
+        c2p = c2p_bench(dev, learned=not args.no_learned)
 
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
@@ -369,6 +355,61 @@ def ours(args, rank, world, local_rank):
         }
         print(json.dumps(line), flush=True)
     g.close()
+
+
+def c2p_bench(dev, learned=True, n=1 << 24, reps=5):
+    cons, _ = workloads.c2p_states(n, seed=5)
+    gc = GRMHDEquationsSystem(params.c2p_bench())
+    c_d = torch.from_numpy(cons).to(dev)
+    del cons
+
+    def timed(use_learned):
+        for _ in range(2):
+            gc.conservs_to_prims(c_d, use_learned=use_learned)
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record()
+        for _ in range(reps):
+            gc.conservs_to_prims(c_d, use_learned=use_learned)
+        a1.record()
+        torch.cuda.synchronize()
+        return n * reps / (a0.elapsed_time(a1) * 1e-3)
+
+    def iters(use_learned):
+        it = torch.zeros(n, dtype=torch.int32, device=dev)
+        gu = torch.zeros(n, dtype=torch.int8, device=dev)
+        pr = gc.conservs_to_prims(c_d, use_learned=use_learned, diag={"iters": it, "guess_used": gu})
+        m = (n // 32) * 32
+        st = {"mean_brent_iters": float(it.double().mean()), "max_brent_iters": int(it.max()),
+              "warp_max_brent_iters": float(it[:m].view(-1, 32).max(1).values.double().mean())}
+        if use_learned:
+            st["guess_used"] = float(gu.double().mean())
+        return pr, st
+
+    out = {"states": n, "tolerance": 1e-12, "plain_solves_per_s": timed(False)}
+    pr_p, out["plain"] = iters(False)
+    if learned:
+        tr, _ = workloads.c2p_states(1 << 20, seed=6)
+        rep = gc.train_c2p_model(torch.from_numpy(tr).to(dev))
+        del tr
+        out["learned_solves_per_s"] = timed(True)
+        pr_l, out["learned"] = iters(True)
+        W = torch.sqrt(1.0 + (pr_p[2:5] ** 2).sum(0))
+        scale = torch.maximum(torch.maximum(pr_p[0].abs(), pr_p[7].abs()),
+                              torch.sqrt((pr_p[2:5] ** 2).sum(0)).clamp_min(1e-30))
+        d = torch.stack([(pr_l[v] - pr_p[v]).abs() for v in (0, 7, 2, 3, 4)]).max(0).values / scale
+        ok = torch.isfinite(d)
+        out["learned_vs_plain"] = {
+            "max_state_residual": float(d[ok].max()),
+            "max_residual_over_W2_tol": float((d[ok] / (1e-12 * torch.clamp(W[ok] ** 2, min=1.0))).max()),
+            "frac_within_1e-12": float((d[ok] <= 1e-12).double().mean())}
+        out["training"] = {k: rep[k] for k in ("states", "labelled", "loss_first", "loss_last", "err_q99",
+                                               "err_q999", "err_max", "delta", "delta_cand", "calib_ms",
+                                               "train_ms")}
+        out["learned_speedup"] = out["learned_solves_per_s"] / out["plain_solves_per_s"]
+    gc.close()
+    return out
 
 
 def main():

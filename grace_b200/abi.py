@@ -27,9 +27,11 @@ RECON_WENOZ, RECON_MC2, RECON_MINMOD, RECON_DONOR = 0, 1, 2, 3
 RIEMANN_HLL, RIEMANN_LLF = 0, 1
 EMF_GS, EMF_UCT = 0, 1
 
-OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_RESERVED = 0, -1, -2, -3, -4
+OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_RESERVED, ERR_NO_MODEL = 0, -1, -2, -3, -4, -5
 STATIC_SCRATCH_BYTES = 64 << 20
 MODE_PLAIN, MODE_TUNED = 0, 1
+MLP_NUM_WEIGHTS, MLP_NUM_PARAMS = 9473, 9488
+MLP_IN = 6
 KIND_NAMES = ["flux", "emf", "fofc_flag", "fofc_fix", "update", "ct", "aux", "linop", "ghost",
               "c2p", "other"]
 
@@ -89,6 +91,23 @@ class Status(C.Structure):
                 ("launches", C.c_int64)]
 
 
+class C2PDiag(C.Structure):
+    _fields_ = [("iters", C.c_void_p), ("guess_used", C.c_void_p), ("mu", C.c_void_p),
+                ("bracket", C.c_void_p)]
+
+
+class TrainConfig(C.Structure):
+    _fields_ = [("steps", C.c_int64), ("batch", C.c_int32), ("lr", C.c_float), ("lr_min", C.c_float),
+                ("seed", C.c_uint64), ("calib_states", C.c_int64)]
+
+
+class TrainReport(C.Structure):
+    _fields_ = [("states", C.c_int64), ("labelled", C.c_int64), ("loss_first", C.c_float),
+                ("loss_last", C.c_float), ("err_q99", C.c_float), ("err_q999", C.c_float),
+                ("err_max", C.c_float), ("delta", C.c_float), ("delta_cand", C.c_float * 4),
+                ("calib_ms", C.c_float * 4), ("train_ms", C.c_double)]
+
+
 # Every extern "C" symbol declared in include/grace_b200.h, with its
 # (restype, argtypes).  The loader binds exactly these.
 PROTOTYPES = {
@@ -113,6 +132,20 @@ PROTOTYPES = {
                                   C.c_double, C.c_void_p]),
     "grb_c2p_batch": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
+    "grb_c2p_batch_diag": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C2PDiag),
+                                     C.c_void_p]),
+    "grb_train_config_defaults": (None, [C.POINTER(TrainConfig)]),
+    "grb_c2p_train": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p,
+                                C.POINTER(TrainConfig), C.POINTER(TrainReport), C.c_void_p]),
+    "grb_c2p_model_get": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "grb_c2p_model_set": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int64]),
+    "grb_c2p_features": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]),
+    "grb_mlp_eval": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p]),
+    "grb_mlp_grad": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_void_p]),
     "grb_set_mode": (C.c_int, [C.c_void_p, C.c_int32]),
     "grb_autotune": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Fields),
                                C.c_void_p, C.c_void_p]),

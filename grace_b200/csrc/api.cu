@@ -7,14 +7,17 @@
 // here synchronises the stream except grb_get_status and grb_reserve.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <random>
 #include <new>
 #include <vector>
 
 #include "grace_b200.h"
+#include "mlp.cuh"
 #include "stage_kernels.cuh"
 
 using namespace grb;
@@ -42,6 +45,10 @@ struct grb_handle {
   std::vector<cudaEvent_t> pool;
   double kind_ms[GRB_KIND_COUNT] = {0};
   int64_t kind_n[GRB_KIND_COUNT] = {0};
+  // learned c2p bracket: FP32 parameter block on the device
+  float* d_mlp = nullptr;
+  bool mlp_ready = false;
+  int c2p_grid[2] = {0, 0};  // persistent grid of k_c2p_batch<plain / learned>
 };
 
 namespace {
@@ -358,6 +365,7 @@ int grb_destroy(grb_handle* h) {
   free_scratch(h);
   cudaFree(h->d_flags);
   cudaFree(h->d_counters);
+  cudaFree(h->d_mlp);
   delete h;
   return GRB_OK;
 }
@@ -557,19 +565,328 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A, const
   return GRB_OK;
 }
 
-int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons, const double* metric, double* prims,
-                  double* cons_out, uint32_t* err, int32_t use_learned, void* stream) {
-  if (!h) return GRB_ERR_INVALID;
-  if (n < 0 || (n > 0 && (!cons || !prims))) return fail(h, GRB_ERR_INVALID);
-  if (use_learned) return fail(h, GRB_ERR_INVALID);  // model loading is separate
-  if (n == 0) return GRB_OK;
-  KScope ks(h, (cudaStream_t)stream, GRB_KIND_C2P);
-  k_c2p_batch<<<nblk(n, 128), 128, 0, (cudaStream_t)stream>>>(h->dp, n, cons, metric, prims, cons_out, err,
-                                                               nullptr, h->d_flags); ++h->launches;
+}  // extern "C"
+
+namespace {
+
+// Persistent grid for k_c2p_batch: all CTAs resident at once, so that the
+// learned variant loads the network into shared memory once per CTA.
+template <bool kLearned>
+int c2p_grid(grb_handle* h) {
+  int& g = h->c2p_grid[kLearned ? 1 : 0];
+  if (g == 0) {
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_c2p_batch<kLearned>, kC2PThreads, 0);
+    g = std::max(1, sms) * std::max(1, occ);
+  }
+  return g;
+}
+
+int launch_c2p(grb_handle* h, int64_t n, const double* cons, const double* metric, double* prims,
+               double* cons_out, uint32_t* err, bool learned, const grb_c2p_diag* diag, cudaStream_t s) {
+  C2PDiagDev d{nullptr, nullptr, nullptr, nullptr};
+  if (diag) d = C2PDiagDev{diag->iters, diag->guess_used, diag->mu, diag->bracket};
+  if (learned) {
+    const unsigned grid = (unsigned)std::min<int64_t>(nblk(n, kC2PThreads), c2p_grid<true>(h));
+    k_c2p_batch<true><<<grid, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, h->d_mlp,
+                                                   h->d_flags);
+  } else {
+    const unsigned grid = (unsigned)std::min<int64_t>(nblk(n, kC2PThreads), c2p_grid<false>(h));
+    k_c2p_batch<false><<<grid, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, nullptr,
+                                                    h->d_flags);
+  }
+  ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;
 }
 
+int ensure_mlp(grb_handle* h) {
+  if (!h->d_mlp) CK(cudaMalloc(&h->d_mlp, sizeof(float) * kMlpNumParams));
+  return GRB_OK;
+}
+
+// He-uniform hidden weights, small output layer, zero biases (host RNG,
+// reproducible for a seed).
+void mlp_init(std::vector<float>& P, uint64_t seed) {
+  std::mt19937_64 rng(seed);
+  std::uniform_real_distribution<float> u(-1.f, 1.f);
+  std::fill(P.begin(), P.end(), 0.f);
+  const float a1 = std::sqrt(6.f / kMlpIn), a2 = std::sqrt(6.f / kMlpH), a4 = std::sqrt(3.f / kMlpH);
+  // high parts and remainders of an input start with the same weight
+  for (int o = 0; o < kMlpH; ++o)
+    for (int k = 0; k < kMlpIn; ++k)
+      P[kMlpOffW1 + o * kMlpK0 + k] = P[kMlpOffW1 + o * kMlpK0 + kMlpIn + k] = a1 * u(rng);
+  for (int t = 0; t < kMlpH * kMlpH; ++t) P[kMlpOffW2 + t] = a2 * u(rng);
+  for (int t = 0; t < kMlpH * kMlpH; ++t) P[kMlpOffW3 + t] = a2 * u(rng);
+  for (int t = 0; t < kMlpH; ++t) P[kMlpOffW4 + t] = a4 * u(rng);
+}
+
+struct DevBuf {
+  void* p = nullptr;
+  ~DevBuf() { cudaFree(p); }
+  template <class T>
+  T* as() { return static_cast<T*>(p); }
+};
+
+}  // namespace
+
+extern "C" {
+
+static_assert(kMlpNumParams == GRB_MLP_NUM_PARAMS, "parameter block size");
+static_assert(kMlpNumWeights == GRB_MLP_NUM_WEIGHTS, "trainable block size");
+
+int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons, const double* metric, double* prims,
+                  double* cons_out, uint32_t* err, int32_t use_learned, void* stream) {
+  return grb_c2p_batch_diag(h, n, cons, metric, prims, cons_out, err, use_learned, nullptr, stream);
+}
+
+int grb_c2p_batch_diag(grb_handle* h, int64_t n, const double* cons, const double* metric, double* prims,
+                       double* cons_out, uint32_t* err, int32_t use_learned, const grb_c2p_diag* diag,
+                       void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (n < 0 || (n > 0 && (!cons || !prims))) return fail(h, GRB_ERR_INVALID);
+  if (use_learned && !h->mlp_ready) return fail(h, GRB_ERR_NO_MODEL);
+  if (n == 0) return GRB_OK;
+  KScope ks(h, (cudaStream_t)stream, GRB_KIND_C2P);
+  return launch_c2p(h, n, cons, metric, prims, cons_out, err, use_learned != 0, diag, (cudaStream_t)stream);
+}
+
+int grb_c2p_features(grb_handle* h, int64_t n, const double* cons, const double* metric, const double* mu,
+                     float* feat, float* target, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (n < 0 || (n > 0 && (!cons || !feat || !target))) return fail(h, GRB_ERR_INVALID);
+  if (n == 0) return GRB_OK;
+  KScope ks(h, (cudaStream_t)stream, GRB_KIND_OTHER);
+  k_mlp_labels<<<(unsigned)std::min<int64_t>(nblk(n, 256), 148 * 8), 256, 0, (cudaStream_t)stream>>>(
+      h->dp, n, cons, metric, mu, feat, target);
+  ++h->launches;
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_mlp_eval(grb_handle* h, int64_t n, const float* params, const float* feat, float* out, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (n < 0 || (n > 0 && (!feat || !out))) return fail(h, GRB_ERR_INVALID);
+  if (!params && !h->mlp_ready) return fail(h, GRB_ERR_NO_MODEL);
+  if (n == 0) return GRB_OK;
+  KScope ks(h, (cudaStream_t)stream, GRB_KIND_OTHER);
+  const unsigned grid = (unsigned)std::min<int64_t>(nblk(n, kC2PThreads), 148 * 8);
+  k_mlp_eval<<<grid, kC2PThreads, 0, (cudaStream_t)stream>>>(params ? params : h->d_mlp, n, feat, out);
+  ++h->launches;
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+}  // extern "C"
+
+namespace {
+int grad_setup(grb_handle* h) {
+  static bool done = false;
+  if (!done) {
+    CK(cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MlpGradSmem)));
+    done = true;
+  }
+  return GRB_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int grb_mlp_grad(grb_handle* h, int64_t n, const float* params, const float* feat, const float* target,
+                 float* grad, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (n < 1 || n > (int64_t)kGradRows * 65535 || !params || !feat || !target || !grad) return fail(h, GRB_ERR_INVALID);
+  if (int rc = grad_setup(h)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const int nparts = (int)nblk(n, kGradRows);
+  DevBuf part;
+  CK(cudaMalloc(&part.p, sizeof(float) * (size_t)nparts * kPW));
+  KScope ks(h, s, GRB_KIND_OTHER);
+  k_mlp_grad<<<nparts, kGradThreads, sizeof(MlpGradSmem), s>>>(params, n, feat, target, n, 0, 0, 1,
+                                                              1.f / (float)n, part.as<float>());
+  k_mlp_reduce<<<nblk(kPW, 256), 256, 0, s>>>(part.as<float>(), nparts, grad);
+  h->launches += 2;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(s));  // part is freed on return
+  return GRB_OK;
+}
+
+void grb_train_config_defaults(grb_train_config* c) {
+  if (!c) return;
+  c->steps = 3000;
+  c->batch = 8192;
+  c->lr = 3e-3f;
+  c->lr_min = 3e-5f;
+  c->seed = 0x6A5CEull;
+  c->calib_states = 1 << 18;
+}
+
+int grb_c2p_train(grb_handle* h, int64_t n, const double* cons, const double* metric, const grb_train_config* cfg,
+                  grb_train_report* rep, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  grb_train_config C;
+  grb_train_config_defaults(&C);
+  if (cfg) C = *cfg;
+  if (n < kGradRows || !cons || C.steps < 1 || C.batch < kGradRows || C.batch % kGradRows ||
+      C.batch > kGradRows * 65535 || !(C.lr > 0.f) || C.lr_min < 0.f || C.calib_states < 0)
+    return fail(h, GRB_ERR_INVALID);
+  if (int rc = ensure_mlp(h)) return rc;
+  if (int rc = grad_setup(h)) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  grb_train_report R{};
+  R.states = n;
+  const int nparts = C.batch / kGradRows;
+  DevBuf prims, mu, feat, tgt, part, m1, m2, loss, stat, pred;
+  CK(cudaMalloc(&prims.p, sizeof(double) * 13 * (size_t)n));
+  CK(cudaMalloc(&mu.p, sizeof(double) * (size_t)n));
+  CK(cudaMalloc(&feat.p, sizeof(float) * kMlpIn * (size_t)n));
+  CK(cudaMalloc(&tgt.p, sizeof(float) * (size_t)n));
+  CK(cudaMalloc(&pred.p, sizeof(float) * (size_t)n));
+  CK(cudaMalloc(&part.p, sizeof(float) * (size_t)nparts * kPW));
+  CK(cudaMalloc(&m1.p, sizeof(float) * kMlpNumWeights));
+  CK(cudaMalloc(&m2.p, sizeof(float) * kMlpNumWeights));
+  CK(cudaMalloc(&loss.p, sizeof(float) * (size_t)C.steps));
+  CK(cudaMalloc(&stat.p, sizeof(double) * kStatBlocks * kStatN));
+  CK(cudaMemsetAsync(m1.p, 0, sizeof(float) * kMlpNumWeights, s));
+  CK(cudaMemsetAsync(m2.p, 0, sizeof(float) * kMlpNumWeights, s));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  CK(cudaEventRecord(e0, s));
+  h->mlp_ready = false;
+  // 1. labels: roots of the plain FP64 c2p, features of the same states
+  grb_c2p_diag dg{nullptr, nullptr, mu.as<double>(), nullptr};
+  if (int rc = launch_c2p(h, n, cons, metric, prims.as<double>(), nullptr, nullptr, false, &dg, s)) return rc;
+  k_mlp_labels<<<(unsigned)std::min<int64_t>(nblk(n, 256), 148 * 8), 256, 0, s>>>(
+      h->dp, n, cons, metric, mu.as<double>(), feat.as<float>(), tgt.as<float>());
+  k_mlp_stats<<<kStatBlocks, 256, 0, s>>>(n, feat.as<float>(), tgt.as<float>(), stat.as<double>());
+  h->launches += 2;
+  CK(cudaGetLastError());
+  std::vector<double> st(kStatBlocks * kStatN);
+  CK(cudaMemcpyAsync(st.data(), stat.p, sizeof(double) * st.size(), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  double sum[kStatN] = {0};
+  for (int b = 0; b < kStatBlocks; ++b)
+    for (int a = 0; a < kStatN; ++a) sum[a] += st[b * kStatN + a];
+  const double cnt = sum[2 * kMlpIn + 2];
+  R.labelled = (int64_t)cnt;
+  if (cnt < kGradRows) return fail(h, GRB_ERR_INVALID);
+  // 2. initial network and normalisation
+  std::vector<float> P(kMlpNumParams);
+  mlp_init(P, C.seed);
+  for (int k = 0; k < kMlpIn; ++k) {
+    const double m = sum[k] / cnt, v = std::max(sum[kMlpIn + k] / cnt - m * m, 0.0);
+    P[kMlpOffNorm + k] = (float)m;
+    P[kMlpOffNorm + kMlpIn + k] = (float)std::max(std::sqrt(v), 1e-3);
+  }
+  {
+    const double m = sum[2 * kMlpIn] / cnt, v = std::max(sum[2 * kMlpIn + 1] / cnt - m * m, 0.0);
+    P[kMlpOffNorm + 2 * kMlpIn] = (float)m;
+    P[kMlpOffNorm + 2 * kMlpIn + 1] = (float)std::max(std::sqrt(v), 1e-6);
+  }
+  P[kMlpOffNorm + 2 * kMlpIn + 2] = 0.1f;
+  CK(cudaMemcpyAsync(h->d_mlp, P.data(), sizeof(float) * kMlpNumParams, cudaMemcpyHostToDevice, s));
+  // 3. Adam with linear warm-up and cosine decay
+  const int64_t warm = std::min<int64_t>(100, C.steps / 10);
+  double b1t = 1.0, b2t = 1.0;
+  for (int64_t it = 0; it < C.steps; ++it) {
+    double lr;
+    if (it < warm) lr = C.lr * (double)(it + 1) / (double)warm;
+    else lr = C.lr_min + 0.5 * (C.lr - C.lr_min) * (1.0 + std::cos(M_PI * (double)(it - warm) / (double)std::max<int64_t>(1, C.steps - warm)));
+    b1t *= 0.9;
+    b2t *= 0.999;
+    k_mlp_grad<<<nparts, kGradThreads, sizeof(MlpGradSmem), s>>>(h->d_mlp, n, feat.as<float>(), tgt.as<float>(),
+                                                                C.batch, C.seed, it, 0, 1.f / (float)C.batch,
+                                                                part.as<float>());
+    k_mlp_adam<<<nblk(kPW, 256), 256, 0, s>>>(h->d_mlp, m1.as<float>(), m2.as<float>(), part.as<float>(), nparts,
+                                               (float)lr, (float)(1.0 - b1t), (float)(1.0 - b2t), loss.as<float>(), it);
+    h->launches += 2;
+  }
+  CK(cudaGetLastError());
+  // 4. prediction error on the training states -> candidate half-widths
+  k_mlp_eval<<<(unsigned)std::min<int64_t>(nblk(n, kC2PThreads), 148 * 8), kC2PThreads, 0, s>>>(
+      h->d_mlp, n, feat.as<float>(), pred.as<float>());
+  ++h->launches;
+  CK(cudaEventRecord(e1, s));
+  std::vector<float> hp(n), ht(n), hl(2);
+  CK(cudaMemcpyAsync(hp.data(), pred.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(ht.data(), tgt.p, sizeof(float) * n, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&hl[0], loss.as<float>(), sizeof(float), cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(&hl[1], loss.as<float>() + C.steps - 1, sizeof(float), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  float tms = 0.f;
+  cudaEventElapsedTime(&tms, e0, e1);
+  R.train_ms = tms;
+  R.loss_first = hl[0];
+  R.loss_last = hl[1];
+  std::vector<float> err;
+  err.reserve(n);
+  for (int64_t t = 0; t < n; ++t)
+    if (std::isfinite(ht[t])) err.push_back(std::fabs(hp[t] - ht[t]));
+  auto quant = [&](double q) {
+    const size_t k = std::min(err.size() - 1, (size_t)(q * (double)(err.size() - 1)));
+    std::nth_element(err.begin(), err.begin() + k, err.end());
+    return err[k];
+  };
+  R.err_q99 = quant(0.99);
+  R.err_q999 = quant(0.999);
+  const float q9999 = quant(0.9999);
+  R.err_max = *std::max_element(err.begin(), err.end());
+  const float cand[4] = {1.2f * R.err_q99, 1.2f * R.err_q999, 1.2f * q9999, 1.1f * R.err_max};
+  // 5. autotune delta: time the learned c2p on the calibration states
+  h->mlp_ready = true;
+  const int64_t nc = std::min<int64_t>(n, C.calib_states > 0 ? C.calib_states : n);
+  int best = 0;
+  for (int ci = 0; ci < 4; ++ci) {
+    const float dlt = std::max(cand[ci], 1e-6f);
+    R.delta_cand[ci] = dlt;
+    CK(cudaMemcpyAsync(h->d_mlp + kMlpOffNorm + 2 * kMlpIn + 2, &dlt, sizeof(float), cudaMemcpyHostToDevice, s));
+    float bestms = 1e30f;
+    for (int rep_i = 0; rep_i < 3; ++rep_i) {
+      CK(cudaEventRecord(e0, s));
+      if (int rc = launch_c2p(h, nc, cons, metric, prims.as<double>(), nullptr, nullptr, true, nullptr, s)) return rc;
+      CK(cudaEventRecord(e1, s));
+      CK(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      bestms = std::min(bestms, ms);
+    }
+    R.calib_ms[ci] = bestms;
+    if (bestms < R.calib_ms[best] || ci == 0) best = ci;
+  }
+  R.delta = R.delta_cand[best];
+  CK(cudaMemcpyAsync(h->d_mlp + kMlpOffNorm + 2 * kMlpIn + 2, &R.delta, sizeof(float), cudaMemcpyHostToDevice, s));
+  CK(cudaStreamSynchronize(s));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rep) *rep = R;
+  return GRB_OK;
+}
+
+int grb_c2p_model_get(grb_handle* h, float* params, int64_t nparams) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!params || nparams != kMlpNumParams) return fail(h, GRB_ERR_INVALID);
+  if (!h->mlp_ready) return fail(h, GRB_ERR_NO_MODEL);
+  CK(cudaMemcpy(params, h->d_mlp, sizeof(float) * kMlpNumParams, cudaMemcpyDeviceToHost));
+  return GRB_OK;
+}
+
+int grb_c2p_model_set(grb_handle* h, const float* params, int64_t nparams) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!params || nparams != kMlpNumParams) return fail(h, GRB_ERR_INVALID);
+  for (int k = 0; k < kMlpNumParams; ++k)
+    if (!std::isfinite(params[k])) return fail(h, GRB_ERR_INVALID);
+  for (int k = 0; k < kMlpIn; ++k)
+    if (!(params[kMlpOffNorm + kMlpIn + k] > 0.f)) return fail(h, GRB_ERR_INVALID);
+  if (!(params[kMlpOffNorm + 2 * kMlpIn + 1] > 0.f) || !(params[kMlpOffNorm + 2 * kMlpIn + 2] > 0.f))
+    return fail(h, GRB_ERR_INVALID);
+  if (int rc = ensure_mlp(h)) return rc;
+  CK(cudaMemcpy(h->d_mlp, params, sizeof(float) * kMlpNumParams, cudaMemcpyHostToDevice));
+  h->mlp_ready = true;
+  return GRB_OK;
+}
 
 int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
                           int32_t nby, int32_t nbz, const int32_t* periodic, void* stream) {

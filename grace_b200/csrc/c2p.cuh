@@ -19,11 +19,12 @@ enum : uint32_t {
 };
 constexpr int kBrentMaxIter = 200;
 
-// Brent's zero finder on [a,b] with tol = 2 eps |b| + t.  F: double(double).
+// Brent's zero finder on [a,b] with tol = 2 eps |b| + t, given f(a) and
+// f(b) already evaluated (fa0, fb0).  F: double(double).
 template <class F>
-GRB_HD double brent(F& f, double a, double b, double t, int& iters) {
+GRB_HD double brent_f(F& f, double a, double b, double fa0, double fb0, double t, int& iters) {
   double sa = a, sb = b;
-  double fa = f(sa), fb = f(sb);
+  double fa = fa0, fb = fb0;
   double c = sa, fc = fa, e = sb - sa, d = e;
   const double macheps = 2.220446049250313e-16;
   for (int it = 0; it < kBrentMaxIter; ++it) {
@@ -63,6 +64,12 @@ GRB_HD double brent(F& f, double a, double b, double t, int& iters) {
     }
   }
   return sb;
+}
+template <class F>
+GRB_HD double brent(F& f, double a, double b, double t, int& iters) {
+  const double fa = f(a);
+  const double fb = f(b);
+  return brent_f(f, a, b, fa, fb, t, iters);
 }
 
 // Kastaun auxiliary function mu sqrt(h0^2 + rbar^2(mu)) - 1 (kastaun_c2p.hh:44-117)
@@ -245,31 +252,42 @@ GRB_HD double kastaun_mu0(const KSc& k) {
   return mu0;
 }
 
-// Optional learned bracket for the Kastaun solve.
+// Optional learned bracket for the Kastaun solve.  mu0 (has_mu0): the plain
+// bracket top already computed from the unchanged state.
 struct Guess {
   bool valid;
   double lo, hi;
+  double mu0;
+  bool has_mu0;
 };
+GRB_HD Guess no_guess() { return Guess{false, 0., 0., 0., false}; }
 
+// kastaun_c2p_t::invert (kastaun_c2p.hh:352-395).  With a learned bracket
+// the unchanged Brent iteration starts from [gs.lo, gs.hi] when f changes
+// sign there (the two end values are the iteration's own first two
+// evaluations), and from the plain [0, mu0] otherwise.
 GRB_HD double kastaun_invert(const DevEos& e, const Met& m, double c[10], double pr[13],
-                             uint32_t& sig, int& iters, const Guess& gs, bool& guess_used) {
+                             uint32_t& sig, int& iters, const Guess& gs, bool& guess_used,
+                             double& mu_out) {
   const KSc k = kscalars(e, m, c);
   const KRt f(e, k);
   double mu;
   guess_used = false;
+  const double mu0 = gs.has_mu0 ? gs.mu0 : kastaun_mu0(k);
   if (gs.valid) {
-    const double flo = f(gs.lo), fhi = f(gs.hi);
-    if (flo * fhi < 0) {
-      mu = brent(f, gs.lo, gs.hi, 1e-15, iters);
-      guess_used = true;
+    const double lo = gs.lo, hi = fmin(gs.hi, mu0);
+    if (hi > lo) {
+      const double flo = f(lo), fhi = f(hi);
+      if (flo * fhi < 0) {
+        mu = brent_f(f, lo, hi, flo, fhi, 1e-15, iters);
+        guess_used = true;
+      }
     }
   }
-  if (!guess_used) {
-    const double mu0 = kastaun_mu0(k);
-    mu = brent(f, 0, mu0, 1e-15, iters);
-  }
+  if (!guess_used) mu = brent(f, 0, mu0, 1e-15, iters);
   double x, w, rho, press, eps, temp, ent;
   const double res = f.eval(mu, true, sig, x, w, rho, press, eps, temp, ent);
+  mu_out = mu;
   pr[GRB_P_EPS] = eps; pr[GRB_P_RHO] = rho; pr[GRB_P_PRESS] = press;
   pr[GRB_P_TEMP] = temp; pr[GRB_P_ENT] = ent;
 #pragma unroll
@@ -377,13 +395,14 @@ struct C2POut {
   int iters;
   bool floored;
   bool guess_used;
+  double mu;  // Kastaun root, 0 where the Kastaun solve did not run
 };
 
 // conservs_to_prims (c2p.cpp:188-414).  c: densitized cons with densitized
 // cell-centred B (in), re-densitized consistent cons (out).
 GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P, double r_sph,
                   bool dry_run, double alp_bh_thresh, const Guess& gs) {
-  C2POut o{0u, 0u, 0, false, false};
+  C2POut o{0u, 0u, 0, false, false, 0.0};
   const DevEos& e = P.eos;
   bool failed = false;
   uint32_t ret = 0;
@@ -422,7 +441,9 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
   }
   if (o.floored && dry_run) return o;
   if (c[0] >= P.rho_fl * (1 + P.atmo_tol)) {
-    const double res = kastaun_invert(e, m, c, pr, ret, o.iters, gs, o.guess_used);
+    Guess g2 = gs;
+    if (o.floored) g2.has_mu0 = false;  // limit_conservatives changed the state
+    const double res = kastaun_invert(e, m, c, pr, ret, o.iters, g2, o.guess_used, o.mu);
     failed = (fabs(res) > P.tol) || (ret & SIG_RHO_HIGH) || (ret & SIG_EPS_HIGH) || !isfinite(res);
     double beta;
     {

@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box
   if (!dmp) {  // the c2p dry run only matters when the DMP test passed
     const Met m = cell_met(G, os, i, j, k, q);
     double pr[13];
-    const Guess none{false, 0., 0.};
+    const Guess none = no_guess();
     floored = c2p(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), true, 1e30, none).floored;
   }
   if (floored || dmp) {
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, 
   aux[a0 + G.cells * GRB_BZ] = c[9] / m.sqrtg;
   const double cbx = c[7], cby = c[8], cbz = c[9];
   double pr[13];
-  const Guess none{false, 0., 0.};
+  const Guess none = no_guess();
   const C2POut o = c2p(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), false, P.alp_bh_thresh, none);
   if (o.fatal) atomicOr(B.flags, o.fatal);
   aux[a0 + G.cells * GRB_RHO] = pr[GRB_P_RHO];
@@ -658,40 +658,6 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, int ax, int fd, 
     const int64_t ls = sidx[0] + (int64_t)n[0] * (sidx[1] + (int64_t)n[1] * sidx[2]) + qsrc * qstride;
     for (int v = 0; v < nv; ++v) a[ld + v * vstride] = a[ls + v * vstride];
   }
-}
-
-// batched c2p on SoA arrays
-__global__ void __launch_bounds__(128) k_c2p_batch(DevParams P, int64_t n, const double* __restrict__ cons,
-                                                    const double* __restrict__ metric,
-                                                    double* __restrict__ prims, double* __restrict__ cons_out,
-                                                    uint32_t* __restrict__ err, int32_t* __restrict__ iters,
-                                                    uint32_t* flags) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  double g[6] = {1, 0, 0, 1, 0, 1}, b[3] = {0, 0, 0}, alp = 1.0;
-  if (metric) {
-#pragma unroll
-    for (int a = 0; a < 6; ++a) g[a] = metric[a * n + t];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) b[a] = metric[(6 + a) * n + t];
-    alp = metric[9 * n + t];
-  }
-  const Met m = make_met(g, b, alp);
-  double c[10], pr[13];
-#pragma unroll
-  for (int v = 0; v < 10; ++v) c[v] = cons[v * n + t];
-  const Guess none{false, 0., 0.};
-  const C2POut o = c2p(c, pr, m, P, 0.0, false, P.alp_bh_thresh, none);
-  if (o.fatal) atomicOr(flags, o.fatal);
-  pr[GRB_P_CS2] = 0.0;
-#pragma unroll
-  for (int v = 0; v < 13; ++v) prims[v * n + t] = pr[v];
-  if (cons_out) {
-#pragma unroll
-    for (int v = 0; v < 10; ++v) cons_out[v * n + t] = c[v];
-  }
-  if (err) err[t] = o.err;
-  if (iters) iters[t] = o.iters;
 }
 
 }  // namespace grb

@@ -153,14 +153,75 @@ class GRMHDEquationsSystem:
                                                   nb[2], per, _stream_ptr(stream)), "grb_fill_ghosts_brick")
 
     def conservs_to_prims(self, cons, metric=None, cons_out=None, err=None, use_learned=False,
-                          stream=None):
-        """Batched c2p: cons (10, n) float64 -> prims (13, n)."""
+                          stream=None, diag=None):
+        """Batched c2p: cons (10, n) float64 -> prims (13, n).  diag: dict
+        with optional device tensors "iters" (int32 [n]), "guess_used"
+        (int8 [n]), "mu" (float64 [n]), "bracket" (float64 [2, n])."""
         n = cons.shape[1]
         prims = torch.empty(abi.P_CS2 + 1, n, dtype=torch.float64, device=cons.device)
-        _lib.check(self.lib.grb_c2p_batch(self.h, n, _ptr(cons), _ptr(metric), _ptr(prims), _ptr(cons_out),
-                                          _ptr(err), 1 if use_learned else 0, _stream_ptr(stream)),
-                   "grb_c2p_batch")
+        if diag is None:
+            _lib.check(self.lib.grb_c2p_batch(self.h, n, _ptr(cons), _ptr(metric), _ptr(prims), _ptr(cons_out),
+                                              _ptr(err), 1 if use_learned else 0, _stream_ptr(stream)),
+                       "grb_c2p_batch")
+        else:
+            d = abi.C2PDiag(*[_ptr(diag.get(k)) for k in ("iters", "guess_used", "mu", "bracket")])
+            _lib.check(self.lib.grb_c2p_batch_diag(self.h, n, _ptr(cons), _ptr(metric), _ptr(prims),
+                                                   _ptr(cons_out), _ptr(err), 1 if use_learned else 0,
+                                                   ctypes.byref(d), _stream_ptr(stream)), "grb_c2p_batch_diag")
         return prims
+
+    # ---- learned c2p bracket -------------------------------------------
+    def train_c2p_model(self, cons, metric=None, stream=None, **cfg):
+        """Train the bracket network on the GPU from the states cons (10, n);
+        cfg: steps, batch, lr, lr_min, seed, calib_states.  Returns the
+        training report as a dict."""
+        c = abi.TrainConfig()
+        self.lib.grb_train_config_defaults(ctypes.byref(c))
+        for k, v in cfg.items():
+            setattr(c, k, v)
+        r = abi.TrainReport()
+        _lib.check(self.lib.grb_c2p_train(self.h, cons.shape[1], _ptr(cons), _ptr(metric), ctypes.byref(c),
+                                          ctypes.byref(r), _stream_ptr(stream)), "grb_c2p_train")
+        out = {k: getattr(r, k) for k, _ in abi.TrainReport._fields_}
+        out["delta_cand"] = list(r.delta_cand)
+        out["calib_ms"] = list(r.calib_ms)
+        return out
+
+    def c2p_model(self):
+        """The model's parameter block (numpy float32 [MLP_NUM_PARAMS])."""
+        import numpy as np
+        P = np.zeros(abi.MLP_NUM_PARAMS, np.float32)
+        _lib.check(self.lib.grb_c2p_model_get(self.h, P.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), P.size),
+                   "grb_c2p_model_get")
+        return P
+
+    def set_c2p_model(self, P):
+        import numpy as np
+        P = np.ascontiguousarray(P, dtype=np.float32)
+        _lib.check(self.lib.grb_c2p_model_set(self.h, P.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), P.size),
+                   "grb_c2p_model_set")
+
+    def c2p_features(self, cons, metric=None, mu=None, stream=None):
+        n = cons.shape[1]
+        feat = torch.empty(abi.MLP_IN, n, dtype=torch.float32, device=cons.device)
+        tgt = torch.empty(n, dtype=torch.float32, device=cons.device)
+        _lib.check(self.lib.grb_c2p_features(self.h, n, _ptr(cons), _ptr(metric), _ptr(mu), _ptr(feat), _ptr(tgt),
+                                             _stream_ptr(stream)), "grb_c2p_features")
+        return feat, tgt
+
+    def mlp_eval(self, feat, params=None, stream=None):
+        n = feat.shape[1]
+        out = torch.empty(n, dtype=torch.float32, device=feat.device)
+        _lib.check(self.lib.grb_mlp_eval(self.h, n, _ptr(params), _ptr(feat), _ptr(out), _stream_ptr(stream)),
+                   "grb_mlp_eval")
+        return out
+
+    def mlp_grad(self, params, feat, tgt, stream=None):
+        """(gradient [MLP_NUM_WEIGHTS], loss) of the batch MSE."""
+        g = torch.empty(abi.MLP_NUM_WEIGHTS + 1, dtype=torch.float32, device=feat.device)
+        _lib.check(self.lib.grb_mlp_grad(self.h, feat.shape[1], _ptr(params), _ptr(feat), _ptr(tgt), _ptr(g),
+                                         _stream_ptr(stream)), "grb_mlp_grad")
+        return g[:-1], float(g[-1])
 
     def set_mode(self, mode):
         """abi.MODE_PLAIN (reference launch ranges, one thread per item) or

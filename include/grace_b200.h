@@ -64,7 +64,8 @@ enum grb_status_code {
   GRB_ERR_INVALID = -1,     /* bad argument / unsupported option */
   GRB_ERR_CUDA = -2,        /* a CUDA runtime call failed */
   GRB_ERR_NOMEM = -3,       /* scratch allocation failed */
-  GRB_ERR_NOT_RESERVED = -4 /* grb_reserve was not called for this grid */
+  GRB_ERR_NOT_RESERVED = -4, /* grb_reserve was not called for this grid */
+  GRB_ERR_NO_MODEL = -5      /* learned c2p requested before a model was trained or set */
 };
 /* bits of grb_status.device_flags: device-side conditions the reference
  * turns into Kokkos::abort (c2p.hh:167-316); the kernels record and go on
@@ -205,11 +206,91 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A,
  *          for the flat metric
  *   prims  [GRB_NUM_PRIMS][n] out; cons_out [GRB_NUM_CONS][n] out or NULL
  *   err    [n] out: c2p_err bits (c2p.hh:98-121); NULL allowed
- *   use_learned: 1 = seed the root bracket with the learned model loaded by
- *          grb_load_c2p_model (falls back per state when it misses). */
+ *   use_learned: 1 = start the Kastaun root solve from the learned bracket
+ *          of the model made by grb_c2p_train or grb_c2p_model_set (per
+ *          state, the plain bracket when the learned one misses the root);
+ *          GRB_ERR_NO_MODEL without a model. */
 int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons,
                   const double* metric, double* prims, double* cons_out,
                   uint32_t* err, int32_t use_learned, void* stream);
+
+/* ---- learned c2p bracket (no counterpart in the reference) --------------
+ * A 12-64-64-64-1 ReLU network (BF16 tensor-core hidden layers, FP32
+ * accumulation) predicts L = log(mu0/mu) for a state: mu is the root of the
+ * Kastaun master function (kastaun_c2p.hh:245-290), mu0 the top of the plain
+ * bracket (kastaun_c2p.hh:355-369).  Features: D, tau/D, |S|/D, |B|^2/D,
+ * cos^2(S,B) (kastaun_c2p.hh:306-337) and log mu0, normalised and split into
+ * BF16 high parts and remainders.  The FP64 Brent solve (1e-15 abscissa
+ * tolerance, as the plain one) runs on [mu0 e^(-L-delta),
+ * min(mu0 e^(-L+delta), mu0)] when the master function changes sign there,
+ * else on the plain [0, mu0]: the network changes only the starting bracket.
+ * Parameters: GRB_MLP_NUM_PARAMS floats, W1[64][16] b1[64] W2[64][64] b2[64]
+ * W3[64][64] b3[64] w4[64] b4 (the GRB_MLP_NUM_WEIGHTS trainable ones), then
+ * feature means[6], feature sds[6], L mean, L sd, delta. */
+#define GRB_MLP_NUM_WEIGHTS 9473
+#define GRB_MLP_NUM_PARAMS 9488
+
+typedef struct grb_c2p_diag {
+  int32_t* iters;      /* [n] Brent iterations of the Kastaun solve, or NULL */
+  int8_t* guess_used;  /* [n] 1 where the learned bracket held the root, or NULL */
+  double* mu;          /* [n] Kastaun root (0 where no Kastaun solve ran), or NULL */
+  double* bracket;     /* [2][n] learned bracket lo, hi (0 where none), or NULL */
+} grb_c2p_diag;
+/* grb_c2p_batch with per-state diagnostics (device arrays). */
+int grb_c2p_batch_diag(grb_handle* h, int64_t n, const double* cons,
+                       const double* metric, double* prims, double* cons_out,
+                       uint32_t* err, int32_t use_learned,
+                       const grb_c2p_diag* diag, void* stream);
+
+typedef struct grb_train_config {
+  int64_t steps;        /* Adam steps (default 3000) */
+  int32_t batch;        /* states per step, a multiple of 64 (default 8192) */
+  float lr;             /* peak learning rate (default 3e-3) */
+  float lr_min;         /* end of the cosine decay (default 3e-5) */
+  uint64_t seed;        /* weight initialisation and sampling */
+  int64_t calib_states; /* states timed to choose delta (default 2^18) */
+} grb_train_config;
+typedef struct grb_train_report {
+  int64_t states;       /* states given */
+  int64_t labelled;     /* states whose plain c2p ran the Kastaun solve */
+  float loss_first;     /* batch MSE of normalised L, first step */
+  float loss_last;      /* ... last step */
+  float err_q99;        /* |L_net - L| quantiles over the states */
+  float err_q999;
+  float err_max;
+  float delta;          /* chosen bracket half-width (in log mu) */
+  float delta_cand[4];  /* candidates: 1.2 q99, 1.2 q999, 1.2 q9999, 1.1 max */
+  float calib_ms[4];    /* learned c2p time on the calibration states */
+  double train_ms;      /* device time: labels + statistics + Adam steps */
+} grb_train_report;
+void grb_train_config_defaults(grb_train_config* c);
+/* Train the bracket network on the GPU from n states (cons/metric as for
+ * grb_c2p_batch): labels are the roots of the plain FP64 c2p of the same
+ * states; the tensor-core forward, the FP32 backward and Adam run as this
+ * library's kernels; delta is then chosen among four quantiles of the
+ * prediction error by timing the learned c2p.  Synchronises the stream. */
+int grb_c2p_train(grb_handle* h, int64_t n, const double* cons,
+                  const double* metric, const grb_train_config* cfg,
+                  grb_train_report* report, void* stream);
+/* Copy the model to / from a host array of GRB_MLP_NUM_PARAMS floats. */
+int grb_c2p_model_get(grb_handle* h, float* params, int64_t nparams);
+int grb_c2p_model_set(grb_handle* h, const float* params, int64_t nparams);
+/* Features [6][n] (FP32) and target L = log(mu0/mu) [n] (NaN where mu <= 0
+ * or mu is NULL) of n states, mu the plain roots; device arrays. */
+int grb_c2p_features(grb_handle* h, int64_t n, const double* cons,
+                     const double* metric, const double* mu, float* feat,
+                     float* target, void* stream);
+/* Network output L [n] for raw features [6][n] with the parameter block
+ * params (device; NULL = the handle's model). */
+int grb_mlp_eval(grb_handle* h, int64_t n, const float* params,
+                 const float* feat, float* out, void* stream);
+/* Gradient of the mean squared error of normalised L over n samples
+ * (targets NaN are skipped but still count in the mean) with respect to the
+ * GRB_MLP_NUM_WEIGHTS trainable parameters; grad[GRB_MLP_NUM_WEIGHTS] receives
+ * the loss.  All device arrays; synchronises the stream. */
+int grb_mlp_grad(grb_handle* h, int64_t n, const float* params,
+                 const float* feat, const float* target, float* grad,
+                 void* stream);
 
 
 /* ---- execution mode and autotuning --------------------------------------- */

@@ -34,7 +34,7 @@ inline C2PParams make_c2p_params(const grb_params& p) {
 enum { FATAL_C2P_RHO_HIGH = 1, FATAL_EOS_RHO_HIGH = 2, FATAL_EOS_EPS_HIGH = 4,
        FATAL_EOS_TEMP_HIGH = 8, FATAL_EOS_PRESS_HIGH = 16 };
 
-struct C2PStats { int brent_iters = 0; int newton_fail = 0; };
+struct C2PStats { int brent_iters = 0; int newton_fail = 0; double mu = 0; int guess_used = 0; };
 
 // Learned-bracket hook: if set, called with the Kastaun scalars; returns
 // true and a bracket [lo, hi] to try before the plain one.
@@ -306,8 +306,8 @@ inline double kastaun_mu0(const KScalars& k) {
 }
 
 // kastaun_c2p_t::invert (kastaun_c2p.hh:352-395).  With a learned guess the
-// Brent solve starts from [guess.lo, guess.hi] when that bracket changes
-// sign, and from the plain [0, mu0] otherwise.
+// Brent solve starts from [guess.lo, min(guess.hi, mu0)] when that bracket
+// changes sign, and from the plain [0, mu0] otherwise.
 inline double kastaun_invert(const Eos& e, const Metric& m, double cons[10], double pr[13],
                              uint32_t& sig, C2PStats* st, const BracketGuess* guess) {
   KScalars k = kastaun_setup(e, m, cons);
@@ -315,16 +315,22 @@ inline double kastaun_invert(const Eos& e, const Metric& m, double cons[10], dou
   double mu;
   bool done = false;
   int* it = st ? &st->brent_iters : nullptr;
+  const double mu0 = kastaun_mu0(k);
   if (guess && guess->valid) {
-    const double flo = f(guess->lo), fhi = f(guess->hi);
-    if (flo * fhi < 0) { mu = brent(f, guess->lo, guess->hi, 1e-15, it); done = true; }
+    const double lo = guess->lo, hi = std::fmin(guess->hi, mu0);
+    if (hi > lo) {
+      const double flo = f(lo), fhi = f(hi);
+      if (flo * fhi < 0) {
+        mu = brent(f, lo, hi, 1e-15, it);
+        done = true;
+        if (st) st->guess_used = 1;
+      }
+    }
   }
-  if (!done) {
-    const double mu0 = kastaun_mu0(k);
-    mu = brent(f, 0, mu0, 1e-15, it);
-  }
+  if (!done) mu = brent(f, 0, mu0, 1e-15, it);
   double x, w, eps, rho, press, temp, ent;
   const double res = f.primitives(mu, sig, x, w, rho, press, eps, temp, ent);
+  if (st) st->mu = mu;
   pr[PR_EPS] = eps; pr[PR_RHO] = rho; pr[PR_PRESS] = press; pr[PR_TEMP] = temp;
   pr[PR_ENT] = ent;
   for (int i = 0; i < 3; ++i) pr[PR_BX + i] = k.B[i];

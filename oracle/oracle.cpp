@@ -121,3 +121,4 @@ struct OracleNumerics {
 #define NUMERICS orc::OracleNumerics
 #define API(name) orc_##name
 #include "api_impl.hpp"
+#include "mlp_oracle.hpp"

@@ -71,6 +71,62 @@ def p(a):
     return a.ctypes.data_as(VP) if a is not None else None
 
 
+def mlp_lib():
+    """liboracle.so with the bracket-network oracle bound (orc_ only)."""
+    L = lib("orc")
+    P = C.POINTER
+    for name, res, args in (
+            ("orc_mlp_num_params", C.c_int, []),
+            ("orc_mlp_features", None, [P(abi.Params), C.c_int64, VP, VP, VP]),
+            ("orc_mlp_forward", None, [VP, C.c_int64, VP, C.c_int32, VP]),
+            ("orc_mlp_loss_grad", C.c_double, [VP, C.c_int64, VP, VP, C.c_int32, VP]),
+            ("orc_c2p_batch_guess", C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP, VP, VP, VP, VP, VP,
+                                              VP, VP])):
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    return L
+
+
+def mlp_features(params, cons, metric=None):
+    n = cons.shape[1]
+    f = np.zeros((abi.MLP_IN, n), np.float32)
+    mlp_lib().orc_mlp_features(C.byref(params), n, p(np.ascontiguousarray(cons)),
+                               p(np.ascontiguousarray(metric) if metric is not None else None), p(f))
+    return f
+
+
+def mlp_forward(P, feat, emulate=True):
+    n = feat.shape[1]
+    out = np.zeros(n)
+    mlp_lib().orc_mlp_forward(p(np.ascontiguousarray(P, np.float32)), n,
+                              p(np.ascontiguousarray(feat, np.float32)), 1 if emulate else 0, p(out))
+    return out
+
+
+def mlp_loss_grad(P, feat, tgt, emulate=True):
+    n = feat.shape[1]
+    g = np.zeros(abi.MLP_NUM_WEIGHTS)
+    loss = mlp_lib().orc_mlp_loss_grad(p(np.ascontiguousarray(P, np.float32)), n,
+                                       p(np.ascontiguousarray(feat, np.float32)),
+                                       p(np.ascontiguousarray(tgt, np.float32)), 1 if emulate else 0, p(g))
+    return loss, g
+
+
+def c2p_batch_guess(params, cons, lo, hi, metric=None):
+    n = cons.shape[1]
+    pr = np.zeros((13, n))
+    co = np.zeros((10, n))
+    err = np.zeros(n, np.uint32)
+    it = np.zeros(n, np.int32)
+    gu = np.zeros(n, np.int8)
+    mu = np.zeros(n)
+    rc = mlp_lib().orc_c2p_batch_guess(C.byref(params), n, p(np.ascontiguousarray(cons)), p(metric),
+                                       p(np.ascontiguousarray(lo)), p(np.ascontiguousarray(hi)), p(pr), p(co),
+                                       p(err), p(it), p(gu), p(mu))
+    return pr, co, err, it, gu, mu, rc
+
+
 class Stage:
     """Oracle stage driver on host numpy arrays (GRACE LayoutLeft shapes)."""
 

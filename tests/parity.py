@@ -8,6 +8,8 @@ per-component relative errors are ill-posed for momenta that are zero up
 to rounding (a resting background with 1e-3 pressure noise)."""
 import numpy as np
 
+from grace_b200 import abi
+
 
 def cons_rel_err(a, b, floor=1e-300):
     """a, b: (nq, >=7, NZ, NY, NX) state arrays (interior slice); returns
@@ -29,3 +31,28 @@ def cons_rel_err(a, b, floor=1e-300):
 
 def interior(x, g):
     return x[..., g:-g, g:-g, g:-g]
+
+
+# ---- c2p primitives -------------------------------------------------------
+PRIM_TOL = 1e-12  # relative, per primitive
+
+
+def state_residual(a, b):
+    """State-normalised infinity-norm residual of test/test_c2p.cpp:80-98:
+    max |a-b| over (rho, eps, z^i) divided by max(|rho|, |eps|, |z|)."""
+    zm = np.sqrt(np.sum(b[abi.P_ZX:abi.P_ZZ + 1] ** 2, axis=0))
+    scale = np.maximum(np.maximum(np.abs(b[abi.P_RHO]), np.abs(b[abi.P_EPS])), np.maximum(zm, 1e-30))
+    d = np.zeros(b.shape[1])
+    for v in (abi.P_RHO, abi.P_EPS, abi.P_ZX, abi.P_ZY, abi.P_ZZ):
+        d = np.maximum(d, np.abs(a[v] - b[v]))
+    return d / scale
+
+
+def prim_tol(prims):
+    """Per-state tolerance: 1e-12, widened by W^2 for fast flows.  Brent stops
+    within t = 1e-15 of the root in mu (kastaun_c2p.hh:372); through
+    W = (1 - rbar^2 mu^2)^(-1/2) an abscissa shift dmu moves W (and
+    rho = D/W) by ~W^2 dmu/mu, so two correct solvers that stop at different
+    points of the tolerance window differ by up to ~1e-13 W^2."""
+    W = np.sqrt(1.0 + np.sum(prims[abi.P_ZX:abi.P_ZZ + 1] ** 2, axis=0))
+    return PRIM_TOL * np.maximum(1.0, W * W)

@@ -1,0 +1,153 @@
+"""Learned c2p bracket on the GPU, through the C ABI: the network's
+features, tensor-core forward and gradient against the CPU oracle, training
+on the GPU, and the learned-bracket c2p against the plain one and against
+the oracle started from the same bracket."""
+import numpy as np
+import pytest
+import torch
+
+import _oracle
+from grace_b200 import abi, params, workloads
+from grace_b200.host import GRMHDEquationsSystem
+from parity import prim_tol, state_residual
+from test_mlp_oracle import feats_targets, random_params
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x)).to("cuda:0")
+
+
+@pytest.fixture(scope="module")
+def sysg():
+    return GRMHDEquationsSystem(params.c2p_bench())
+
+
+@pytest.fixture(scope="module")
+def trained():
+    """A handle with a model trained on 2^18 seeded states."""
+    s = GRMHDEquationsSystem(params.c2p_bench())
+    cons, _ = workloads.c2p_states(1 << 18, seed=42)
+    rep = s.train_c2p_model(dev(cons), steps=1500, calib_states=1 << 16)
+    return s, rep
+
+
+def test_features_match_oracle(sysg):
+    P = params.c2p_bench()
+    cons, _ = workloads.c2p_states(20000, seed=41)
+    f_g, t_g = sysg.c2p_features(dev(cons))
+    f_o = _oracle.mlp_features(P, cons)
+    f_g = f_g.cpu().numpy()
+    assert np.max(np.abs(f_g[:5] - f_o[:5])) < 1e-5
+    # log mu0: the same EOS-free Newton solve on both sides
+    assert np.max(np.abs(f_g[5] - f_o[5])) < 1e-6
+    assert torch.isnan(t_g).all()  # no roots given -> no labels
+
+
+def test_forward_matches_oracle(sysg):
+    P = random_params(7)
+    _, f, _ = feats_targets(8192, 44)
+    y_g = sysg.mlp_eval(dev(f), params=dev(P)).cpu().numpy()
+    y_o = _oracle.mlp_forward(P, f, emulate=True)
+    d = np.abs(y_g - y_o)
+    scale = 1e-5 * (1 + np.abs(y_o))
+    # FP32 tensor-core accumulation vs FP64 sums: identical up to the rare
+    # activation that lands on the other side of a BF16 rounding boundary
+    assert np.mean(d < scale) > 0.99, np.quantile(d, 0.99)
+    assert np.max(d) < 2e-3
+
+
+def test_gradient_matches_oracle(sysg):
+    P = random_params(8)
+    _, f, t = feats_targets(4096, 45)
+    t[::97] = np.nan  # unlabelled states contribute nothing
+    g_g, loss_g = sysg.mlp_grad(dev(P), dev(f), dev(t))
+    g_g = g_g.cpu().numpy().astype(np.float64)
+    loss_o, g_o = _oracle.mlp_loss_grad(P, f, t, emulate=True)
+    assert abs(loss_g - loss_o) <= 1e-4 * loss_o
+    H = 64
+    blocks = {"W1": (0, H * 16), "b1": (H * 16, H), "W2": (H * 17, H * H), "b2": (H * 17 + H * H, H),
+              "W3": (H * 18 + H * H, H * H), "b3": (H * 18 + 2 * H * H, H), "w4": (H * 19 + 2 * H * H, H),
+              "b4": (H * 20 + 2 * H * H, 1)}
+    assert blocks["b4"][0] + 1 == abi.MLP_NUM_WEIGHTS
+    for name, (o, n) in blocks.items():
+        a, b = g_g[o:o + n], g_o[o:o + n]
+        rel = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30)
+        assert rel < 2e-3, (name, rel)
+
+
+def test_learned_without_model_fails():
+    s = GRMHDEquationsSystem(params.c2p_bench())
+    cons, _ = workloads.c2p_states(256, seed=46)
+    with pytest.raises(RuntimeError, match=str(abi.ERR_NO_MODEL)):
+        s.conservs_to_prims(dev(cons), use_learned=True)
+
+
+def test_training_and_learned_c2p(trained):
+    """Training converges; the learned-bracket c2p returns the plain c2p's
+    primitives (W^2-aware 1e-12, the c2p tolerance window) and the oracle's
+    primitives when the oracle starts from the same brackets; and what the
+    network gains over the plain bracket is measured, on held-out states,
+    as Brent iterations per state and per warp (the GPU pays the slowest
+    lane of each warp)."""
+    s, rep = trained
+    assert rep["labelled"] > 0.99 * (1 << 18)
+    assert rep["loss_last"] < 0.05 * rep["loss_first"], rep
+    assert rep["delta"] in rep["delta_cand"]
+    P = params.c2p_bench()
+    cons, _ = workloads.c2p_states(1 << 16, seed=43)
+    n = cons.shape[1]
+    c = dev(cons)
+    it_p = torch.zeros(n, dtype=torch.int32, device="cuda:0")
+    it_l = torch.zeros_like(it_p)
+    gu = torch.zeros(n, dtype=torch.int8, device="cuda:0")
+    br = torch.zeros(2, n, dtype=torch.float64, device="cuda:0")
+    e_p = torch.zeros(n, dtype=torch.int32, device="cuda:0")
+    e_l = torch.zeros_like(e_p)
+    pr_p = s.conservs_to_prims(c, err=e_p, diag={"iters": it_p}).cpu().numpy()
+    pr_l = s.conservs_to_prims(c, err=e_l, use_learned=True,
+                               diag={"iters": it_l, "guess_used": gu, "bracket": br}).cpu().numpy()
+    e_p, e_l = e_p.cpu().numpy(), e_l.cpu().numpy()
+    it_p, it_l, gu, br = it_p.cpu().numpy(), it_l.cpu().numpy(), gu.cpu().numpy(), br.cpu().numpy()
+    used = gu == 1
+    assert used.mean() > 0.9, used.mean()
+    same = e_p == e_l
+    assert same.mean() > 0.999
+    res = state_residual(pr_l[:, same], pr_p[:, same])
+    assert np.all(res < prim_tol(pr_p)[same]), res.max()
+    # the oracle from the same brackets
+    pr_o, _, e_o, it_o, gu_o, _, _ = _oracle.c2p_batch_guess(P, cons, br[0], br[1])
+    assert (gu_o == gu).mean() > 0.999
+    same = e_o == e_l
+    assert same.mean() > 0.999
+    res = state_residual(pr_l[:, same], pr_o[:, same])
+    assert np.all(res < prim_tol(pr_o)[same]), res.max()
+    # gains over the plain bracket (reported; the plain bracket's top is
+    # already within 5e-5 of the root for half of these states)
+    m = (n // 32) * 32
+    gain = {
+        "mean_iters_plain": float(it_p.mean()), "mean_iters_learned": float(it_l.mean()),
+        "warp_max_plain": float(it_p[:m].reshape(-1, 32).max(1).mean()),
+        "warp_max_learned": float(it_l[:m].reshape(-1, 32).max(1).mean()),
+        "guess_used": float(used.mean()), "delta": rep["delta"],
+    }
+    print("learned-bracket gain:", gain)
+    assert gain["mean_iters_learned"] < gain["mean_iters_plain"] + 2.0
+
+
+def test_model_roundtrip(trained):
+    s, _ = trained
+    Pm = s.c2p_model()
+    assert Pm.shape == (abi.MLP_NUM_PARAMS,) and np.all(np.isfinite(Pm))
+    s2 = GRMHDEquationsSystem(params.c2p_bench())
+    s2.set_c2p_model(Pm)
+    cons, _ = workloads.c2p_states(4096, seed=47)
+    c = dev(cons)
+    a = s.conservs_to_prims(c, use_learned=True).cpu().numpy()
+    b = s2.conservs_to_prims(c, use_learned=True).cpu().numpy()
+    assert np.array_equal(a, b)
+    bad = Pm.copy()
+    bad[abi.MLP_NUM_WEIGHTS] = np.nan
+    with pytest.raises(RuntimeError):
+        s2.set_c2p_model(bad)
