@@ -103,7 +103,8 @@ class TrainConfig(C.Structure):
 
 class TrainReport(C.Structure):
     _fields_ = [("states", C.c_int64), ("labelled", C.c_int64), ("loss_first", C.c_float),
-                ("loss_last", C.c_float), ("err_q99", C.c_float), ("err_q999", C.c_float),
+                ("loss_last", C.c_float), ("err_q50", C.c_float), ("err_q90", C.c_float),
+                ("err_q99", C.c_float), ("err_q999", C.c_float),
                 ("err_max", C.c_float), ("delta", C.c_float), ("delta_cand", C.c_float * 4),
                 ("calib_ms", C.c_float * 4), ("train_ms", C.c_double)]
 

@@ -47,8 +47,8 @@ struct grb_handle {
   int64_t kind_n[GRB_KIND_COUNT] = {0};
   // learned c2p bracket: FP32 parameter block on the device
   float* d_mlp = nullptr;
+  MlpSmem* d_mlp_pack = nullptr;  // shared-memory image of the network
   bool mlp_ready = false;
-  int c2p_grid[2] = {0, 0};  // persistent grid of k_c2p_batch<plain / learned>
 };
 
 namespace {
@@ -366,6 +366,7 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_flags);
   cudaFree(h->d_counters);
   cudaFree(h->d_mlp);
+  cudaFree(h->d_mlp_pack);
   delete h;
   return GRB_OK;
 }
@@ -569,34 +570,17 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A, const
 
 namespace {
 
-// Persistent grid for k_c2p_batch: all CTAs resident at once, so that the
-// learned variant loads the network into shared memory once per CTA.
-template <bool kLearned>
-int c2p_grid(grb_handle* h) {
-  int& g = h->c2p_grid[kLearned ? 1 : 0];
-  if (g == 0) {
-    int dev = 0, sms = 0, occ = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_c2p_batch<kLearned>, kC2PThreads, 0);
-    g = std::max(1, sms) * std::max(1, occ);
-  }
-  return g;
-}
-
 int launch_c2p(grb_handle* h, int64_t n, const double* cons, const double* metric, double* prims,
                double* cons_out, uint32_t* err, bool learned, const grb_c2p_diag* diag, cudaStream_t s) {
   C2PDiagDev d{nullptr, nullptr, nullptr, nullptr};
   if (diag) d = C2PDiagDev{diag->iters, diag->guess_used, diag->mu, diag->bracket};
-  if (learned) {
-    const unsigned grid = (unsigned)std::min<int64_t>(nblk(n, kC2PThreads), c2p_grid<true>(h));
-    k_c2p_batch<true><<<grid, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, h->d_mlp,
-                                                   h->d_flags);
-  } else {
-    const unsigned grid = (unsigned)std::min<int64_t>(nblk(n, kC2PThreads), c2p_grid<false>(h));
-    k_c2p_batch<false><<<grid, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, nullptr,
-                                                    h->d_flags);
-  }
+  if (n > (int64_t)kC2PThreads * 0x7fffffff) return fail(h, GRB_ERR_INVALID);
+  if (learned)
+    k_c2p_batch<true><<<nblk(n, kC2PThreads), kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err,
+                                                                   d, h->d_mlp_pack, h->d_flags);
+  else
+    k_c2p_batch<false><<<nblk(n, kC2PThreads), kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err,
+                                                                    d, nullptr, h->d_flags);
   ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;
@@ -604,6 +588,15 @@ int launch_c2p(grb_handle* h, int64_t n, const double* cons, const double* metri
 
 int ensure_mlp(grb_handle* h) {
   if (!h->d_mlp) CK(cudaMalloc(&h->d_mlp, sizeof(float) * kMlpNumParams));
+  if (!h->d_mlp_pack) CK(cudaMalloc(&h->d_mlp_pack, sizeof(MlpSmem)));
+  return GRB_OK;
+}
+
+// Rebuild the shared-memory image after the parameters changed.
+int pack_mlp(grb_handle* h, cudaStream_t s) {
+  k_mlp_pack<<<1, 256, 0, s>>>(h->d_mlp, h->d_mlp_pack);
+  ++h->launches;
+  CK(cudaGetLastError());
   return GRB_OK;
 }
 
@@ -715,8 +708,8 @@ int grb_mlp_grad(grb_handle* h, int64_t n, const float* params, const float* fea
 
 void grb_train_config_defaults(grb_train_config* c) {
   if (!c) return;
-  c->steps = 3000;
-  c->batch = 8192;
+  c->steps = 8000;
+  c->batch = 16384;
   c->lr = 3e-3f;
   c->lr_min = 3e-5f;
   c->seed = 0x6A5CEull;
@@ -830,11 +823,13 @@ int grb_c2p_train(grb_handle* h, int64_t n, const double* cons, const double* me
     std::nth_element(err.begin(), err.begin() + k, err.end());
     return err[k];
   };
+  R.err_q50 = quant(0.5);
+  R.err_q90 = quant(0.9);
   R.err_q99 = quant(0.99);
   R.err_q999 = quant(0.999);
   const float q9999 = quant(0.9999);
   R.err_max = *std::max_element(err.begin(), err.end());
-  const float cand[4] = {1.2f * R.err_q99, 1.2f * R.err_q999, 1.2f * q9999, 1.1f * R.err_max};
+  const float cand[4] = {1.2f * R.err_q90, 1.2f * R.err_q99, 1.2f * R.err_q999, 1.2f * q9999};
   // 5. autotune delta: time the learned c2p on the calibration states
   h->mlp_ready = true;
   const int64_t nc = std::min<int64_t>(n, C.calib_states > 0 ? C.calib_states : n);
@@ -843,6 +838,7 @@ int grb_c2p_train(grb_handle* h, int64_t n, const double* cons, const double* me
     const float dlt = std::max(cand[ci], 1e-6f);
     R.delta_cand[ci] = dlt;
     CK(cudaMemcpyAsync(h->d_mlp + kMlpOffNorm + 2 * kMlpIn + 2, &dlt, sizeof(float), cudaMemcpyHostToDevice, s));
+    if (int rc = pack_mlp(h, s)) return rc;
     float bestms = 1e30f;
     for (int rep_i = 0; rep_i < 3; ++rep_i) {
       CK(cudaEventRecord(e0, s));
@@ -858,6 +854,7 @@ int grb_c2p_train(grb_handle* h, int64_t n, const double* cons, const double* me
   }
   R.delta = R.delta_cand[best];
   CK(cudaMemcpyAsync(h->d_mlp + kMlpOffNorm + 2 * kMlpIn + 2, &R.delta, sizeof(float), cudaMemcpyHostToDevice, s));
+  if (int rc = pack_mlp(h, s)) return rc;
   CK(cudaStreamSynchronize(s));
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -884,6 +881,8 @@ int grb_c2p_model_set(grb_handle* h, const float* params, int64_t nparams) {
     return fail(h, GRB_ERR_INVALID);
   if (int rc = ensure_mlp(h)) return rc;
   CK(cudaMemcpy(h->d_mlp, params, sizeof(float) * kMlpNumParams, cudaMemcpyHostToDevice));
+  if (int rc = pack_mlp(h, 0)) return rc;
+  CK(cudaDeviceSynchronize());
   h->mlp_ready = true;
   return GRB_OK;
 }

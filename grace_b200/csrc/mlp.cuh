@@ -1,18 +1,19 @@
 // Learned bracket for the Kastaun c2p.
 //
-// A 12 -> 64 -> 64 -> 64 -> 1 ReLU network predicts L = log(mu0 / mu), mu
-// the root of the Kastaun master function f(mu) = mu - 1/(hbw + rbar^2 mu)
-// (kastaun_c2p.hh:245-290) and mu0 the top of the plain bracket
-// (kastaun_c2p.hh:355-369, an EOS-free Newton solve the plain path runs
-// anyway).  Features: the Kastaun scalars of the state (kastaun_c2p.hh:306-337:
+// A 12 -> 64 -> 64 -> 64 -> 1 ReLU network predicts y = asinh(L / L0) with
+// L = log(mu0 / mu) and L0 = 1e-4: mu is the root of the Kastaun master
+// function f(mu) = mu - 1/(hbw + rbar^2 mu) (kastaun_c2p.hh:245-290), mu0 the
+// top of the plain bracket (kastaun_c2p.hh:355-369, an EOS-free Newton solve
+// the plain path runs anyway).  L spans 1e-10..3; the asinh keeps small gaps
+// linear and large ones logarithmic, so no tail dominates the squared error.  Features: the Kastaun scalars of the state (kastaun_c2p.hh:306-337:
 // D, q = tau/D, |r|, |B~|^2, cos^2(r, B~)) and log mu0, normalised, each
 // split into a BF16 high part and a BF16 remainder (12 inputs).  Hidden
 // layers run on the tensor cores (mma.sync m16n8k16, BF16 operands, FP32
 // accumulation); the output layer is FP32 on the BF16-rounded activations.
 // The unchanged FP64 Brent iteration then starts from
-// [mu0 e^(-L-delta), min(mu0 e^(-L+delta), mu0)] when f changes sign there,
-// and from the plain [0, mu0] otherwise, so the network only moves where the
-// iteration starts.
+// [mu0 e^(-L0 sinh(y+delta)), min(mu0 e^(-L0 sinh(y-delta)), mu0)] when f
+// changes sign there, and from the plain [0, mu0] otherwise, so the network
+// only moves where the iteration starts.
 //
 // Training (all on the GPU): labels come from the roots of the plain FP64
 // c2p on the caller's states; k_mlp_grad runs the same tensor-core forward on
@@ -32,9 +33,10 @@ namespace grb {
 constexpr int kMlpIn = 6;    // features; inputs 0..5 high parts, 6..11 remainders
 constexpr int kMlpK0 = 16;   // input width padded to one MMA k-chunk
 constexpr int kMlpH = 64;    // hidden width
+constexpr double kMlpL0 = 1e-4;  // scale of the asinh target
 // FP32 parameter block, in this order: W1[64][16], b1[64], W2[64][64], b2[64],
 // W3[64][64], b3[64], w4[64], b4 (trainable), then the normalisation
-// fmu[6], fsd[6], tmu, tsd and the bracket half-width delta (in log mu).
+// fmu[6], fsd[6], tmu, tsd and the bracket half-width delta (in y).
 constexpr int kMlpOffW1 = 0;
 constexpr int kMlpOffB1 = kMlpOffW1 + kMlpH * kMlpK0;
 constexpr int kMlpOffW2 = kMlpOffB1 + kMlpH;
@@ -260,7 +262,7 @@ __device__ __forceinline__ void mlp_tile16(const MlpSmem& s, const __nv_bfloat16
 }
 
 // Whole warp, one state per lane: network inputs in, network output
-// (normalised L) of the lane's own state out.  xs: per-warp shared buffer of
+// (normalised y) of the lane's own state out.  xs: per-warp shared buffer of
 // 32 rows x kXP BF16.  All 32 lanes must call.
 __device__ __forceinline__ float mlp_warp32(const MlpSmem& s, __nv_bfloat16* xs, const __nv_bfloat16 x[kMlpK0]) {
   const int lane = threadIdx.x & 31;
@@ -281,13 +283,14 @@ __device__ __forceinline__ float mlp_warp32(const MlpSmem& s, __nv_bfloat16* xs,
   return lane >= 16 ? (row >= 8 ? v3 : v2) : (row >= 8 ? v1 : v0);
 }
 
-// Learned bracket of one state from the network output and the plain mu0:
-// [mu0 e^(-L-delta), min(mu0 e^(-L+delta), mu0)].
+// Learned bracket of one state from the network output and the plain mu0.
 __device__ __forceinline__ Guess mlp_bracket(const MlpNorm& nrm, float out, double mu0) {
-  const float L = fmaf(out, nrm.tsd, nrm.tmu);
+  const float y = fmaf(out, nrm.tsd, nrm.tmu);
+  const float Llo = (float)kMlpL0 * sinhf(y - nrm.delta);
+  const float Lhi = (float)kMlpL0 * sinhf(y + nrm.delta);
   Guess g;
-  g.lo = mu0 * (double)expf(-L - nrm.delta);
-  g.hi = fmin(mu0 * (double)expf(-L + nrm.delta), mu0);
+  g.lo = mu0 * (double)expf(-Lhi);
+  g.hi = fmin(mu0 * (double)expf(-Llo), mu0);
   g.valid = mu0 > 0.0 && g.lo > 0.0 && g.hi > g.lo && isfinite(g.hi);
   g.mu0 = mu0;
   g.has_mu0 = mu0 > 0.0;
@@ -327,23 +330,32 @@ struct C2PLearnedSmem {
   MlpSmem net;
   __nv_bfloat16 xs[kC2PThreads / 32][32 * kXP];
 };
+static_assert(sizeof(MlpSmem) % 16 == 0, "the packed network is copied in 16-byte words");
 
-// Persistent grid-stride loop over chunks of kC2PThreads states; every
-// iteration is CTA-uniform so that all lanes reach the warp-wide network.
+// Packs the FP32 parameter block into the shared-memory image of the network
+// (BF16 weights in padded rows), once per model; c2p CTAs copy the image.
+__global__ void __launch_bounds__(256) k_mlp_pack(const float* __restrict__ P, MlpSmem* __restrict__ out) {
+  mlp_load_smem(*out, P);
+}
+
+// One state per thread.  With the learned bracket every lane of a warp takes
+// part in the network (lanes past n with neutral inputs), then returns.
 template <bool kLearned>
 __global__ void __launch_bounds__(kC2PThreads) k_c2p_batch(DevParams P, int64_t n, const double* __restrict__ cons,
                                                           const double* __restrict__ metric,
                                                           double* __restrict__ prims, double* __restrict__ cons_out,
                                                           uint32_t* __restrict__ err, C2PDiagDev diag,
-                                                          const float* __restrict__ model, uint32_t* flags) {
+                                                          const MlpSmem* __restrict__ net, uint32_t* flags) {
   __shared__ __align__(16) unsigned char smraw[kLearned ? sizeof(C2PLearnedSmem) : 16];
   C2PLearnedSmem& S = *reinterpret_cast<C2PLearnedSmem*>(smraw);
   if (kLearned) {
-    mlp_load_smem(S.net, model);
+    const uint4* src = reinterpret_cast<const uint4*>(net);
+    uint4* dst = reinterpret_cast<uint4*>(&S.net);
+    for (int w = threadIdx.x; w < (int)(sizeof(MlpSmem) / 16); w += kC2PThreads) dst[w] = src[w];
     __syncthreads();
   }
-  for (int64_t base = (int64_t)blockIdx.x * kC2PThreads; base < n; base += (int64_t)gridDim.x * kC2PThreads) {
-    const int64_t t = base + threadIdx.x;
+  {
+    const int64_t t = (int64_t)blockIdx.x * kC2PThreads + threadIdx.x;
     const bool active = t < n;
     const int64_t ts = active ? t : 0;
     const Met m = batch_metric(metric, n, ts);
@@ -364,7 +376,7 @@ __global__ void __launch_bounds__(kC2PThreads) k_c2p_batch(DevParams P, int64_t 
       const float out = mlp_warp32(S.net, S.xs[threadIdx.x >> 5], x);
       gs = mlp_bracket(S.net.nrm, out, mu0);
     }
-    if (!active) continue;
+    if (!active) return;
     const C2POut o = c2p(c, pr, m, P, 0.0, false, P.alp_bh_thresh, gs);
     if (o.fatal) atomicOr(flags, o.fatal);
     pr[GRB_P_CS2] = 0.0;
@@ -386,8 +398,9 @@ __global__ void __launch_bounds__(kC2PThreads) k_c2p_batch(DevParams P, int64_t 
 }
 
 // ---- training data ----------------------------------------------------------
-// Raw features [6][n] and target L = log(mu0 / mu) [n] (NaN where the plain
-// c2p did not reach the Kastaun solve) from the states and the plain roots.
+// Raw features [6][n] and target y = asinh(log(mu0 / mu) / L0) [n] (NaN where
+// the plain c2p did not reach the Kastaun solve) from the states and the
+// plain roots.
 __global__ void __launch_bounds__(256) k_mlp_labels(DevParams P, int64_t n, const double* __restrict__ cons,
                                                     const double* __restrict__ metric,
                                                     const double* __restrict__ mu, float* __restrict__ feat,
@@ -407,7 +420,8 @@ __global__ void __launch_bounds__(256) k_mlp_labels(DevParams P, int64_t n, cons
       ok = ok && isfinite(f[k]);
     }
     const double u = mu ? mu[t] : 0.0;
-    tgt[t] = (ok && u > 0.0 && isfinite(u)) ? (float)(log(mu0) - log(u)) : __int_as_float(0x7fc00000);
+    tgt[t] = (ok && u > 0.0 && isfinite(u)) ? (float)asinh((log(mu0) - log(u)) / kMlpL0)
+                                            : __int_as_float(0x7fc00000);
   }
 }
 
@@ -450,7 +464,7 @@ __global__ void __launch_bounds__(256) k_mlp_stats(int64_t n, const float* __res
 
 // ---- gradient of the batch loss -------------------------------------------
 // loss = sum_s w_s (y_s - t_s)^2 with w_s = inv_count for valid samples,
-// y and t in normalised log mu.
+// y and t normalised.
 constexpr int kGradRows = 64;            // states per CTA
 constexpr int kGradThreads = 256;
 constexpr int kSP = kGradRows + 1;       // pitch of the [feature][state] arrays
@@ -634,7 +648,7 @@ __global__ void __launch_bounds__(256) k_mlp_adam(float* __restrict__ P, float* 
   P[p] -= lr * (a / bc1) / (sqrtf(b / bc2) + 1e-8f);
 }
 
-// Network outputs (L, denormalised) for n raw feature rows [6][n].
+// Network outputs (y, denormalised) for n raw feature rows [6][n].
 __global__ void __launch_bounds__(kC2PThreads) k_mlp_eval(const float* __restrict__ P, int64_t n,
                                                           const float* __restrict__ feat, float* __restrict__ out) {
   __shared__ __align__(16) C2PLearnedSmem S;

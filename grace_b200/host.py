@@ -277,3 +277,16 @@ class GRMHDEquationsSystem:
         bc(state)
         self.compute_auxiliary_quantities(state, aux, stream)
         self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
+
+    def capture_rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0):
+        """Capture one rk3_step (same arguments) into a CUDA graph.  The
+        arrays and dt are baked into the graph: each graph.replay() advances
+        the same arrays by one step with no host work per kernel.  Call after
+        at least one eager step (first-call set-up such as shared-memory
+        attributes and autotuning happens outside the capture).  Returns
+        (graph, kernels launched per replay)."""
+        n0 = self.status().launches
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self.rk3_step(dt, state, state_p, state_pp, aux, bc, t)
+        return graph, self.status().launches - n0

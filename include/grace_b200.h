@@ -216,17 +216,18 @@ int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons,
 
 /* ---- learned c2p bracket (no counterpart in the reference) --------------
  * A 12-64-64-64-1 ReLU network (BF16 tensor-core hidden layers, FP32
- * accumulation) predicts L = log(mu0/mu) for a state: mu is the root of the
- * Kastaun master function (kastaun_c2p.hh:245-290), mu0 the top of the plain
- * bracket (kastaun_c2p.hh:355-369).  Features: D, tau/D, |S|/D, |B|^2/D,
- * cos^2(S,B) (kastaun_c2p.hh:306-337) and log mu0, normalised and split into
- * BF16 high parts and remainders.  The FP64 Brent solve (1e-15 abscissa
- * tolerance, as the plain one) runs on [mu0 e^(-L-delta),
- * min(mu0 e^(-L+delta), mu0)] when the master function changes sign there,
- * else on the plain [0, mu0]: the network changes only the starting bracket.
+ * accumulation) predicts y = asinh(L / 1e-4), L = log(mu0/mu), for a state:
+ * mu is the root of the Kastaun master function (kastaun_c2p.hh:245-290),
+ * mu0 the top of the plain bracket (kastaun_c2p.hh:355-369).  Features: D,
+ * tau/D, |S|/D, |B|^2/D, cos^2(S,B) (kastaun_c2p.hh:306-337) and log mu0,
+ * normalised and split into BF16 high parts and remainders.  The FP64 Brent
+ * solve (1e-15 abscissa tolerance, as the plain one) runs on
+ * [mu0 e^(-1e-4 sinh(y+delta)), min(mu0 e^(-1e-4 sinh(y-delta)), mu0)] when
+ * the master function changes sign there, else on the plain [0, mu0]: the
+ * network changes only the starting bracket.
  * Parameters: GRB_MLP_NUM_PARAMS floats, W1[64][16] b1[64] W2[64][64] b2[64]
  * W3[64][64] b3[64] w4[64] b4 (the GRB_MLP_NUM_WEIGHTS trainable ones), then
- * feature means[6], feature sds[6], L mean, L sd, delta. */
+ * feature means[6], feature sds[6], y mean, y sd, delta. */
 #define GRB_MLP_NUM_WEIGHTS 9473
 #define GRB_MLP_NUM_PARAMS 9488
 
@@ -243,8 +244,8 @@ int grb_c2p_batch_diag(grb_handle* h, int64_t n, const double* cons,
                        const grb_c2p_diag* diag, void* stream);
 
 typedef struct grb_train_config {
-  int64_t steps;        /* Adam steps (default 3000) */
-  int32_t batch;        /* states per step, a multiple of 64 (default 8192) */
+  int64_t steps;        /* Adam steps (default 8000) */
+  int32_t batch;        /* states per step, a multiple of 64 (default 16384) */
   float lr;             /* peak learning rate (default 3e-3) */
   float lr_min;         /* end of the cosine decay (default 3e-5) */
   uint64_t seed;        /* weight initialisation and sampling */
@@ -253,13 +254,15 @@ typedef struct grb_train_config {
 typedef struct grb_train_report {
   int64_t states;       /* states given */
   int64_t labelled;     /* states whose plain c2p ran the Kastaun solve */
-  float loss_first;     /* batch MSE of normalised L, first step */
+  float loss_first;     /* batch MSE of normalised y, first step */
   float loss_last;      /* ... last step */
-  float err_q99;        /* |L_net - L| quantiles over the states */
+  float err_q50;        /* |y_net - y| quantiles over the states */
+  float err_q90;
+  float err_q99;
   float err_q999;
   float err_max;
-  float delta;          /* chosen bracket half-width (in log mu) */
-  float delta_cand[4];  /* candidates: 1.2 q99, 1.2 q999, 1.2 q9999, 1.1 max */
+  float delta;          /* chosen bracket half-width (in y) */
+  float delta_cand[4];  /* candidates: 1.2 x the q90, q99, q999, q9999 errors */
   float calib_ms[4];    /* learned c2p time on the calibration states */
   double train_ms;      /* device time: labels + statistics + Adam steps */
 } grb_train_report;
@@ -275,16 +278,16 @@ int grb_c2p_train(grb_handle* h, int64_t n, const double* cons,
 /* Copy the model to / from a host array of GRB_MLP_NUM_PARAMS floats. */
 int grb_c2p_model_get(grb_handle* h, float* params, int64_t nparams);
 int grb_c2p_model_set(grb_handle* h, const float* params, int64_t nparams);
-/* Features [6][n] (FP32) and target L = log(mu0/mu) [n] (NaN where mu <= 0
- * or mu is NULL) of n states, mu the plain roots; device arrays. */
+/* Features [6][n] (FP32) and target y [n] (NaN where mu <= 0 or mu is NULL)
+ * of n states, mu the plain roots; device arrays. */
 int grb_c2p_features(grb_handle* h, int64_t n, const double* cons,
                      const double* metric, const double* mu, float* feat,
                      float* target, void* stream);
-/* Network output L [n] for raw features [6][n] with the parameter block
+/* Network output y [n] for raw features [6][n] with the parameter block
  * params (device; NULL = the handle's model). */
 int grb_mlp_eval(grb_handle* h, int64_t n, const float* params,
                  const float* feat, float* out, void* stream);
-/* Gradient of the mean squared error of normalised L over n samples
+/* Gradient of the mean squared error of normalised y over n samples
  * (targets NaN are skipped but still count in the mean) with respect to the
  * GRB_MLP_NUM_WEIGHTS trainable parameters; grad[GRB_MLP_NUM_WEIGHTS] receives
  * the loss.  All device arrays; synchronises the stream. */
