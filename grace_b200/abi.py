@@ -126,6 +126,11 @@ PROTOTYPES = {
     "grb_compute_auxiliary_quantities": (C.c_int, [C.c_void_p, C.POINTER(Grid),
                                                    C.POINTER(Fields), C.c_void_p,
                                                    C.c_void_p]),
+    "grb_compute_auxiliary_quantities_dt": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields),
+                                                      C.c_void_p, C.c_void_p, C.c_double, C.c_void_p,
+                                                      C.c_void_p]),
+    "grb_find_stable_timestep": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.c_void_p,
+                                           C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]),
     "grb_reset_c2p_diagnostics": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.c_void_p,
                                             C.c_void_p]),
     "grb_linop_apply": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields),

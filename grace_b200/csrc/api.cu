@@ -195,7 +195,14 @@ void launch_update_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P,
 }
 void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                       double* st, const double* bx, const double* by, const double* bz, double* aux,
-                      const double* idx, const double* crd, const StageBufs& B) {
+                      const double* idx, const double* crd, const StageBufs& B,
+                      const DtArgs* dta = nullptr) {
+  if (dta) {
+    if (v == 1) k_aux<4, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+    else if (v == 2) k_aux<5, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+    else k_aux<1, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+    return;
+  }
   if (v == 1) k_aux<4><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
   else if (v == 2) k_aux<5><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
   else k_aux<1><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
@@ -501,22 +508,54 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt, d
 
 int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g, const grb_fields* st,
                                      double* aux, void* stream) {
+  return grb_compute_auxiliary_quantities_dt(h, g, st, aux, nullptr, 0.0, nullptr, stream);
+}
+
+int grb_compute_auxiliary_quantities_dt(grb_handle* h, const grb_grid* g, const grb_fields* st, double* aux,
+                                        const double* dx, double cfl, double* dt_out, void* stream) {
   if (!h) return GRB_ERR_INVALID;
   int rc = check_grid(h, g);
   if (rc) return fail(h, rc);
   if (!st || !st->state || !st->bx || !st->by || !st->bz || !aux) return fail(h, GRB_ERR_INVALID);
+  if (dt_out && (!dx || !(cfl > 0.0))) return fail(h, GRB_ERR_INVALID);
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   const Box b = box(0, 0, 0, G.NX, G.NY, G.NZ, G.nq);
-  KScope ks(h, (cudaStream_t)stream, GRB_KIND_AUX);
-  if (h->mode == GRB_MODE_TUNED) {
-    launch_aux_tuned(h->var_aux, nblk(b.count(), 128), (cudaStream_t)stream, h->dp, G, b, st->state, st->bx,
-                     st->by, st->bz, aux, g->idx, g->coords, h->B);
+  cudaStream_t s = (cudaStream_t)stream;
+  KScope ks(h, s, GRB_KIND_AUX);
+  const DtArgs dta{dx, cfl, reinterpret_cast<unsigned long long*>(dt_out)};
+  if (dt_out) {
+    k_dt_init<<<1, 1, 0, s>>>(dta.out);
     ++h->launches;
-    CK(cudaGetLastError());
-    return GRB_OK;
   }
-  k_aux<1><<<nblk(b.count(), 128), 128, 0, (cudaStream_t)stream>>>(h->dp, G, b, st->state, st->bx, st->by,
-                                                                  st->bz, aux, g->idx, g->coords, h->B); ++h->launches;
+  if (h->mode == GRB_MODE_TUNED) {
+    launch_aux_tuned(h->var_aux, nblk(b.count(), 128), s, h->dp, G, b, st->state, st->bx, st->by, st->bz, aux,
+                     g->idx, g->coords, h->B, dt_out ? &dta : nullptr);
+  } else if (dt_out) {
+    k_aux<1, true><<<nblk(b.count(), 128), 128, 0, s>>>(h->dp, G, b, st->state, st->bx, st->by, st->bz, aux,
+                                                        g->idx, g->coords, h->B, dta);
+  } else {
+    k_aux<1><<<nblk(b.count(), 128), 128, 0, s>>>(h->dp, G, b, st->state, st->bx, st->by, st->bz, aux, g->idx,
+                                                  g->coords, h->B);
+  }
+  ++h->launches;
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_find_stable_timestep(grb_handle* h, const grb_grid* g, const grb_fields* st, const double* aux,
+                             const double* dx, double cfl, double* dt_out, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  int rc = check_grid(h, g);
+  if (rc) return fail(h, rc);
+  if (!st || !st->state || !aux || !dx || !dt_out || !(cfl > 0.0)) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  const Box b = box(G.g, G.g, G.g, G.nx, G.ny, G.nz, G.nq);
+  cudaStream_t s = (cudaStream_t)stream;
+  KScope ks(h, s, GRB_KIND_OTHER);
+  const DtArgs dta{dx, cfl, reinterpret_cast<unsigned long long*>(dt_out)};
+  k_dt_init<<<1, 1, 0, s>>>(dta.out);
+  k_dt<<<nblk(b.count(), 128), 128, 0, s>>>(h->dp, G, b, st->state, aux, dta);
+  h->launches += 2;
   CK(cudaGetLastError());
   return GRB_OK;
 }

@@ -175,6 +175,24 @@ GRB_HD double eos_PT(const DevEos& e, double& eps, double& cs2, double* ent, dou
   if (ent) *ent = hy_ent(e, eth, rho);
   return p;
 }
+// cs2 from (T, rho) as press_h_csnd2__temp_rho_ye computes it
+// (hybrid_eos.hh:227-240, ideal_gas_eos.hh:224-234: h summed as
+// 1 + eps_cold + eps_th + P/rho); rho and T clamped in place
+GRB_HD double eos_cs2_T(const DevEos& e, double& t, double& rho, uint32_t& q) {
+  if (e.kind == GRB_EOS_IDEAL_GAS) {
+    id_temp(e, t, q);
+    const double eps = t / e.gm1;
+    return e.ggm1 * eps / (1.0 + e.g * eps);
+  }
+  hy_rho(e, rho, q);
+  hy_temp(e, t, q);
+  double ec;
+  const double pc = pw_cold(e, ec, rho);
+  const double eth = fmax(0.0, t / e.gthm1);
+  const double p = pc + eth * rho * e.gthm1;
+  const double h = 1. + ec + eth + p / rho;
+  return (pw_dpdrho(e, rho) + e.gthm1 * (e.gthm1 + 1) * eth) / h;
+}
 // P from (eps, rho): hybrid_eos.hh:78-85, ideal_gas_eos.hh:88-92
 GRB_HD double eos_Peps(const DevEos& e, double& eps, double& rho, uint32_t& q) {
   if (e.kind == GRB_EOS_IDEAL_GAS) { id_eps(e, eps, q); return e.gm1 * eps * rho; }

@@ -525,18 +525,83 @@ __global__ void __launch_bounds__(128) k_ct(Geo G, Box box, double dt, double dt
                                     (E[emi(G, i, j, k, 1, q)] - E[emi(G, i + 1, j, k, 1, q)]) * ix[0]);
 }
 
+// ---- time step: compute_max_eigenspeed (grmhd.hh:444-519) ----------------
+// Largest |characteristic speed| over the three directions of one cell from
+// its primitives (as stored in aux) and the cell metric.
+GRB_HD double max_eigenspeed(const DevEos& e, const Met& m, const double pr[13]) {
+  double rho = pr[GRB_P_RHO], T = pr[GRB_P_TEMP];
+  uint32_t q = 0;
+  const double cs2 = eos_cs2_T(e, T, rho, q);
+  const double W = lorentz(m.g, pr + GRB_P_ZX);
+  double b[4], b2, vt[3];
+  comoving_b(m.alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, W, b, b2);
+  vtilde(m.alp, m.beta, pr + GRB_P_ZX, W, vt);
+  const double gdd[3] = {m.gi[0], m.gi[3], m.gi[5]};
+  double cmax = 0.0;
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double cm, cp;
+    char_speeds(m.alp, m.beta[d], rho, pr[GRB_P_PRESS], pr[GRB_P_EPS], cs2, W, b2, vt[d], gdd[d], cm, cp);
+    cmax = fmax(cmax, fmax(fabs(cp), fabs(cm)));
+  }
+  return cmax;
+}
+// find_stable_timestep_impl (find_stable_timestep.cpp:73-125): the minimum
+// of cfl / cmax * dx(0, q) over interior cells, reduced into *out as the
+// bit pattern of a positive double (ordered like an unsigned integer).
+struct DtArgs {
+  const double* dx;  // spacings (3, nq)
+  double cfl;
+  unsigned long long* out;
+};
+__device__ __forceinline__ void dt_reduce(double v, unsigned long long* out) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0 && v < INFINITY) atomicMin(out, (unsigned long long)__double_as_longlong(v));
+}
+__global__ void k_dt_init(unsigned long long* out) { *out = (unsigned long long)__double_as_longlong(INFINITY); }
+
+// Separate reduction pass over interior cells (one thread per cell); every
+// thread of the CTA reaches the warp reduction.
+__global__ void __launch_bounds__(128) k_dt(DevParams P, Geo G, Box box, const double* __restrict__ st,
+                                            const double* __restrict__ aux, DtArgs dt) {
+  int i = 0, j = 0, k = 0;
+  int64_t q = 0;
+  double v = INFINITY;
+  if (decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) {
+    const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
+    double pr[13];
+    pr[GRB_P_RHO] = aux[a0 + G.cells * GRB_RHO];
+    pr[GRB_P_TEMP] = aux[a0 + G.cells * GRB_TEMP];
+    pr[GRB_P_EPS] = aux[a0 + G.cells * GRB_EPS];
+    pr[GRB_P_PRESS] = aux[a0 + G.cells * GRB_PRESS];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      pr[GRB_P_ZX + a] = aux[a0 + G.cells * (GRB_ZVECX + a)];
+      pr[GRB_P_BX + a] = aux[a0 + G.cells * (GRB_BX + a)];
+    }
+    const Met m = cell_met(G, st, i, j, k, q);
+    v = dt.cfl / max_eigenspeed(P.eos, m, pr) * dt.dx[3 * q];
+  }
+  dt_reduce(v, dt.out);
+}
+
 // ---- aux: c2p on every cell + resets + C2P_ERR + BDIV + cell-centred E -----
-template <int MINB = 1>
+// kDt: also the time-step reduction over the interior cells, from the
+// primitives just computed (the aux pass that ends an RK step).
+template <int MINB = 1, bool kDt = false>
 __global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, double* __restrict__ st,
                                               const double* __restrict__ bx,
                                               const double* __restrict__ by,
                                               const double* __restrict__ bz,
                                               double* __restrict__ aux,
                                               const double* __restrict__ idx,
-                                              const double* __restrict__ coords, StageBufs B) {
-  int i, j, k;
-  int64_t q;
-  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+                                              const double* __restrict__ coords, StageBufs B,
+                                              DtArgs dta = DtArgs{nullptr, 0.0, nullptr}) {
+  int i = 0, j = 0, k = 0;
+  int64_t q = 0;
+  double dtc = INFINITY;
+  if (decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) {
   const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
   const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
   const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
@@ -590,6 +655,10 @@ __global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, 
     B.ecenter[eci(G, i, j, k, 1, q)] = -cbx * vt[2] + cbz * vt[0];
     B.ecenter[eci(G, i, j, k, 2, q)] = cbx * vt[1] - cby * vt[0];
   }
+  if (kDt && i >= G.g && i < G.nx + G.g && j >= G.g && j < G.ny + G.g && k >= G.g && k < G.nz + G.g)
+    dtc = dta.cfl / max_eigenspeed(P.eos, m, pr) * dta.dx[3 * q];
+  }
+  if (kDt) dt_reduce(dtc, dta.out);
 }
 
 // reset_c2p_diagnostics (evolve.cpp:154-161)
@@ -656,7 +725,15 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, int ax, int fd, 
     sidx[ax] = src;
     const int64_t ld = d[0] + (int64_t)n[0] * (d[1] + (int64_t)n[1] * d[2]) + q * qstride;
     const int64_t ls = sidx[0] + (int64_t)n[0] * (sidx[1] + (int64_t)n[1] * sidx[2]) + qsrc * qstride;
-    for (int v = 0; v < nv; ++v) a[ld + v * vstride] = a[ls + v * vstride];
+    // all loads before any store: source and destination share one array,
+    // so interleaved copies would each wait a full memory latency
+    double tmp[GRB_N_HRSC];
+#pragma unroll
+    for (int v = 0; v < GRB_N_HRSC; ++v)
+      if (v < nv) tmp[v] = a[ls + v * vstride];
+#pragma unroll
+    for (int v = 0; v < GRB_N_HRSC; ++v)
+      if (v < nv) a[ld + v * vstride] = tmp[v];
   }
 }
 

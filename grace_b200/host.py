@@ -132,6 +132,24 @@ class GRMHDEquationsSystem:
                                                              _ptr(aux), _stream_ptr(stream)),
                    "grb_compute_auxiliary_quantities")
 
+    def compute_auxiliary_quantities_dt(self, state, aux, dx, cfl, dt_out, stream=None):
+        """compute_auxiliary_quantities fused with find_stable_timestep_impl:
+        dt_out (float64 device tensor, one element) receives the minimum of
+        cfl / cmax * dx(0, q) over the interior cells."""
+        g = self.blocks.c()
+        f = state.c()
+        _lib.check(self.lib.grb_compute_auxiliary_quantities_dt(self.h, ctypes.byref(g), ctypes.byref(f), _ptr(aux),
+                                                                _ptr(dx), cfl, _ptr(dt_out), _stream_ptr(stream)),
+                   "grb_compute_auxiliary_quantities_dt")
+
+    def find_stable_timestep(self, state, aux, dx, cfl, dt_out, stream=None):
+        """find_stable_timestep_impl on this rank's blocks (separate pass)."""
+        g = self.blocks.c()
+        f = state.c()
+        _lib.check(self.lib.grb_find_stable_timestep(self.h, ctypes.byref(g), ctypes.byref(f), _ptr(aux), _ptr(dx),
+                                                     cfl, _ptr(dt_out), _stream_ptr(stream)),
+                   "grb_find_stable_timestep")
+
     def reset_c2p_diagnostics(self, aux, stream=None):
         g = self.blocks.c()
         _lib.check(self.lib.grb_reset_c2p_diagnostics(self.h, ctypes.byref(g), _ptr(aux),
@@ -260,10 +278,12 @@ class GRMHDEquationsSystem:
         return st
 
     # --- evolve_impl<eos_t>() RK3 branch (evolve.cpp:147-225, 427-428) -----
-    def rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, stream=None):
+    def rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, stream=None, next_dt=None):
         """One SSP-RK3 step.  `bc(fields)` applies the boundary conditions
         (GRACE's amr::apply_boundary_conditions); on entry aux holds the
-        primitives of `state` and state_p equals state."""
+        primitives of `state` and state_p equals state.  next_dt = (dx, cfl,
+        dt_out): the last aux pass also reduces the next stable time step
+        into dt_out (find_stable_timestep after the step)."""
         self.reset_c2p_diagnostics(aux, stream)
         self.advance_substep(t, dt, 1.0, state_p, state, aux, stream)
         bc(state_p)
@@ -275,10 +295,13 @@ class GRMHDEquationsSystem:
         self.linop_apply(state, state, state_pp, 1.0 / 3, 2.0 / 3.0, stream)
         self.advance_substep(t, dt, 2.0 / 3.0, state, state_pp, aux, stream)
         bc(state)
-        self.compute_auxiliary_quantities(state, aux, stream)
+        if next_dt is None:
+            self.compute_auxiliary_quantities(state, aux, stream)
+        else:
+            self.compute_auxiliary_quantities_dt(state, aux, *next_dt, stream=stream)
         self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
 
-    def capture_rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0):
+    def capture_rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, next_dt=None):
         """Capture one rk3_step (same arguments) into a CUDA graph.  The
         arrays and dt are baked into the graph: each graph.replay() advances
         the same arrays by one step with no host work per kernel.  Call after
@@ -288,5 +311,5 @@ class GRMHDEquationsSystem:
         n0 = self.status().launches
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
-            self.rk3_step(dt, state, state_p, state_pp, aux, bc, t)
+            self.rk3_step(dt, state, state_p, state_pp, aux, bc, t, next_dt=next_dt)
         return graph, self.status().launches - n0

@@ -191,6 +191,23 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt,
 int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g,
                                      const grb_fields* state, double* aux,
                                      void* stream);
+/* compute_auxiliary_quantities fused with the time-step reduction of
+ *   find_stable_timestep_impl (src/evolution/find_stable_timestep.cpp:73-125,
+ *   compute_max_eigenspeed grmhd.hh:444-519) over the interior cells, from
+ *   the primitives this pass computes: *dt_out (device double) becomes
+ *   min over interior cells of cfl / cmax * dx(0, q); dx is the (3, nq)
+ *   device view of getspacings().  dt_out == NULL: plain aux pass.  The
+ *   cross-rank MPI minimum stays with the caller. */
+int grb_compute_auxiliary_quantities_dt(grb_handle* h, const grb_grid* g,
+                                        const grb_fields* state, double* aux,
+                                        const double* dx, double cfl,
+                                        double* dt_out, void* stream);
+/* = find_stable_timestep_impl on this rank's blocks, as a separate pass over
+ *   aux and the metric (same result as the fused form). */
+int grb_find_stable_timestep(grb_handle* h, const grb_grid* g,
+                             const grb_fields* state, const double* aux,
+                             const double* dx, double cfl, double* dt_out,
+                             void* stream);
 /* = the reset_c2p_diagnostics kernel at the top of evolve_impl
  *   (evolve.cpp:154-161). */
 int grb_reset_c2p_diagnostics(grb_handle* h, const grb_grid* g, double* aux,

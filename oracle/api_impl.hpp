@@ -45,6 +45,9 @@ int API(compute_aux)(void* hh, const double* idx, const double* coords, double* 
   return st.fatal;
 }
 void API(reset_diag)(void* hh, double* aux) { static_cast<Handle*>(hh)->st.reset_diag(aux); }
+double API(find_stable_timestep)(void* hh, double* s, const double* aux, const double* dx, double cfl) {
+  return static_cast<Handle*>(hh)->st.find_stable_timestep(mk(s, nullptr, nullptr, nullptr), aux, dx, cfl);
+}
 void API(linop)(void* hh, double* as, double* abx, double* aby, double* abz, double* bs,
                 double* bbx, double* bby, double* bbz, double* cs, double* cbx, double* cby,
                 double* cbz, double b, double c) {

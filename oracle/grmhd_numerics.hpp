@@ -210,6 +210,28 @@ inline double press_eps_csnd2__temp_rho(const Eos& e, double& eps, double& cs2,
   cs2 = hy_cs2(e, rho, eth, h);
   return p;
 }
+// P, h, cs2 from (T, rho): hybrid_eos.hh:227-240, ideal_gas_eos.hh:224-234
+// (h summed as 1 + eps_cold + eps_th + P/rho, as the reference does there)
+inline double press_h_csnd2__temp_rho(const Eos& e, double& h, double& cs2, double& temp,
+                                      double& rho, uint32_t& err) {
+  if (e.kind == GRB_EOS_IDEAL_GAS) {
+    id_limit_temp(e, temp, err);
+    const double eps = temp / e.g_m1;
+    const double p = e.g_m1 * eps * rho;
+    h = 1.0 + e.g * eps;
+    cs2 = e.gg_m1 * eps / h;
+    return p;
+  }
+  hy_check_rho(e, rho, err);
+  hy_check_temp(e, temp, err);
+  double ec;
+  const double pc = pw_press_cold(e, ec, rho);
+  const double eth = std::fmax(0.0, temp / e.gth_m1);
+  const double p = pc + eth * rho * e.gth_m1;
+  h = 1. + ec + eth + p / rho;
+  cs2 = hy_cs2(e, rho, eth, h);
+  return p;
+}
 // P, eps, cs2, s from (T, rho): hybrid_eos.hh:276-291, ideal_gas_eos.hh:277-288
 inline double press_eps_csnd2_entropy__temp_rho(const Eos& e, double& eps, double& cs2,
                                                 double& ent, double& temp, double& rho,

@@ -20,6 +20,10 @@ struct OracleNumerics {
     uint32_t err = 0;
     return orc::press_eps_csnd2__temp_rho(e, eps, cs2, t, r, err);
   }
+  static double press_h_csnd2__temp_rho(const Eos& e, double& h, double& cs2, double& t, double& r) {
+    uint32_t err = 0;
+    return orc::press_h_csnd2__temp_rho(e, h, cs2, t, r, err);
+  }
   static double lorentz(const double g[6], const double z[3]) { return orc::lorentz(g, z); }
   static void comoving_b(double alp, const double* beta, const double* g, const double* B,
                          const double* z, double W, double b[4], double& b2) {

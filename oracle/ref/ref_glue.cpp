@@ -116,6 +116,12 @@ struct RefNumerics {
     if (e.kind == GRB_EOS_IDEAL_GAS) return e.ideal.press_eps_csnd2__temp_rho_ye(eps, cs2, t, r, ye, err);
     return e.hyb.press_eps_csnd2__temp_rho_ye(eps, cs2, t, r, ye, err);
   }
+  static double press_h_csnd2__temp_rho(const Eos& e, double& h, double& cs2, double& t, double& r) {
+    grace::eos_err_t err;
+    double ye = 0.0;
+    if (e.kind == GRB_EOS_IDEAL_GAS) return e.ideal.press_h_csnd2__temp_rho_ye(h, cs2, t, r, ye, err);
+    return e.hyb.press_h_csnd2__temp_rho_ye(h, cs2, t, r, ye, err);
+  }
   static double lorentz(const double g[6], const double z[3]) {
     double W;
     grmhd_get_W(g, z, &W);

@@ -589,6 +589,49 @@ struct Stage {
     }
   }
 
+  // compute_max_eigenspeed (grmhd.hh:444-519) of one cell from its primitives
+  // in aux and the metric in the state
+  double max_eigenspeed(double* s, const double* aux, int i, int j, int k, int64_t q) const {
+    double* a = const_cast<double*>(aux);
+    const double z[3] = {A(a, i, j, k, GRB_ZVECX, q), A(a, i, j, k, GRB_ZVECY, q), A(a, i, j, k, GRB_ZVECZ, q)};
+    const double B[3] = {A(a, i, j, k, GRB_BX, q), A(a, i, j, k, GRB_BY, q), A(a, i, j, k, GRB_BZ, q)};
+    double rho = A(a, i, j, k, GRB_RHO, q), T = A(a, i, j, k, GRB_TEMP, q);
+    const double eps = A(a, i, j, k, GRB_EPS, q), press = A(a, i, j, k, GRB_PRESS, q);
+    const Metric m = cell_metric(s, i, j, k, q);
+    double h, cs2;
+    N::press_h_csnd2__temp_rho(eos, h, cs2, T, rho);
+    const double W = N::lorentz(m.g, z);
+    double b[4], b2;
+    N::comoving_b(m.alp, m.beta, m.g, B, z, W, b, b2);
+    double vt[3];
+    N::vtilde(m.alp, m.beta, z, W, vt);
+    const int diag[3] = {0, 3, 5};
+    double cmax = 0.0;
+    for (int dir = 0; dir < 3; ++dir) {
+      double cm, cp;
+      N::char_speeds(m.alp, m.beta, rho, press, eps, cs2, W, b2, vt, m.ginv[diag[dir]], dir, cm, cp);
+      cmax = std::fmax(cmax, std::fmax(std::fabs(cp), std::fabs(cm)));
+    }
+    return cmax;
+  }
+
+  // find_stable_timestep_impl (find_stable_timestep.cpp:73-125) on this
+  // rank's blocks: min over interior cells of CFL / cmax * dx(0, q)
+  double find_stable_timestep(const Fields& st, const double* aux, const double* dx, double cfl) const {
+    double dt = std::numeric_limits<double>::max();
+#pragma omp parallel for collapse(2) schedule(static) reduction(min : dt)
+    for (int64_t q = 0; q < d.nq; ++q)
+      for (int k = d.g; k < d.nz + d.g; ++k)
+        for (int j = d.g; j < d.ny + d.g; ++j)
+          for (int i = d.g; i < d.nx + d.g; ++i) {
+            const double cmax = max_eigenspeed(st.state, aux, i, j, k, q);
+            const double L = dx[3 * q];
+            const double c = cfl / cmax * L;
+            dt = dt > c ? c : dt;
+          }
+    return dt;
+  }
+
   // reset_c2p_diagnostics (evolve.cpp:154-161)
   void reset_diag(double* aux) {
     for (int64_t q = 0; q < d.nq; ++q) {

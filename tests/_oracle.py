@@ -24,6 +24,7 @@ def _bind(lib, pre):
         "advance_substep": (C.c_int, [VP, VP, VP, C.c_double, C.c_double] + [VP] * 9),
         "compute_aux": (C.c_int, [VP, VP, VP] + [VP] * 5),
         "reset_diag": (None, [VP, VP]),
+        "find_stable_timestep": (C.c_double, [VP, VP, VP, VP, C.c_double]),
         "linop": (None, [VP] + [VP] * 12 + [C.c_double, C.c_double]),
         "scratch": (C.c_int64, [VP, C.c_int, VP]),
         "fofc_counts": (None, [VP, P(C.c_int64), P(C.c_int64)]),
@@ -153,6 +154,11 @@ class Stage:
 
     def reset_diag(self, aux):
         getattr(self.L, self.pre + "reset_diag")(self.h, p(aux))
+
+    def find_stable_timestep(self, st, aux, dx, cfl):
+        """find_stable_timestep_impl: min over interior cells of
+        cfl / cmax * dx(0, q)."""
+        return getattr(self.L, self.pre + "find_stable_timestep")(self.h, p(st[0]), p(aux), p(dx), cfl)
 
     def linop(self, A, B, Cf, b, c):
         Cp = [p(x) for x in Cf] if Cf is not None else [None] * 4

@@ -162,3 +162,34 @@ def test_graph_replay_matches_eager(mode):
     for x, y in zip(eager, replayed):
         assert np.array_equal(x, y, equal_nan=True)
     assert g.status().device_flags == 0
+
+
+@pytest.mark.parametrize("name", ["blast", "balsara"])
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_timestep_reduction(name, mode):
+    """find_stable_timestep on the GPU, fused into the aux pass and as a
+    separate pass, against the oracle's find_stable_timestep_impl on the
+    same arrays; the fused aux pass leaves aux and state bit-identical to
+    the plain one."""
+    P, su, f, dt = _setup(name)
+    (st, bx, by, bz), aux, g = _gpu_run(P, su, f, dt, 1, mode)
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    dx = np.ascontiguousarray(1.0 / su.idx())
+    cfl = 0.4
+    state = Fields(T(st), T(bx), T(by), T(bz))
+    aux_a, aux_b = T(aux), T(aux)
+    state_b = state.clone()
+    dt_f = torch.zeros(1, dtype=torch.float64, device=dev)
+    dt_s = torch.zeros(1, dtype=torch.float64, device=dev)
+    g.compute_auxiliary_quantities(state, aux_a)
+    g.compute_auxiliary_quantities_dt(state_b, aux_b, T(dx), cfl, dt_f)
+    g.find_stable_timestep(state_b, aux_b, T(dx), cfl, dt_s)
+    torch.cuda.synchronize()
+    assert torch.equal(aux_a, aux_b) and torch.equal(state.state, state_b.state)
+    assert dt_f.item() == dt_s.item()
+    S = _oracle.Stage(P, su.n[0], su.n[1], su.n[2], su.ngz, su.nq)
+    host = [state_b.state.cpu().numpy(), None, None, None]
+    dt_o = S.find_stable_timestep(host, aux_b.cpu().numpy(), dx, cfl)
+    assert abs(dt_f.item() - dt_o) <= 1e-13 * dt_o, (dt_f.item(), dt_o)
+    assert 0.0 < dt_o < 1.0
