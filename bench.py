@@ -42,6 +42,11 @@ ALGO_BYTES = {
     # per interior cell: 21 face fluxes, 9 aux, 16 metric/curvature, 7 cons RMW
     "update": 8 * (21 + 9 + 16 + 14),
 }
+# DRAM bytes per face of the tuned flux kernel, measured by ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum = 129.5 MB for one launch of
+# 64 blocks x 19x18x18 faces, cold L2; profiles/flux_tuned_blast64blocks_ncu_full.md),
+# scaled to a full launch by the faces it computes
+FLUX_DRAM_BYTES_PER_FACE = 129.51e6 / (64 * 19 * 18 * 18)
 
 
 def parse():
@@ -58,6 +63,8 @@ def parse():
     ap.add_argument("--eager", action="store_true", help="launch the timed steps eagerly, not as a CUDA graph")
     ap.add_argument("--no-c2p", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="c2p leg: plain bracket only")
+    ap.add_argument("--c2p-only", action="store_true", help="run only the c2p micro-benchmark")
+    ap.add_argument("--c2p-states", type=int, default=1 << 24, help="states of the c2p micro-benchmark")
     ap.add_argument("--mode", default="tuned", choices=["tuned", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
     return ap.parse_args()
@@ -221,15 +228,29 @@ def ours(args, rank, world, local_rank):
     dx_d = torch.from_numpy(np.ascontiguousarray(1.0 / su.idx())).to(dev)
     dt_next = torch.zeros(1, dtype=torch.float64, device=dev)
     nd = (dx_d, args.cfl, dt_next)
-    # warm-up: eager steps, then the step captured as one CUDA graph
-    for _ in range(max(1, args.warmup - 1)):
+    # warm-up: eager steps (one with the dt reduction fused into the last aux
+    # pass, one with it as a separate pass: the faster form is kept), then the
+    # step captured as one CUDA graph
+    for _ in range(max(1, args.warmup - 3)):
         g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd)
+
+    def step_ms(fused):
+        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a0.record()
+        g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd, fused_dt=fused)
+        a1.record()
+        torch.cuda.synchronize()
+        return a0.elapsed_time(a1)
+
+    dt_pass = {"separate_step_ms": step_ms(False), "fused_step_ms": step_ms(True)}
+    fused = dt_pass["fused_step_ms"] < dt_pass["separate_step_ms"]
+    dt_pass["used"] = "fused" if fused else "separate"
     graph, per_step = None, None
     if not args.eager:
-        graph, per_step = g.capture_rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd)
+        graph, per_step = g.capture_rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd, fused_dt=fused)
         graph.replay()
     else:
-        g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd)
+        g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd, fused_dt=fused)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
@@ -243,7 +264,7 @@ def ours(args, rank, world, local_rank):
         if graph is not None:
             graph.replay()
         else:
-            g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd)
+            g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd, fused_dt=fused)
     e1.record()
     torch.cuda.synchronize()
     barrier()
@@ -254,7 +275,7 @@ def ours(args, rank, world, local_rank):
     launches = per_step * args.steps if graph is not None else st1.launches - st0.launches
     # per-kernel device times: one more eager step with event timing
     g.set_kernel_timing(True)
-    g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd)
+    g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd, fused_dt=fused)
     torch.cuda.synchronize()
     kt = g.kernel_times()
     g.set_kernel_timing(False)
@@ -332,8 +353,12 @@ def ours(args, rank, world, local_rank):
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     top = max(kt.items(), key=lambda kv: kv[1][0])
     name, (kms, kcnt) = top
+    # faces one flux launch (one direction) computes: the reference's full
+    # transverse ghost range in the plain form, only the faces the stage
+    # reads in the tuned form (GS: n+2 transverse, UCT: n+6)
+    tr = (n + 8) if args.mode != "tuned" else ((n + 2) if P.emf == abi.EMF_GS else (n + 6))
     items = {
-        "flux": 3 * su.nq * (n + 3) * (n + 8) ** 2 / 3.0,
+        "flux": su.nq * (n + 3) * tr ** 2,
         "aux": su.nq * (n + 8) ** 3,
         "update": su.nq * n ** 3,
     }
@@ -342,8 +367,10 @@ def ours(args, rank, world, local_rank):
         bytes_per_launch = ALGO_BYTES[name] * items[name]
         per_launch_ms = kms / kcnt
         ach = bytes_per_launch / (per_launch_ms * 1e-3) / 1e9
+        traffic = FLUX_DRAM_BYTES_PER_FACE * items[name] if (name == "flux" and args.mode == "tuned") else None
         roof = {"bound": "hbm", "kernel": name, "achieved": ach, "peak": hbm, "unit": "GB/s",
-                "frac": ach / hbm, "peak_source": peak_src, "traffic": None,
+                "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_per_launch, "items_per_launch": items[name],
                 "launch_ms": per_launch_ms,
                 "note": "FP64 arithmetic, not HBM, binds this kernel (see profiles/)"}
 
@@ -371,7 +398,7 @@ def ours(args, rank, world, local_rank):
                        "launch": "cuda_graph" if graph is not None else "eager",
                        "step": "3 x (advance_substep + ghost fill + aux) + linops; the last aux pass "
                                "also reduces the next stable dt (dt itself held fixed)",
-                       "next_dt": float(dt_next.item())},
+                       "next_dt": float(dt_next.item()), "dt_pass": dt_pass},
             "clocks": clk, "gpu_launches": launches,
             "kernel_ms": {k: round(v[0], 3) for k, v in kt.items() if v[1]},
             "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "c2p": c2p,
@@ -447,6 +474,12 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank)
+        return
+    if args.c2p_only:
+        # the c2p micro-benchmark alone (for profiling; not the bench line)
+        import torch
+        if rank == 0:
+            print(json.dumps(c2p_bench(torch.device("cuda:0"), learned=not args.no_learned, n=args.c2p_states)))
         return
     if world > 1:
         import datetime

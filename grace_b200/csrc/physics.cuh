@@ -114,15 +114,23 @@ GRB_HD int pw_idx(const DevEos& e, double& rho) {
     if (rho > e.R[ii] && rho <= e.R[ii + 1]) return ii;
   return e.n - 1;
 }
+// rho^G of the cold polytrope.  G = 2 (the usual neutron-star index) and
+// G = 1 are exact products, rho*rho being the correctly rounded square;
+// other indices call pow.  The branch is uniform: G is a run constant.
+GRB_HD double pw_pow(double rho, double G) {
+  if (G == 2.0) return rho * rho;
+  if (G == 1.0) return rho;
+  return pow(rho, G);
+}
 GRB_HD double pw_cold(const DevEos& e, double& ec, double& rho) {
   const int i = pw_idx(e, rho);
-  const double pc = e.K[i] * pow(rho, e.G[i]);
+  const double pc = e.K[i] * pw_pow(rho, e.G[i]);
   ec = e.E[i] + pc / (rho * (e.G[i] - 1.));
   return pc;
 }
 GRB_HD double pw_dpdrho(const DevEos& e, double& rho) {
   const int i = pw_idx(e, rho);
-  return e.G[i] * (e.K[i] * pow(rho, e.G[i])) / rho;
+  return e.G[i] * (e.K[i] * pw_pow(rho, e.G[i])) / rho;
 }
 GRB_HD void hy_rho(const DevEos& e, double& rho, uint32_t& q) {
   if (rho < e.rhomin) { q |= EOS_RHO_LOW; rho = e.rhomin; }

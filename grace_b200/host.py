@@ -278,12 +278,13 @@ class GRMHDEquationsSystem:
         return st
 
     # --- evolve_impl<eos_t>() RK3 branch (evolve.cpp:147-225, 427-428) -----
-    def rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, stream=None, next_dt=None):
+    def rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, stream=None, next_dt=None,
+                 fused_dt=False):
         """One SSP-RK3 step.  `bc(fields)` applies the boundary conditions
         (GRACE's amr::apply_boundary_conditions); on entry aux holds the
         primitives of `state` and state_p equals state.  next_dt = (dx, cfl,
-        dt_out): the last aux pass also reduces the next stable time step
-        into dt_out (find_stable_timestep after the step)."""
+        dt_out): the step ends with find_stable_timestep into dt_out, as a
+        separate pass after the last aux pass or, with fused_dt, inside it."""
         self.reset_c2p_diagnostics(aux, stream)
         self.advance_substep(t, dt, 1.0, state_p, state, aux, stream)
         bc(state_p)
@@ -295,13 +296,15 @@ class GRMHDEquationsSystem:
         self.linop_apply(state, state, state_pp, 1.0 / 3, 2.0 / 3.0, stream)
         self.advance_substep(t, dt, 2.0 / 3.0, state, state_pp, aux, stream)
         bc(state)
-        if next_dt is None:
-            self.compute_auxiliary_quantities(state, aux, stream)
-        else:
+        if next_dt is not None and fused_dt:
             self.compute_auxiliary_quantities_dt(state, aux, *next_dt, stream=stream)
+        else:
+            self.compute_auxiliary_quantities(state, aux, stream)
+            if next_dt is not None:
+                self.find_stable_timestep(state, aux, *next_dt, stream=stream)
         self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
 
-    def capture_rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, next_dt=None):
+    def capture_rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, next_dt=None, fused_dt=False):
         """Capture one rk3_step (same arguments) into a CUDA graph.  The
         arrays and dt are baked into the graph: each graph.replay() advances
         the same arrays by one step with no host work per kernel.  Call after
@@ -311,5 +314,5 @@ class GRMHDEquationsSystem:
         n0 = self.status().launches
         graph = torch.cuda.CUDAGraph()
         with torch.cuda.graph(graph):
-            self.rk3_step(dt, state, state_p, state_pp, aux, bc, t, next_dt=next_dt)
+            self.rk3_step(dt, state, state_p, state_pp, aux, bc, t, next_dt=next_dt, fused_dt=fused_dt)
         return graph, self.status().launches - n0
