@@ -930,7 +930,7 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
                           int32_t nby, int32_t nbz, const int32_t* periodic, void* stream) {
   if (!h) return GRB_ERR_INVALID;
   if (!g || !f || !f->state || !f->bx || !f->by || !f->bz || !periodic || g->ngz < 1 ||
-      nbx < 1 || nby < 1 || nbz < 1 || (int64_t)nbx * nby * nbz != g->nq)
+      nbx < 1 || nby < 1 || nbz < 1 || (int64_t)nbx * nby * nbz != g->nq || g->nq > 65535)
     return fail(h, GRB_ERR_INVALID);
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   Brick br;
@@ -939,16 +939,13 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
   cudaStream_t s = (cudaStream_t)stream;
   double* bf[3] = {f->bx, f->by, f->bz};
   KScope ks(h, s, GRB_KIND_GHOST);
-  for (int ax = 0; ax < 3; ++ax) {
-    for (int fd = -1; fd < 3; ++fd) {
-      int n[3] = {G.NX, G.NY, G.NZ};
-      if (fd >= 0) n[fd] += 1;
-      n[ax] = 2 * G.g;
-      const int total = n[0] * n[1] * n[2];
-      const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq);
-      k_ghost<<<grid, 256, 0, s>>>(G, br, ax, fd, fd < 0 ? f->state : bf[fd]);
-      ++h->launches;
-    }
+  for (int fd = -1; fd < 3; ++fd) {
+    int n[3] = {G.NX, G.NY, G.NZ};
+    if (fd >= 0) n[fd] += 1;
+    const int total = n[0] * n[1] * n[2];
+    const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq);
+    k_ghost<<<grid, 256, 0, s>>>(G, br, fd, fd < 0 ? f->state : bf[fd]);
+    ++h->launches;
   }
   CK(cudaGetLastError());
   return GRB_OK;

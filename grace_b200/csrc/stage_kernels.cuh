@@ -680,61 +680,70 @@ __global__ void k_linop(int64_t n, double* __restrict__ a, const double* __restr
 
 
 // ---- ghost fill for a brick of same-level blocks ---------------------------
-// One sweep along axis `ax` over the full extent of the other two axes, so
-// three sweeps (x, y, z) also fill edges and corners.  Periodic axes copy
-// from the neighbouring block (wrapping), others copy the nearest interior
-// cell or face (zero-gradient outflow).  Only the 7 evolved HRSC variables
-// and the three face-B arrays are exchanged; the Cowling metric is static.
-// Threads run x-fastest over the ghost slab of one block (blockIdx.y = q),
-// so the y and z sweeps read and write whole contiguous rows.
+// Periodic axes copy from the neighbouring block (wrapping), the others copy
+// the nearest interior cell or face (zero-gradient outflow).  These copies
+// compose axis by axis, so each ghost cell (edges and corners included) is
+// copied once, directly from the interior cell that the x, y and z sweeps
+// of phys_bc / copy kernels would carry into it, with identical values.
+// Only the 7 evolved HRSC variables and the three face-B arrays are
+// exchanged; the Cowling metric is static.
 struct Brick {
   int nbx, nby, nbz;
   int periodic[3];
 };
-// `fd` = -1: cell-centred HRSC vars of `a`; 0..2: face array staggered along fd.
-__global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, int ax, int fd, double* __restrict__ a) {
+// One coordinate along one axis: true when x is a ghost index; then (sx,
+// off) is the source index and the block offset (-1, 0, +1) along the axis.
+// stag: the array is staggered along this axis (faces 0 .. nin + 2g).
+__device__ __forceinline__ bool ghost_map(int x, int nin, int g, bool stag, bool periodic, int qc, int nb,
+                                          int& sx, int& off) {
+  off = 0;
+  sx = x;
+  if (x < g) {
+    if (qc == 0 && !periodic) sx = g;
+    else { sx = x + nin; off = -1; }
+    return true;
+  }
+  if (x >= (stag ? nin + g + 1 : nin + g)) {
+    if (qc == nb - 1 && !periodic) sx = stag ? nin + g : nin + g - 1;
+    else { sx = x - nin; off = 1; }
+    return true;
+  }
+  return false;
+}
+// `fd` = -1: cell-centred HRSC vars of `a`; 0..2: face array staggered
+// along fd.  One thread per cell of one block (blockIdx.y = q), x fastest.
+__global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, int fd, double* __restrict__ a) {
   const int64_t q = blockIdx.y;
   int n[3] = {G.NX, G.NY, G.NZ};
   if (fd >= 0) n[fd] += 1;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n[0] * n[1] * n[2]) return;
   const int nin[3] = {G.nx, G.ny, G.nz};
-  const bool stag = (fd == ax);
-  int box[3] = {n[0], n[1], n[2]};
-  box[ax] = 2 * G.g;
-  const int total = box[0] * box[1] * box[2];
   const int nb[3] = {br.nbx, br.nby, br.nbz};
   const int qc[3] = {(int)(q % br.nbx), (int)((q / br.nbx) % br.nby), (int)(q / ((int64_t)br.nbx * br.nby))};
-  const int64_t nv = fd < 0 ? GRB_N_HRSC : 1;
+  const int c[3] = {t % n[0], (t / n[0]) % n[1], t / (n[0] * n[1])};
+  int sidx[3], off[3];
+  bool ghost = false;
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax)
+    ghost |= ghost_map(c[ax], nin[ax], G.g, fd == ax, br.periodic[ax] != 0, qc[ax], nb[ax], sidx[ax], off[ax]);
+  if (!ghost) return;
+  int qs[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) qs[ax] = (qc[ax] + off[ax] + nb[ax]) % nb[ax];
+  const int64_t qsrc = qs[0] + (int64_t)br.nbx * (qs[1] + (int64_t)br.nby * qs[2]);
+  const int nv = fd < 0 ? GRB_N_HRSC : 1;
   const int64_t vstride = (int64_t)n[0] * n[1] * n[2];
   const int64_t qstride = vstride * (fd < 0 ? GRB_N_EVOL_VARS : 1);
-  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    int c[3];
-    c[0] = t % box[0];
-    c[1] = (t / box[0]) % box[1];
-    c[2] = t / (box[0] * box[1]);
-    const int gi = c[ax];
-    const bool lo = gi < G.g;
-    const int ig = lo ? gi : (stag ? nin[ax] + G.g + 1 + (gi - G.g) : nin[ax] + gi);
-    int src = lo ? ig + nin[ax] : ig - nin[ax];
-    int qs[3] = {qc[0], qc[1], qc[2]};
-    const bool edge = lo ? (qc[ax] == 0) : (qc[ax] == nb[ax] - 1);
-    if (edge && !br.periodic[ax]) src = lo ? G.g : (stag ? nin[ax] + G.g : nin[ax] + G.g - 1);
-    else qs[ax] = (qc[ax] + (lo ? nb[ax] - 1 : 1)) % nb[ax];
-    const int64_t qsrc = qs[0] + (int64_t)br.nbx * (qs[1] + (int64_t)br.nby * qs[2]);
-    int d[3] = {c[0], c[1], c[2]}, sidx[3] = {c[0], c[1], c[2]};
-    d[ax] = ig;
-    sidx[ax] = src;
-    const int64_t ld = d[0] + (int64_t)n[0] * (d[1] + (int64_t)n[1] * d[2]) + q * qstride;
-    const int64_t ls = sidx[0] + (int64_t)n[0] * (sidx[1] + (int64_t)n[1] * sidx[2]) + qsrc * qstride;
-    // all loads before any store: source and destination share one array,
-    // so interleaved copies would each wait a full memory latency
-    double tmp[GRB_N_HRSC];
+  const int64_t ld = c[0] + (int64_t)n[0] * (c[1] + (int64_t)n[1] * c[2]) + q * qstride;
+  const int64_t ls = sidx[0] + (int64_t)n[0] * (sidx[1] + (int64_t)n[1] * sidx[2]) + qsrc * qstride;
+  double tmp[GRB_N_HRSC];
 #pragma unroll
-    for (int v = 0; v < GRB_N_HRSC; ++v)
-      if (v < nv) tmp[v] = a[ls + v * vstride];
+  for (int v = 0; v < GRB_N_HRSC; ++v)
+    if (v < nv) tmp[v] = a[ls + v * vstride];
 #pragma unroll
-    for (int v = 0; v < GRB_N_HRSC; ++v)
-      if (v < nv) a[ld + v * vstride] = tmp[v];
-  }
+  for (int v = 0; v < GRB_N_HRSC; ++v)
+    if (v < nv) a[ld + v * vstride] = tmp[v];
 }
 
 }  // namespace grb

@@ -169,8 +169,10 @@ def test_graph_replay_matches_eager(mode):
 def test_timestep_reduction(name, mode):
     """find_stable_timestep on the GPU, fused into the aux pass and as a
     separate pass, against the oracle's find_stable_timestep_impl on the
-    same arrays; the fused aux pass leaves aux and state bit-identical to
-    the plain one."""
+    same arrays; the fused aux pass gives the plain pass's aux and state.
+    The two aux kernels are separate compiled instantiations (and, tuned,
+    under different register caps), so they agree to rounding, not bit for
+    bit."""
     P, su, f, dt = _setup(name)
     (st, bx, by, bz), aux, g = _gpu_run(P, su, f, dt, 1, mode)
     dev = torch.device("cuda:0")
@@ -186,8 +188,12 @@ def test_timestep_reduction(name, mode):
     g.compute_auxiliary_quantities_dt(state_b, aux_b, T(dx), cfl, dt_f)
     g.find_stable_timestep(state_b, aux_b, T(dx), cfl, dt_s)
     torch.cuda.synchronize()
-    assert torch.equal(aux_a, aux_b) and torch.equal(state.state, state_b.state)
-    assert dt_f.item() == dt_s.item()
+    a, b = aux_a.cpu().numpy(), aux_b.cpu().numpy()
+    da = np.abs(a - b) / np.maximum(np.abs(a), 1e-300)
+    assert np.max(da[np.isfinite(da)]) < 1e-12, np.max(da)
+    sa, sb = state.state.cpu().numpy(), state_b.state.cpu().numpy()
+    assert np.max(np.abs(sa - sb) / np.maximum(np.abs(sa), 1e-300)) < 1e-12
+    assert abs(dt_f.item() - dt_s.item()) <= 1e-14 * dt_s.item()
     S = _oracle.Stage(P, su.n[0], su.n[1], su.n[2], su.ngz, su.nq)
     host = [state_b.state.cpu().numpy(), None, None, None]
     dt_o = S.find_stable_timestep(host, aux_b.cpu().numpy(), dx, cfl)
