@@ -156,6 +156,7 @@ PROTOTYPES = {
     "grb_autotune": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Fields),
                                C.c_void_p, C.c_void_p]),
     "grb_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
+    "grb_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "grb_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "grb_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                    C.c_int32]),

@@ -5,6 +5,8 @@
 // src/data_structures/variables.cpp:100-211), and launches the kernels of
 // stage_kernels.cuh / fused_kernels.cuh on the caller's stream.  No call
 // here synchronises the stream except grb_get_status and grb_reserve.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +19,7 @@
 #include <vector>
 
 #include "grace_b200.h"
+#include "flux_tma.cuh"
 #include "mlp.cuh"
 #include "stage_kernels.cuh"
 
@@ -171,12 +174,84 @@ struct KScope {
 constexpr int kMinB[3] = {1, 4, 5};
 constexpr int kNumVar = 3;
 
+// ---- TMA-staged flux kernel: tensor maps and tile geometry ----------------
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no -lcuda).
+PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &qr) == cudaSuccess &&
+        qr == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+// Tile of direction dir for the face box b (one block's face ranges).
+FluxTile flux_tile(int dir, const Geo& G, const Box& b) {
+  FluxTile T;
+  for (int a = 0; a < 3; ++a) { T.lo[a] = b.lo[a]; T.n[a] = b.n[a]; }
+  T.R = 128 / T.n[0];
+  T.BY = dir == 0 ? T.R : dir == 1 ? T.R + 5 : 1;
+  T.BZ = dir == 2 ? T.R + 5 : 1;
+  (void)G;
+  return T;
+}
+// Tensor map over a LayoutLeft (NX, NY, NZ, nv, nq) double array, box
+// (NX, BY, BZ, 10 variables, 1 block).  False when the array or the box does
+// not meet the copy engine's rules (then the global-load kernel runs).
+bool make_tmap(CUtensorMap* tm, const double* base, const Geo& G, int nv, int64_t nq, const FluxTile& T) {
+  auto enc = tma_encoder();
+  if (!enc || ((uintptr_t)base & 15) || (G.NX * sizeof(double)) % 16 || G.NX > 256 || T.BY > 256 ||
+      T.BZ > 256 || T.R < 1)
+    return false;
+  const cuuint64_t dims[5] = {(cuuint64_t)G.NX, (cuuint64_t)G.NY, (cuuint64_t)G.NZ, (cuuint64_t)nv,
+                              (cuuint64_t)nq};
+  const cuuint64_t strides[4] = {(cuuint64_t)G.NX * 8, (cuuint64_t)G.NX * G.NY * 8, (cuuint64_t)G.cells * 8,
+                                 (cuuint64_t)G.cells * nv * 8};
+  const cuuint32_t box[5] = {(cuuint32_t)G.NX, (cuuint32_t)T.BY, (cuuint32_t)T.BZ, 10u, 1u};
+  const cuuint32_t es[5] = {1, 1, 1, 1, 1};
+  return enc(tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 5, const_cast<double*>(base), dims, strides, box, es,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+template <int dir, int MINB>
+bool launch_flux_tma(cudaStream_t s, const DevParams& P, const Geo& G, const Box& b, const double* st,
+                     const double* aux, const double* bf, const StageBufs& B) {
+  const FluxTile T = flux_tile(dir, G, b);
+  if (T.n[0] > 128 || b.nq > 65535) return false;
+  CUtensorMap ta, tm;
+  if (!make_tmap(&ta, aux, G, GRB_N_AUX_VARS, b.nq, T) || !make_tmap(&tm, st, G, GRB_N_EVOL_VARS, b.nq, T))
+    return false;
+  const size_t smem = flux_tile_smem(G, T);
+  static size_t attr = 0;
+  if (smem > attr) {
+    if (cudaFuncSetAttribute(k_flux_tma<dir, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return false;
+    attr = smem;
+  }
+  const int nrow = dir == 2 ? T.n[2] : T.n[1];
+  const int nother = dir == 2 ? T.n[1] : T.n[2];
+  const dim3 grid((unsigned)((nrow + T.R - 1) / T.R), (unsigned)nother, (unsigned)b.nq);
+  k_flux_tma<dir, MINB><<<grid, 128, smem, s>>>(P, G, T, ta, tm, bf, B);
+  return true;
+}
+
+// Flux candidates of the tuned mode: the global-load kernel capped at 4
+// CTAs/SM, and the TMA-staged kernel capped at 4 or 5.  Reported by
+// grb_get_tuning as min CTAs/SM, plus 100 for the TMA-staged kernel.
+constexpr int kFluxMinB[3] = {4, 4, 5};
+constexpr bool kFluxTma[3] = {false, true, true};
+
 template <int dir>
 void launch_flux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                        const double* st, const double* aux, const double* bf, const StageBufs& B) {
-  if (v == 1) k_flux<dir, true, 4><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
-  else if (v == 2) k_flux<dir, true, 5><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
-  else k_flux<dir, true, 1><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
+  if (v == 1 && launch_flux_tma<dir, 4>(s, P, G, b, st, aux, bf, B)) return;
+  if (v == 2 && launch_flux_tma<dir, 5>(s, P, G, b, st, aux, bf, B)) return;
+  k_flux<dir, true, 4><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
 }
 void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                        double dt, double dtfact, const double* ns, const double* os, const double* bx,
@@ -1067,13 +1142,25 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
 
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   if (!h || !variant) return GRB_ERR_INVALID;
-  variant[0] = kMinB[h->var_flux];
+  variant[0] = kFluxMinB[h->var_flux] + (kFluxTma[h->var_flux] ? 100 : 0);
   variant[1] = kMinB[h->var_flag];
   variant[2] = kMinB[h->var_update];
   variant[3] = kMinB[h->var_aux];
   if (ms)
     for (int f = 0; f < 4; ++f)
       for (int v = 0; v < kNumVar; ++v) ms[f * kNumVar + v] = h->tune_ms[f][v];
+  return GRB_OK;
+}
+
+int grb_set_tuning(grb_handle* h, const int32_t* variant) {
+  if (!h || !variant) return GRB_ERR_INVALID;
+  for (int f = 0; f < 4; ++f)
+    if (variant[f] < 0 || variant[f] >= kNumVar) return fail(h, GRB_ERR_INVALID);
+  h->var_flux = variant[0];
+  h->var_flag = variant[1];
+  h->var_update = variant[2];
+  h->var_aux = variant[3];
+  h->autotuned = true;
   return GRB_OK;
 }
 

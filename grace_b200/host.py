@@ -261,6 +261,11 @@ class GRMHDEquationsSystem:
         return {f: {"min_ctas_per_sm": v[i], "ms": [round(ms[3 * i + k], 4) for k in range(3)]}
                 for i, f in enumerate(fam)}
 
+    def set_tuning(self, flux=0, flag=0, update=0, aux=0):
+        """Pick tuned-mode candidates (indices 0..2) without timing."""
+        v = (ctypes.c_int32 * 4)(flux, flag, update, aux)
+        _lib.check(self.lib.grb_set_tuning(self.h, v), "grb_set_tuning")
+
     def set_kernel_timing(self, on):
         _lib.check(self.lib.grb_set_kernel_timing(self.h, 1 if on else 0), "grb_set_kernel_timing")
 

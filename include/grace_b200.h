@@ -76,7 +76,9 @@ enum grb_device_flag {
   GRB_FLAG_EOS_EPS_TOO_HIGH = 1u << 2,
   GRB_FLAG_EOS_TEMP_TOO_HIGH = 1u << 3,
   GRB_FLAG_EOS_PRESS_TOO_HIGH = 1u << 4,
-  GRB_FLAG_BAD_LEARNED_BRACKET = 1u << 8 /* informational: fallback taken */
+  GRB_FLAG_BAD_LEARNED_BRACKET = 1u << 8, /* informational: fallback taken */
+  GRB_FLAG_WAIT_TIMEOUT = 1u << 9         /* a bounded wait in a kernel gave up
+                                             (its results are not valid) */
 };
 
 /* ---- scheme selectors (runtime; the reference picks them in CMake) ------- */
@@ -330,9 +332,14 @@ int grb_set_mode(grb_handle* h, int32_t mode);
  * Allocates and frees temporary copies; synchronises the stream. */
 int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* new_state,
                  const grb_fields* old_state, const double* aux, void* stream);
-/* variant[4]: chosen minimum-CTAs-per-SM of flux, flag, update, aux;
+/* variant[4]: chosen minimum-CTAs-per-SM of flux, flag, update, aux (flux:
+ * plus 100 when the TMA-staged shared-memory kernel was chosen);
  * ms[12] (or NULL): timed milliseconds of the 3 candidates per family. */
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms);
+/* Choose the tuned-mode candidates without timing: variant[4] = candidate
+ * index 0..2 of flux, flag, update, aux (flux: 0 global-load kernel, 1 and 2
+ * TMA-staged kernel at 4 and 5 CTAs/SM; others: 1, 4, 5 CTAs/SM). */
+int grb_set_tuning(grb_handle* h, const int32_t* variant);
 
 /* ---- measurement helpers -------------------------------------------------- */
 /* Kernel kinds for grb_kernel_times. */

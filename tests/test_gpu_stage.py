@@ -25,7 +25,7 @@ def _setup(name):
     return P, su, f, cfl / su.idx()[0, 0]
 
 
-def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN):
+def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN, tuning=None):
     dev = torch.device("cuda:0")
     st, bx, by, bz, aux = f
     blocks = Blocks(su.n[0], su.n[1], su.n[2], su.ngz, su.nq, su.idx(), device=dev)
@@ -40,7 +40,10 @@ def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN):
     g.compute_auxiliary_quantities(state, aux_d)
     sp, spp = state.clone(), state.clone()
     if mode == abi.MODE_TUNED:
-        g.autotune(sp, state, aux_d)
+        if tuning is None:
+            g.autotune(sp, state, aux_d)
+        else:
+            g.set_tuning(*tuning)
     for _ in range(nsteps):
         g.rk3_step(dt, state, sp, spp, aux_d, bc)
     torch.cuda.synchronize()
@@ -76,6 +79,24 @@ def test_one_rk3_step_matches_oracle(name, mode):
         r = np.max(np.abs(ga[:, v] - oa[:, v]) / np.abs(oa[:, v]))
         assert r < STEP_TOL, (v, r)
     np.testing.assert_array_equal(ga[:, abi.C2P_ERR], oa[:, abi.C2P_ERR])
+
+
+@pytest.mark.parametrize("flux", [0, 1, 2])
+@pytest.mark.parametrize("name", ["blast", "balsara"])
+def test_tuned_flux_candidates_match_oracle(name, flux):
+    """Each tuned flux candidate (global loads; TMA-staged shared-memory
+    tiles at 4 and 5 CTAs/SM) gives one RK3 step within the step tolerance
+    of the oracle, GS (blast) and UCT (Balsara-1) transverse ranges."""
+    P, su, f, dt = _setup(name)
+    gs, ga, g = _gpu_run(P, su, f, dt, 1, abi.MODE_TUNED, tuning=(flux, 0, 0, 0))
+    assert g.tuning()["flux"]["min_ctas_per_sm"] == [4, 104, 105][flux]
+    os_, oa, S = _oracle_run(P, su, f, dt, 1)
+    e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
+    assert e.max() < STEP_TOL, e
+    for a, b in zip(gs[1:], os_[1:]):
+        d = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+        assert d < STEP_TOL
+    assert g.status().device_flags == 0
 
 
 @pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
