@@ -5,7 +5,9 @@ relative error: D, tau, Ye*D and s*D relative to their own magnitude,
 the momenta S_i relative to max(|S|, tau + D) — the bound |S| <= tau + D
 that the c2p's limit_conservatives enforces (c2p.cpp:138-150).  Plain
 per-component relative errors are ill-posed for momenta that are zero up
-to rounding (a resting background with 1e-3 pressure noise)."""
+to rounding (a resting background with 1e-3 pressure noise).  The entropy density
+s* = D s is taken relative to D max(|s|, 1): s is a logarithm that may
+cross zero."""
 import numpy as np
 
 from grace_b200 import abi
@@ -22,6 +24,10 @@ def cons_rel_err(a, b, floor=1e-300):
         d = np.abs(a[:, v] - b[:, v])
         if 1 <= v <= 3:
             s = scale_S
+        elif v == 6:
+            # s* = D s with the specific entropy s a logarithm: relative to
+            # D max(|s|, 1), ill-posed where s crosses zero otherwise
+            s = np.maximum(np.abs(b[:, v]), np.abs(b[:, 0]))
         else:
             s = np.abs(b[:, v])
         ok = (s > floor) | (d > 0)
