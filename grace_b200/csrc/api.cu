@@ -51,6 +51,8 @@ struct grb_handle {
   // learned c2p bracket: FP32 parameter block on the device
   float* d_mlp = nullptr;
   MlpSmem* d_mlp_pack = nullptr;  // shared-memory image of the network
+  unsigned long long* d_queue = nullptr;  // work-queue counter of the aux pass
+  float tune_aux_queue_ms = 0.f;
   bool mlp_ready = false;
 };
 
@@ -268,10 +270,44 @@ void launch_update_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P,
   else if (v == 2) k_update<5><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B);
   else k_update<1><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B);
 }
+// Work-queue aux pass: one wave of CTAs (occupancy x SMs) pulling tiles.
+template <int MINB, bool kDt>
+void launch_aux_queue(cudaStream_t s, const DevParams& P, const Geo& G, const Box& b, double* st, const double* bx,
+                      const double* by, const double* bz, double* aux, const double* idx, const double* crd,
+                      const StageBufs& B, unsigned long long* queue, const DtArgs& dta) {
+  static int grid = 0;
+  if (grid == 0) {
+    int dev = 0, sms = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_aux_queue<MINB, kDt>, 128, 0);
+    grid = (sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+  }
+  cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+  k_aux_queue<MINB, kDt><<<grid, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, dta);
+}
+
+// Aux candidates: 0..2 one thread per cell at kMinB[v] CTAs/SM; 3..5 the
+// work-queue form at kMinB[v - 3].
 void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                       double* st, const double* bx, const double* by, const double* bz, double* aux,
                       const double* idx, const double* crd, const StageBufs& B,
-                      const DtArgs* dta = nullptr) {
+                      const DtArgs* dta = nullptr, unsigned long long* queue = nullptr) {
+  if (v >= 3 && queue) {
+    const DtArgs d0{nullptr, 0.0, nullptr};
+    const int m = v - 3;
+    if (dta) {
+      if (m == 1) launch_aux_queue<4, true>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, *dta);
+      else if (m == 2) launch_aux_queue<5, true>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, *dta);
+      else launch_aux_queue<1, true>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, *dta);
+    } else {
+      if (m == 1) launch_aux_queue<4, false>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, d0);
+      else if (m == 2) launch_aux_queue<5, false>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, d0);
+      else launch_aux_queue<1, false>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, d0);
+    }
+    return;
+  }
+  if (v >= 3) v -= 3;
   if (dta) {
     if (v == 1) k_aux<4, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
     else if (v == 2) k_aux<5, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
@@ -420,8 +456,10 @@ int grb_create(grb_handle** out, const grb_params* p) {
   h->p = *p;
   h->dp = to_dev(*p);
   if (cudaMalloc(&h->d_flags, sizeof(uint32_t)) != cudaSuccess ||
-      cudaMalloc(&h->d_counters, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMalloc(&h->d_counters, 2 * sizeof(unsigned long long)) != cudaSuccess ||
+      cudaMalloc(&h->d_queue, sizeof(unsigned long long)) != cudaSuccess) {
     cudaFree(h->d_flags);
+    cudaFree(h->d_counters);
     delete h;
     return GRB_ERR_CUDA;
   }
@@ -449,6 +487,7 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_counters);
   cudaFree(h->d_mlp);
   cudaFree(h->d_mlp_pack);
+  cudaFree(h->d_queue);
   delete h;
   return GRB_OK;
 }
@@ -604,7 +643,7 @@ int grb_compute_auxiliary_quantities_dt(grb_handle* h, const grb_grid* g, const 
   }
   if (h->mode == GRB_MODE_TUNED) {
     launch_aux_tuned(h->var_aux, nblk(b.count(), 128), s, h->dp, G, b, st->state, st->bx, st->by, st->bz, aux,
-                     g->idx, g->coords, h->B, dt_out ? &dta : nullptr);
+                     g->idx, g->coords, h->B, dt_out ? &dta : nullptr, h->d_queue);
   } else if (dt_out) {
     k_aux<1, true><<<nblk(b.count(), 128), 128, 0, s>>>(h->dp, G, b, st->state, st->bx, st->by, st->bz, aux,
                                                         g->idx, g->coords, h->B, dta);
@@ -1126,6 +1165,12 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
       if (t < bt) { bt = t; best[fam] = v; }
     }
   }
+  // the work-queue form of the chosen aux register cap
+  h->tune_aux_queue_ms = time_it([&] {
+    launch_aux_tuned(best[3] + 3, nblk(ab.count(), 128), s, P, G, ab, ns, fn.bx, fn.by, fn.bz, ax, gs.idx,
+                     gs.coords, B, nullptr, h->d_queue);
+  });
+  if (h->tune_aux_queue_ms < h->tune_ms[3][best[3]]) best[3] += 3;
   h->var_flux = best[0];
   h->var_flag = best[1];
   h->var_update = best[2];
@@ -1145,7 +1190,7 @@ int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   variant[0] = kFluxMinB[h->var_flux] + (kFluxTma[h->var_flux] ? 100 : 0);
   variant[1] = kMinB[h->var_flag];
   variant[2] = kMinB[h->var_update];
-  variant[3] = kMinB[h->var_aux];
+  variant[3] = kMinB[h->var_aux % 3] + (h->var_aux >= 3 ? 100 : 0);
   if (ms)
     for (int f = 0; f < 4; ++f)
       for (int v = 0; v < kNumVar; ++v) ms[f * kNumVar + v] = h->tune_ms[f][v];
@@ -1155,7 +1200,7 @@ int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
 int grb_set_tuning(grb_handle* h, const int32_t* variant) {
   if (!h || !variant) return GRB_ERR_INVALID;
   for (int f = 0; f < 4; ++f)
-    if (variant[f] < 0 || variant[f] >= kNumVar) return fail(h, GRB_ERR_INVALID);
+    if (variant[f] < 0 || variant[f] >= (f == 3 ? 2 * kNumVar : kNumVar)) return fail(h, GRB_ERR_INVALID);
   h->var_flux = variant[0];
   h->var_flag = variant[1];
   h->var_update = variant[2];

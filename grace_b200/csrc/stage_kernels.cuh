@@ -589,19 +589,16 @@ __global__ void __launch_bounds__(128) k_dt(DevParams P, Geo G, Box box, const d
 // ---- aux: c2p on every cell + resets + C2P_ERR + BDIV + cell-centred E -----
 // kDt: also the time-step reduction over the interior cells, from the
 // primitives just computed (the aux pass that ends an RK step).
-template <int MINB = 1, bool kDt = false>
-__global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, double* __restrict__ st,
-                                              const double* __restrict__ bx,
-                                              const double* __restrict__ by,
-                                              const double* __restrict__ bz,
-                                              double* __restrict__ aux,
-                                              const double* __restrict__ idx,
-                                              const double* __restrict__ coords, StageBufs B,
-                                              DtArgs dta = DtArgs{nullptr, 0.0, nullptr}) {
-  int i = 0, j = 0, k = 0;
-  int64_t q = 0;
+// One cell of the aux pass; returns the cell's dt candidate (kDt, interior
+// cells) or +inf.
+template <bool kDt>
+__device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
+                                           double* __restrict__ st, const double* __restrict__ bx,
+                                           const double* __restrict__ by, const double* __restrict__ bz,
+                                           double* __restrict__ aux, const double* __restrict__ idx,
+                                           const double* __restrict__ coords, const StageBufs& B,
+                                           const DtArgs& dta) {
   double dtc = INFINITY;
-  if (decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) {
   const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
   const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
   const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
@@ -657,8 +654,59 @@ __global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, 
   }
   if (kDt && i >= G.g && i < G.nx + G.g && j >= G.g && j < G.ny + G.g && k >= G.g && k < G.nz + G.g)
     dtc = dta.cfl / max_eigenspeed(P.eos, m, pr) * dta.dx[3 * q];
-  }
+  return dtc;
+}
+
+// One thread per cell over the box.
+template <int MINB = 1, bool kDt = false>
+__global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, double* __restrict__ st,
+                                              const double* __restrict__ bx,
+                                              const double* __restrict__ by,
+                                              const double* __restrict__ bz,
+                                              double* __restrict__ aux,
+                                              const double* __restrict__ idx,
+                                              const double* __restrict__ coords, StageBufs B,
+                                              DtArgs dta = DtArgs{nullptr, 0.0, nullptr}) {
+  int i = 0, j = 0, k = 0;
+  int64_t q = 0;
+  double dtc = INFINITY;
+  if (decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q))
+    dtc = aux_cell<kDt>(P, G, i, j, k, q, st, bx, by, bz, aux, idx, coords, B, dta);
   if (kDt) dt_reduce(dtc, dta.out);
+}
+
+// Persistent form: one wave of CTAs; each pulls chunks of kAuxChunk tiles of
+// 128 cells (tiles numbered block by block, so a chunk stays inside one or
+// two blocks) from the device work queue *queue (zeroed before the launch)
+// until the box is exhausted.  Per-cell work is the same function.
+constexpr int kAuxChunk = 8;
+template <int MINB = 1, bool kDt = false>
+__global__ void __launch_bounds__(128, MINB) k_aux_queue(DevParams P, Geo G, Box box, double* __restrict__ st,
+                                                    const double* __restrict__ bx,
+                                                    const double* __restrict__ by,
+                                                    const double* __restrict__ bz,
+                                                    double* __restrict__ aux,
+                                                    const double* __restrict__ idx,
+                                                    const double* __restrict__ coords, StageBufs B,
+                                                    unsigned long long* __restrict__ queue,
+                                                    DtArgs dta = DtArgs{nullptr, 0.0, nullptr}) {
+  __shared__ unsigned long long item;
+  const int64_t ntiles = (box.count() + 127) / 128;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(queue, (unsigned long long)kAuxChunk);
+    __syncthreads();
+    const int64_t first = (int64_t)item;
+    __syncthreads();
+    if (first >= ntiles) break;
+    for (int c = 0; c < kAuxChunk; ++c) {
+      int i = 0, j = 0, k = 0;
+      int64_t q = 0;
+      double dtc = INFINITY;
+      if (first + c < ntiles && decode(box, (first + c) * 128 + threadIdx.x, i, j, k, q))
+        dtc = aux_cell<kDt>(P, G, i, j, k, q, st, bx, by, bz, aux, idx, coords, B, dta);
+      if (kDt) dt_reduce(dtc, dta.out);
+    }
+  }
 }
 
 // reset_c2p_diagnostics (evolve.cpp:154-161)

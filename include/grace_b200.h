@@ -333,12 +333,15 @@ int grb_set_mode(grb_handle* h, int32_t mode);
 int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* new_state,
                  const grb_fields* old_state, const double* aux, void* stream);
 /* variant[4]: chosen minimum-CTAs-per-SM of flux, flag, update, aux (flux:
- * plus 100 when the TMA-staged shared-memory kernel was chosen);
+ * plus 100 when the TMA-staged shared-memory kernel was chosen; aux: plus
+ * 100 when the work-queue form was chosen);
  * ms[12] (or NULL): timed milliseconds of the 3 candidates per family. */
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms);
 /* Choose the tuned-mode candidates without timing: variant[4] = candidate
  * index 0..2 of flux, flag, update, aux (flux: 0 global-load kernel, 1 and 2
- * TMA-staged kernel at 4 and 5 CTAs/SM; others: 1, 4, 5 CTAs/SM). */
+ * TMA-staged kernel at 4 and 5 CTAs/SM; others: 1, 4, 5 CTAs/SM; aux also
+ * 3..5: the work-queue form — one wave of CTAs pulling chunks of 128-cell
+ * tiles from a device counter — at 1, 4, 5 CTAs/SM). */
 int grb_set_tuning(grb_handle* h, const int32_t* variant);
 
 /* ---- measurement helpers -------------------------------------------------- */

@@ -99,6 +99,37 @@ def test_tuned_flux_candidates_match_oracle(name, flux):
     assert g.status().device_flags == 0
 
 
+@pytest.mark.parametrize("aux", [3, 4, 5])
+@pytest.mark.parametrize("name", ["blast", "balsara"])
+def test_aux_work_queue_matches_oracle(name, aux):
+    """The work-queue form of the aux pass (one wave of CTAs pulling 128-cell
+    tiles from a device counter) at each register cap: one RK3 step within
+    the step tolerance of the oracle, and its fused dt reduction equal to the
+    separate pass to rounding."""
+    P, su, f, dt = _setup(name)
+    gs, ga, g = _gpu_run(P, su, f, dt, 1, abi.MODE_TUNED, tuning=(1, 0, 0, aux))
+    assert g.tuning()["aux"]["min_ctas_per_sm"] == [101, 104, 105][aux - 3]
+    os_, oa, S = _oracle_run(P, su, f, dt, 1)
+    e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
+    assert e.max() < STEP_TOL, e
+    for v in (abi.RHO, abi.PRESS, abi.EPS):
+        r = np.max(np.abs(ga[:, v] - oa[:, v]) / np.abs(oa[:, v]))
+        assert r < STEP_TOL, (v, r)
+    np.testing.assert_array_equal(ga[:, abi.C2P_ERR], oa[:, abi.C2P_ERR])
+    dev = torch.device("cuda:0")
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    state = Fields(*[T(x) for x in gs])
+    aux_d = T(ga)
+    dx = T(1.0 / su.idx())
+    d1 = torch.zeros(1, dtype=torch.float64, device=dev)
+    d2 = torch.zeros(1, dtype=torch.float64, device=dev)
+    g.compute_auxiliary_quantities_dt(state, aux_d, dx, 0.4, d1)
+    g.find_stable_timestep(state, aux_d, dx, 0.4, d2)
+    torch.cuda.synchronize()
+    assert abs(d1.item() - d2.item()) <= 1e-14 * d2.item()
+    assert g.status().device_flags == 0
+
+
 @pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
 def test_div_b_and_conservation_blast(mode):
     P, su, f, dt = _setup("blast")
