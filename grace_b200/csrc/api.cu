@@ -259,9 +259,9 @@ void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, c
                        double dt, double dtfact, const double* ns, const double* os, const double* bx,
                        const double* by, const double* bz, const double* idx, const double* crd,
                        const StageBufs& B) {
-  if (v == 1) k_fofc_flag<4><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
-  else if (v == 2) k_fofc_flag<5><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
-  else k_fofc_flag<1><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
+  if (v == 1) k_fofc_flag<4, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
+  else if (v == 2) k_fofc_flag<5, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
+  else k_fofc_flag<1, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
 }
 void launch_update_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                          double dt, double dtfact, double* ns, const double* os, const double* aux,
@@ -280,11 +280,11 @@ void launch_aux_queue(cudaStream_t s, const DevParams& P, const Geo& G, const Bo
     int dev = 0, sms = 0, occ = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_aux_queue<MINB, kDt>, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_aux_queue<MINB, kDt, true>, 128, 0);
     grid = (sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
   }
   cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
-  k_aux_queue<MINB, kDt><<<grid, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, dta);
+  k_aux_queue<MINB, kDt, true><<<grid, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, dta);
 }
 
 // Aux candidates: 0..2 one thread per cell at kMinB[v] CTAs/SM; 3..5 the
@@ -309,14 +309,14 @@ void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, co
   }
   if (v >= 3) v -= 3;
   if (dta) {
-    if (v == 1) k_aux<4, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
-    else if (v == 2) k_aux<5, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
-    else k_aux<1, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+    if (v == 1) k_aux<4, true, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+    else if (v == 2) k_aux<5, true, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+    else k_aux<1, true, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
     return;
   }
-  if (v == 1) k_aux<4><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
-  else if (v == 2) k_aux<5><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
-  else k_aux<1><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
+  if (v == 1) k_aux<4, false, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
+  else if (v == 2) k_aux<5, false, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
+  else k_aux<1, false, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
 }
 
 // linop on the evolved HRSC variables and the face arrays only

@@ -139,7 +139,10 @@ GRB_HD KSc kscalars(const DevEos& e, const Met& m, double c[10]) {
   return k;
 }
 
-// Kastaun master function (kastaun_c2p.hh:122-295)
+// Kastaun master function (kastaun_c2p.hh:122-295).  FAST (tuned mode):
+// rho = D sqrt(1 - v^2) and h/W = h sqrt(1 - v^2) instead of two divisions
+// by W = 1/sqrt(1 - v^2); the same function up to rounding.
+template <bool FAST = false>
 struct KRt {
   const DevEos* e;
   double d, qtot, rsqr, bsqr, rbsqr, brosqr, vsqrmax, wmax;
@@ -158,9 +161,18 @@ struct KRt {
     const double mx = mu * x;
     const double qf = qtot - 0.5 * (bsqr + mx * mx * brosqr);
     const double vsqr = rf * mu * mu;
-    if (vsqr > vsqrmax) { w = wmax; if (full) sig |= SIG_VEL_HIGH; }
-    else w = 1 / sqrt(1 - vsqr);
-    rho = d / w;
+    double iw = 0.0;
+    if (vsqr > vsqrmax) {
+      w = wmax;
+      if (full) sig |= SIG_VEL_HIGH;
+      if (FAST) iw = 1.0 / wmax;
+    } else if (FAST) {
+      iw = sqrt(1 - vsqr);
+      w = 1 / iw;
+    } else {
+      w = 1 / sqrt(1 - vsqr);
+    }
+    rho = FAST ? d * iw : d / w;
     if (full) {
       if (rho >= e->rhomax) { sig |= SIG_RHO_HIGH; rho = e->rhomax; }
       else if (rho <= e->rhomin) { sig |= SIG_RHO_LOW; rho = e->rhomin; }
@@ -182,7 +194,7 @@ struct KRt {
     }
     const double a = press / (rho * (1 + eps));
     const double h = (1 + eps) * (1 + a);
-    const double hbw = fmax((1 + a) * (1 + qf - mu * rf), h / w);
+    const double hbw = fmax((1 + a) * (1 + qf - mu * rf), FAST ? h * iw : h / w);
     return mu - 1. / (hbw + rf * mu);
   }
   GRB_HD double operator()(double mu) const {
@@ -266,11 +278,12 @@ GRB_HD Guess no_guess() { return Guess{false, 0., 0., 0., false}; }
 // the unchanged Brent iteration starts from [gs.lo, gs.hi] when f changes
 // sign there (the two end values are the iteration's own first two
 // evaluations), and from the plain [0, mu0] otherwise.
+template <bool FAST = false>
 GRB_HD double kastaun_invert(const DevEos& e, const Met& m, double c[10], double pr[13],
                              uint32_t& sig, int& iters, const Guess& gs, bool& guess_used,
                              double& mu_out) {
   const KSc k = kscalars(e, m, c);
-  const KRt f(e, k);
+  const KRt<FAST> f(e, k);
   double mu;
   guess_used = false;
   const double mu0 = gs.has_mu0 ? gs.mu0 : kastaun_mu0(k);
@@ -400,6 +413,10 @@ struct C2POut {
 
 // conservs_to_prims (c2p.cpp:188-414).  c: densitized cons with densitized
 // cell-centred B (in), re-densitized consistent cons (out).
+// FAST (tuned mode): multiplications by 1/sqrt(gamma) and 1/D where the
+// reference divides repeatedly by the same value, and the FAST master
+// function; equal to the reference's operations up to rounding.
+template <bool FAST = false>
 GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P, double r_sph,
                   bool dry_run, double alp_bh_thresh, const Guess& gs) {
   C2POut o{0u, 0u, 0, false, false, 0.0};
@@ -409,7 +426,7 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
   o.err = ERR_RESET_ENTROPY;
   const double isg = 1.0 / m.sqrtg;
 #pragma unroll
-  for (int v = 0; v < 10; ++v) c[v] = c[v] / m.sqrtg;
+  for (int v = 0; v < 10; ++v) c[v] = FAST ? c[v] * isg : c[v] / m.sqrtg;
   (void)isg;
   pr[GRB_P_BX] = c[7]; pr[GRB_P_BY] = c[8]; pr[GRB_P_BZ] = c[9];
   if (c[0] < 0) {
@@ -417,7 +434,8 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
     o.floored = true;
     return o;
   }
-  pr[GRB_P_YE] = c[5] / c[0];
+  const double iD0 = FAST ? 1.0 / c[0] : 0.0;
+  pr[GRB_P_YE] = FAST ? c[5] * iD0 : c[5] / c[0];
   if (pr[GRB_P_YE] > e.yemax) { pr[GRB_P_YE] = e.yemax; o.err |= ERR_RESET_YE; }
   if (pr[GRB_P_YE] < 0.0) { pr[GRB_P_YE] = 0.0; o.err |= ERR_RESET_YE; }
   const bool lenient = m.alp < alp_bh_thresh;
@@ -425,13 +443,13 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
     double lo, hi;
     eos_eps_range(e, lo, hi, c[0]);
     const double B2 = sqs(m.g, c + 7);
-    if (c[4] / c[0] - 0.5 * B2 / c[0] < fmin(0.0, lo)) {
+    if ((FAST ? c[4] * iD0 - 0.5 * B2 * iD0 : c[4] / c[0] - 0.5 * B2 / c[0]) < fmin(0.0, lo)) {
       c[4] = lo * c[0] + 0.5 * B2;
       o.err |= ERR_RESET_TAU;
       o.floored = true;
     }
-    const double qd = c[4] / c[0] + 1;
-    const double st2 = sqs(m.gi, c + 1) / (c[0] * c[0]);
+    const double qd = (FAST ? c[4] * iD0 : c[4] / c[0]) + 1;
+    const double st2 = FAST ? sqs(m.gi, c + 1) * (iD0 * iD0) : sqs(m.gi, c + 1) / (c[0] * c[0]);
     if (st2 > qd * qd) {
       const double f = sqrt(qd * qd / st2);
       c[1] *= f; c[2] *= f; c[3] *= f;
@@ -443,7 +461,7 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
   if (c[0] >= P.rho_fl * (1 + P.atmo_tol)) {
     Guess g2 = gs;
     if (o.floored) g2.has_mu0 = false;  // limit_conservatives changed the state
-    const double res = kastaun_invert(e, m, c, pr, ret, o.iters, g2, o.guess_used, o.mu);
+    const double res = kastaun_invert<FAST>(e, m, c, pr, ret, o.iters, g2, o.guess_used, o.mu);
     failed = (fabs(res) > P.tol) || (ret & SIG_RHO_HIGH) || (ret & SIG_EPS_HIGH) || !isfinite(res);
     double beta;
     {

@@ -341,7 +341,7 @@ __device__ __forceinline__ double cell_r(const Geo& G, const double* coords, con
 }
 
 // flag_fofc_cells (evolve.cpp:456-635) over cells [g-1, n+g]^3
-template <int MINB = 1>
+template <int MINB = 1, bool kFast = false>
 __global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box box, double dt,
                                                     double dtfact, const double* __restrict__ ns,
                                                     const double* __restrict__ os,
@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box
     const Met m = cell_met(G, os, i, j, k, q);
     double pr[13];
     const Guess none = no_guess();
-    floored = c2p(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), true, 1e30, none).floored;
+    floored = c2p<kFast>(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), true, 1e30, none).floored;
   }
   if (floored || dmp) {
     int8_t* T = B.ftag;
@@ -591,7 +591,7 @@ __global__ void __launch_bounds__(128) k_dt(DevParams P, Geo G, Box box, const d
 // primitives just computed (the aux pass that ends an RK step).
 // One cell of the aux pass; returns the cell's dt candidate (kDt, interior
 // cells) or +inf.
-template <bool kDt>
+template <bool kDt, bool kFast>
 __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
                                            double* __restrict__ st, const double* __restrict__ bx,
                                            const double* __restrict__ by, const double* __restrict__ bz,
@@ -612,13 +612,14 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
   c[8] = 0.5 * (by0 + by1);
   c[9] = 0.5 * (bz0 + bz1);
   const Met m = cell_met(G, st, i, j, k, q);
-  aux[a0 + G.cells * GRB_BX] = c[7] / m.sqrtg;
-  aux[a0 + G.cells * GRB_BY] = c[8] / m.sqrtg;
-  aux[a0 + G.cells * GRB_BZ] = c[9] / m.sqrtg;
+  const double isg = kFast ? 1.0 / m.sqrtg : 0.0;
+  aux[a0 + G.cells * GRB_BX] = kFast ? c[7] * isg : c[7] / m.sqrtg;
+  aux[a0 + G.cells * GRB_BY] = kFast ? c[8] * isg : c[8] / m.sqrtg;
+  aux[a0 + G.cells * GRB_BZ] = kFast ? c[9] * isg : c[9] / m.sqrtg;
   const double cbx = c[7], cby = c[8], cbz = c[9];
   double pr[13];
   const Guess none = no_guess();
-  const C2POut o = c2p(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), false, P.alp_bh_thresh, none);
+  const C2POut o = c2p<kFast>(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), false, P.alp_bh_thresh, none);
   if (o.fatal) atomicOr(B.flags, o.fatal);
   aux[a0 + G.cells * GRB_RHO] = pr[GRB_P_RHO];
   aux[a0 + G.cells * GRB_EPS] = pr[GRB_P_EPS];
@@ -642,12 +643,16 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
     const uint64_t prev = (uint64_t)aux[a0 + G.cells * GRB_C2P_ERR];
     aux[a0 + G.cells * GRB_C2P_ERR] = (double)(prev | (uint64_t)o.err);
   }
-  aux[a0 + G.cells * GRB_BDIV] = ((bx1 - bx0) * ix[0] + (by1 - by0) * ix[1] + (bz1 - bz0) * ix[2]) / m.sqrtg;
+  {
+    const double dv = (bx1 - bx0) * ix[0] + (by1 - by0) * ix[1] + (bz1 - bz0) * ix[2];
+    aux[a0 + G.cells * GRB_BDIV] = kFast ? dv * isg : dv / m.sqrtg;
+  }
   if (P.emf == GRB_EMF_GS) {
     const double W = sqrt(1. + sqs(m.g, pr + GRB_P_ZX));
     double vt[3];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) vt[a] = m.alp * pr[GRB_P_ZX + a] / W - m.beta[a];
+    const double iW = kFast ? 1.0 / W : 0.0;
+    for (int a = 0; a < 3; ++a) vt[a] = (kFast ? m.alp * pr[GRB_P_ZX + a] * iW : m.alp * pr[GRB_P_ZX + a] / W) - m.beta[a];
     B.ecenter[eci(G, i, j, k, 0, q)] = cby * vt[2] - cbz * vt[1];
     B.ecenter[eci(G, i, j, k, 1, q)] = -cbx * vt[2] + cbz * vt[0];
     B.ecenter[eci(G, i, j, k, 2, q)] = cbx * vt[1] - cby * vt[0];
@@ -658,7 +663,7 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
 }
 
 // One thread per cell over the box.
-template <int MINB = 1, bool kDt = false>
+template <int MINB = 1, bool kDt = false, bool kFast = false>
 __global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, double* __restrict__ st,
                                               const double* __restrict__ bx,
                                               const double* __restrict__ by,
@@ -671,7 +676,7 @@ __global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, 
   int64_t q = 0;
   double dtc = INFINITY;
   if (decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q))
-    dtc = aux_cell<kDt>(P, G, i, j, k, q, st, bx, by, bz, aux, idx, coords, B, dta);
+    dtc = aux_cell<kDt, kFast>(P, G, i, j, k, q, st, bx, by, bz, aux, idx, coords, B, dta);
   if (kDt) dt_reduce(dtc, dta.out);
 }
 
@@ -680,7 +685,7 @@ __global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, 
 // two blocks) from the device work queue *queue (zeroed before the launch)
 // until the box is exhausted.  Per-cell work is the same function.
 constexpr int kAuxChunk = 8;
-template <int MINB = 1, bool kDt = false>
+template <int MINB = 1, bool kDt = false, bool kFast = false>
 __global__ void __launch_bounds__(128, MINB) k_aux_queue(DevParams P, Geo G, Box box, double* __restrict__ st,
                                                     const double* __restrict__ bx,
                                                     const double* __restrict__ by,
@@ -703,7 +708,7 @@ __global__ void __launch_bounds__(128, MINB) k_aux_queue(DevParams P, Geo G, Box
       int64_t q = 0;
       double dtc = INFINITY;
       if (first + c < ntiles && decode(box, (first + c) * 128 + threadIdx.x, i, j, k, q))
-        dtc = aux_cell<kDt>(P, G, i, j, k, q, st, bx, by, bz, aux, idx, coords, B, dta);
+        dtc = aux_cell<kDt, kFast>(P, G, i, j, k, q, st, bx, by, bz, aux, idx, coords, B, dta);
       if (kDt) dt_reduce(dtc, dta.out);
     }
   }
