@@ -305,6 +305,42 @@ GRB_HD void char_speeds(double alp, double betad, double rho, double press, doub
   cm = fmin(l1, l2);
   cp = fmax(l1, l2);
 }
+// Tuned-mode forms of the three helpers above: the same expressions with the
+// face's 1/alpha (ialp) and the side's 1/W (iW) computed once and multiplied
+// in, instead of 5 divisions by alpha and 2 by W per side; equal up to
+// rounding.
+GRB_HD void comoving_b_f(double alp, double ialp, const double beta[3], const double g[6], const double B[3],
+                         const double z[3], double W, double iW, double b[4], double& b2) {
+  double zl[3];
+  mvs(g, z, zl);
+  const double Bz = B[0] * zl[0] + B[1] * zl[1] + B[2] * zl[2];
+  const double b0 = Bz * ialp;
+  b[0] = b0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) b[i + 1] = (B[i] + alp * b0 * (z[i] - W * beta[i] * ialp)) * iW;
+  b2 = (sqs(g, B) + Bz * Bz) * iW * iW;
+}
+GRB_HD void vtilde_f(double alp, const double beta[3], const double z[3], double iW, double vt[3]) {
+  const double aw = alp * iW;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) vt[i] = aw * z[i] - beta[i];
+}
+GRB_HD void char_speeds_f(double ialp, double betad, double rho, double press, double eps, double cs2,
+                          double W, double b2, double vtd, double guu_dd, double& cm, double& cp) {
+  const double va2 = b2 / (b2 + rho * (1. + eps) + press);
+  const double c2 = va2 + cs2 * (1. - va2);
+  const double ia2 = ialp * ialp;
+  const double u0 = W * ialp;
+  const double ud = W * vtd * ialp;
+  const double A = (1. - c2) * u0 * u0 + c2 * ia2;
+  const double B = -2. * (1. - c2) * u0 * ud + 2. * c2 * betad * ia2;
+  const double C = (1. - c2) * ud * ud - c2 * (guu_dd - betad * betad * ia2);
+  const double disc = sqrt(fmax(0., B * B - 4. * A * C));
+  const double i2A = 0.5 / A;
+  const double l1 = (-B + disc) * i2A, l2 = (-B - disc) * i2A;
+  cm = fmin(l1, l2);
+  cp = fmax(l1, l2);
+}
 // conserved + fluxes along d (grmhd_subexpressions.hh:97-156, 294-331)
 struct ConsFlux {
   double D, tau, S[3], ents, fD, ftau, fS[3], fent;

@@ -33,16 +33,28 @@ __device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
   const double alp = m.alp, sqrtg = m.sqrtg;
   const double wl = lorentz(m.g, pl + GRB_P_ZX), wr = lorentz(m.g, pr + GRB_P_ZX);
   double bl[4], br[4], b2l, b2r, vtl[3], vtr[3];
-  comoving_b(alp, m.beta, m.g, pl + GRB_P_BX, pl + GRB_P_ZX, wl, bl, b2l);
-  comoving_b(alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, wr, br, b2r);
-  vtilde(alp, m.beta, pl + GRB_P_ZX, wl, vtl);
-  vtilde(alp, m.beta, pr + GRB_P_ZX, wr, vtr);
   const double gdd = dir == 0 ? m.gi[0] : dir == 1 ? m.gi[3] : m.gi[5];
   double cml, cpl, cmr, cpr, cmin, cmax;
-  char_speeds(alp, m.beta[dir], pl[GRB_P_RHO], pl[GRB_P_PRESS], pl[GRB_P_EPS], pl[GRB_P_CS2], wl,
-              b2l, vtl[dir], gdd, cml, cpl);
-  char_speeds(alp, m.beta[dir], pr[GRB_P_RHO], pr[GRB_P_PRESS], pr[GRB_P_EPS], pr[GRB_P_CS2], wr,
-              b2r, vtr[dir], gdd, cmr, cpr);
+  if (FAST) {
+    const double ialp = 1.0 / alp, iwl = 1.0 / wl, iwr = 1.0 / wr;
+    comoving_b_f(alp, ialp, m.beta, m.g, pl + GRB_P_BX, pl + GRB_P_ZX, wl, iwl, bl, b2l);
+    comoving_b_f(alp, ialp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, wr, iwr, br, b2r);
+    vtilde_f(alp, m.beta, pl + GRB_P_ZX, iwl, vtl);
+    vtilde_f(alp, m.beta, pr + GRB_P_ZX, iwr, vtr);
+    char_speeds_f(ialp, m.beta[dir], pl[GRB_P_RHO], pl[GRB_P_PRESS], pl[GRB_P_EPS], pl[GRB_P_CS2], wl, b2l,
+                  vtl[dir], gdd, cml, cpl);
+    char_speeds_f(ialp, m.beta[dir], pr[GRB_P_RHO], pr[GRB_P_PRESS], pr[GRB_P_EPS], pr[GRB_P_CS2], wr, b2r,
+                  vtr[dir], gdd, cmr, cpr);
+  } else {
+    comoving_b(alp, m.beta, m.g, pl + GRB_P_BX, pl + GRB_P_ZX, wl, bl, b2l);
+    comoving_b(alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, wr, br, b2r);
+    vtilde(alp, m.beta, pl + GRB_P_ZX, wl, vtl);
+    vtilde(alp, m.beta, pr + GRB_P_ZX, wr, vtr);
+    char_speeds(alp, m.beta[dir], pl[GRB_P_RHO], pl[GRB_P_PRESS], pl[GRB_P_EPS], pl[GRB_P_CS2], wl,
+                b2l, vtl[dir], gdd, cml, cpl);
+    char_speeds(alp, m.beta[dir], pr[GRB_P_RHO], pr[GRB_P_PRESS], pr[GRB_P_EPS], pr[GRB_P_CS2], wr,
+                b2r, vtr[dir], gdd, cmr, cpr);
+  }
   if (rusanov) {
     cmax = fmax(fmax(fabs(cml), fabs(cmr)), fmax(fabs(cpl), fabs(cpr)));
     if (fmin(pl[GRB_P_RHO], pr[GRB_P_RHO]) < P.rusanov_c_limit)
