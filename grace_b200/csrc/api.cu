@@ -319,16 +319,31 @@ void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, co
   else k_aux<1, false, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
 }
 
-// linop on the evolved HRSC variables and the face arrays only
-__global__ void k_linop_hrsc(Geo G, double* __restrict__ a, const double* __restrict__ x,
-                             const double* __restrict__ y, double b, double c) {
-  const int64_t per = G.cells * GRB_N_HRSC;
-  const int64_t n = per * G.nq;
-  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t q = t / per, r = t - q * per;
-    const int64_t o = q * G.cells * GRB_N_EVOL_VARS + r;
-    a[o] = y ? b * x[o] + c * y[o] : b * x[o];
-  }
+// A = b X (+ c Y) on the planes z in [zlo, zlo + nz) and rows y in [ylo,
+// ylo + ny) of a LayoutLeft array (N0, N1, N2, nv_total, nq) at full x
+// extent, for nv variables: each plane's rows are one contiguous span, so
+// every warp reads and writes consecutive doubles.  grid (span / 256,
+// nz * nv, nq); no 64-bit index division.
+struct LinBox {
+  int N0, N1, N2;
+  int ylo, ny, zlo, nz;
+  int64_t vstride, qstride;
+};
+__global__ void __launch_bounds__(256) k_linop_box(LinBox L, int nv, double* __restrict__ a,
+                                                   const double* __restrict__ x, const double* __restrict__ y,
+                                                   double b, double c) {
+  const int span = L.ny * L.N0;
+  const int e = blockIdx.x * 256 + threadIdx.x;
+  if (e >= span) return;
+  const int zi = blockIdx.y % L.nz, v = blockIdx.y / L.nz;
+  const int64_t o = (int64_t)v * L.vstride + (int64_t)blockIdx.z * L.qstride +
+                    ((int64_t)(L.zlo + zi) * L.N1 + L.ylo) * L.N0 + e;
+  a[o] = y ? b * x[o] + c * y[o] : b * x[o];
+}
+void launch_linop_box(cudaStream_t s, const LinBox& L, int nv, int64_t nq, double* a, const double* x,
+                      const double* y, double b, double c) {
+  const dim3 grid((unsigned)((L.ny * L.N0 + 255) / 256), (unsigned)(L.nz * nv), (unsigned)nq);
+  k_linop_box<<<grid, 256, 0, s>>>(L, nv, a, x, y, b, c);
 }
 
 // The stage in tuned mode: only the faces the stage reads, FAST flux math,
@@ -700,12 +715,23 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A, const
   const double* y[4] = {Cf ? Cf->state : nullptr, Cf ? Cf->bx : nullptr, Cf ? Cf->by : nullptr, Cf ? Cf->bz : nullptr};
   KScope ks(h, s, GRB_KIND_LINOP);
   if (h->mode == GRB_MODE_TUNED) {
-    // The Cowling metric and curvature are static: combine only the
-    // evolved HRSC variables (and the face arrays below).
-    k_linop_hrsc<<<148 * 16, 256, 0, s>>>(G, a[0], x[0], y[0], b, c);
+    // The Cowling metric and curvature are static, and the next stage reads
+    // the combination only on the HRSC variables of cells [g-2, n+g+2) (the
+    // FOFC flag window) and on the faces the CT update advances before the
+    // ghost exchange refills the rest: combine just those.
+    const int gz = G.g;
+    if (G.nq > 65535 || gz < 2) return fail(h, GRB_ERR_INVALID);
+    LinBox Lc{G.NX, G.NY, G.NZ, gz - 2, G.ny + 4, gz - 2, G.nz + 4, (int64_t)G.cells,
+              (int64_t)G.cells * GRB_N_EVOL_VARS};
+    launch_linop_box(s, Lc, GRB_N_HRSC, G.nq, a[0], x[0], y[0], b, c);
     ++h->launches;
-    for (int v = 1; v < 4; ++v) {
-      k_linop<<<148 * 16, 256, 0, s>>>(n[v], a[v], x[v], y[v], b, c);
+    for (int fd = 0; fd < 3; ++fd) {
+      int N[3] = {G.NX, G.NY, G.NZ}, nn[3] = {G.nx, G.ny, G.nz};
+      N[fd] += 1;
+      nn[fd] += 1;
+      const int64_t fc = (int64_t)N[0] * N[1] * N[2];
+      LinBox Lf{N[0], N[1], N[2], gz, nn[1], gz, nn[2], fc, fc};
+      launch_linop_box(s, Lf, 1, G.nq, a[1 + fd], x[1 + fd], y[1 + fd], b, c);
       ++h->launches;
     }
     CK(cudaGetLastError());

@@ -662,8 +662,8 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
   if (P.emf == GRB_EMF_GS) {
     const double W = sqrt(1. + sqs(m.g, pr + GRB_P_ZX));
     double vt[3];
-#pragma unroll
     const double iW = kFast ? 1.0 / W : 0.0;
+#pragma unroll
     for (int a = 0; a < 3; ++a) vt[a] = (kFast ? m.alp * pr[GRB_P_ZX + a] * iW : m.alp * pr[GRB_P_ZX + a] / W) - m.beta[a];
     B.ecenter[eci(G, i, j, k, 0, q)] = cby * vt[2] - cbz * vt[1];
     B.ecenter[eci(G, i, j, k, 1, q)] = -cbx * vt[2] + cbz * vt[0];

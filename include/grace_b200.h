@@ -215,7 +215,12 @@ int grb_find_stable_timestep(grb_handle* h, const grb_grid* g,
 int grb_reset_c2p_diagnostics(grb_handle* h, const grb_grid* g, double* aux,
                               void* stream);
 /* = grace::linop_apply (include/grace/utils/tstep_utils.hh:54-229):
- *   A = b*B (C == NULL) or A = b*B + c*C on cells and faces, all 23 vars. */
+ *   A = b*B (C == NULL) or A = b*B + c*C on cells and faces, all 23 vars.
+ *   GRB_MODE_TUNED combines only what the next advance_substep reads before
+ *   the ghost exchange: the 7 evolved HRSC variables on the cells with
+ *   y, z in [ngz-2, n+ngz+2) (all x) and the faces with y, z in the
+ *   interior (all x) (the metric is static in Cowling); the caller's ghost exchange must refill A's ghost zones before
+ *   anything else reads them, as evolve_impl does after every stage. */
 int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A,
                     const grb_fields* B, const grb_fields* C, double b,
                     double c, void* stream);
