@@ -1079,14 +1079,13 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
   cudaStream_t s = (cudaStream_t)stream;
   double* bf[3] = {f->bx, f->by, f->bz};
   KScope ks(h, s, GRB_KIND_GHOST);
-  for (int fd = -1; fd < 3; ++fd) {
-    int n[3] = {G.NX, G.NY, G.NZ};
-    if (fd >= 0) n[fd] += 1;
-    const int total = n[0] * n[1] * n[2];
-    const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq);
-    k_ghost<<<grid, 256, 0, s>>>(G, br, fd, fd < 0 ? f->state : bf[fd]);
-    ++h->launches;
-  }
+  // cells of the largest array (a face array)
+  const int64_t total = (int64_t)std::max({G.NX + 1, G.NY + 1, G.NZ + 1}) *
+                        std::max({G.NX * G.NY, G.NY * G.NZ, G.NX * G.NZ});
+  if (total > (1ll << 31) - 256) return fail(h, GRB_ERR_INVALID);
+  const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq, 4u);
+  k_ghost<<<grid, 256, 0, s>>>(G, br, f->state, bf[0], bf[1], bf[2]);
+  ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;
 }

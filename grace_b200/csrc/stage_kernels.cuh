@@ -775,17 +775,24 @@ __device__ __forceinline__ bool ghost_map(int x, int nin, int g, bool stag, bool
   }
   return false;
 }
-// `fd` = -1: cell-centred HRSC vars of `a`; 0..2: face array staggered
-// along fd.  One thread per cell of one block (blockIdx.y = q), x fastest.
-__global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, int fd, double* __restrict__ a) {
-  const int64_t q = blockIdx.y;
+// One launch for the four arrays: blockIdx.z = 0 the cell-centred HRSC
+// variables, 1..3 the face array staggered along blockIdx.z - 1.  One
+// thread per cell of one block (blockIdx.y = q), x fastest; 32-bit index
+// arithmetic (q < 65536, a block's cells < 2^31).
+__global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, double* __restrict__ cells,
+                                              double* __restrict__ fx, double* __restrict__ fy,
+                                              double* __restrict__ fz) {
+  const int fd = (int)blockIdx.z - 1;
+  const int q = blockIdx.y;
   int n[3] = {G.NX, G.NY, G.NZ};
   if (fd >= 0) n[fd] += 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n[0] * n[1] * n[2]) return;
+  double* a = fd < 0 ? cells : fd == 0 ? fx : fd == 1 ? fy : fz;
   const int nin[3] = {G.nx, G.ny, G.nz};
   const int nb[3] = {br.nbx, br.nby, br.nbz};
-  const int qc[3] = {(int)(q % br.nbx), (int)((q / br.nbx) % br.nby), (int)(q / ((int64_t)br.nbx * br.nby))};
+  const int qyz = q / br.nbx;
+  const int qc[3] = {q - qyz * br.nbx, qyz % br.nby, qyz / br.nby};
   const int c[3] = {t % n[0], (t / n[0]) % n[1], t / (n[0] * n[1])};
   int sidx[3], off[3];
   bool ghost = false;
@@ -796,12 +803,12 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, int fd, double* 
   int qs[3];
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax) qs[ax] = (qc[ax] + off[ax] + nb[ax]) % nb[ax];
-  const int64_t qsrc = qs[0] + (int64_t)br.nbx * (qs[1] + (int64_t)br.nby * qs[2]);
+  const int qsrc = qs[0] + br.nbx * (qs[1] + br.nby * qs[2]);
   const int nv = fd < 0 ? GRB_N_HRSC : 1;
   const int64_t vstride = (int64_t)n[0] * n[1] * n[2];
   const int64_t qstride = vstride * (fd < 0 ? GRB_N_EVOL_VARS : 1);
-  const int64_t ld = c[0] + (int64_t)n[0] * (c[1] + (int64_t)n[1] * c[2]) + q * qstride;
-  const int64_t ls = sidx[0] + (int64_t)n[0] * (sidx[1] + (int64_t)n[1] * sidx[2]) + qsrc * qstride;
+  const int64_t ld = (c[0] + n[0] * (c[1] + n[1] * c[2])) + (int64_t)q * qstride;
+  const int64_t ls = (sidx[0] + n[0] * (sidx[1] + n[1] * sidx[2])) + (int64_t)qsrc * qstride;
   double tmp[GRB_N_HRSC];
 #pragma unroll
   for (int v = 0; v < GRB_N_HRSC; ++v)

@@ -99,6 +99,25 @@ def test_tuned_flux_candidates_match_oracle(name, flux):
     assert g.status().device_flags == 0
 
 
+@pytest.mark.parametrize("flux", [0, 1])
+@pytest.mark.parametrize("recon", [abi.RECON_MC2, abi.RECON_MINMOD, abi.RECON_DONOR])
+def test_tuned_flux_reconstructions_match_oracle(recon, flux):
+    """The per-cell reconstruction of the TMA-staged flux kernel (both face
+    values of a cell at once) and the per-face one of the global-load
+    kernel, for the limiter and donor schemes, within the step tolerance of
+    the oracle on the blast wave."""
+    P, su, f, dt = _setup("blast")
+    P.recon = recon
+    gs, ga, g = _gpu_run(P, su, f, dt, 1, abi.MODE_TUNED, tuning=(flux, 0, 0, 0))
+    os_, oa, S = _oracle_run(P, su, f, dt, 1)
+    e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
+    assert e.max() < STEP_TOL, e
+    for a, b in zip(gs[1:], os_[1:]):
+        d = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+        assert d < STEP_TOL
+    assert g.status().device_flags == 0
+
+
 @pytest.mark.parametrize("aux", [3, 4, 5])
 @pytest.mark.parametrize("name", ["blast", "balsara"])
 def test_aux_work_queue_matches_oracle(name, aux):
@@ -272,4 +291,27 @@ def test_curved_metric_step_matches_oracle(emf, mode):
         assert d < STEP_TOL
     bmax = max(np.max(np.abs(x)) for x in gs[1:])
     assert np.max(np.abs(interior(ga[:, abi.BDIV], su.ngz))) * su.dx[0] < 1e-13 * bmax
+    assert g.status().device_flags == 0
+
+
+@pytest.mark.parametrize("tuning", [None, (0, 0, 0, 0), (1, 0, 0, 0)])
+def test_curved_excision_donor_faces_match_oracle(tuning):
+    """Excision by lapse on the curved setup: with alp_ex = 0.8 the cells
+    with x below ~3.56 are excised by the c2p and every face next to one is
+    a donor face (first-order states, grmhd.hh getflux); plain mode and both
+    tuned flux kernels against the oracle."""
+    from curved import curved_setup
+    P, su, f = curved_setup(emf=abi.EMF_GS, fofc=1)
+    P.alp_ex = 0.8
+    alp = f[0][:, abi.ALP]
+    assert alp.min() < 0.8 < alp.max()
+    dt = 0.25 / su.idx()[0, 0]
+    mode = abi.MODE_PLAIN if tuning is None else abi.MODE_TUNED
+    gs, ga, g = _gpu_run(P, su, f, dt, 1, mode, tuning=tuning)
+    os_, oa, S = _oracle_run(P, su, f, dt, 1)
+    e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
+    assert e.max() < STEP_TOL, e
+    for a, b in zip(gs[1:], os_[1:]):
+        d = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
+        assert d < STEP_TOL
     assert g.status().device_flags == 0
