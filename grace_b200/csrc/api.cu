@@ -136,6 +136,7 @@ inline Box box(int l0, int l1, int l2, int n0, int n1, int n2, int64_t nq) {
   b.lo[0] = l0; b.lo[1] = l1; b.lo[2] = l2;
   b.n[0] = n0; b.n[1] = n1; b.n[2] = n2;
   b.nq = nq;
+  for (int a = 0; a < 3; ++a) b.dv[a] = make_fastdiv((uint32_t)std::max(b.n[a], 1));
   return b;
 }
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }

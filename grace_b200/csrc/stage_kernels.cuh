@@ -9,6 +9,7 @@
 //   linop_apply             include/grace/utils/tstep_utils.hh:54-229
 #pragma once
 #include "c2p.cuh"
+#include "fastdiv.cuh"
 #include "layout.cuh"
 
 namespace grb {
@@ -167,13 +168,26 @@ __device__ __forceinline__ void store_face(const Geo& G, const StageBufs& B, int
 }
 
 // Box of items: [lo, hi) per axis, decoded from a linear thread index.
+// dv: the divisors n[0..2], set by the host (box()); an unset or stale
+// divisor sends decode to the 64-bit division path.
 struct Box {
   int lo[3], n[3];
   int64_t nq;
+  FastDiv dv[3];
   __host__ __device__ int64_t count() const { return (int64_t)n[0] * n[1] * n[2] * nq; }
 };
 __device__ __forceinline__ bool decode(const Box& b, int64_t t, int& i, int& j, int& k, int64_t& q) {
   if (t >= b.count()) return false;
+  if (t <= 0xffffffffll && b.dv[0].d == (uint32_t)b.n[0] && b.dv[1].d == (uint32_t)b.n[1] &&
+      b.dv[2].d == (uint32_t)b.n[2]) {
+    const uint32_t u = (uint32_t)t;
+    const uint32_t u1 = fast_div(u, b.dv[0]), u2 = fast_div(u1, b.dv[1]), u3 = fast_div(u2, b.dv[2]);
+    i = b.lo[0] + (int)(u - u1 * (uint32_t)b.n[0]);
+    j = b.lo[1] + (int)(u1 - u2 * (uint32_t)b.n[1]);
+    k = b.lo[2] + (int)(u2 - u3 * (uint32_t)b.n[2]);
+    q = u3;
+    return true;
+  }
   i = b.lo[0] + (int)(t % b.n[0]); t /= b.n[0];
   j = b.lo[1] + (int)(t % b.n[1]); t /= b.n[1];
   k = b.lo[2] + (int)(t % b.n[2]); t /= b.n[2];
