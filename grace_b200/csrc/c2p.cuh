@@ -359,6 +359,53 @@ GRB_HD void prims_to_cons(const double pr[13], double c[10], const Met& m) {
   c[5] = c[0] * pr[GRB_P_YE];
 }
 
+// Lorentz factor and comoving-field scalars of one set of primitives (tuned
+// mode), kept while z and B stay unchanged: z2 = z_i z^i, W = sqrt(1 + z2),
+// Bz = B^i z_i, b^2 = (B_i B^i + Bz^2) / W^2 (comoving_b's b^2).
+struct WB {
+  double z2, W, iW, Bz, b2;
+};
+GRB_HD WB wb_of(const Met& m, const double pr[13]) {
+  WB o;
+  double zl[3];
+  mvs(m.g, pr + GRB_P_ZX, zl);
+  const double* z = pr + GRB_P_ZX;
+  const double* B = pr + GRB_P_BX;
+  o.z2 = z[0] * zl[0] + z[1] * zl[1] + z[2] * zl[2];
+  o.W = sqrt(1. + o.z2);
+  o.iW = 1.0 / o.W;
+  o.Bz = B[0] * zl[0] + B[1] * zl[1] + B[2] * zl[2];
+  o.b2 = (sqs(m.g, B) + o.Bz * o.Bz) * o.iW * o.iW;
+  return o;
+}
+// prims_to_cons from a cached WB; with `need` holding no ERR_RESET_STILDE
+// or ERR_RESET_TAU bit the momenta and tau (and b^mu) are not formed (D,
+// Ye* and the entropy density always are).
+GRB_HD void prims_to_cons_wb(const double pr[13], double c[10], const Met& m, const WB& q, double ialp,
+                             uint32_t need) {
+  const double D = pr[GRB_P_RHO] * q.W;
+  c[0] = m.sqrtg * D;
+  c[6] = m.sqrtg * (pr[GRB_P_ENT] * D);
+  c[5] = c[0] * pr[GRB_P_YE];
+  if (need & (ERR_RESET_STILDE | ERR_RESET_TAU)) {
+    const double b0 = q.Bz * ialp;
+    double b[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      b[i] = (pr[GRB_P_BX + i] + m.alp * b0 * (pr[GRB_P_ZX + i] - q.W * m.beta[i] * ialp)) * q.iW;
+    const double rhoh = pr[GRB_P_RHO] * (1. + pr[GRB_P_EPS]) + pr[GRB_P_PRESS] + q.b2;
+    const double pstar = pr[GRB_P_PRESS] + 0.5 * q.b2;
+    double bl[3], betal[3], zl[3];
+    mvs(m.g, b, bl);
+    mvs(m.g, m.beta, betal);
+    mvs(m.g, pr + GRB_P_ZX, zl);
+    const double tau = rhoh * q.W * q.W - pstar - m.alp * m.alp * b0 * b0 - D;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) c[1 + i] = m.sqrtg * (rhoh * q.W * zl[i] - m.alp * b0 * (bl[i] + betal[i] * b0));
+    c[4] = m.sqrtg * tau;
+  }
+}
+
 GRB_HD void handle_sig(uint32_t sig, bool lenient, uint32_t& err, uint32_t& fatal) {
   if (sig & SIG_RHO_HIGH) {
     err |= ERR_SIG_RHO_HIGH | ERR_ALL_RESETS;
@@ -409,17 +456,24 @@ struct C2POut {
   bool floored;
   bool guess_used;
   double mu;  // Kastaun root, 0 where the Kastaun solve did not run
+  double W, iW;  // Lorentz factor of the final primitives (tuned mode)
 };
 
 // conservs_to_prims (c2p.cpp:188-414).  c: densitized cons with densitized
 // cell-centred B (in), re-densitized consistent cons (out).
 // FAST (tuned mode): multiplications by 1/sqrt(gamma) and 1/D where the
-// reference divides repeatedly by the same value, and the FAST master
-// function; equal to the reference's operations up to rounding.
-template <bool FAST = false>
+// reference divides repeatedly by the same value, the FAST master function,
+// and W, b^mu, b^2 formed once per set of primitives (WB) instead of in
+// each of the beta test, limit_primitives and prims_to_cons; equal to the
+// reference's operations up to rounding.  kAllCons false (tuned mode):
+// the returned cons hold only what the reset flags in o.err ask for.
+template <bool FAST = false, bool kAllCons = true>
 GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P, double r_sph,
                   bool dry_run, double alp_bh_thresh, const Guess& gs) {
-  C2POut o{0u, 0u, 0, false, false, 0.0};
+  C2POut o{0u, 0u, 0, false, false, 0.0, 0.0, 0.0};
+  const double ialp = FAST ? 1.0 / m.alp : 0.0;
+  WB wb{};
+  bool wb_ok = false;  // wb belongs to the current z and B
   const DevEos& e = P.eos;
   bool failed = false;
   uint32_t ret = 0;
@@ -464,7 +518,11 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
     const double res = kastaun_invert<FAST>(e, m, c, pr, ret, o.iters, g2, o.guess_used, o.mu);
     failed = (fabs(res) > P.tol) || (ret & SIG_RHO_HIGH) || (ret & SIG_EPS_HIGH) || !isfinite(res);
     double beta;
-    {
+    if (FAST) {
+      wb = wb_of(m, pr);
+      wb_ok = true;
+      beta = 2.0 * pr[GRB_P_PRESS] / fmax(wb.b2, 1e-50);
+    } else {
       const double W = lorentz(m.g, pr + GRB_P_ZX);
       double b[4], b2;
       comoving_b(m.alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, W, b, b2);
@@ -482,9 +540,12 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
         ret = bret;
         failed = false;
         o.err |= ERR_ENT_BACKUP;
+        wb_ok = false;
       } else if (!failed) {
 #pragma unroll
         for (int v = 0; v < 13; ++v) pr[v] = save[v];
+      } else {
+        wb_ok = false;
       }
     }
     if (ret & (SIG_EPS_HIGH | SIG_RHO_LOW | SIG_RHO_HIGH | SIG_VEL_HIGH)) o.floored = true;
@@ -497,6 +558,7 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
   if (failed || excise || pr[GRB_P_RHO] < (1. + P.atmo_tol) * P.rho_fl) {
     reset_atmo(c, pr, m, P, o.err);
     o.floored = true;
+    wb_ok = false;
   } else if (pr[GRB_P_TEMP] < P.temp_fl) {
     pr[GRB_P_TEMP] = P.temp_fl;
     double cs2;
@@ -508,15 +570,22 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
   } else {  // limit_primitives (c2p.cpp:63-115)
     uint32_t s2 = 0;
     const double z2max = P.max_w * P.max_w - 1.;
-    const double z2 = sqs(m.g, pr + GRB_P_ZX);
+    if (FAST && !wb_ok) { wb = wb_of(m, pr); wb_ok = true; }
+    const double z2 = FAST ? wb.z2 : sqs(m.g, pr + GRB_P_ZX);
     if (z2 >= z2max) {
       const double zn = 0.99 * sqrt(z2max / z2);
       pr[GRB_P_ZX] *= zn; pr[GRB_P_ZY] *= zn; pr[GRB_P_ZZ] *= zn;
       s2 |= SIG_VEL_HIGH;
+      if (FAST) wb = wb_of(m, pr);
     }
-    const double W = lorentz(m.g, pr + GRB_P_ZX);
-    double b[4], b2;
-    comoving_b(m.alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, W, b, b2);
+    double b2;
+    if (FAST) {
+      b2 = wb.b2;
+    } else {
+      const double W = lorentz(m.g, pr + GRB_P_ZX);
+      double b[4];
+      comoving_b(m.alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, W, b, b2);
+    }
     const double sigma = b2 / pr[GRB_P_RHO];
     if (sigma >= P.max_sigma) {
       pr[GRB_P_RHO] *= 1.001 * sigma / P.max_sigma;
@@ -528,7 +597,14 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
     handle_sig(s2, lenient, o.err, o.fatal);
     if (s2 & (SIG_VEL_HIGH | SIG_SIGMA_HIGH)) o.floored = true;
   }
-  prims_to_cons(pr, c, m);
+  if (FAST) {
+    if (!wb_ok) wb = wb_of(m, pr);
+    prims_to_cons_wb(pr, c, m, wb, ialp, kAllCons ? ~0u : o.err);
+    o.W = wb.W;
+    o.iW = wb.iW;
+  } else {
+    prims_to_cons(pr, c, m);
+  }
   return o;
 }
 

@@ -645,7 +645,8 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
   const double cbx = c[7], cby = c[8], cbz = c[9];
   double pr[13];
   const Guess none = no_guess();
-  const C2POut o = c2p<kFast>(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), false, P.alp_bh_thresh, none);
+  const C2POut o =
+      c2p<kFast, !kFast>(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), false, P.alp_bh_thresh, none);
   if (o.fatal) atomicOr(B.flags, o.fatal);
   aux[a0 + G.cells * GRB_RHO] = pr[GRB_P_RHO];
   aux[a0 + G.cells * GRB_EPS] = pr[GRB_P_EPS];
@@ -674,11 +675,12 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
     aux[a0 + G.cells * GRB_BDIV] = kFast ? dv * isg : dv / m.sqrtg;
   }
   if (P.emf == GRB_EMF_GS) {
-    const double W = sqrt(1. + sqs(m.g, pr + GRB_P_ZX));
+    // tuned mode: 1/W of the final primitives from the c2p
+    const double W = kFast ? o.W : sqrt(1. + sqs(m.g, pr + GRB_P_ZX));
     double vt[3];
-    const double iW = kFast ? 1.0 / W : 0.0;
 #pragma unroll
-    for (int a = 0; a < 3; ++a) vt[a] = (kFast ? m.alp * pr[GRB_P_ZX + a] * iW : m.alp * pr[GRB_P_ZX + a] / W) - m.beta[a];
+    for (int a = 0; a < 3; ++a)
+      vt[a] = (kFast ? m.alp * pr[GRB_P_ZX + a] * o.iW : m.alp * pr[GRB_P_ZX + a] / W) - m.beta[a];
     B.ecenter[eci(G, i, j, k, 0, q)] = cby * vt[2] - cbz * vt[1];
     B.ecenter[eci(G, i, j, k, 1, q)] = -cbx * vt[2] + cbz * vt[0];
     B.ecenter[eci(G, i, j, k, 2, q)] = cbx * vt[1] - cby * vt[0];
