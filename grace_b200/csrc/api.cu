@@ -52,6 +52,9 @@ struct grb_handle {
   float* d_mlp = nullptr;
   MlpSmem* d_mlp_pack = nullptr;  // shared-memory image of the network
   unsigned long long* d_queue = nullptr;  // work-queue counter of the aux pass
+  uint32_t* d_auxlist = nullptr;          // cells of the tuned aux pass in one block
+  uint32_t auxlist_n = 0;
+  int auxlist_key[4] = {0, 0, 0, 0};      // nx, ny, nz, ngz it was built for
   float tune_aux_queue_ms = 0.f;
   bool mlp_ready = false;
 };
@@ -504,6 +507,7 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_mlp);
   cudaFree(h->d_mlp_pack);
   cudaFree(h->d_queue);
+  cudaFree(h->d_auxlist);
   delete h;
   return GRB_OK;
 }
@@ -641,6 +645,60 @@ int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g, const grb
   return grb_compute_auxiliary_quantities_dt(h, g, st, aux, nullptr, 0.0, nullptr, stream);
 }
 
+// The cells whose primitives (and c2p resets) the next tuned stage reads
+// before the ghost exchange refills the rest, with the Gardiner-Stone EMF:
+// the face fluxes reconstruct along each axis over the whole block from
+// cells whose two other indices lie in [g-1, n+g+1) (cells with at least
+// two indices there), and the FOFC flag's DMP test reads the new
+// conservatives, which the c2p may reset, on [g-2, n+g+2)^3.  The flag, the
+// FOFC face and edge corrections, the cell-centred E of the EMF and the
+// update stay inside these.  Packed i | j << 8 | k << 16, x fastest.
+std::vector<uint32_t> tuned_aux_cells(const Geo& G) {
+  const int N[3] = {G.NX, G.NY, G.NZ}, n[3] = {G.nx, G.ny, G.nz};
+  std::vector<uint32_t> v;
+  for (int k = 0; k < N[2]; ++k)
+    for (int j = 0; j < N[1]; ++j)
+      for (int i = 0; i < N[0]; ++i) {
+        const int c[3] = {i, j, k};
+        int in_t = 0, in_d = 0;
+        for (int a = 0; a < 3; ++a) {
+          in_t += c[a] >= G.g - 1 && c[a] < n[a] + G.g + 1;
+          in_d += c[a] >= G.g - 2 && c[a] < n[a] + G.g + 2;
+        }
+        if (in_t >= 2 || in_d == 3) v.push_back((uint32_t)i | (uint32_t)j << 8 | (uint32_t)k << 16);
+      }
+  return v;
+}
+// The aux box of the tuned mode: the cell list above when it applies (GS
+// EMF, blocks up to 256 cells a side, the list already built for this
+// geometry or buildable now, i.e. not inside a stream capture), else the
+// whole block.
+Box tuned_aux_box(grb_handle* h, const Geo& G, cudaStream_t s) {
+  Box b = box(0, 0, 0, G.NX, G.NY, G.NZ, G.nq);
+  if (h->dp.emf != GRB_EMF_GS || G.NX > 256 || G.NY > 256 || G.NZ > 256 || G.g < 2) return b;
+  const int key[4] = {G.nx, G.ny, G.nz, G.g};
+  if (!h->d_auxlist || !std::equal(key, key + 4, h->auxlist_key)) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return b;
+    const std::vector<uint32_t> v = tuned_aux_cells(G);
+    uint32_t* d = nullptr;
+    if (cudaMalloc(&d, v.size() * sizeof(uint32_t)) != cudaSuccess) return b;
+    if (cudaMemcpy(d, v.data(), v.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+      cudaFree(d);
+      return b;
+    }
+    cudaFree(h->d_auxlist);
+    h->d_auxlist = d;
+    h->auxlist_n = (uint32_t)v.size();
+    std::copy(key, key + 4, h->auxlist_key);
+  }
+  if ((int64_t)h->auxlist_n * G.nq >= (1ll << 32)) return b;
+  b.list = h->d_auxlist;
+  b.nlist = h->auxlist_n;
+  b.dl = make_fastdiv(h->auxlist_n);
+  return b;
+}
+
 int grb_compute_auxiliary_quantities_dt(grb_handle* h, const grb_grid* g, const grb_fields* st, double* aux,
                                         const double* dx, double cfl, double* dt_out, void* stream) {
   if (!h) return GRB_ERR_INVALID;
@@ -658,7 +716,8 @@ int grb_compute_auxiliary_quantities_dt(grb_handle* h, const grb_grid* g, const 
     ++h->launches;
   }
   if (h->mode == GRB_MODE_TUNED) {
-    launch_aux_tuned(h->var_aux, nblk(b.count(), 128), s, h->dp, G, b, st->state, st->bx, st->by, st->bz, aux,
+    const Box tb = tuned_aux_box(h, G, s);
+    launch_aux_tuned(h->var_aux, nblk(tb.count(), 128), s, h->dp, G, tb, st->state, st->bx, st->by, st->bz, aux,
                      g->idx, g->coords, h->B, dt_out ? &dta : nullptr, h->d_queue);
   } else if (dt_out) {
     k_aux<1, true><<<nblk(b.count(), 128), 128, 0, s>>>(h->dp, G, b, st->state, st->bx, st->by, st->bz, aux,
@@ -1170,7 +1229,8 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
   const Box fbx = box(lo[0], lo[1], lo[2], n[0], n[1], n[2], nt);
   const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, nt);
   const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, nt);
-  const Box ab = box(0, 0, 0, G.NX, G.NY, G.NZ, nt);
+  Box ab = tuned_aux_box(h, G, s);
+  ab.nq = nt;
   int best[4] = {0, 0, 0, 0};
   for (int fam = 0; fam < 4; ++fam) {
     float bt = 1e30f;

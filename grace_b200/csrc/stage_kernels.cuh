@@ -169,15 +169,32 @@ __device__ __forceinline__ void store_face(const Geo& G, const StageBufs& B, int
 
 // Box of items: [lo, hi) per axis, decoded from a linear thread index.
 // dv: the divisors n[0..2], set by the host (box()); an unset or stale
-// divisor sends decode to the 64-bit division path.
+// divisor sends decode to the 64-bit division path.  list (optional): the
+// items are instead the nlist cells of list[] in every block, each packed as
+// i | j << 8 | k << 16 (dl: the divisor nlist; nlist * nq < 2^32).
 struct Box {
   int lo[3], n[3];
   int64_t nq;
   FastDiv dv[3];
-  __host__ __device__ int64_t count() const { return (int64_t)n[0] * n[1] * n[2] * nq; }
+  const uint32_t* list = nullptr;
+  uint32_t nlist = 0;
+  FastDiv dl;
+  __host__ __device__ int64_t count() const {
+    return list ? (int64_t)nlist * nq : (int64_t)n[0] * n[1] * n[2] * nq;
+  }
 };
 __device__ __forceinline__ bool decode(const Box& b, int64_t t, int& i, int& j, int& k, int64_t& q) {
   if (t >= b.count()) return false;
+  if (b.list) {
+    const uint32_t u = (uint32_t)t;
+    const uint32_t qq = fast_div(u, b.dl);
+    const uint32_t c = __ldg(b.list + (u - qq * b.nlist));
+    i = (int)(c & 0xffu);
+    j = (int)((c >> 8) & 0xffu);
+    k = (int)(c >> 16);
+    q = qq;
+    return true;
+  }
   if (t <= 0xffffffffll && b.dv[0].d == (uint32_t)b.n[0] && b.dv[1].d == (uint32_t)b.n[1] &&
       b.dv[2].d == (uint32_t)b.n[2]) {
     const uint32_t u = (uint32_t)t;

@@ -189,7 +189,12 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt,
 /* = grace::compute_auxiliary_quantities<eos_t>(state, sstate, aux)
  *   (src/evolution/auxiliaries.cpp:81-180): c2p on every cell including
  *   ghosts, conservative rewrites, C2P_ERR sticky-OR, BDIV, and (GS) the
- *   cell-centred E used by the next stage's EMF. */
+ *   cell-centred E used by the next stage's EMF.
+ *   GRB_MODE_TUNED with the GS EMF covers only the cells the next
+ *   advance_substep reads before the ghost exchange refills the rest: those
+ *   with at least two indices in [ngz-1, n+ngz+1), and [ngz-2, n+ngz+2)^3
+ *   (14 % fewer cells for 16^3 blocks with 4 ghosts); aux and the
+ *   conservative rewrites of the other ghost cells are left as they were. */
 int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g,
                                      const grb_fields* state, double* aux,
                                      void* stream);

@@ -62,3 +62,19 @@ def prim_tol(prims):
     points of the tolerance window differ by up to ~1e-13 W^2."""
     W = np.sqrt(1.0 + np.sum(prims[abi.P_ZX:abi.P_ZZ + 1] ** 2, axis=0))
     return PRIM_TOL * np.maximum(1.0, W * W)
+
+
+def tuned_aux_mask(su):
+    """Cells that the tuned aux pass (GS EMF) maintains in every block: at
+    least two indices in [g-1, n+g+1), or all three in [g-2, n+g+2).
+    Boolean array (NZ, NY, NX)."""
+    g = su.ngz
+    axes = []
+    for n in (su.n[2], su.n[1], su.n[0]):
+        c = np.arange(n + 2 * g)
+        axes.append(((c >= g - 1) & (c < n + g + 1), (c >= g - 2) & (c < n + g + 2)))
+    tz, ty, tx = (a[0] for a in axes)
+    dz, dy, dx = (a[1] for a in axes)
+    T = (tz[:, None, None].astype(int) + ty[None, :, None].astype(int) + tx[None, None, :].astype(int))
+    D = dz[:, None, None] & dy[None, :, None] & dx[None, None, :]
+    return (T >= 2) | D
