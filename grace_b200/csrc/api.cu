@@ -1151,6 +1151,54 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
 }
 
 
+// Device view of a host array: the pointer the GPU uses for page-locked,
+// mapped host memory, or null.
+static double* host_view(double* p) {
+  cudaPointerAttributes a;
+  if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+  return static_cast<double*>(a.devicePointer);
+}
+
+int grb_copy_evolved_interior(grb_handle* h, const grb_grid* g, const grb_fields* host, int32_t host_state_nvars,
+                              const grb_fields* dev, int32_t to_device, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!g || !host || !dev || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->ngz < 1 || g->nq < 1 ||
+      (host_state_nvars != GRB_N_HRSC && host_state_nvars != GRB_N_EVOL_VARS))
+    return fail(h, GRB_ERR_INVALID);
+  double* hv[4] = {host_view(host->state), host_view(host->bx), host_view(host->by), host_view(host->bz)};
+  double* dv[4] = {dev->state, dev->bx, dev->by, dev->bz};
+  for (int a = 0; a < 4; ++a)
+    if (!hv[a] || !dv[a]) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  if ((int64_t)GRB_N_HRSC * G.nq >= (1ll << 32) - 1) return fail(h, GRB_ERR_INVALID);
+  cudaStream_t s = (cudaStream_t)stream;
+  KScope ks(h, s, GRB_KIND_OTHER);
+  for (int a = 0; a < 4; ++a) {
+    int N[3] = {G.NX, G.NY, G.NZ}, n[3] = {G.nx, G.ny, G.nz};
+    if (a > 0) { N[a - 1] += 1; n[a - 1] += 1; }
+    const int nv = a == 0 ? GRB_N_HRSC : 1;
+    const int64_t vstride = (int64_t)N[0] * N[1] * N[2];
+    const int64_t qdev = vstride * (a == 0 ? GRB_N_EVOL_VARS : 1);
+    const int64_t qhost = vstride * (a == 0 ? host_state_nvars : 1);
+    double* dst = to_device ? dv[a] : hv[a];
+    const double* src = to_device ? hv[a] : dv[a];
+    const int64_t qd = to_device ? qdev : qhost, qs = to_device ? qhost : qdev;
+    // whole rows of the interior (y, z) range; an upload stores only the
+    // interior x, a download also the x-ghosts of those rows
+    const Box b = box(0, G.g, G.g, N[0], n[1], n[2], (int64_t)nv * G.nq);
+    const int xlo = to_device ? G.g : 0, xhi = to_device ? G.g + n[0] : N[0];
+    k_copy_rows<<<nblk(b.count(), 256), 256, 0, s>>>(b, xlo, xhi, nv, make_fastdiv((uint32_t)nv), N[0], N[1],
+                                                     vstride, qd, qs, dst, src);
+    ++h->launches;
+  }
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
 int grb_set_mode(grb_handle* h, int32_t mode) {
   if (!h || (mode != GRB_MODE_PLAIN && mode != GRB_MODE_TUNED)) return GRB_ERR_INVALID;
   h->mode = mode;

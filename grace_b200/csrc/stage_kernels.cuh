@@ -851,4 +851,25 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, double* __restri
     if (v < nv) a[ld + v * vstride] = tmp[v];
 }
 
+// Interior rows of one array between device memory and mapped host
+// memory.  box: rows at full x extent (x = 0 .. N0-1) of the interior y and
+// z ranges, x (nv variables x nq blocks) folded into the box's block index,
+// so each (variable, block, z) plane is one contiguous run of memory that
+// the bus moves in whole lines; dst and src are LayoutLeft arrays with the
+// same cell layout, variable stride vstride and block strides qdst, qsrc
+// (doubles).  Only x in [xlo, xhi) is stored (the loads cover the whole
+// row, volatile so that they are not narrowed to the stored part).
+__global__ void __launch_bounds__(256) k_copy_rows(Box box, int xlo, int xhi, int nv, FastDiv dnv, int N0,
+                                                    int N1, int64_t vstride, int64_t qdst, int64_t qsrc,
+                                                    double* dst, const double* src) {
+  int i, j, k;
+  int64_t qv;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, qv)) return;
+  const uint32_t q = fast_div((uint32_t)qv, dnv);
+  const uint32_t v = (uint32_t)qv - q * (uint32_t)nv;
+  const int64_t o = (int64_t)v * vstride + ((int64_t)k * N1 + j) * N0 + i;
+  const double x = *reinterpret_cast<const volatile double*>(src + o + (int64_t)q * qsrc);
+  if (i >= xlo && i < xhi) dst[o + (int64_t)q * qdst] = x;
+}
+
 }  // namespace grb

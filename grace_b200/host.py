@@ -170,6 +170,26 @@ class GRMHDEquationsSystem:
         _lib.check(self.lib.grb_fill_ghosts_brick(self.h, ctypes.byref(g), ctypes.byref(f), nb[0], nb[1],
                                                   nb[2], per, _stream_ptr(stream)), "grb_fill_ghosts_brick")
 
+    def copy_evolved_interior(self, host, dev, to_device, stream=None):
+        """Interior of the evolved variables between pinned host tensors and
+        the device Fields `dev` (grb_copy_evolved_interior).  host: Fields of
+        pinned CPU tensors shaped like dev's, except that host.state may hold
+        only the 7 HRSC variables, (nq, 7, NZ, NY, NX)."""
+        for h, d in zip((host.state, host.bx, host.by, host.bz), (dev.state, dev.bx, dev.by, dev.bz)):
+            if h.device.type != "cpu" or not h.is_pinned() or not h.is_contiguous() or h.dtype != torch.float64:
+                raise ValueError("host arrays must be contiguous pinned float64 CPU tensors")
+            if h is not host.state and tuple(h.shape) != tuple(d.shape):
+                raise ValueError("host face array shape differs from the device one")
+        nv = host.state.shape[1]
+        if tuple(host.state.shape) != (dev.state.shape[0], nv) + tuple(dev.state.shape[2:]) or \
+                nv not in (abi.N_HRSC, dev.state.shape[1]):
+            raise ValueError("host state must be (nq, 7 or 23, NZ, NY, NX) like the device state")
+        g = self.blocks.c()
+        fh, fd = host.c(), dev.c()
+        _lib.check(self.lib.grb_copy_evolved_interior(self.h, ctypes.byref(g), ctypes.byref(fh), int(nv),
+                                                      ctypes.byref(fd), 1 if to_device else 0,
+                                                      _stream_ptr(stream)), "grb_copy_evolved_interior")
+
     def conservs_to_prims(self, cons, metric=None, cons_out=None, err=None, use_learned=False,
                           stream=None, diag=None):
         """Batched c2p: cons (10, n) float64 -> prims (13, n).  diag: dict

@@ -378,6 +378,23 @@ int grb_kernel_times(grb_handle* h, double* ms, int64_t* counts, int32_t nkinds)
  * 7 evolved HRSC variables and the three face-B arrays. */
 int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
                           int32_t nby, int32_t nbz, const int32_t* periodic, void* stream);
+/* No counterpart in the reference (its state stays on the device): copies
+ * the interior of the evolved variables, i.e. the 7 HRSC variables on the
+ * interior cells and the three face-B arrays on the interior faces
+ * (staggered index in [ngz, n+ngz]), between host arrays and the device
+ * arrays `dev` of the same layout, to_device = 1 host -> device, 0 device ->
+ * host.  host_state_nvars: variables per block in host->state, either
+ * GRB_N_EVOL_VARS (the device layout) or GRB_N_HRSC (the evolved
+ * variables only).  The host arrays must be pinned and mapped (cudaHostAlloc, or any
+ * page-locked allocation visible to the device); one kernel per array
+ * reads or writes them over the bus in whole rows of the interior (y, z)
+ * range.  An upload leaves the device ghost zones as they were (refill them
+ * with the ghost exchange); a download also writes the x-ghost cells of the
+ * interior rows of the host arrays.  GRB_ERR_INVALID when a host array is
+ * not device-accessible. */
+int grb_copy_evolved_interior(grb_handle* h, const grb_grid* g, const grb_fields* host,
+                              int32_t host_state_nvars, const grb_fields* dev, int32_t to_device,
+                              void* stream);
 
 /* ---- scratch-free stage -------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -1,0 +1,108 @@
+"""Interior copies between pinned host memory and the device
+(grb_copy_evolved_interior): exact round trips, ghost zones untouched, and
+upload + ghost fill equal to copying whole arrays."""
+import numpy as np
+import pytest
+import torch
+
+from grace_b200 import abi, params, workloads
+from grace_b200.host import Blocks, Fields, GRMHDEquationsSystem
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(su, P):
+    dev = torch.device("cuda:0")
+    blocks = Blocks(su.n[0], su.n[1], su.n[2], su.ngz, su.nq, su.idx(), device=dev)
+    g = GRMHDEquationsSystem(P)
+    g.reserve(blocks)
+    return g, dev
+
+
+def _interior_masks(su, whole_rows=False):
+    """Interior cells / faces of the cell array and the three face arrays;
+    whole_rows: the rows of the interior (y, z) range at every x."""
+    g = su.ngz
+    nx, ny, nz = su.n
+    NX, NY, NZ = nx + 2 * g, ny + 2 * g, nz + 2 * g
+
+    def m(shape, stag):
+        out = np.zeros(shape, dtype=bool)
+        hi = [nz + g, ny + g, nx + g]
+        if stag is not None:
+            hi[stag] += 1
+        out[g:hi[0], g:hi[1], (0 if whole_rows else g):(shape[2] if whole_rows else hi[2])] = True
+        return out
+    return (m((NZ, NY, NX), None), m((NZ, NY, NX + 1), 2), m((NZ, NY + 1, NX), 1),
+            m((NZ + 1, NY, NX), 0))
+
+
+@pytest.mark.parametrize("nvars", [abi.N_HRSC, abi.N_EVOL_VARS])
+def test_interior_round_trip_is_exact(nvars):
+    su, f = workloads.blast(nb=(2, 2, 1), n=(8, 8, 8))
+    g, dev = _system(su, params.blast())
+    rng = np.random.default_rng(7)
+    st, bx, by, bz = [np.ascontiguousarray(x) for x in f[:4]]
+    dstate = Fields(*[torch.from_numpy(x).to(dev) for x in (st, bx, by, bz)])
+    host = Fields(torch.from_numpy(rng.standard_normal((su.nq, nvars) + st.shape[2:])).pin_memory(),
+                  *[torch.from_numpy(rng.standard_normal(x.shape)).pin_memory() for x in (bx, by, bz)])
+    before = [x.cpu().numpy().copy() for x in (dstate.state, dstate.bx, dstate.by, dstate.bz)]
+    g.copy_evolved_interior(host, dstate, to_device=True)
+    torch.cuda.synchronize()
+    after = [x.cpu().numpy() for x in (dstate.state, dstate.bx, dstate.by, dstate.bz)]
+    masks = _interior_masks(su)
+    hs = host.state.numpy()
+    # cells: HRSC vars take the host interior, everything else is unchanged
+    for v in range(abi.N_EVOL_VARS):
+        a, b = after[0][:, v], before[0][:, v]
+        if v < abi.N_HRSC:
+            np.testing.assert_array_equal(a[:, masks[0]], hs[:, v][:, masks[0]])
+            np.testing.assert_array_equal(a[:, ~masks[0]], b[:, ~masks[0]])
+        else:
+            np.testing.assert_array_equal(a, b)
+    for a, b, h, m in zip(after[1:], before[1:], (host.bx, host.by, host.bz), masks[1:]):
+        np.testing.assert_array_equal(a[:, m], h.numpy()[:, m])
+        np.testing.assert_array_equal(a[:, ~m], b[:, ~m])
+    # and back into zeroed host arrays: the interior rows at every x
+    back = Fields(torch.zeros_like(host.state).pin_memory(), *[torch.zeros_like(x).pin_memory()
+                                                              for x in (host.bx, host.by, host.bz)])
+    g.copy_evolved_interior(back, dstate, to_device=False)
+    torch.cuda.synchronize()
+    rows = _interior_masks(su, whole_rows=True)
+    bs = back.state.numpy()
+    for v in range(nvars):
+        exp = after[0][:, v] if v < abi.N_HRSC else np.zeros_like(bs[:, v])
+        np.testing.assert_array_equal(bs[:, v][:, rows[0]], exp[:, rows[0]])
+        assert not bs[:, v][:, ~rows[0]].any()
+    for b, a, m in zip((back.bx, back.by, back.bz), after[1:], rows[1:]):
+        np.testing.assert_array_equal(b.numpy()[:, m], a[:, m])
+        assert not b.numpy()[:, ~m].any()
+
+
+def test_upload_and_ghost_fill_equals_whole_copy():
+    """The e2e leg's upload (interior copy, then the ghost fill) gives the
+    device state, ghosts included, of copying the whole arrays."""
+    su, f = workloads.blast(nb=(2, 2, 2), n=(8, 8, 8))
+    g, dev = _system(su, params.blast())
+    st, bx, by, bz = [np.ascontiguousarray(x) for x in f[:4]]
+    ref = Fields(*[torch.from_numpy(x).to(dev) for x in (st, bx, by, bz)])
+    g.fill_ghosts_brick(ref, su.nb, su.periodic)
+    host = Fields(*[x.cpu().pin_memory() for x in (ref.state[:, :abi.N_HRSC].contiguous(), ref.bx, ref.by,
+                                                   ref.bz)])
+    up = Fields(ref.state.clone(), *[torch.full_like(x, np.nan) for x in (ref.bx, ref.by, ref.bz)])
+    up.state[:, :abi.N_HRSC] = np.nan
+    g.copy_evolved_interior(host, up, to_device=True)
+    g.fill_ghosts_brick(up, su.nb, su.periodic)
+    torch.cuda.synchronize()
+    for a, b in zip((up.state, up.bx, up.by, up.bz), (ref.state, ref.bx, ref.by, ref.bz)):
+        assert torch.equal(a, b)
+
+
+def test_unpinned_host_arrays_are_rejected():
+    su, f = workloads.blast(nb=(1, 1, 1), n=(8, 8, 8))
+    g, dev = _system(su, params.blast())
+    st, bx, by, bz = [np.ascontiguousarray(x) for x in f[:4]]
+    dstate = Fields(*[torch.from_numpy(x).to(dev) for x in (st, bx, by, bz)])
+    host = Fields(*[torch.from_numpy(x.copy()) for x in (st, bx, by, bz)])
+    with pytest.raises(ValueError):
+        g.copy_evolved_interior(host, dstate, to_device=True)
