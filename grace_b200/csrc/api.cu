@@ -52,6 +52,11 @@ struct grb_handle {
   float* d_mlp = nullptr;
   MlpSmem* d_mlp_pack = nullptr;  // shared-memory image of the network
   unsigned long long* d_queue = nullptr;  // work-queue counter of the aux pass
+  double* d_metder = nullptr;             // static-metric cache (grb_set_static_metric)
+  size_t metder_bytes = 0;
+  int metder_key[4] = {0, 0, 0, 0};       // nx, ny, nz, ngz it was built for
+  int64_t metder_nq = 0;                  // blocks it covers
+  const double* metder_idx = nullptr;     // the spacings it was built with
   uint32_t* d_auxlist = nullptr;          // cells of the tuned aux pass in one block
   uint32_t auxlist_n = 0;
   int auxlist_key[4] = {0, 0, 0, 0};      // nx, ny, nz, ngz it was built for
@@ -178,6 +183,8 @@ struct KScope {
 // kMinB[v]: minimum resident CTAs of 128 threads per SM requested from the
 // compiler; 1 leaves the register count free, 4 caps it at 128, 5 at 102.
 constexpr int kMinB[3] = {1, 4, 5};
+// The update kernel that reads the static-metric cache: 1, 3, 4.
+constexpr int kMinBCached[3] = {1, 3, 4};
 constexpr int kNumVar = 3;
 
 // ---- TMA-staged flux kernel: tensor maps and tile geometry ----------------
@@ -267,9 +274,18 @@ void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, c
   else if (v == 2) k_fofc_flag<5, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
   else k_fofc_flag<1, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
 }
+// Update candidates: 0..2 at 1, 4, 5 CTAs/SM; with the static-metric
+// cache md the kernel that reads it (capped at 1, 3, 4 CTAs/SM).
 void launch_update_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                          double dt, double dtfact, double* ns, const double* os, const double* aux,
-                         const double* idx, const StageBufs& B) {
+                         const double* idx, const StageBufs& B, const double* md = nullptr) {
+  if (md) {
+    static_assert(kMinBCached[1] == 3 && kMinBCached[2] == 4, "update candidates");
+    if (v == 1) k_update<3, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B, md);
+    else if (v == 2) k_update<4, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B, md);
+    else k_update<1, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B, md);
+    return;
+  }
   if (v == 1) k_update<4><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B);
   else if (v == 2) k_update<5><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B);
   else k_update<1><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B);
@@ -350,6 +366,14 @@ void launch_linop_box(cudaStream_t s, const LinBox& L, int nv, int64_t nq, doubl
   k_linop_box<<<grid, 256, 0, s>>>(L, nv, a, x, y, b, c);
 }
 
+// The static-metric cache when it was built for this geometry and these
+// spacings and covers these blocks, else null.
+const double* static_metric(const grb_handle* h, const Geo& G, const double* idx) {
+  if (!h->d_metder || idx != h->metder_idx || G.nq > h->metder_nq) return nullptr;
+  const int key[4] = {G.nx, G.ny, G.nz, G.g};
+  return std::equal(key, key + 4, h->metder_key) ? h->d_metder : nullptr;
+}
+
 // The stage in tuned mode: only the faces the stage reads, FAST flux math,
 // tuned register caps.  Returns the number of kernels launched.
 int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, double dtfact,
@@ -405,7 +429,7 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
   {
     KScope ks(h, s, GRB_KIND_UPDATE);
     launch_update_tuned(h->var_update, nblk(ub.count(), T), s, P, G, ub, dt, dtfact, nw->state, old->state,
-                        aux, g->idx, B);
+                        aux, g->idx, B, static_metric(h, G, g->idx));
     ++launches;
   }
   {
@@ -508,6 +532,7 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_mlp_pack);
   cudaFree(h->d_queue);
   cudaFree(h->d_auxlist);
+  cudaFree(h->d_metder);
   delete h;
   return GRB_OK;
 }
@@ -1199,6 +1224,42 @@ int grb_copy_evolved_interior(grb_handle* h, const grb_grid* g, const grb_fields
   return GRB_OK;
 }
 
+int grb_set_static_metric(grb_handle* h, const grb_grid* g, const grb_fields* st, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!st) {
+    cudaFree(h->d_metder);
+    h->d_metder = nullptr;
+    h->metder_bytes = 0;
+    h->metder_idx = nullptr;
+    h->metder_nq = 0;
+    return GRB_OK;
+  }
+  if (!g || !st->state || !g->idx || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->ngz < 3 || g->nq < 1)
+    return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  const size_t bytes = sizeof(double) * kMetDer * (size_t)G.nx * G.ny * G.nz * (size_t)G.nq;
+  if (bytes > h->metder_bytes) {
+    cudaFree(h->d_metder);
+    h->d_metder = nullptr;
+    h->metder_bytes = 0;
+    if (cudaMalloc(&h->d_metder, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, GRB_ERR_NOMEM);
+    }
+    h->metder_bytes = bytes;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const Box b = box(G.g, G.g, G.g, G.nx, G.ny, G.nz, G.nq);
+  k_metric_derivs<<<nblk(b.count(), 128), 128, 0, s>>>(G, b, st->state, g->idx, h->d_metder);
+  ++h->launches;
+  CK(cudaGetLastError());
+  const int key[4] = {G.nx, G.ny, G.nz, G.g};
+  std::copy(key, key + 4, h->metder_key);
+  h->metder_nq = G.nq;
+  h->metder_idx = g->idx;
+  return GRB_OK;
+}
+
 int grb_set_mode(grb_handle* h, int32_t mode) {
   if (!h || (mode != GRB_MODE_PLAIN && mode != GRB_MODE_TUNED)) return GRB_ERR_INVALID;
   h->mode = mode;
@@ -1291,7 +1352,7 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
                                             fo.by, fo.bz, gs.idx, gs.coords, B); });
       else if (fam == 2)
         t = time_it([&] { launch_update_tuned(v, nblk(ub.count(), 128), s, P, G, ub, 1e-12, 1.0, ns, os, ax,
-                                              gs.idx, B); });
+                                              gs.idx, B, static_metric(h, G, gs.idx)); });
       else
         t = time_it([&] { launch_aux_tuned(v, nblk(ab.count(), 128), s, P, G, ab, ns, fn.bx, fn.by, fn.bz,
                                            ax, gs.idx, gs.coords, B); });
@@ -1323,7 +1384,7 @@ int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   if (!h || !variant) return GRB_ERR_INVALID;
   variant[0] = kFluxMinB[h->var_flux] + (kFluxTma[h->var_flux] ? 100 : 0);
   variant[1] = kMinB[h->var_flag];
-  variant[2] = kMinB[h->var_update];
+  variant[2] = h->d_metder ? kMinBCached[h->var_update] : kMinB[h->var_update];
   variant[3] = kMinB[h->var_aux % 3] + (h->var_aux >= 3 ? 100 : 0);
   if (ms)
     for (int f = 0; f < 4; ++f)

@@ -490,22 +490,14 @@ __global__ void __launch_bounds__(128) k_fofc_edges(Geo G, Box box, StageBufs B)
 }
 
 // ---- flux divergence + geometric sources on interior cells -----------------
-template <int MINB = 1>
-__global__ void __launch_bounds__(128, MINB) k_update(DevParams P, Geo G, Box box, double dt, double dtfact,
-                                                 double* __restrict__ ns, const double* __restrict__ os,
-                                                 const double* __restrict__ aux,
-                                                 const double* __restrict__ idx, StageBufs B) {
-  int i, j, k;
-  int64_t q;
-  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
-  const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
-  const Met m = cell_met(G, os, i, j, k, q);
-  const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
-  const double z[3] = {aux[a0 + G.cells * GRB_ZVECX], aux[a0 + G.cells * GRB_ZVECY], aux[a0 + G.cells * GRB_ZVECZ]};
-  const double Bv[3] = {aux[a0 + G.cells * GRB_BX], aux[a0 + G.cells * GRB_BY], aux[a0 + G.cells * GRB_BZ]};
-  const double W = lorentz(m.g, z);
-  const double h = ix[0];  // one spacing for all axes, as in grmhd.hh:232-235
-  const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
+// Sixth-order centred derivatives of the lapse, shift and 3-metric at one
+// cell (os + c0: the cell's variable 0), one spacing h for all axes as in
+// grmhd.hh:232-235: dalp[jd], db[3 jd + c] = d_jd beta^c,
+// dg[6 jd + c] = d_jd g_c.  The 30 values in this order are also the
+// layout of the static-metric cache (kMetDer doubles per cell).
+constexpr int kMetDer = 30;
+__device__ __forceinline__ void metric_derivs(const Geo& G, const double* __restrict__ os, int64_t c0, double h,
+                                              double dalp[3], double db[9], double dg[18]) {
   const int64_t sy = G.NX, sz = (int64_t)G.NX * G.NY;
   auto der = [&](int v, double o[3]) {
     const double* p = os + c0 + G.cells * v;
@@ -513,7 +505,7 @@ __global__ void __launch_bounds__(128, MINB) k_update(DevParams P, Geo G, Box bo
     o[1] = fd6(p[-3 * sy], p[-2 * sy], p[-sy], p[sy], p[2 * sy], p[3 * sy], h);
     o[2] = fd6(p[-3 * sz], p[-2 * sz], p[-sz], p[sz], p[2 * sz], p[3 * sz], h);
   };
-  double dalp[3], db[9], dg[18], t3[3];
+  double t3[3];
   der(GRB_ALP, dalp);
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
@@ -525,11 +517,56 @@ __global__ void __launch_bounds__(128, MINB) k_update(DevParams P, Geo G, Box bo
     der(GRB_GXX + c, t3);
     dg[c] = t3[0]; dg[6 + c] = t3[1]; dg[12 + c] = t3[2];
   }
+}
+// Offset of derivative d of interior cell (i, j, k) of block q in the
+// static-metric cache: [q][d][k - g][j - g][i - g].
+__device__ __forceinline__ int64_t mdi(const Geo& G, int i, int j, int k, int d, int64_t q) {
+  return (((q * kMetDer + d) * G.nz + (k - G.g)) * G.ny + (j - G.g)) * G.nx + (i - G.g);
+}
+// Fills the static-metric cache on interior cells.
+__global__ void __launch_bounds__(128) k_metric_derivs(Geo G, Box box, const double* __restrict__ os,
+                                                       const double* __restrict__ idx, double* __restrict__ md) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  double d[kMetDer];
+  metric_derivs(G, os, cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q), idx[3 * q], d, d + 3, d + 12);
+#pragma unroll
+  for (int c = 0; c < kMetDer; ++c) md[mdi(G, i, j, k, c, q)] = d[c];
+}
+
+// add_fluxes_and_source_terms.  kCached: read the metric derivatives from
+// the static-metric cache md (tuned mode, Cowling) instead of
+// differentiating the metric here.
+template <int MINB = 1, bool kCached = false>
+__global__ void __launch_bounds__(128, MINB) k_update(DevParams P, Geo G, Box box, double dt, double dtfact,
+                                                 double* __restrict__ ns, const double* __restrict__ os,
+                                                 const double* __restrict__ aux,
+                                                 const double* __restrict__ idx, StageBufs B,
+                                                 const double* __restrict__ md = nullptr) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
+  const Met m = cell_met(G, os, i, j, k, q);
+  const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
+  const double z[3] = {aux[a0 + G.cells * GRB_ZVECX], aux[a0 + G.cells * GRB_ZVECY], aux[a0 + G.cells * GRB_ZVECZ]};
+  const double Bv[3] = {aux[a0 + G.cells * GRB_BX], aux[a0 + G.cells * GRB_BY], aux[a0 + G.cells * GRB_BZ]};
+  const double W = lorentz(m.g, z);
+  const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
+  double d[kMetDer];
+  if (kCached) {
+    const int64_t m0 = mdi(G, i, j, k, 0, q), ms = (int64_t)G.nx * G.ny * G.nz;
+#pragma unroll
+    for (int c = 0; c < kMetDer; ++c) d[c] = md[m0 + c * ms];
+  } else {
+    metric_derivs(G, os, c0, ix[0], d, d + 3, d + 12);
+  }
   double K[6];
 #pragma unroll
   for (int c = 0; c < 6; ++c) K[c] = os[c0 + G.cells * (GRB_KXX + c)];
   double stau, sS[3];
-  geom_sources(m, K, dalp, dg, db, aux[a0 + G.cells * GRB_RHO], aux[a0 + G.cells * GRB_PRESS],
+  geom_sources(m, K, d, d + 12, d + 3, aux[a0 + G.cells * GRB_RHO], aux[a0 + G.cells * GRB_PRESS],
                aux[a0 + G.cells * GRB_EPS], Bv, z, W, stau, sS);
   const double* F = B.flux;
   const double sd = m.sqrtg * dt * dtfact;

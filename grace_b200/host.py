@@ -170,6 +170,14 @@ class GRMHDEquationsSystem:
         _lib.check(self.lib.grb_fill_ghosts_brick(self.h, ctypes.byref(g), ctypes.byref(f), nb[0], nb[1],
                                                   nb[2], per, _stream_ptr(stream)), "grb_fill_ghosts_brick")
 
+    def set_static_metric(self, fields=None, stream=None):
+        """Cowling: cache the metric derivatives of `fields` for the tuned
+        update (grb_set_static_metric); None frees the cache."""
+        g = self.blocks.c()
+        f = fields.c() if fields is not None else None
+        _lib.check(self.lib.grb_set_static_metric(self.h, ctypes.byref(g), ctypes.byref(f) if f is not None else None,
+                                                  _stream_ptr(stream)), "grb_set_static_metric")
+
     def copy_evolved_interior(self, host, dev, to_device, stream=None):
         """Interior of the evolved variables between pinned host tensors and
         the device Fields `dev` (grb_copy_evolved_interior).  host: Fields of

@@ -186,6 +186,19 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt,
                         double dtfact, const grb_fields* new_state,
                         const grb_fields* old_state, const double* aux,
                         void* stream);
+/* No counterpart in the reference (it differentiates the metric at every
+ * stage).  Cowling: declares the lapse, shift and 3-metric of st->state
+ * static and computes, once, the sixth-order derivatives that
+ * add_fluxes_and_source_terms (grmhd.hh:232-330) takes of them on every
+ * interior cell: 30 doubles per cell in device memory owned by the handle,
+ * the same arithmetic as the stage's.  GRB_MODE_TUNED stages on a grid of
+ * the same block geometry, the same idx pointer and at most these nq blocks
+ * then read them instead of differentiating the metric (identical
+ * results); the plain mode ignores them.  Call again after changing the
+ * metric or the spacings; st = NULL frees them.  GRB_ERR_NOMEM when the
+ * cache cannot be allocated. */
+int grb_set_static_metric(grb_handle* h, const grb_grid* g, const grb_fields* st,
+                          void* stream);
 /* = grace::compute_auxiliary_quantities<eos_t>(state, sstate, aux)
  *   (src/evolution/auxiliaries.cpp:81-180): c2p on every cell including
  *   ghosts, conservative rewrites, C2P_ERR sticky-OR, BDIV, and (GS) the
@@ -343,7 +356,8 @@ int grb_set_mode(grb_handle* h, int32_t mode);
 int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* new_state,
                  const grb_fields* old_state, const double* aux, void* stream);
 /* variant[4]: chosen minimum-CTAs-per-SM of flux, flag, update, aux (flux:
- * plus 100 when the TMA-staged shared-memory kernel was chosen; aux: plus
+ * plus 100 when the TMA-staged shared-memory kernel was chosen; update: of
+ * the kernel that reads the static-metric cache when one is set; aux: plus
  * 100 when the work-queue form was chosen);
  * ms[12] (or NULL): timed milliseconds of the 3 candidates per family. */
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms);

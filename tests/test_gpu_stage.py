@@ -25,7 +25,7 @@ def _setup(name):
     return P, su, f, cfl / su.idx()[0, 0]
 
 
-def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN, tuning=None):
+def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN, tuning=None, static_metric=False):
     dev = torch.device("cuda:0")
     st, bx, by, bz, aux = f
     blocks = Blocks(su.n[0], su.n[1], su.n[2], su.ngz, su.nq, su.idx(), device=dev)
@@ -39,6 +39,8 @@ def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN, tuning=None):
     bc(state)
     g.compute_auxiliary_quantities(state, aux_d)
     sp, spp = state.clone(), state.clone()
+    if static_metric:
+        g.set_static_metric(state)
     if mode == abi.MODE_TUNED:
         if tuning is None:
             g.autotune(sp, state, aux_d)
@@ -325,3 +327,28 @@ def test_curved_excision_donor_faces_match_oracle(tuning):
         d = np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300)
         assert d < STEP_TOL
     assert g.status().device_flags == 0
+
+
+@pytest.mark.parametrize("update", [0, 1, 2])
+@pytest.mark.parametrize("case", ["blast", "curved"])
+def test_static_metric_cache_gives_identical_steps(case, update):
+    """The tuned update reading the static-metric cache (grb_set_static_metric)
+    gives bit-for-bit the step of the tuned update that differentiates the
+    metric itself, at each register cap; on the curved setup the cached step
+    also matches the oracle."""
+    if case == "blast":
+        P, su, f, dt = _setup("blast")
+    else:
+        from curved import curved_setup
+        P, su, f = curved_setup(emf=abi.EMF_GS, fofc=1)
+        dt = 0.25 / su.idx()[0, 0]
+    gs0, ga0, _ = _gpu_run(P, su, f, dt, 2, abi.MODE_TUNED, tuning=(1, 0, update, 0))
+    gs1, ga1, g = _gpu_run(P, su, f, dt, 2, abi.MODE_TUNED, tuning=(1, 0, update, 0), static_metric=True)
+    for a, b in zip(gs0 + [ga0], gs1 + [ga1]):
+        np.testing.assert_array_equal(a, b)
+    assert g.status().device_flags == 0
+    if case == "curved":
+        os_, oa, S = _oracle_run(P, su, f, dt, 2)
+        e = cons_rel_err(interior(gs1[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
+        assert e.max() < STEP_TOL, e
+    g.set_static_metric(None)
