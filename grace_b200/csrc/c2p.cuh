@@ -115,7 +115,7 @@ GRB_HD double newton_br(double sa, double sb, const KBr& g, int maxiter, double 
 
 // Kastaun scalars (kastaun_c2p.hh:306-337)
 struct KSc {
-  double D, q, s, ye, r2, Bt2, rBt, rBt2, h0;
+  double D, iD, q, s, ye, r2, Bt2, rBt, rBt2, h0;
   double rup[3], Bt[3], B[3];
 };
 GRB_HD KSc kscalars(const DevEos& e, const Met& m, double c[10]) {
@@ -124,6 +124,7 @@ GRB_HD KSc kscalars(const DevEos& e, const Met& m, double c[10]) {
   c[0] = fmax(0., c[0]);
   k.D = c[0];
   const double iD = 1.0 / k.D;
+  k.iD = iD;
   k.q = c[4] * iD;
   k.s = c[6] * iD;
   const double r[3] = {c[1] * iD, c[2] * iD, c[3] * iD};
@@ -139,13 +140,20 @@ GRB_HD KSc kscalars(const DevEos& e, const Met& m, double c[10]) {
   return k;
 }
 
-// Kastaun master function (kastaun_c2p.hh:122-295).  FAST (tuned mode):
-// rho = D sqrt(1 - v^2) and h/W = h sqrt(1 - v^2) instead of two divisions
-// by W = 1/sqrt(1 - v^2); the same function up to rounding.
+// Kastaun master function (kastaun_c2p.hh:122-295).  FAST (tuned mode): the
+// same function up to rounding with three divisions per evaluation instead
+// of five: rho = D sqrt(1 - v^2) and h/W = h sqrt(1 - v^2); W and
+// W/(1+W) = 1/(1 + 1/W) from one reciprocal of (1/W)(1 + 1/W);
+// h = (1+eps)(1+a) with a = P/(rho(1+eps)) formed as 1 + eps + P/rho, with
+// 1/rho = W/D; and nu = max(nu_A, nu_B), nu_A = (1+a)(1+q-mu r^2) =
+// h (1+q-mu r^2)/(1+eps), nu_B = h/W, decided by comparing
+// 1+q-mu r^2 with (1+eps)/W (h, 1+eps > 0), so that 1/(nu + mu r^2) takes
+// one division either way.
 template <bool FAST = false>
 struct KRt {
   const DevEos* e;
   double d, qtot, rsqr, bsqr, rbsqr, brosqr, vsqrmax, wmax;
+  double id, iwmax, w1max;  // FAST: 1/D, 1/wmax, wmax/(1+wmax)
   GRB_HD KRt(const DevEos& eos, const KSc& k) : e(&eos) {
     d = k.D; qtot = k.q; rsqr = k.r2; bsqr = k.Bt2; rbsqr = k.rBt2;
     brosqr = rsqr * bsqr - rbsqr;
@@ -153,26 +161,76 @@ struct KRt {
     const double ws = 1 + zs;
     wmax = sqrt(ws);
     vsqrmax = zs / ws;
+    id = iwmax = w1max = 0.0;
+    if (FAST) {
+      id = k.iD;
+      iwmax = 1.0 / wmax;
+      w1max = wmax / (1 + wmax);
+    }
   }
-  GRB_HD double eval(double mu, bool full, uint32_t& sig, double& x, double& w, double& rho,
-                     double& press, double& eps, double& temp, double& ent) const {
+  // FAST form of eval (same arguments and results).
+  GRB_HD double eval_f(double mu, bool full, uint32_t& sig, double& x, double& w, double& rho,
+                       double& press, double& eps, double& temp, double& ent) const {
     x = 1. / (1. + mu * bsqr);
     const double rf = x * (rsqr * x + mu * (x + 1.0) * rbsqr);
     const double mx = mu * x;
     const double qf = qtot - 0.5 * (bsqr + mx * mx * brosqr);
     const double vsqr = rf * mu * mu;
-    double iw = 0.0;
+    double iw, w1;  // 1/W and W/(1+W)
+    if (vsqr > vsqrmax) {
+      w = wmax;
+      iw = iwmax;
+      w1 = w1max;
+      if (full) sig |= SIG_VEL_HIGH;
+    } else {
+      iw = sqrt(1 - vsqr);
+      const double r = 1.0 / (iw * (1.0 + iw));
+      w = (1.0 + iw) * r;
+      w1 = iw * r;
+    }
+    rho = d * iw;
+    const double rho0 = rho;
+    if (full) {
+      if (rho >= e->rhomax) { sig |= SIG_RHO_HIGH; rho = e->rhomax; }
+      else if (rho <= e->rhomin) { sig |= SIG_RHO_LOW; rho = e->rhomin; }
+    } else {
+      rho = fmin(e->rhomax, fmax(e->rhomin, rho));
+    }
+    const double irho = rho == rho0 ? w * id : 1.0 / rho;
+    eps = w * (qf - mu * rf * (1.0 - mu * w1));
+    double lo, hi;
+    eos_eps_range(*e, lo, hi, rho);
+    uint32_t qe = 0;
+    if (full) {
+      hi = fmin(hi, e->eps_max);
+      if (eps >= hi) { sig |= SIG_EPS_HIGH; eps = hi * 0.999; }
+      else if (eps < lo) { sig |= SIG_EPS_LOW; eps = lo; }
+      press = eos_Peps_full(*e, temp, ent, eps, rho, qe);
+    } else {
+      eps = fmin(hi, fmax(lo, eps));
+      press = eos_Peps(*e, eps, rho, qe);
+    }
+    const double h = 1 + eps + press * irho;
+    const double qa = 1 + qf - mu * rf;
+    const double rmu = rf * mu;
+    if (qa >= iw * (1 + eps)) return mu - (1 + eps) / (h * qa + rmu * (1 + eps));
+    return mu - 1. / (h * iw + rmu);
+  }
+  GRB_HD double eval(double mu, bool full, uint32_t& sig, double& x, double& w, double& rho,
+                     double& press, double& eps, double& temp, double& ent) const {
+    if (FAST) return eval_f(mu, full, sig, x, w, rho, press, eps, temp, ent);
+    x = 1. / (1. + mu * bsqr);
+    const double rf = x * (rsqr * x + mu * (x + 1.0) * rbsqr);
+    const double mx = mu * x;
+    const double qf = qtot - 0.5 * (bsqr + mx * mx * brosqr);
+    const double vsqr = rf * mu * mu;
     if (vsqr > vsqrmax) {
       w = wmax;
       if (full) sig |= SIG_VEL_HIGH;
-      if (FAST) iw = 1.0 / wmax;
-    } else if (FAST) {
-      iw = sqrt(1 - vsqr);
-      w = 1 / iw;
     } else {
       w = 1 / sqrt(1 - vsqr);
     }
-    rho = FAST ? d * iw : d / w;
+    rho = d / w;
     if (full) {
       if (rho >= e->rhomax) { sig |= SIG_RHO_HIGH; rho = e->rhomax; }
       else if (rho <= e->rhomin) { sig |= SIG_RHO_LOW; rho = e->rhomin; }
@@ -194,7 +252,7 @@ struct KRt {
     }
     const double a = press / (rho * (1 + eps));
     const double h = (1 + eps) * (1 + a);
-    const double hbw = fmax((1 + a) * (1 + qf - mu * rf), FAST ? h * iw : h / w);
+    const double hbw = fmax((1 + a) * (1 + qf - mu * rf), h / w);
     return mu - 1. / (hbw + rf * mu);
   }
   GRB_HD double operator()(double mu) const {

@@ -549,8 +549,18 @@ GRB_HD void recon6_fast(int kind, const double u[6], double& uL, double& uR) {
 GRB_HD double face4(double um2, double um1, double u0, double up1) {
   return 0.5625 * (um1 + u0) + (-0.0625) * (um2 + up1);
 }
+// Sixth-order centred first derivative.  On the device every operation is
+// rounded on its own (no contraction into fused multiply-adds), so the value
+// is the same bits wherever the stencil is inlined (the stage, the
+// static-metric cache) and matches a host evaluation without FMA.
 GRB_HD double fd6(double m3, double m2, double m1, double p1, double p2, double p3, double h) {
+#ifdef __CUDA_ARCH__
+  const double s = __dadd_rn(__dsub_rn(__dmul_rn(45.0, __dsub_rn(p1, m1)), __dmul_rn(9.0, __dsub_rn(p2, m2))),
+                             __dsub_rn(p3, m3));
+  return __dmul_rn(__dmul_rn(1.0 / 60.0, h), s);
+#else
   return (1.0 / 60.0) * h * (45.0 * (p1 - m1) - 9.0 * (p2 - m2) + (p3 - m3));
+#endif
 }
 
 }  // namespace grb
