@@ -325,29 +325,50 @@ GRB_HD void vtilde_f(double alp, const double beta[3], const double z[3], double
 #pragma unroll
   for (int i = 0; i < 3; ++i) vt[i] = aw * z[i] - beta[i];
 }
-GRB_HD void char_speeds_f(double ialp, double betad, double rho, double press, double eps, double cs2,
-                          double W, double b2, double vtd, double guu_dd, double& cm, double& cp) {
-  const double va2 = b2 / (b2 + rho * (1. + eps) + press);
-  const double c2 = va2 + cs2 * (1. - va2);
+// char_speeds with 1/alpha multiplied in, for the two states of a face at
+// once (tuned mode): the two va^2 denominators share one reciprocal, and so
+// do the two 2A (all four positive and of physical size, far from the
+// double range's ends).
+GRB_HD void char_speeds_f2(double ialp, double betad, double guu_dd, const double* pl, const double* pr,
+                           double wl, double wr, double b2l, double b2r, double vtdl, double vtdr, double& cml,
+                           double& cpl, double& cmr, double& cpr) {
+  const double dl = b2l + pl[GRB_P_RHO] * (1. + pl[GRB_P_EPS]) + pl[GRB_P_PRESS];
+  const double dr = b2r + pr[GRB_P_RHO] * (1. + pr[GRB_P_EPS]) + pr[GRB_P_PRESS];
+  const double rd = 1.0 / (dl * dr);
+  const double va2[2] = {b2l * dr * rd, b2r * dl * rd};
+  const double cs2[2] = {pl[GRB_P_CS2], pr[GRB_P_CS2]};
+  const double W[2] = {wl, wr}, vtd[2] = {vtdl, vtdr};
   const double ia2 = ialp * ialp;
-  const double u0 = W * ialp;
-  const double ud = W * vtd * ialp;
-  const double A = (1. - c2) * u0 * u0 + c2 * ia2;
-  const double B = -2. * (1. - c2) * u0 * ud + 2. * c2 * betad * ia2;
-  const double C = (1. - c2) * ud * ud - c2 * (guu_dd - betad * betad * ia2);
-  const double disc = sqrt(fmax(0., B * B - 4. * A * C));
-  const double i2A = 0.5 / A;
-  const double l1 = (-B + disc) * i2A, l2 = (-B - disc) * i2A;
-  cm = fmin(l1, l2);
-  cp = fmax(l1, l2);
+  double A[2], B[2], C[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const double c2 = va2[s] + cs2[s] * (1. - va2[s]);
+    const double u0 = W[s] * ialp;
+    const double ud = W[s] * vtd[s] * ialp;
+    A[s] = (1. - c2) * u0 * u0 + c2 * ia2;
+    B[s] = -2. * (1. - c2) * u0 * ud + 2. * c2 * betad * ia2;
+    C[s] = (1. - c2) * ud * ud - c2 * (guu_dd - betad * betad * ia2);
+  }
+  const double ra = 0.5 / (A[0] * A[1]);
+  const double i2A[2] = {A[1] * ra, A[0] * ra};
+  double cm[2], cp[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const double disc = sqrt(fmax(0., B[s] * B[s] - 4. * A[s] * C[s]));
+    const double l1 = (-B[s] + disc) * i2A[s], l2 = (-B[s] - disc) * i2A[s];
+    cm[s] = fmin(l1, l2);
+    cp[s] = fmax(l1, l2);
+  }
+  cml = cm[0]; cpl = cp[0]; cmr = cm[1]; cpr = cp[1];
 }
 // conserved + fluxes along d (grmhd_subexpressions.hh:97-156, 294-331)
 struct ConsFlux {
   double D, tau, S[3], ents, fD, ftau, fS[3], fent;
 };
+// ialp > 0 (tuned mode): 1/alpha, multiplied in instead of dividing.
 GRB_HD ConsFlux cons_flux(double alp, const double beta[3], const double g[6], double rho,
                           double press, double eps, const double z[3], double s, double W,
-                          double b2, const double b[4], const double vt[3], int d) {
+                          double b2, const double b[4], const double vt[3], int d, double ialp = 0.0) {
   ConsFlux o;
   const double rhoh = rho * (1. + eps) + press + b2;
   const double pstar = press + 0.5 * b2;
@@ -366,7 +387,7 @@ GRB_HD ConsFlux cons_flux(double alp, const double beta[3], const double g[6], d
   o.ents = s * o.D;
   o.fD = o.D * vt[d];
   o.ftau = W2rhoh * vt[d] + pstar * beta[d] - alp * alp * b[0] * b[d + 1] - o.fD;
-  const double c = W2rhoh * vt[d] / alp;
+  const double c = ialp > 0.0 ? W2rhoh * vt[d] * ialp : W2rhoh * vt[d] / alp;
 #pragma unroll
   for (int j = 0; j < 3; ++j)
     o.fS[j] = c * (betal[j] + vtl[j]) + alp * ((j == d ? pstar : 0.) - b[d + 1] * bl[j]);
@@ -517,9 +538,44 @@ GRB_HD double wz_side(double b0, double b1, double b2, double f0, double f1, dou
   const double w2 = d2 * (e2 + t2) * (e0 * e1);
   return (f0 * w0 + f1 * w1 + f2 * w2) / (6.0 * (w0 + w1 + w2));
 }
+// wz_side as a numerator and a positive, normal denominator (>= 6e-253).
+GRB_HD void wz_side_nd(double b0, double b1, double b2, double f0, double f1, double f2, double d0, double d1,
+                       double d2, double& num, double& den) {
+  const double ep = 1.0e-42;
+  const double t5 = fabs(b0 - b2);
+  const double t2 = t5 * t5;
+  const double e0 = (b0 + ep) * (b0 + ep), e1 = (b1 + ep) * (b1 + ep), e2 = (b2 + ep) * (b2 + ep);
+  const double w0 = d0 * (e0 + t2) * (e1 * e2);
+  const double w1 = d1 * (e1 + t2) * (e0 * e2);
+  const double w2 = d2 * (e2 + t2) * (e0 * e1);
+  num = f0 * w0 + f1 * w1 + f2 * w2;
+  den = 6.0 * (w0 + w1 + w2);
+}
+// 2^-e for a positive normal d = m 2^e (m in [1, 2)), exact.
+GRB_HD double inv_pow2_exponent(double d) {
+#ifdef __CUDA_ARCH__
+  const long long be = (__double_as_longlong(d) >> 52) & 0x7ff;
+  return __longlong_as_double((2046ll - be) << 52);
+#else
+  int e;
+  frexp(d, &e);  // d = f 2^e, f in [0.5, 1)
+  return ldexp(1.0, 1 - e);
+#endif
+}
+// n1 / d1 and n2 / d2 with one division (tuned mode): the denominators,
+// positive and normal, are first scaled by powers of two into [1, 2)
+// (exact), so that their product neither overflows nor underflows.
+GRB_HD void div_pair(double n1, double d1, double n2, double d2, double& q1, double& q2) {
+  const double s1 = inv_pow2_exponent(d1), s2 = inv_pow2_exponent(d2);
+  const double a1 = d1 * s1, a2 = d2 * s2;
+  const double r = 1.0 / (a1 * a2);
+  q1 = (n1 * s1) * a2 * r;
+  q2 = (n2 * s2) * a1 * r;
+}
 GRB_HD void weno_z_fast(double um3, double um2, double um1, double u0, double up1, double up2,
                         double& uL, double& uR) {
   const double c13 = 13.0 / 12.0, c14 = 0.25;
+  double nR, dR, nL, dL;
   {
     const double t0 = um2 + u0 - 2.0 * um1, s0 = um2 + 3.0 * u0 - 4.0 * um1;
     const double t1 = um1 + up1 - 2.0 * u0, s1 = um1 - up1;
@@ -528,8 +584,8 @@ GRB_HD void weno_z_fast(double um3, double um2, double um1, double u0, double up
     const double b1 = c13 * t1 * t1 + c14 * s1 * s1;
     const double b2 = c13 * t2 * t2 + c14 * s2 * s2;
     // uR: stencil k pairs with beta_{2-k} (weno_reconstruction.hh:214-243)
-    uR = wz_side(b2, b1, b0, 2.0 * up2 - 7.0 * up1 + 11.0 * u0, -up1 + 5.0 * u0 + 2.0 * um1,
-                 2.0 * u0 + 5.0 * um1 - um2, 0.1, 0.6, 0.3);
+    wz_side_nd(b2, b1, b0, 2.0 * up2 - 7.0 * up1 + 11.0 * u0, -up1 + 5.0 * u0 + 2.0 * um1,
+               2.0 * u0 + 5.0 * um1 - um2, 0.1, 0.6, 0.3, nR, dR);
   }
   {
     const double t0 = um3 + um1 - 2.0 * um2, s0 = um3 + 3.0 * um1 - 4.0 * um2;
@@ -538,9 +594,10 @@ GRB_HD void weno_z_fast(double um3, double um2, double um1, double u0, double up
     const double b0 = c13 * t0 * t0 + c14 * s0 * s0;
     const double b1 = c13 * t1 * t1 + c14 * s1 * s1;
     const double b2 = c13 * t2 * t2 + c14 * s2 * s2;
-    uL = wz_side(b0, b1, b2, 2.0 * um3 - 7.0 * um2 + 11.0 * um1, -um2 + 5.0 * um1 + 2.0 * u0,
-                 2.0 * um1 + 5.0 * u0 - up1, 0.1, 0.6, 0.3);
+    wz_side_nd(b0, b1, b2, 2.0 * um3 - 7.0 * um2 + 11.0 * um1, -um2 + 5.0 * um1 + 2.0 * u0,
+               2.0 * um1 + 5.0 * u0 - up1, 0.1, 0.6, 0.3, nL, dL);
   }
+  div_pair(nL, dL, nR, dR, uL, uR);
 }
 GRB_HD void recon6_fast(int kind, const double u[6], double& uL, double& uR) {
   if (kind == GRB_RECON_WENOZ) { weno_z_fast(u[0], u[1], u[2], u[3], u[4], u[5], uL, uR); return; }

@@ -36,16 +36,14 @@ __device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
   double bl[4], br[4], b2l, b2r, vtl[3], vtr[3];
   const double gdd = dir == 0 ? m.gi[0] : dir == 1 ? m.gi[3] : m.gi[5];
   double cml, cpl, cmr, cpr, cmin, cmax;
+  const double ialp = FAST ? 1.0 / alp : 0.0;
   if (FAST) {
-    const double ialp = 1.0 / alp, iwl = 1.0 / wl, iwr = 1.0 / wr;
+    const double iwl = 1.0 / wl, iwr = 1.0 / wr;
     comoving_b_f(alp, ialp, m.beta, m.g, pl + GRB_P_BX, pl + GRB_P_ZX, wl, iwl, bl, b2l);
     comoving_b_f(alp, ialp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, wr, iwr, br, b2r);
     vtilde_f(alp, m.beta, pl + GRB_P_ZX, iwl, vtl);
     vtilde_f(alp, m.beta, pr + GRB_P_ZX, iwr, vtr);
-    char_speeds_f(ialp, m.beta[dir], pl[GRB_P_RHO], pl[GRB_P_PRESS], pl[GRB_P_EPS], pl[GRB_P_CS2], wl, b2l,
-                  vtl[dir], gdd, cml, cpl);
-    char_speeds_f(ialp, m.beta[dir], pr[GRB_P_RHO], pr[GRB_P_PRESS], pr[GRB_P_EPS], pr[GRB_P_CS2], wr, b2r,
-                  vtr[dir], gdd, cmr, cpr);
+    char_speeds_f2(ialp, m.beta[dir], gdd, pl, pr, wl, wr, b2l, b2r, vtl[dir], vtr[dir], cml, cpl, cmr, cpr);
   } else {
     comoving_b(alp, m.beta, m.g, pl + GRB_P_BX, pl + GRB_P_ZX, wl, bl, b2l);
     comoving_b(alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, wr, br, b2r);
@@ -79,9 +77,9 @@ __device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
     vb[3] = cmax;
   }
   const ConsFlux L = cons_flux(alp, m.beta, m.g, pl[GRB_P_RHO], pl[GRB_P_PRESS], pl[GRB_P_EPS],
-                               pl + GRB_P_ZX, pl[GRB_P_ENT], wl, b2l, bl, vtl, dir);
+                               pl + GRB_P_ZX, pl[GRB_P_ENT], wl, b2l, bl, vtl, dir, ialp);
   const ConsFlux R = cons_flux(alp, m.beta, m.g, pr[GRB_P_RHO], pr[GRB_P_PRESS], pr[GRB_P_EPS],
-                               pr + GRB_P_ZX, pr[GRB_P_ENT], wr, b2r, br, vtr, dir);
+                               pr + GRB_P_ZX, pr[GRB_P_ENT], wr, b2r, br, vtr, dir, ialp);
   f[GRB_DENS] = sqrtg * hll(L.fD, R.fD, L.D, R.D, cmin, cmax);
   f[GRB_ENTROPYSTAR] = sqrtg * hll(L.fent, R.fent, L.ents, R.ents, cmin, cmax);
   f[GRB_TAU] = sqrtg * hll(L.ftau, R.ftau, L.tau, R.tau, cmin, cmax);
