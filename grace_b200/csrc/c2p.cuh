@@ -536,10 +536,9 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
   bool failed = false;
   uint32_t ret = 0;
   o.err = ERR_RESET_ENTROPY;
-  const double isg = 1.0 / m.sqrtg;
+  const double isg = FAST ? 1.0 / m.sqrtg : 0.0;
 #pragma unroll
   for (int v = 0; v < 10; ++v) c[v] = FAST ? c[v] * isg : c[v] / m.sqrtg;
-  (void)isg;
   pr[GRB_P_BX] = c[7]; pr[GRB_P_BY] = c[8]; pr[GRB_P_BZ] = c[9];
   if (c[0] < 0) {
     reset_atmo(c, pr, m, P, o.err);

@@ -68,7 +68,7 @@ __device__ __forceinline__ void getflux_tile(const DevParams& P, int recon, bool
     const double* p = M + a * vs;
     gm[a] = face4(p[st], p[2 * st], p[3 * st], p[4 * st]);
   }
-  const Met m = make_met(gm, gm + 7, gm[6]);
+  const Met m = make_met<true>(gm, gm + 7, gm[6]);
   const int av[10] = {GRB_RHO, GRB_ZVECX, GRB_ZVECY, GRB_ZVECZ, GRB_YE, GRB_TEMP, GRB_ENTROPY, GRB_BX, GRB_BY, GRB_BZ};
   const int pv[10] = {GRB_P_RHO, GRB_P_ZX, GRB_P_ZY, GRB_P_ZZ, GRB_P_YE, GRB_P_TEMP, GRB_P_ENT, GRB_P_BX, GRB_P_BY, GRB_P_BZ};
   double pl[13], pr[13];
@@ -86,7 +86,7 @@ __device__ __forceinline__ void getflux_tile(const DevParams& P, int recon, bool
       recon6_fast(recon, u, pl[pv[r]], pr[pv[r]]);
     }
   }
-  const double bn = bface / m.sqrtg;
+  const double bn = bface * m.isqrtg;
   pl[GRB_P_BX + dir] = bn;
   pr[GRB_P_BX + dir] = bn;
   uint32_t q0 = 0;

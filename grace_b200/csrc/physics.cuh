@@ -73,9 +73,14 @@ struct DevParams {
 };
 
 // ---- metric ---------------------------------------------------------------
+// isqrtg, ialp: 1/sqrt(gamma) and 1/alpha, set by make_met<true> (tuned
+// mode) only.
 struct Met {
-  double g[6], beta[3], alp, gi[6], sqrtg;
+  double g[6], beta[3], alp, gi[6], sqrtg, isqrtg, ialp;
 };
+// FAST (tuned mode): 1/det and 1/alpha from one reciprocal of det * alpha,
+// and 1/sqrt(gamma) = sqrt(gamma) / det.
+template <bool FAST = false>
 GRB_HD Met make_met(const double g[6], const double b[3], double alp) {
   Met m;
 #pragma unroll
@@ -87,7 +92,15 @@ GRB_HD Met make_met(const double g[6], const double b[3], double alp) {
   const double c1 = g[2] * g[4] - g[1] * g[5];
   const double c2 = g[1] * g[4] - g[2] * g[3];
   const double det = g[0] * c0 + g[1] * c1 + g[2] * c2;
-  const double id = 1.0 / det;
+  double id;
+  if (FAST) {
+    const double r = 1.0 / (det * alp);
+    id = alp * r;
+    m.ialp = det * r;
+  } else {
+    id = 1.0 / det;
+    m.ialp = 0.0;
+  }
   m.gi[0] = c0 * id;
   m.gi[1] = c1 * id;
   m.gi[2] = c2 * id;
@@ -95,6 +108,7 @@ GRB_HD Met make_met(const double g[6], const double b[3], double alp) {
   m.gi[4] = (g[1] * g[2] - g[0] * g[4]) * id;
   m.gi[5] = (g[0] * g[3] - g[1] * g[1]) * id;
   m.sqrtg = sqrt(det);
+  m.isqrtg = FAST ? m.sqrtg * id : 0.0;
   return m;
 }
 GRB_HD double sqs(const double s[6], const double v[3]) {
@@ -551,7 +565,7 @@ GRB_HD void wz_side_nd(double b0, double b1, double b2, double f0, double f1, do
   num = f0 * w0 + f1 * w1 + f2 * w2;
   den = 6.0 * (w0 + w1 + w2);
 }
-// 2^-e for a positive normal d = m 2^e (m in [1, 2)), exact.
+// 2^-e for a nonzero normal d = +-m 2^e (m in [1, 2)), exact.
 GRB_HD double inv_pow2_exponent(double d) {
 #ifdef __CUDA_ARCH__
   const long long be = (__double_as_longlong(d) >> 52) & 0x7ff;
@@ -563,8 +577,8 @@ GRB_HD double inv_pow2_exponent(double d) {
 #endif
 }
 // n1 / d1 and n2 / d2 with one division (tuned mode): the denominators,
-// positive and normal, are first scaled by powers of two into [1, 2)
-// (exact), so that their product neither overflows nor underflows.
+// nonzero and normal, are first scaled by powers of two to magnitudes in
+// [1, 2) (exact), so that their product neither overflows nor underflows.
 GRB_HD void div_pair(double n1, double d1, double n2, double d2, double& q1, double& q2) {
   const double s1 = inv_pow2_exponent(d1), s2 = inv_pow2_exponent(d2);
   const double a1 = d1 * s1, a2 = d2 * s2;

@@ -36,9 +36,10 @@ __device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
   double bl[4], br[4], b2l, b2r, vtl[3], vtr[3];
   const double gdd = dir == 0 ? m.gi[0] : dir == 1 ? m.gi[3] : m.gi[5];
   double cml, cpl, cmr, cpr, cmin, cmax;
-  const double ialp = FAST ? 1.0 / alp : 0.0;
+  const double ialp = m.ialp;  // FAST: set by make_met<true>
   if (FAST) {
-    const double iwl = 1.0 / wl, iwr = 1.0 / wr;
+    double iwl, iwr;
+    div_pair(1.0, wl, 1.0, wr, iwl, iwr);
     comoving_b_f(alp, ialp, m.beta, m.g, pl + GRB_P_BX, pl + GRB_P_ZX, wl, iwl, bl, b2l);
     comoving_b_f(alp, ialp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, wr, iwr, br, b2r);
     vtilde_f(alp, m.beta, pl + GRB_P_ZX, iwl, vtl);
@@ -122,7 +123,7 @@ __device__ __forceinline__ void getflux(const DevParams& P, const Geo& G, int i,
     const double* p = st + c0 + G.cells * (GRB_GXX + a);
     gm[a] = face4(__ldg(p - 2 * s), __ldg(p - s), __ldg(p), __ldg(p + s));
   }
-  const Met m = make_met(gm, gm + 7, gm[6]);
+  const Met m = make_met<FAST>(gm, gm + 7, gm[6]);
   const int av[10] = {GRB_RHO, GRB_ZVECX, GRB_ZVECY, GRB_ZVECZ, GRB_YE, GRB_TEMP, GRB_ENTROPY, GRB_BX, GRB_BY, GRB_BZ};
   const int pv[10] = {GRB_P_RHO, GRB_P_ZX, GRB_P_ZY, GRB_P_ZZ, GRB_P_YE, GRB_P_TEMP, GRB_P_ENT, GRB_P_BX, GRB_P_BY, GRB_P_BZ};
   double pl[13], pr[13];
@@ -142,7 +143,7 @@ __device__ __forceinline__ void getflux(const DevParams& P, const Geo& G, int i,
     }
   }
   const int64_t bi = dir == 0 ? bxi(G, i, j, k, q) : dir == 1 ? byi(G, i, j, k, q) : bzi(G, i, j, k, q);
-  const double bn = __ldg(bface + bi) / m.sqrtg;
+  const double bn = FAST ? __ldg(bface + bi) * m.isqrtg : __ldg(bface + bi) / m.sqrtg;
   pl[GRB_P_BX + dir] = bn;
   pr[GRB_P_BX + dir] = bn;
   uint32_t q0 = 0;
@@ -365,6 +366,7 @@ __device__ __forceinline__ double ct_bz(const Geo& G, const double* bz, const do
                                          (E[emi(G, i, j, k, 1, q)] - E[emi(G, i + 1, j, k, 1, q)]) * ix[0]);
 }
 
+template <bool FAST = false>
 __device__ __forceinline__ Met cell_met(const Geo& G, const double* st, int i, int j, int k, int64_t q) {
   const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
   double g[6], b[3];
@@ -372,7 +374,7 @@ __device__ __forceinline__ Met cell_met(const Geo& G, const double* st, int i, i
   for (int a = 0; a < 6; ++a) g[a] = st[c0 + G.cells * (GRB_GXX + a)];
 #pragma unroll
   for (int a = 0; a < 3; ++a) b[a] = st[c0 + G.cells * (GRB_BETAX + a)];
-  return make_met(g, b, st[c0 + G.cells * GRB_ALP]);
+  return make_met<FAST>(g, b, st[c0 + G.cells * GRB_ALP]);
 }
 __device__ __forceinline__ double cell_r(const Geo& G, const double* coords, const double* ix, int i,
                                          int j, int k, int64_t q) {
