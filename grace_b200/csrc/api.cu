@@ -88,6 +88,7 @@ DevParams to_dev(const grb_params& p) {
     e.gm1 = p.eos.gamma - 1.;
     e.g = e.gm1 + 1.;
     e.ggm1 = e.g * e.gm1;
+    e.igm1 = 1.0 / e.gm1;
     e.ent_min = (p.eos.temp_atm > 0.0) ? (p.eos.temp_atm / e.gm1) : 1e-100;
     e.n = 1;
   } else {
@@ -102,6 +103,7 @@ DevParams to_dev(const grb_params& p) {
       e.R[i] = p.eos.pw_rho[i]; e.E[i] = p.eos.pw_eps[i];
     }
   }
+  e.ih0 = 1.0 / e.h_min;
   d.rho_fl = p.rho_fl; d.ye_fl = p.ye_fl; d.temp_fl = p.temp_fl; d.atmo_tol = p.atmo_tol;
   d.excise_by_radius = p.excise_by_radius; d.r_ex = p.r_ex; d.alp_ex = p.alp_ex;
   d.tol = p.c2p_tol; d.max_w = p.max_w; d.max_sigma = p.max_sigma;

@@ -115,12 +115,13 @@ GRB_HD double newton_br(double sa, double sb, const KBr& g, int maxiter, double 
 
 // Kastaun scalars (kastaun_c2p.hh:306-337)
 struct KSc {
-  double D, iD, q, s, ye, r2, Bt2, rBt, rBt2, h0;
+  double D, iD, q, s, ye, r2, Bt2, rBt, rBt2, h0, ih0;
   double rup[3], Bt[3], B[3];
 };
 GRB_HD KSc kscalars(const DevEos& e, const Met& m, double c[10]) {
   KSc k;
   k.h0 = e.h_min;
+  k.ih0 = e.ih0;  // 1/h_min, correctly rounded on the host as 1 / k.h0 is here
   c[0] = fmax(0., c[0]);
   k.D = c[0];
   const double iD = 1.0 / k.D;
@@ -157,15 +158,22 @@ struct KRt {
   GRB_HD KRt(const DevEos& eos, const KSc& k) : e(&eos) {
     d = k.D; qtot = k.q; rsqr = k.r2; bsqr = k.Bt2; rbsqr = k.rBt2;
     brosqr = rsqr * bsqr - rbsqr;
-    const double zs = rsqr / (k.h0 * k.h0);
-    const double ws = 1 + zs;
-    wmax = sqrt(ws);
-    vsqrmax = zs / ws;
     id = iwmax = w1max = 0.0;
     if (FAST) {
+      // 1/ws, 1/wmax and 1/(1 + wmax) from one reciprocal (all >= 1)
+      const double zs = rsqr * (k.ih0 * k.ih0);
+      const double ws = 1 + zs;
+      wmax = sqrt(ws);
+      const double r = 1.0 / (ws * wmax * (1 + wmax));
+      vsqrmax = zs * (wmax * (1 + wmax)) * r;
+      iwmax = ws * (1 + wmax) * r;
+      w1max = wmax * (ws * wmax) * r;
       id = k.iD;
-      iwmax = 1.0 / wmax;
-      w1max = wmax / (1 + wmax);
+    } else {
+      const double zs = rsqr / (k.h0 * k.h0);
+      const double ws = 1 + zs;
+      wmax = sqrt(ws);
+      vsqrmax = zs / ws;
     }
   }
   // FAST form of eval (same arguments and results).
@@ -305,7 +313,7 @@ struct ERt {
 };
 
 GRB_HD double kastaun_mu0(const KSc& k) {
-  double mu0 = 1 / k.h0;
+  double mu0 = k.ih0;  // = 1 / k.h0
   if (k.r2 >= k.h0 * k.h0) {
     KBr g{k.r2, k.Bt2, k.rBt2, k.h0 * k.h0};
     double lo = 1. / (g.h0sqr + g.rsqr);
@@ -317,7 +325,7 @@ GRB_HD double kastaun_mu0(const KSc& k) {
     int err;
     mu0 = newton_br(lo, hi, g, 30, 1e-10, err);
     if (err == 0) mu0 *= 1 + 1e-10;
-    else mu0 = 1.0 / k.h0;
+    else mu0 = k.ih0;
   }
   return mu0;
 }

@@ -73,25 +73,43 @@ __device__ __forceinline__ void getflux_tile(const DevParams& P, int recon, bool
   const int pv[10] = {GRB_P_RHO, GRB_P_ZX, GRB_P_ZY, GRB_P_ZZ, GRB_P_YE, GRB_P_TEMP, GRB_P_ENT, GRB_P_BX, GRB_P_BY, GRB_P_BZ};
   double pl[13], pr[13];
   const bool donor = (alpl <= P.alp_ex || alpr <= P.alp_ex);
+  if (!donor && recon == GRB_RECON_WENOZ) {
+    // two variables per division: their four WENO-Z states through div_quad
 #pragma unroll
-  for (int r = 0; r < 10; ++r) {
-    const double* p = A + av[r] * vs;
-    if (donor) {
-      pl[pv[r]] = p[2 * st];
-      pr[pv[r]] = p[3 * st];
-    } else {
-      double u[6];
+    for (int r = 0; r < 10; r += 2) {
+      double u0[6], u1[6], n[4], d[4], q[4];
 #pragma unroll
-      for (int o = 0; o < 6; ++o) u[o] = p[o * st];
-      recon6_fast(recon, u, pl[pv[r]], pr[pv[r]]);
+      for (int o = 0; o < 6; ++o) {
+        u0[o] = A[av[r] * vs + o * st];
+        u1[o] = A[av[r + 1] * vs + o * st];
+      }
+      weno_z_nd(u0, n[0], d[0], n[1], d[1]);
+      weno_z_nd(u1, n[2], d[2], n[3], d[3]);
+      div_quad(n, d, q);
+      pl[pv[r]] = q[0];
+      pr[pv[r]] = q[1];
+      pl[pv[r + 1]] = q[2];
+      pr[pv[r + 1]] = q[3];
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+      const double* p = A + av[r] * vs;
+      if (donor) {
+        pl[pv[r]] = p[2 * st];
+        pr[pv[r]] = p[3 * st];
+      } else {
+        double u[6];
+#pragma unroll
+        for (int o = 0; o < 6; ++o) u[o] = p[o * st];
+        recon6_fast(recon, u, pl[pv[r]], pr[pv[r]]);
+      }
     }
   }
   const double bn = bface * m.isqrtg;
   pl[GRB_P_BX + dir] = bn;
   pr[GRB_P_BX + dir] = bn;
-  uint32_t q0 = 0;
-  pl[GRB_P_PRESS] = eos_PT(P.eos, pl[GRB_P_EPS], pl[GRB_P_CS2], nullptr, pl[GRB_P_TEMP], pl[GRB_P_RHO], q0);
-  pr[GRB_P_PRESS] = eos_PT(P.eos, pr[GRB_P_EPS], pr[GRB_P_CS2], nullptr, pr[GRB_P_TEMP], pr[GRB_P_RHO], q0);
+  eos_PT_pair_f(P.eos, pl, pr);
   mhd_fluxes<dir, true>(P, rusanov, pl, pr, m, f, vb);
 }
 

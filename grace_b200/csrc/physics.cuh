@@ -57,6 +57,7 @@ struct DevEos {
   double rhomax, rhomin, tempmax, yemax, eps_max, h_min;
   double gm1, g, ggm1, ent_min;        // ideal gas
   double gthm1, entropy_min;           // hybrid thermal part
+  double igm1, ih0;                    // 1/gm1 (ideal gas), 1/h_min
   double K[GRB_MAX_PIECES], G[GRB_MAX_PIECES], R[GRB_MAX_PIECES], E[GRB_MAX_PIECES];
 };
 struct DevParams {
@@ -196,6 +197,30 @@ GRB_HD double eos_PT(const DevEos& e, double& eps, double& cs2, double* ent, dou
   cs2 = (pw_dpdrho(e, rho) + e.gthm1 * (e.gthm1 + 1) * eth) / h;
   if (ent) *ent = hy_ent(e, eth, rho);
   return p;
+}
+// eos_PT for the two reconstructed states of a face (tuned mode; states
+// in the local primitive layout, no entropy): for the ideal gas
+// eps = T * (1/(Gamma-1)) and both sound speeds from one reciprocal of
+// (1 + Gamma eps_l)(1 + Gamma eps_r) (both >= 1); the hybrid EOS calls
+// eos_PT per state.
+GRB_HD void eos_PT_pair_f(const DevEos& e, double* pl, double* pr) {
+  uint32_t q0 = 0;
+  if (e.kind == GRB_EOS_IDEAL_GAS) {
+    id_temp(e, pl[GRB_P_TEMP], q0);
+    id_temp(e, pr[GRB_P_TEMP], q0);
+    const double el = pl[GRB_P_TEMP] * e.igm1, er = pr[GRB_P_TEMP] * e.igm1;
+    pl[GRB_P_EPS] = el;
+    pr[GRB_P_EPS] = er;
+    pl[GRB_P_PRESS] = e.gm1 * el * pl[GRB_P_RHO];
+    pr[GRB_P_PRESS] = e.gm1 * er * pr[GRB_P_RHO];
+    const double dl = 1.0 + e.g * el, dr = 1.0 + e.g * er;
+    const double r = 1.0 / (dl * dr);
+    pl[GRB_P_CS2] = e.ggm1 * el * dr * r;
+    pr[GRB_P_CS2] = e.ggm1 * er * dl * r;
+    return;
+  }
+  pl[GRB_P_PRESS] = eos_PT(e, pl[GRB_P_EPS], pl[GRB_P_CS2], nullptr, pl[GRB_P_TEMP], pl[GRB_P_RHO], q0);
+  pr[GRB_P_PRESS] = eos_PT(e, pr[GRB_P_EPS], pr[GRB_P_CS2], nullptr, pr[GRB_P_TEMP], pr[GRB_P_RHO], q0);
 }
 // cs2 from (T, rho) as press_h_csnd2__temp_rho_ye computes it
 // (hybrid_eos.hh:227-240, ideal_gas_eos.hh:224-234: h summed as
@@ -586,10 +611,11 @@ GRB_HD void div_pair(double n1, double d1, double n2, double d2, double& q1, dou
   q1 = (n1 * s1) * a2 * r;
   q2 = (n2 * s2) * a1 * r;
 }
-GRB_HD void weno_z_fast(double um3, double um2, double um1, double u0, double up1, double up2,
-                        double& uL, double& uR) {
+// WENO-Z at face i-1/2 as numerators and denominators (tuned mode): the
+// states are nL / dL and nR / dR (dL, dR positive and normal).
+GRB_HD void weno_z_nd(const double u[6], double& nL, double& dL, double& nR, double& dR) {
+  const double um3 = u[0], um2 = u[1], um1 = u[2], u0 = u[3], up1 = u[4], up2 = u[5];
   const double c13 = 13.0 / 12.0, c14 = 0.25;
-  double nR, dR, nL, dL;
   {
     const double t0 = um2 + u0 - 2.0 * um1, s0 = um2 + 3.0 * u0 - 4.0 * um1;
     const double t1 = um1 + up1 - 2.0 * u0, s1 = um1 - up1;
@@ -597,7 +623,6 @@ GRB_HD void weno_z_fast(double um3, double um2, double um1, double u0, double up
     const double b0 = c13 * t0 * t0 + c14 * s0 * s0;
     const double b1 = c13 * t1 * t1 + c14 * s1 * s1;
     const double b2 = c13 * t2 * t2 + c14 * s2 * s2;
-    // uR: stencil k pairs with beta_{2-k} (weno_reconstruction.hh:214-243)
     wz_side_nd(b2, b1, b0, 2.0 * up2 - 7.0 * up1 + 11.0 * u0, -up1 + 5.0 * u0 + 2.0 * um1,
                2.0 * u0 + 5.0 * um1 - um2, 0.1, 0.6, 0.3, nR, dR);
   }
@@ -611,6 +636,29 @@ GRB_HD void weno_z_fast(double um3, double um2, double um1, double u0, double up
     wz_side_nd(b0, b1, b2, 2.0 * um3 - 7.0 * um2 + 11.0 * um1, -um2 + 5.0 * um1 + 2.0 * u0,
                2.0 * um1 + 5.0 * u0 - up1, 0.1, 0.6, 0.3, nL, dL);
   }
+}
+// n[k] / d[k], k = 0..3, with one division (tuned mode): as div_pair, the
+// four denominators scaled to magnitudes in [1, 2) first.
+GRB_HD void div_quad(const double n[4], const double d[4], double q[4]) {
+  double s[4], a[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    s[k] = inv_pow2_exponent(d[k]);
+    a[k] = d[k] * s[k];
+  }
+  const double p01 = a[0] * a[1], p23 = a[2] * a[3];
+  const double r = 1.0 / (p01 * p23);
+  const double r01 = p23 * r, r23 = p01 * r;
+  q[0] = (n[0] * s[0]) * a[1] * r01;
+  q[1] = (n[1] * s[1]) * a[0] * r01;
+  q[2] = (n[2] * s[2]) * a[3] * r23;
+  q[3] = (n[3] * s[3]) * a[2] * r23;
+}
+GRB_HD void weno_z_fast(double um3, double um2, double um1, double u0, double up1, double up2,
+                        double& uL, double& uR) {
+  const double u[6] = {um3, um2, um1, u0, up1, up2};
+  double nL, dL, nR, dR;
+  weno_z_nd(u, nL, dL, nR, dR);
   div_pair(nL, dL, nR, dR, uL, uR);
 }
 GRB_HD void recon6_fast(int kind, const double u[6], double& uL, double& uR) {
