@@ -358,3 +358,95 @@ def test_static_metric_cache_gives_identical_steps(case, update):
         e = cons_rel_err(interior(gs1[0][:, :7], su.ngz), interior(os_[0][:, :7], su.ngz))
         assert e.max() < STEP_TOL, e
     g.set_static_metric(None)
+
+
+def _two_level_blast():
+    """Two levels of the blast wave in one block array: the [-6, 6]^3 brick
+    (dx 0.75) and a finer [-3, 3]^3 brick (dx 0.375), 8 blocks of 8^3 each,
+    as an FMR hierarchy hands its blocks of every level to one launch.
+    Returns the concatenated arrays, per-block idx and the two setups."""
+    lv = [workloads.blast(nb=(2, 2, 2), n=(8, 8, 8)),
+          workloads.blast(nb=(2, 2, 2), n=(8, 8, 8), lo=(-3, -3, -3), hi=(3, 3, 3))]
+    sus = [x[0] for x in lv]
+    f = [np.ascontiguousarray(np.concatenate([x[1][a] for x in lv])) for a in range(5)]
+    idx = np.concatenate([s.idx() for s in sus])
+    return sus, f, idx
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_two_level_blocks_in_one_launch_match_oracle(mode):
+    """Blocks of two refinement levels (different spacings) advanced by the
+    same launches: every kernel takes its spacing per block.  Ghosts are
+    filled per level; one RK3 step at the fine level's CFL against the
+    oracle, and the stable dt reduced over both levels with dx(0, q)."""
+    P = params.blast()
+    sus, f, idx = _two_level_blast()
+    nq = sum(s.nq for s in sus)
+    dt = 0.25 / idx[:, 0].max()
+    ngz, n = sus[0].ngz, sus[0].n
+    cut = [0, sus[0].nq, nq]
+    # GPU: one system for the stage, one per level for its ghost fill
+    dev = torch.device("cuda:0")
+    g = GRMHDEquationsSystem(P)
+    g.reserve(Blocks(n[0], n[1], n[2], ngz, nq, idx, device=dev))
+    g.set_mode(mode)
+    lvl = []
+    for s in sus:
+        gl = GRMHDEquationsSystem(P)
+        gl.reserve(Blocks(n[0], n[1], n[2], ngz, s.nq, s.idx(), device=dev))
+        lvl.append(gl)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    def bc(fl):
+        for t, (s, gl) in enumerate(zip(sus, lvl)):
+            a, b = cut[t], cut[t + 1]
+            gl.fill_ghosts_brick(Fields(fl.state[a:b], fl.bx[a:b], fl.by[a:b], fl.bz[a:b]), s.nb, s.periodic)
+
+    state = Fields(T(f[0]), T(f[1]), T(f[2]), T(f[3]))
+    aux = T(f[4])
+    bc(state)
+    g.compute_auxiliary_quantities(state, aux)
+    sp, spp = state.clone(), state.clone()
+    if mode == abi.MODE_TUNED:
+        g.set_static_metric(state)
+        g.autotune(sp, state, aux)
+    g.rk3_step(dt, state, sp, spp, aux, bc)
+    dx = torch.from_numpy(np.ascontiguousarray(1.0 / idx)).to(dev)  # dx(d, q) at [3 q + d]
+    dtd = torch.zeros(1, dtype=torch.float64, device=dev)
+    g.find_stable_timestep(state, aux, dx, 0.25, dtd)
+    torch.cuda.synchronize()
+    gs = [x.cpu().numpy() for x in (state.state, state.bx, state.by, state.bz)]
+    # oracle: the same hierarchy on the CPU
+    st_, bx_, by_, bz_, ax_ = [x.copy() for x in f]
+    S = _oracle.Stage(P, n[0], n[1], n[2], ngz, nq)
+    ost = [st_, bx_, by_, bz_]
+
+    def obc(fl):
+        for t, s in enumerate(sus):
+            a, b = cut[t], cut[t + 1]
+            _oracle.fill_ghosts("orc", s, [x[a:b] for x in fl])
+
+    obc(ost)
+    S.compute_aux(idx.copy(), ost, ax_)
+    osp = [x.copy() for x in ost]
+    ospp = [x.copy() for x in ost]
+    i2 = idx.copy()
+    S.reset_diag(ax_)
+    S.advance_substep(i2, dt, 1.0, osp, ost, ax_)
+    obc(osp)
+    S.compute_aux(i2, osp, ax_)
+    S.linop(ospp, ost, osp, 0.75, 0.25)
+    S.advance_substep(i2, dt, 0.25, ospp, osp, ax_)
+    obc(ospp)
+    S.compute_aux(i2, ospp, ax_)
+    S.linop(ost, ost, ospp, 1.0 / 3, 2.0 / 3.0)
+    S.advance_substep(i2, dt, 2.0 / 3.0, ost, ospp, ax_)
+    obc(ost)
+    S.compute_aux(i2, ost, ax_)
+    e = cons_rel_err(interior(gs[0][:, :7], ngz), interior(ost[0][:, :7], ngz))
+    assert e.max() < STEP_TOL, e.max()
+    for a, b in zip(gs[1:], ost[1:]):
+        assert np.max(np.abs(a - b)) < STEP_TOL * max(np.max(np.abs(b)), 1e-300)
+    dto = S.find_stable_timestep(ost, ax_, np.ascontiguousarray(1.0 / idx), 0.25)
+    assert abs(dtd.item() - dto) <= 1e-12 * dto, (dtd.item(), dto)
+    assert g.status().device_flags == 0
