@@ -167,6 +167,8 @@ PROTOTYPES = {
                                         C.c_int32, C.c_int32, C.c_int32,
                                         C.POINTER(C.c_int32), C.c_void_p]),
     "grb_set_static_metric": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.c_void_p]),
+    "grb_copy_evolved_packed": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Fields),
+                                          C.c_int32, C.c_void_p]),
     "grb_copy_evolved_interior": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.c_int32,
                                             C.POINTER(Fields), C.c_int32, C.c_void_p]),
 }

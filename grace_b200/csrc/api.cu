@@ -57,6 +57,8 @@ struct grb_handle {
   int metder_key[4] = {0, 0, 0, 0};       // nx, ny, nz, ngz it was built for
   int64_t metder_nq = 0;                  // blocks it covers
   const double* metder_idx = nullptr;     // the spacings it was built with
+  double* d_stage_io = nullptr;           // staging of grb_copy_evolved_packed
+  size_t stage_io_bytes = 0;
   uint32_t* d_auxlist = nullptr;          // cells of the tuned aux pass in one block
   uint32_t auxlist_n = 0;
   int auxlist_key[4] = {0, 0, 0, 0};      // nx, ny, nz, ngz it was built for
@@ -534,6 +536,7 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_mlp_pack);
   cudaFree(h->d_queue);
   cudaFree(h->d_auxlist);
+  cudaFree(h->d_stage_io);
   cudaFree(h->d_metder);
   delete h;
   return GRB_OK;
@@ -1259,6 +1262,67 @@ int grb_set_static_metric(grb_handle* h, const grb_grid* g, const grb_fields* st
   std::copy(key, key + 4, h->metder_key);
   h->metder_nq = G.nq;
   h->metder_idx = g->idx;
+  return GRB_OK;
+}
+
+int grb_copy_evolved_packed(grb_handle* h, const grb_grid* g, const grb_fields* host, const grb_fields* dev,
+                            int32_t to_device, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!g || !host || !dev || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->ngz < 1 || g->nq < 1)
+    return fail(h, GRB_ERR_INVALID);
+  double* hp[4] = {host->state, host->bx, host->by, host->bz};
+  double* dp[4] = {dev->state, dev->bx, dev->by, dev->bz};
+  for (int a = 0; a < 4; ++a)
+    if (!hp[a] || !dp[a]) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  if ((int64_t)GRB_N_HRSC * G.nq >= (1ll << 32) - 1) return fail(h, GRB_ERR_INVALID);
+  cudaStream_t s = (cudaStream_t)stream;
+  // packed sizes (doubles) and offsets of the four arrays in the staging
+  int64_t cnt[4], off[4], tot = 0;
+  for (int a = 0; a < 4; ++a) {
+    int n[3] = {G.nx, G.ny, G.nz};
+    if (a > 0) n[a - 1] += 1;
+    cnt[a] = (int64_t)n[0] * n[1] * n[2] * (a == 0 ? GRB_N_HRSC : 1) * G.nq;
+    off[a] = tot;
+    tot += (cnt[a] + 31) / 32 * 32;  // 256-byte aligned starts
+  }
+  if (cnt[0] >= (1ll << 32)) return fail(h, GRB_ERR_INVALID);
+  const size_t bytes = sizeof(double) * (size_t)tot;
+  if (bytes > h->stage_io_bytes) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+      return fail(h, GRB_ERR_INVALID);  // first call must come before any capture
+    cudaFree(h->d_stage_io);
+    h->d_stage_io = nullptr;
+    h->stage_io_bytes = 0;
+    if (cudaMalloc(&h->d_stage_io, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, GRB_ERR_NOMEM);
+    }
+    h->stage_io_bytes = bytes;
+  }
+  KScope ks(h, s, GRB_KIND_OTHER);
+  for (int a = 0; a < 4; ++a) {
+    int N[3] = {G.NX, G.NY, G.NZ}, n[3] = {G.nx, G.ny, G.nz};
+    if (a > 0) { N[a - 1] += 1; n[a - 1] += 1; }
+    const int nv = a == 0 ? GRB_N_HRSC : 1;
+    const int64_t vstride = (int64_t)N[0] * N[1] * N[2];
+    const int64_t qdev = vstride * (a == 0 ? GRB_N_EVOL_VARS : 1);
+    const Box b = box(G.g, G.g, G.g, n[0], n[1], n[2], (int64_t)nv * G.nq);
+    double* stg = h->d_stage_io + off[a];
+    const size_t nb = sizeof(double) * (size_t)cnt[a];
+    if (to_device) {
+      CK(cudaMemcpyAsync(stg, hp[a], nb, cudaMemcpyHostToDevice, s));
+      k_pack_interior<<<nblk(b.count(), 256), 256, 0, s>>>(b, nv, make_fastdiv((uint32_t)nv), N[0], N[1],
+                                                           vstride, qdev, false, dp[a], stg);
+    } else {
+      k_pack_interior<<<nblk(b.count(), 256), 256, 0, s>>>(b, nv, make_fastdiv((uint32_t)nv), N[0], N[1],
+                                                           vstride, qdev, true, dp[a], stg);
+      CK(cudaMemcpyAsync(hp[a], stg, nb, cudaMemcpyDeviceToHost, s));
+    }
+    ++h->launches;
+  }
+  CK(cudaGetLastError());
   return GRB_OK;
 }
 

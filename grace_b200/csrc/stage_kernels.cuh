@@ -888,6 +888,24 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, double* __restri
     if (v < nv) a[ld + v * vstride] = tmp[v];
 }
 
+// Interior of one array between the device layout and a packed interior
+// layout [nq][nv][n2][n1][n0] (no ghosts): box = the interior (lo = g),
+// x (nv variables x nq blocks) folded into the box's block index;
+// qdev: block stride of the device array; to_packed selects the direction.
+__global__ void __launch_bounds__(256) k_pack_interior(Box box, int nv, FastDiv dnv, int N0, int N1,
+                                                       int64_t vstride, int64_t qdev, bool to_packed,
+                                                       double* __restrict__ dev, double* __restrict__ packed) {
+  int i, j, k;
+  int64_t qv;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (!decode(box, t, i, j, k, qv)) return;
+  const uint32_t q = fast_div((uint32_t)qv, dnv);
+  const uint32_t v = (uint32_t)qv - q * (uint32_t)nv;
+  const int64_t o = (int64_t)q * qdev + (int64_t)v * vstride + ((int64_t)k * N1 + j) * N0 + i;
+  if (to_packed) packed[t] = dev[o];
+  else dev[o] = packed[t];
+}
+
 // Interior rows of one array between device memory and mapped host
 // memory.  box: rows at full x extent (x = 0 .. N0-1) of the interior y and
 // z ranges, x (nv variables x nq blocks) folded into the box's block index,

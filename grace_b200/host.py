@@ -178,6 +178,29 @@ class GRMHDEquationsSystem:
         _lib.check(self.lib.grb_set_static_metric(self.h, ctypes.byref(g), ctypes.byref(f) if f is not None else None,
                                                   _stream_ptr(stream)), "grb_set_static_metric")
 
+    def packed_host_fields(self, pin=True):
+        """Host Fields in the packed interior layout of grb_copy_evolved_packed."""
+        b = self.blocks
+        e = lambda *s: torch.empty(*s, dtype=torch.float64, pin_memory=pin)
+        return Fields(e(b.nq, abi.N_HRSC, b.nz, b.ny, b.nx), e(b.nq, b.nz, b.ny, b.nx + 1),
+                      e(b.nq, b.nz, b.ny + 1, b.nx), e(b.nq, b.nz + 1, b.ny, b.nx))
+
+    def copy_evolved_packed(self, host, dev, to_device, stream=None):
+        """Interior of the evolved variables between packed host tensors
+        (packed_host_fields) and the device Fields (grb_copy_evolved_packed)."""
+        b = self.blocks
+        shapes = [(b.nq, abi.N_HRSC, b.nz, b.ny, b.nx), (b.nq, b.nz, b.ny, b.nx + 1),
+                  (b.nq, b.nz, b.ny + 1, b.nx), (b.nq, b.nz + 1, b.ny, b.nx)]
+        for h, shp in zip((host.state, host.bx, host.by, host.bz), shapes):
+            if h.device.type != "cpu" or not h.is_contiguous() or h.dtype != torch.float64 or \
+                    tuple(h.shape) != shp:
+                raise ValueError(f"packed host array must be a contiguous float64 CPU tensor of shape {shp}")
+        g = b.c()
+        fh, fd = host.c(), dev.c()
+        _lib.check(self.lib.grb_copy_evolved_packed(self.h, ctypes.byref(g), ctypes.byref(fh), ctypes.byref(fd),
+                                                    1 if to_device else 0, _stream_ptr(stream)),
+                   "grb_copy_evolved_packed")
+
     def copy_evolved_interior(self, host, dev, to_device, stream=None):
         """Interior of the evolved variables between pinned host tensors and
         the device Fields `dev` (grb_copy_evolved_interior).  host: Fields of

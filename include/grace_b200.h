@@ -409,6 +409,18 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
 int grb_copy_evolved_interior(grb_handle* h, const grb_grid* g, const grb_fields* host,
                               int32_t host_state_nvars, const grb_fields* dev, int32_t to_device,
                               void* stream);
+/* No counterpart in the reference: the same interior as
+ * grb_copy_evolved_interior, with host arrays in a packed interior layout
+ * (no ghosts, LayoutLeft): host->state [nq][GRB_N_HRSC][nz][ny][nx],
+ * host->bx [nq][nz][ny][nx+1], host->by [nq][nz][ny+1][nx],
+ * host->bz [nq][nz+1][ny][nx].  Each array crosses the bus as one
+ * contiguous DMA copy through a device staging buffer owned by the handle
+ * (packed or unpacked on the device by one kernel), so the copy engine
+ * moves only interior bytes at its full rate; host arrays should be pinned.
+ * The first call allocates the staging (make it before any stream
+ * capture); an upload leaves the device ghost zones as they were. */
+int grb_copy_evolved_packed(grb_handle* h, const grb_grid* g, const grb_fields* host,
+                            const grb_fields* dev, int32_t to_device, void* stream);
 
 /* ---- scratch-free stage -------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

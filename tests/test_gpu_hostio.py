@@ -106,3 +106,36 @@ def test_unpinned_host_arrays_are_rejected():
     host = Fields(*[torch.from_numpy(x.copy()) for x in (st, bx, by, bz)])
     with pytest.raises(ValueError):
         g.copy_evolved_interior(host, dstate, to_device=True)
+
+
+def test_packed_round_trip_is_exact():
+    """grb_copy_evolved_packed: the packed host arrays hold exactly the
+    interior of the device arrays (download), an upload writes exactly the
+    interior back and leaves ghosts and the non-evolved variables alone."""
+    su, f = workloads.blast(nb=(2, 2, 1), n=(8, 8, 8))
+    g, dev = _system(su, params.blast())
+    st, bx, by, bz = [np.ascontiguousarray(x) for x in f[:4]]
+    d = Fields(*[torch.from_numpy(x).to(dev) for x in (st, bx, by, bz)])
+    host = g.packed_host_fields()
+    g.copy_evolved_packed(host, d, to_device=False)
+    torch.cuda.synchronize()
+    G = su.ngz
+    nx, ny, nz = su.n
+    np.testing.assert_array_equal(host.state.numpy(), st[:, :abi.N_HRSC, G:G + nz, G:G + ny, G:G + nx])
+    np.testing.assert_array_equal(host.bx.numpy(), bx[:, G:G + nz, G:G + ny, G:G + nx + 1])
+    np.testing.assert_array_equal(host.by.numpy(), by[:, G:G + nz, G:G + ny + 1, G:G + nx])
+    np.testing.assert_array_equal(host.bz.numpy(), bz[:, G:G + nz + 1, G:G + ny, G:G + nx])
+    rng = np.random.default_rng(3)
+    for h in (host.state, host.bx, host.by, host.bz):
+        h.copy_(torch.from_numpy(rng.standard_normal(tuple(h.shape))))
+    before = [x.cpu().numpy().copy() for x in (d.state, d.bx, d.by, d.bz)]
+    g.copy_evolved_packed(host, d, to_device=True)
+    torch.cuda.synchronize()
+    after = [x.cpu().numpy() for x in (d.state, d.bx, d.by, d.bz)]
+    exp = [before[0].copy(), before[1].copy(), before[2].copy(), before[3].copy()]
+    exp[0][:, :abi.N_HRSC, G:G + nz, G:G + ny, G:G + nx] = host.state.numpy()
+    exp[1][:, G:G + nz, G:G + ny, G:G + nx + 1] = host.bx.numpy()
+    exp[2][:, G:G + nz, G:G + ny + 1, G:G + nx] = host.by.numpy()
+    exp[3][:, G:G + nz + 1, G:G + ny, G:G + nx] = host.bz.numpy()
+    for a, b in zip(after, exp):
+        np.testing.assert_array_equal(a, b)
