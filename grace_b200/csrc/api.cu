@@ -1273,11 +1273,13 @@ int grb_copy_evolved_packed(grb_handle* h, const grb_grid* g, const grb_fields* 
   double* hp[4] = {host->state, host->bx, host->by, host->bz};
   double* dp[4] = {dev->state, dev->bx, dev->by, dev->bz};
   for (int a = 0; a < 4; ++a)
-    if (!hp[a] || !dp[a]) return fail(h, GRB_ERR_INVALID);
+    if (!hp[a] != !dp[a]) return fail(h, GRB_ERR_INVALID);  // both null: array skipped
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   if ((int64_t)GRB_N_HRSC * G.nq >= (1ll << 32) - 1) return fail(h, GRB_ERR_INVALID);
   cudaStream_t s = (cudaStream_t)stream;
   // packed sizes (doubles) and offsets of the four arrays in the staging
+  // (each array has its own region, so calls on different streams that
+  // move different arrays do not share staging)
   int64_t cnt[4], off[4], tot = 0;
   for (int a = 0; a < 4; ++a) {
     int n[3] = {G.nx, G.ny, G.nz};
@@ -1303,6 +1305,7 @@ int grb_copy_evolved_packed(grb_handle* h, const grb_grid* g, const grb_fields* 
   }
   KScope ks(h, s, GRB_KIND_OTHER);
   for (int a = 0; a < 4; ++a) {
+    if (!hp[a]) continue;
     int N[3] = {G.NX, G.NY, G.NZ}, n[3] = {G.nx, G.ny, G.nz};
     if (a > 0) { N[a - 1] += 1; n[a - 1] += 1; }
     const int nv = a == 0 ? GRB_N_HRSC : 1;

@@ -185,9 +185,10 @@ class GRMHDEquationsSystem:
         return Fields(e(b.nq, abi.N_HRSC, b.nz, b.ny, b.nx), e(b.nq, b.nz, b.ny, b.nx + 1),
                       e(b.nq, b.nz, b.ny + 1, b.nx), e(b.nq, b.nz + 1, b.ny, b.nx))
 
-    def copy_evolved_packed(self, host, dev, to_device, stream=None):
+    def copy_evolved_packed(self, host, dev, to_device, stream=None, arrays=(True, True, True, True)):
         """Interior of the evolved variables between packed host tensors
-        (packed_host_fields) and the device Fields (grb_copy_evolved_packed)."""
+        (packed_host_fields) and the device Fields (grb_copy_evolved_packed);
+        `arrays` selects state, bx, by, bz."""
         b = self.blocks
         shapes = [(b.nq, abi.N_HRSC, b.nz, b.ny, b.nx), (b.nq, b.nz, b.ny, b.nx + 1),
                   (b.nq, b.nz, b.ny + 1, b.nx), (b.nq, b.nz + 1, b.ny, b.nx)]
@@ -196,7 +197,9 @@ class GRMHDEquationsSystem:
                     tuple(h.shape) != shp:
                 raise ValueError(f"packed host array must be a contiguous float64 CPU tensor of shape {shp}")
         g = b.c()
-        fh, fd = host.c(), dev.c()
+        ph = [x.data_ptr() if on else None for x, on in zip((host.state, host.bx, host.by, host.bz), arrays)]
+        pd = [x.data_ptr() if on else None for x, on in zip((dev.state, dev.bx, dev.by, dev.bz), arrays)]
+        fh, fd = abi.Fields(*ph), abi.Fields(*pd)
         _lib.check(self.lib.grb_copy_evolved_packed(self.h, ctypes.byref(g), ctypes.byref(fh), ctypes.byref(fd),
                                                     1 if to_device else 0, _stream_ptr(stream)),
                    "grb_copy_evolved_packed")
@@ -335,12 +338,16 @@ class GRMHDEquationsSystem:
 
     # --- evolve_impl<eos_t>() RK3 branch (evolve.cpp:147-225, 427-428) -----
     def rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, stream=None, next_dt=None,
-                 fused_dt=False):
+                 fused_dt=False, after_update=None):
         """One SSP-RK3 step.  `bc(fields)` applies the boundary conditions
         (GRACE's amr::apply_boundary_conditions); on entry aux holds the
         primitives of `state` and state_p equals state.  next_dt = (dx, cfl,
         dt_out): the step ends with find_stable_timestep into dt_out, as a
-        separate pass after the last aux pass or, with fused_dt, inside it."""
+        separate pass after the last aux pass or, with fused_dt, inside it.
+        after_update(): called (host side, stream order) right after the last
+        substep, when the interior face B of `state` is final (the boundary
+        fill and the aux pass that follow change only ghosts and cell
+        variables)."""
         self.reset_c2p_diagnostics(aux, stream)
         self.advance_substep(t, dt, 1.0, state_p, state, aux, stream)
         bc(state_p)
@@ -351,6 +358,8 @@ class GRMHDEquationsSystem:
         self.compute_auxiliary_quantities(state_pp, aux, stream)
         self.linop_apply(state, state, state_pp, 1.0 / 3, 2.0 / 3.0, stream)
         self.advance_substep(t, dt, 2.0 / 3.0, state, state_pp, aux, stream)
+        if after_update is not None:
+            after_update()
         bc(state)
         if next_dt is not None and fused_dt:
             self.compute_auxiliary_quantities_dt(state, aux, *next_dt, stream=stream)

@@ -418,7 +418,10 @@ int grb_copy_evolved_interior(grb_handle* h, const grb_grid* g, const grb_fields
  * (packed or unpacked on the device by one kernel), so the copy engine
  * moves only interior bytes at its full rate; host arrays should be pinned.
  * The first call allocates the staging (make it before any stream
- * capture); an upload leaves the device ghost zones as they were. */
+ * capture); an upload leaves the device ghost zones as they were.  An array
+ * whose host and device pointers are both NULL is skipped; each array has
+ * its own staging region, so calls that move different arrays may run on
+ * different streams at the same time. */
 int grb_copy_evolved_packed(grb_handle* h, const grb_grid* g, const grb_fields* host,
                             const grb_fields* dev, int32_t to_device, void* stream);
 

@@ -139,3 +139,22 @@ def test_packed_round_trip_is_exact():
     exp[3][:, G:G + nz + 1, G:G + ny, G:G + nx] = host.bz.numpy()
     for a, b in zip(after, exp):
         np.testing.assert_array_equal(a, b)
+
+
+def test_packed_copy_by_array_on_two_streams():
+    """Face B downloaded on a second stream and the cell variables on the
+    current one (the e2e leg's overlap) give the one-call download."""
+    su, f = workloads.blast(nb=(2, 1, 1), n=(8, 8, 8))
+    g, dev = _system(su, params.blast())
+    d = Fields(*[torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in f[:4]])
+    ref, split = g.packed_host_fields(), g.packed_host_fields()
+    for h in (split.state, split.bx, split.by, split.bz):
+        h.zero_()
+    g.copy_evolved_packed(ref, d, to_device=False)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    g.copy_evolved_packed(split, d, to_device=False, stream=side, arrays=(False, True, True, True))
+    g.copy_evolved_packed(split, d, to_device=False, arrays=(True, False, False, False))
+    torch.cuda.synchronize()
+    for a, b in zip((split.state, split.bx, split.by, split.bz), (ref.state, ref.bx, ref.by, ref.bz)):
+        assert torch.equal(a, b)
