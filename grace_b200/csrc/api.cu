@@ -186,6 +186,7 @@ struct KScope {
 // ---- tuned-mode variant dispatch (launch-bounds register caps) -------------
 // kMinB[v]: minimum resident CTAs of 128 threads per SM requested from the
 // compiler; 1 leaves the register count free, 4 caps it at 128, 5 at 102.
+constexpr int kMaxDevices = 64;  // device ordinals tracked by per-device launch set-up
 constexpr int kMinB[3] = {1, 4, 5};
 // The update kernel that reads the static-metric cache: 1, 3, 4.
 constexpr int kMinBCached[3] = {1, 3, 4};
@@ -243,12 +244,15 @@ bool launch_flux_tma(cudaStream_t s, const DevParams& P, const Geo& G, const Box
   if (!make_tmap(&ta, aux, G, GRB_N_AUX_VARS, b.nq, T) || !make_tmap(&tm, st, G, GRB_N_EVOL_VARS, b.nq, T))
     return false;
   const size_t smem = flux_tile_smem(G, T);
-  static size_t attr = 0;
-  if (smem > attr) {
+  // the attribute is per device: remember what each device ordinal got
+  static size_t attr[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+  if (smem > attr[dev]) {
     if (cudaFuncSetAttribute(k_flux_tma<dir, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
       return false;
-    attr = smem;
+    attr[dev] = smem;
   }
   const int nrow = dir == 2 ? T.n[2] : T.n[1];
   const int nother = dir == 2 ? T.n[1] : T.n[2];
@@ -299,13 +303,18 @@ template <int MINB, bool kDt>
 void launch_aux_queue(cudaStream_t s, const DevParams& P, const Geo& G, const Box& b, double* st, const double* bx,
                       const double* by, const double* bz, double* aux, const double* idx, const double* crd,
                       const StageBufs& B, unsigned long long* queue, const DtArgs& dta) {
-  static int grid = 0;
+  // one wave of CTAs, per device ordinal
+  static int grids[kMaxDevices] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int grid = 0;
+  if (dev >= 0 && dev < kMaxDevices) grid = grids[dev];
   if (grid == 0) {
-    int dev = 0, sms = 0, occ = 0;
-    cudaGetDevice(&dev);
+    int sms = 0, occ = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_aux_queue<MINB, kDt, true>, 128, 0);
     grid = (sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+    if (dev >= 0 && dev < kMaxDevices) grids[dev] = grid;
   }
   cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
   k_aux_queue<MINB, kDt, true><<<grid, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, dta);
