@@ -24,6 +24,15 @@
  * entry point returns GRB_OK (0) or a negative GRB_ERR_* code; device-side
  * fatal conditions (the reference's Kokkos::abort sites) are recorded in a
  * device status word read back by grb_get_status(), never by a trap.
+ *
+ * A handle belongs to one host thread and one device at a time (GRACE: one
+ * rank, one stream): its scratch, work-queue counter, tuned-mode lists and
+ * caches are shared by the calls made through it, so two calls on the same
+ * handle must not overlap on the GPU (order them on one stream, or use one
+ * handle per stream).  The exception is grb_copy_evolved_packed on
+ * different arrays, documented there.  First calls that allocate (reserve,
+ * the tuned aux list, the copy staging, the static-metric cache) must come
+ * before any stream capture that records the handle's work.
  */
 #ifndef GRACE_B200_H
 #define GRACE_B200_H
