@@ -438,8 +438,8 @@ GRB_HD WB wb_of(const Met& m, const double pr[13]) {
   const double* z = pr + GRB_P_ZX;
   const double* B = pr + GRB_P_BX;
   o.z2 = z[0] * zl[0] + z[1] * zl[1] + z[2] * zl[2];
-  o.W = sqrt(1. + o.z2);
-  o.iW = 1.0 / o.W;
+  o.iW = rsqrt(1. + o.z2);  // 1/W; W = (1 + z^2) / W without a square root
+  o.W = (1. + o.z2) * o.iW;
   o.Bz = B[0] * zl[0] + B[1] * zl[1] + B[2] * zl[2];
   o.b2 = (sqs(m.g, B) + o.Bz * o.Bz) * o.iW * o.iW;
   return o;

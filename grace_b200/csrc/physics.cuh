@@ -79,8 +79,8 @@ struct DevParams {
 struct Met {
   double g[6], beta[3], alp, gi[6], sqrtg, isqrtg, ialp;
 };
-// FAST (tuned mode): 1/det and 1/alpha from one reciprocal of det * alpha,
-// and 1/sqrt(gamma) = sqrt(gamma) / det.
+// FAST (tuned mode): 1/sqrt(gamma) = rsqrt(det), sqrt(gamma) = det / sqrt(det)
+// and 1/det = (1/sqrt(gamma))^2, so no square root and one division (1/alpha).
 template <bool FAST = false>
 GRB_HD Met make_met(const double g[6], const double b[3], double alp) {
   Met m;
@@ -93,11 +93,11 @@ GRB_HD Met make_met(const double g[6], const double b[3], double alp) {
   const double c1 = g[2] * g[4] - g[1] * g[5];
   const double c2 = g[1] * g[4] - g[2] * g[3];
   const double det = g[0] * c0 + g[1] * c1 + g[2] * c2;
-  double id;
+  double id, isg = 0.0;
   if (FAST) {
-    const double r = 1.0 / (det * alp);
-    id = alp * r;
-    m.ialp = det * r;
+    isg = rsqrt(det);
+    id = isg * isg;
+    m.ialp = 1.0 / alp;
   } else {
     id = 1.0 / det;
     m.ialp = 0.0;
@@ -108,8 +108,8 @@ GRB_HD Met make_met(const double g[6], const double b[3], double alp) {
   m.gi[3] = (g[0] * g[5] - g[2] * g[2]) * id;
   m.gi[4] = (g[1] * g[2] - g[0] * g[4]) * id;
   m.gi[5] = (g[0] * g[3] - g[1] * g[1]) * id;
-  m.sqrtg = sqrt(det);
-  m.isqrtg = FAST ? m.sqrtg * id : 0.0;
+  m.sqrtg = FAST ? det * isg : sqrt(det);
+  m.isqrtg = isg;
   return m;
 }
 GRB_HD double sqs(const double s[6], const double v[3]) {

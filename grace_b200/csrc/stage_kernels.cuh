@@ -32,14 +32,23 @@ __device__ __forceinline__ void mhd_fluxes(const DevParams& P, bool rusanov,
                                            double* pl, double* pr, const Met& m, double f[7],
                                            double vb[4]) {
   const double alp = m.alp, sqrtg = m.sqrtg;
-  const double wl = lorentz(m.g, pl + GRB_P_ZX), wr = lorentz(m.g, pr + GRB_P_ZX);
+  double wl, wr, iwl = 0.0, iwr = 0.0;
+  if (FAST) {
+    // 1/W = rsqrt(1 + z^2), W = (1 + z^2) / W: no square root, no division
+    const double ql = 1. + sqs(m.g, pl + GRB_P_ZX), qr = 1. + sqs(m.g, pr + GRB_P_ZX);
+    iwl = rsqrt(ql);
+    iwr = rsqrt(qr);
+    wl = ql * iwl;
+    wr = qr * iwr;
+  } else {
+    wl = lorentz(m.g, pl + GRB_P_ZX);
+    wr = lorentz(m.g, pr + GRB_P_ZX);
+  }
   double bl[4], br[4], b2l, b2r, vtl[3], vtr[3];
   const double gdd = dir == 0 ? m.gi[0] : dir == 1 ? m.gi[3] : m.gi[5];
   double cml, cpl, cmr, cpr, cmin, cmax;
   const double ialp = m.ialp;  // FAST: set by make_met<true>
   if (FAST) {
-    double iwl, iwr;
-    div_pair(1.0, wl, 1.0, wr, iwl, iwr);
     comoving_b_f(alp, ialp, m.beta, m.g, pl + GRB_P_BX, pl + GRB_P_ZX, wl, iwl, bl, b2l);
     comoving_b_f(alp, ialp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, wr, iwr, br, b2r);
     vtilde_f(alp, m.beta, pl + GRB_P_ZX, iwl, vtl);
