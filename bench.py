@@ -430,7 +430,7 @@ def ours(args, rank, world, local_rank):
 
 def c2p_bench(dev, learned=True, n=1 << 24, reps=5):
     import torch
-    from grace_b200 import params, workloads
+    from grace_b200 import abi, params, workloads
     from grace_b200.host import GRMHDEquationsSystem
     cons, _ = workloads.c2p_states(n, seed=5)
     gc = GRMHDEquationsSystem(params.c2p_bench())
@@ -463,6 +463,10 @@ def c2p_bench(dev, learned=True, n=1 << 24, reps=5):
 
     out = {"states": n, "tolerance": 1e-12, "plain_solves_per_s": timed(False)}
     pr_p, out["plain"] = iters(False)
+    # the tuned-mode c2p arithmetic on the same states (plain bracket)
+    gc.set_mode(abi.MODE_TUNED)
+    out["tuned_solves_per_s"] = timed(False)
+    gc.set_mode(abi.MODE_PLAIN)
     if learned:
         tr, _ = workloads.c2p_states(1 << 20, seed=6)
         rep = gc.train_c2p_model(torch.from_numpy(tr).to(dev))

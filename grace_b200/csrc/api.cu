@@ -853,12 +853,20 @@ int launch_c2p(grb_handle* h, int64_t n, const double* cons, const double* metri
   C2PDiagDev d{nullptr, nullptr, nullptr, nullptr};
   if (diag) d = C2PDiagDev{diag->iters, diag->guess_used, diag->mu, diag->bracket};
   if (n > (int64_t)kC2PThreads * 0x7fffffff) return fail(h, GRB_ERR_INVALID);
-  if (learned)
-    k_c2p_batch<true><<<nblk(n, kC2PThreads), kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err,
-                                                                   d, h->d_mlp_pack, h->d_flags);
+  const unsigned nb = nblk(n, kC2PThreads);
+  const bool fast = h->mode == GRB_MODE_TUNED;
+  if (learned && fast)
+    k_c2p_batch<true, true><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d,
+                                                       h->d_mlp_pack, h->d_flags);
+  else if (learned)
+    k_c2p_batch<true><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, h->d_mlp_pack,
+                                                 h->d_flags);
+  else if (fast)
+    k_c2p_batch<false, true><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, nullptr,
+                                                        h->d_flags);
   else
-    k_c2p_batch<false><<<nblk(n, kC2PThreads), kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err,
-                                                                    d, nullptr, h->d_flags);
+    k_c2p_batch<false><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, nullptr,
+                                                  h->d_flags);
   ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;

@@ -340,7 +340,8 @@ __global__ void __launch_bounds__(256) k_mlp_pack(const float* __restrict__ P, M
 
 // One state per thread.  With the learned bracket every lane of a warp takes
 // part in the network (lanes past n with neutral inputs), then returns.
-template <bool kLearned>
+// kFast: the tuned-mode c2p arithmetic (same functions up to rounding).
+template <bool kLearned, bool kFast = false>
 __global__ void __launch_bounds__(kC2PThreads) k_c2p_batch(DevParams P, int64_t n, const double* __restrict__ cons,
                                                           const double* __restrict__ metric,
                                                           double* __restrict__ prims, double* __restrict__ cons_out,
@@ -377,7 +378,7 @@ __global__ void __launch_bounds__(kC2PThreads) k_c2p_batch(DevParams P, int64_t 
       gs = mlp_bracket(S.net.nrm, out, mu0);
     }
     if (!active) return;
-    const C2POut o = c2p(c, pr, m, P, 0.0, false, P.alp_bh_thresh, gs);
+    const C2POut o = c2p<kFast>(c, pr, m, P, 0.0, false, P.alp_bh_thresh, gs);
     if (o.fatal) atomicOr(flags, o.fatal);
     pr[GRB_P_CS2] = 0.0;
 #pragma unroll

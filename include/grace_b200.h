@@ -260,7 +260,9 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A,
  *   use_learned: 1 = start the Kastaun root solve from the learned bracket
  *          of the model made by grb_c2p_train or grb_c2p_model_set (per
  *          state, the plain bracket when the learned one misses the root);
- *          GRB_ERR_NO_MODEL without a model. */
+ *          GRB_ERR_NO_MODEL without a model.
+ * GRB_MODE_TUNED evaluates the c2p with the tuned-mode arithmetic (the same
+ * functions up to rounding: fewer divisions, W and b^2 formed once). */
 int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons,
                   const double* metric, double* prims, double* cons_out,
                   uint32_t* err, int32_t use_learned, void* stream);

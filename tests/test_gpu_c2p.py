@@ -11,9 +11,10 @@ from parity import PRIM_TOL, prim_tol, state_residual
 pytestmark = pytest.mark.gpu
 
 
-def _compare(P, cons, metric=None):
+def _compare(P, cons, metric=None, mode=abi.MODE_PLAIN):
     dev = torch.device("cuda:0")
     sysg = GRMHDEquationsSystem(P)
+    sysg.set_mode(mode)
     c_d = torch.from_numpy(np.ascontiguousarray(cons)).to(dev)
     m_d = torch.from_numpy(np.ascontiguousarray(metric)).to(dev) if metric is not None else None
     n = cons.shape[1]
@@ -25,13 +26,15 @@ def _compare(P, cons, metric=None):
     return pr_g, co_d.cpu().numpy(), err_g, pr_o, co_o, err_o
 
 
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
 @pytest.mark.parametrize("preset", ["c2p_bench", "blast"])
-def test_c2p_batch_matches_oracle(preset):
+def test_c2p_batch_matches_oracle(preset, mode):
+    """Plain mode: the reference's operations; tuned mode: the tuned c2p
+    arithmetic (same functions up to rounding), both within the W^2-aware
+    1e-12 bound of the oracle."""
     P = getattr(params, preset)()
     cons, _ = workloads.c2p_states(50000, seed=11)
-    if preset == "blast":  # ideal gas: reinterpret the same states
-        pass
-    pr_g, co_g, err_g, pr_o, co_o, err_o = _compare(P, cons)
+    pr_g, co_g, err_g, pr_o, co_o, err_o = _compare(P, cons, mode=mode)
     assert (err_g == err_o).mean() > 0.999
     same = err_g == err_o
     tol = prim_tol(pr_o)[same]
