@@ -59,6 +59,9 @@ struct grb_handle {
   const double* metder_idx = nullptr;     // the spacings it was built with
   double* d_stage_io = nullptr;           // staging of grb_copy_evolved_packed
   size_t stage_io_bytes = 0;
+  uint32_t* d_ghostruns = nullptr;        // ghost runs of k_ghost_runs, 3 arrays
+  int ghost_off[3] = {0, 0, 0}, ghost_cnt[3] = {0, 0, 0};
+  int ghost_key[4] = {0, 0, 0, 0};        // nx, ny, nz, ngz they were built for
   uint32_t* d_auxlist = nullptr;          // cells of the tuned aux pass in one block
   uint32_t auxlist_n = 0;
   int auxlist_key[4] = {0, 0, 0, 0};      // nx, ny, nz, ngz it was built for
@@ -545,6 +548,7 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_mlp_pack);
   cudaFree(h->d_queue);
   cudaFree(h->d_auxlist);
+  cudaFree(h->d_ghostruns);
   cudaFree(h->d_stage_io);
   cudaFree(h->d_metder);
   delete h;
@@ -1173,6 +1177,50 @@ int grb_c2p_model_set(grb_handle* h, const float* params, int64_t nparams) {
   return GRB_OK;
 }
 
+// Ghost runs of k_ghost_runs for this block geometry (ghost width 4,
+// interiors multiples of 4 along x, blocks up to 255 rows a side), built
+// now if needed and possible (not inside a stream capture); false when the
+// run form does not apply.
+static bool ghost_runs(grb_handle* h, const Geo& G, cudaStream_t s) {
+  if (G.g != 4 || G.nx % 4 || G.NY + 1 > 255 || G.NZ + 1 > 255 || G.NX / 4 > 255) return false;
+  const int key[4] = {G.nx, G.ny, G.nz, G.g};
+  if (h->d_ghostruns && std::equal(key, key + 4, h->ghost_key)) return true;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return false;
+  std::vector<uint32_t> v;
+  int off[3], cnt[3];
+  const int nr = G.NX / 4;
+  for (int a = 0; a < 3; ++a) {  // cells, faces staggered along y, z
+    const int N1 = G.NY + (a == 1), N2 = G.NZ + (a == 2);
+    const int hi1 = G.ny + G.g + (a == 1), hi2 = G.nz + G.g + (a == 2);
+    off[a] = (int)v.size();
+    for (int k = 0; k < N2; ++k)
+      for (int j = 0; j < N1; ++j) {
+        const bool row_ghost = j < G.g || j >= hi1 || k < G.g || k >= hi2;
+        for (int r = 0; r < nr; ++r)
+          if (row_ghost || r == 0 || r == nr - 1)
+            v.push_back((uint32_t)r | (uint32_t)j << 8 | (uint32_t)k << 16);
+      }
+    cnt[a] = (int)v.size() - off[a];
+  }
+  uint32_t* d = nullptr;
+  if (cudaMalloc(&d, v.size() * sizeof(uint32_t)) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (cudaMemcpy(d, v.data(), v.size() * sizeof(uint32_t), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(d);
+    cudaGetLastError();
+    return false;
+  }
+  cudaFree(h->d_ghostruns);
+  h->d_ghostruns = d;
+  std::copy(off, off + 3, h->ghost_off);
+  std::copy(cnt, cnt + 3, h->ghost_cnt);
+  std::copy(key, key + 4, h->ghost_key);
+  return true;
+}
+
 int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
                           int32_t nby, int32_t nbz, const int32_t* periodic, void* stream) {
   if (!h) return GRB_ERR_INVALID;
@@ -1190,9 +1238,24 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
   const int64_t total = (int64_t)std::max({G.NX + 1, G.NY + 1, G.NZ + 1}) *
                         std::max({G.NX * G.NY, G.NY * G.NZ, G.NX * G.NZ});
   if (total > (1ll << 31) - 256) return fail(h, GRB_ERR_INVALID);
-  const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq, 4u);
-  k_ghost<<<grid, 256, 0, s>>>(G, br, f->state, bf[0], bf[1], bf[2]);
-  ++h->launches;
+  const bool aligned = (((uintptr_t)f->state | (uintptr_t)bf[1] | (uintptr_t)bf[2]) & 15) == 0;
+  if (aligned && ghost_runs(h, G, s)) {
+    // 4-cell runs for the cells and the y, z face arrays; the x face array
+    // (rows of NX+1) by the per-cell kernel
+    const int* o = h->ghost_off;
+    const int* c = h->ghost_cnt;
+    const int mx = std::max({c[0], c[1], c[2]});
+    const dim3 gr((unsigned)((mx + 127) / 128), (unsigned)G.nq, 3u);
+    k_ghost_runs<<<gr, 128, 0, s>>>(G, br, h->d_ghostruns, make_int3(o[0], o[1], o[2]), make_int3(c[0], c[1], c[2]),
+                                    f->state, bf[1], bf[2]);
+    const dim3 gx((unsigned)((total + 255) / 256), (unsigned)G.nq, 1u);
+    k_ghost<<<gx, 256, 0, s>>>(G, br, f->state, bf[0], bf[1], bf[2], 1);
+    h->launches += 2;
+  } else {
+    const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq, 4u);
+    k_ghost<<<grid, 256, 0, s>>>(G, br, f->state, bf[0], bf[1], bf[2]);
+    ++h->launches;
+  }
   CK(cudaGetLastError());
   return GRB_OK;
 }

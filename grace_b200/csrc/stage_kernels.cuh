@@ -860,8 +860,8 @@ __device__ __forceinline__ bool ghost_map(int x, int nin, int g, bool stag, bool
 // arithmetic (q < 65536, a block's cells < 2^31).
 __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, double* __restrict__ cells,
                                               double* __restrict__ fx, double* __restrict__ fy,
-                                              double* __restrict__ fz) {
-  const int fd = (int)blockIdx.z - 1;
+                                              double* __restrict__ fz, int z0 = 0) {
+  const int fd = (int)blockIdx.z + z0 - 1;
   const int q = blockIdx.y;
   int n[3] = {G.NX, G.NY, G.NZ};
   if (fd >= 0) n[fd] += 1;
@@ -895,6 +895,66 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, double* __restri
 #pragma unroll
   for (int v = 0; v < GRB_N_HRSC; ++v)
     if (v < nv) a[ld + v * vstride] = tmp[v];
+}
+
+// The same fill in runs of 4 cells along x, for ghost width 4 and interior
+// extents along x that are multiples of 4 (so runs never straddle the
+// interior's edge) on arrays whose rows are 4-aligned (not staggered along
+// x): blockIdx.z = 0 the cell-centred HRSC variables, 1, 2 the face arrays
+// staggered along y, z; runs + off[a] lists array a's ghost runs, packed
+// r | j << 8 | k << 16 (x in [4r, 4r + 4) of row (j, k)).  Each thread
+// copies one run with 16-byte loads and stores: the matching run of its
+// source row, or one cell repeated where zero-gradient applies along x.
+__global__ void __launch_bounds__(128) k_ghost_runs(Geo G, Brick br, const uint32_t* __restrict__ runs,
+                                                   int3 off, int3 cnt, double* __restrict__ cells,
+                                                   double* __restrict__ fy, double* __restrict__ fz) {
+  const int arr = blockIdx.z;
+  const int len = arr == 0 ? cnt.x : arr == 1 ? cnt.y : cnt.z;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= len) return;
+  const uint32_t e = __ldg(runs + (arr == 0 ? off.x : arr == 1 ? off.y : off.z) + t);
+  const int r = (int)(e & 0xffu), c1 = (int)((e >> 8) & 0xffu), c2 = (int)(e >> 16);
+  const int fd = arr == 0 ? -1 : arr;  // staggered axis (1: y, 2: z)
+  int n[3] = {G.NX, G.NY, G.NZ};
+  if (fd > 0) n[fd] += 1;
+  double* a = arr == 0 ? cells : arr == 1 ? fy : fz;
+  const int q = blockIdx.y;
+  const int nin[3] = {G.nx, G.ny, G.nz};
+  const int nb[3] = {br.nbx, br.nby, br.nbz};
+  const int qyz = q / br.nbx;
+  const int qc[3] = {q - qyz * br.nbx, qyz % br.nby, qyz / br.nby};
+  int sx, sy, sz, ox, oy, oz;
+  const int x0 = 4 * r;
+  ghost_map(x0, nin[0], G.g, false, br.periodic[0] != 0, qc[0], nb[0], sx, ox);
+  ghost_map(c1, nin[1], G.g, fd == 1, br.periodic[1] != 0, qc[1], nb[1], sy, oy);
+  ghost_map(c2, nin[2], G.g, fd == 2, br.periodic[2] != 0, qc[2], nb[2], sz, oz);
+  // along x: a ghost run whose first cell maps to the boundary cell is a
+  // zero-gradient run (every cell copies that one cell); otherwise the
+  // run maps to the run at the same offset
+  int sxe;
+  int oxe;
+  ghost_map(x0 + 3, nin[0], G.g, false, br.periodic[0] != 0, qc[0], nb[0], sxe, oxe);
+  const bool bcast = sxe == sx;
+  const int qs = (qc[0] + ox + nb[0]) % nb[0] +
+                 br.nbx * ((qc[1] + oy + nb[1]) % nb[1] + br.nby * ((qc[2] + oz + nb[2]) % nb[2]));
+  const int nv = arr == 0 ? GRB_N_HRSC : 1;
+  const int64_t vstride = (int64_t)n[0] * n[1] * n[2];
+  const int64_t qstride = vstride * (arr == 0 ? GRB_N_EVOL_VARS : 1);
+  const int64_t ld = (x0 + n[0] * (c1 + n[1] * c2)) + (int64_t)q * qstride;
+  const int64_t ls = (sx + n[0] * (sy + n[1] * sz)) + (int64_t)qs * qstride;
+  for (int v = 0; v < nv; ++v) {
+    double2* d = reinterpret_cast<double2*>(a + ld + v * vstride);
+    if (bcast) {
+      const double x = a[ls + v * vstride];
+      d[0] = make_double2(x, x);
+      d[1] = make_double2(x, x);
+    } else {
+      const double2* sp = reinterpret_cast<const double2*>(a + ls + v * vstride);
+      const double2 u0 = sp[0], u1 = sp[1];
+      d[0] = u0;
+      d[1] = u1;
+    }
+  }
 }
 
 // Interior of one array between the device layout and a packed interior
