@@ -62,6 +62,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--eager", action="store_true", help="launch the timed steps eagerly, not as a CUDA graph")
     ap.add_argument("--no-c2p", action="store_true")
+    ap.add_argument("--no-restrict", action="store_true", help="skip the FMR restriction measurement")
     ap.add_argument("--no-learned", action="store_true", help="c2p leg: plain bracket only")
     ap.add_argument("--c2p-only", action="store_true", help="run only the c2p micro-benchmark")
     ap.add_argument("--c2p-states", type=int, default=1 << 24, help="states of the c2p micro-benchmark")
@@ -368,6 +369,40 @@ def ours(args, rank, world, local_rank):
                        "substep has made it final); each step refills the ghost zones and recomputes the "
                        "primitives of the uploaded state first"}
 
+    # --- FMR restriction into coarse buffers (a separate measurement, not
+    # part of the step): every block restricted into a buffer, the 7 HRSC
+    # variables by the 8-cell average, the 16 metric and curvature variables
+    # by the 5-point Lagrange operator, and the three face-B arrays
+    restrict = None
+    if not args.no_restrict and args.mode == "tuned":
+        nq = su.nq
+        qs = torch.arange(nq, dtype=torch.int64, device=dev)
+        ch = (qs % 8).to(torch.uint8)
+        lo, hi = list(range(abi.N_HRSC)), list(range(abi.N_HRSC, abi.N_EVOL_VARS))
+        run = lambda: g.restrict_to_coarse(state, spp, qs, qs, ch, lo, hi)
+        for _ in range(2):
+            run()
+        torch.cuda.synchronize()
+        r0 = torch.cuda.Event(enable_timing=True)
+        r1 = torch.cuda.Event(enable_timing=True)
+        reps = 5
+        r0.record()
+        for _ in range(reps):
+            run()
+        r1.record()
+        torch.cuda.synchronize()
+        rms = r0.elapsed_time(r1) / reps
+        # algorithmic bytes: fine interior read once, coarse interior written
+        cells, ccells = n ** 3, (n // 2) ** 3
+        fcells = (n + 1) * n * n
+        cfaces = (n // 2 + 1) * (n // 2) ** 2
+        rbytes = 8 * nq * (abi.N_EVOL_VARS * (cells + ccells) + 3 * (fcells + cfaces))
+        restrict = {"quads": nq, "ms": rms, "fine_cells_per_s": nq * cells / (rms * 1e-3),
+                    "achieved_GBps": rbytes / (rms * 1e-3) / 1e9,
+                    "note": "23 state variables (7 by the 8-cell average, 16 by the 5-point Lagrange "
+                            "restriction) and the three face-B arrays of every block; bytes = the fine "
+                            "interior read once plus the coarse image written"}
+
     # --- dominant kernel roofline (HBM), measured over the timed region
     peaks = {}
     try:
@@ -376,6 +411,9 @@ def ours(args, rank, world, local_rank):
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    if restrict is not None:
+        restrict["hbm_frac"] = restrict["achieved_GBps"] / hbm
+        restrict["peak_source"] = peak_src
     top = max(kt.items(), key=lambda kv: kv[1][0])
     name, (kms, kcnt) = top
     # faces one flux launch (one direction) computes: the reference's full
@@ -429,7 +467,7 @@ def ours(args, rank, world, local_rank):
             "clocks": clk, "gpu_launches": launches,
             "kernel_ms": {k: round(v[0], 3) for k, v in kt.items() if v[1]},
             "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "c2p": c2p,
-            "mode": args.mode, "plain_form": plain, "tuning": tuning,
+            "mode": args.mode, "plain_form": plain, "tuning": tuning, "restrict": restrict,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "grace_b200.h"
+#include "amr.cuh"
 #include "flux_tma.cuh"
 #include "mlp.cuh"
 #include "stage_kernels.cuh"
@@ -1403,6 +1404,58 @@ int grb_copy_evolved_packed(grb_handle* h, const grb_grid* g, const grb_fields* 
                                                            vstride, qdev, true, dp[a], stg);
       CK(cudaMemcpyAsync(hp[a], stg, nb, cudaMemcpyDeviceToHost, s));
     }
+    ++h->launches;
+  }
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_restrict_to_coarse(grb_handle* h, const grb_grid* g, const grb_fields* fine, const grb_fields* cbuf,
+                           int64_t nquads, const int64_t* src_q, const int64_t* dst_q, const uint8_t* child_id,
+                           const int32_t* vars_lo, int32_t nlo, const int32_t* vars_ho, int32_t nho,
+                           void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!g || !fine || !cbuf || nquads < 0 || g->nx < 2 || g->ny < 2 || g->nz < 2 || g->ngz < 3 ||
+      g->nx % 2 || g->ny % 2 || g->nz % 2 || nlo < 0 || nho < 0 || nlo > GRB_N_EVOL_VARS ||
+      nho > GRB_N_EVOL_VARS || (nlo && !vars_lo) || (nho && !vars_ho) || !src_q || !dst_q)
+    return fail(h, GRB_ERR_INVALID);
+  if (nquads == 0) return GRB_OK;
+  if (nho && !child_id) return fail(h, GRB_ERR_INVALID);
+  // the 5-point stencils reach 3 fine cells beyond the interior's edge cell
+  if (nho && (g->nx < 4 || g->ny < 4 || g->nz < 4)) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, nquads);
+  cudaStream_t s = (cudaStream_t)stream;
+  KScope ks(h, s, GRB_KIND_OTHER);
+  for (int pass = 0; pass < 2; ++pass) {
+    const int nl = pass == 0 ? nlo : nho;
+    const int32_t* vl = pass == 0 ? vars_lo : vars_ho;
+    if (!nl) continue;
+    if (!fine->state || !cbuf->state) return fail(h, GRB_ERR_INVALID);
+    RestrictVars V{};
+    V.n = nl;
+    for (int t = 0; t < nl; ++t) {
+      if (vl[t] < 0 || vl[t] >= GRB_N_EVOL_VARS) return fail(h, GRB_ERR_INVALID);
+      V.v[t] = vl[t];
+    }
+    if ((int64_t)nl * nquads >= (1ll << 32)) return fail(h, GRB_ERR_INVALID);
+    const Box b = box(0, 0, 0, G.nx / 2, G.ny / 2, G.nz / 2, (int64_t)nl * nquads);
+    if (pass == 0)
+      k_restrict_cells<false><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V, make_fastdiv((uint32_t)nl), fine->state,
+                                                                   cbuf->state, src_q, dst_q, child_id);
+    else
+      k_restrict_cells<true><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V, make_fastdiv((uint32_t)nl), fine->state,
+                                                                  cbuf->state, src_q, dst_q, child_id);
+    ++h->launches;
+  }
+  const double* fs[3] = {fine->bx, fine->by, fine->bz};
+  double* cs[3] = {cbuf->bx, cbuf->by, cbuf->bz};
+  for (int d = 0; d < 3; ++d) {
+    if (!fs[d] && !cs[d]) continue;
+    if (!fs[d] || !cs[d]) return fail(h, GRB_ERR_INVALID);
+    const Box b = box(0, 0, 0, G.nx / 2 + (d == 0), G.ny / 2 + (d == 1), G.nz / 2 + (d == 2), nquads);
+    if (d == 0) k_restrict_faces<0><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, fs[d], cs[d], src_q, dst_q);
+    if (d == 1) k_restrict_faces<1><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, fs[d], cs[d], src_q, dst_q);
+    if (d == 2) k_restrict_faces<2><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, fs[d], cs[d], src_q, dst_q);
     ++h->launches;
   }
   CK(cudaGetLastError());

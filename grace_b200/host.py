@@ -170,6 +170,27 @@ class GRMHDEquationsSystem:
         _lib.check(self.lib.grb_fill_ghosts_brick(self.h, ctypes.byref(g), ctypes.byref(f), nb[0], nb[1],
                                                   nb[2], per, _stream_ptr(stream)), "grb_fill_ghosts_brick")
 
+    def restrict_to_coarse(self, fine, cbuf, src_q, dst_q, child_id=None, vars_lo=(), vars_ho=(),
+                           faces=True, stream=None):
+        """FMR restriction into coarse buffers (grb_restrict_to_coarse).
+        fine, cbuf: Fields on the device (same block geometry); src_q,
+        dst_q: int64 device tensors; child_id: uint8 device tensor (needed
+        with vars_ho); faces: also restrict face B."""
+        g = self.blocks.c()
+        ff = abi.Fields(fine.state.data_ptr(), *(x.data_ptr() if faces else None for x in (fine.bx, fine.by, fine.bz)))
+        fc = abi.Fields(cbuf.state.data_ptr(), *(x.data_ptr() if faces else None for x in (cbuf.bx, cbuf.by, cbuf.bz)))
+        for t, dt in ((src_q, torch.int64), (dst_q, torch.int64)):
+            if t.dtype != dt or not t.is_cuda or not t.is_contiguous():
+                raise ValueError("src_q / dst_q must be contiguous int64 device tensors")
+        if child_id is not None and (child_id.dtype != torch.uint8 or not child_id.is_cuda):
+            raise ValueError("child_id must be a uint8 device tensor")
+        lo = (ctypes.c_int32 * max(1, len(vars_lo)))(*vars_lo)
+        hi = (ctypes.c_int32 * max(1, len(vars_ho)))(*vars_ho)
+        _lib.check(self.lib.grb_restrict_to_coarse(
+            self.h, ctypes.byref(g), ctypes.byref(ff), ctypes.byref(fc), src_q.numel(), src_q.data_ptr(),
+            dst_q.data_ptr(), child_id.data_ptr() if child_id is not None else None, lo, len(vars_lo), hi,
+            len(vars_ho), _stream_ptr(stream)), "grb_restrict_to_coarse")
+
     def set_static_metric(self, fields=None, stream=None):
         """Cowling: cache the metric derivatives of `fields` for the tuned
         update (grb_set_static_metric); None frees the cache."""

@@ -436,6 +436,32 @@ int grb_copy_evolved_interior(grb_handle* h, const grb_grid* g, const grb_fields
 int grb_copy_evolved_packed(grb_handle* h, const grb_grid* g, const grb_fields* host,
                             const grb_fields* dev, int32_t to_device, void* stream);
 
+/* ---- FMR: restriction into coarse buffers ---------------------------------- */
+/* = the ghost-zone restriction of GRACE's AMR
+ *   (include/grace/amr/ghostzone_kernels/restriction_task_factories.hh:64-
+ *   200, restrict_kernels.hh:42-165): for each of the nquads fine
+ *   quadrants, block src_q[i] of `fine` writes the coarse-resolution image
+ *   of its interior into block dst_q[i] of the coarse buffers `cbuf` (same
+ *   block geometry; coarse cells (ngz + [0, n/2))^3):
+ *     state variables vars_lo[0..nlo) by the 8-cell average
+ *       (second_order_restrict_op, pr_helpers.hh:187-213);
+ *     state variables vars_ho[0..nho) by the 5-point Lagrange restriction
+ *       (lagrange_restrict_op<4>, pr_helpers.hh:216-322, the coefficients of
+ *       fill_fifth_order_restriction_coefficients), its interior stencils
+ *       mirrored by the quadrant's half of its parent: bits 0, 1, 2 of
+ *       child_id[i] (the p4est Morton child id) for x, y, z;
+ *     face B (the arrays not NULL in both `fine` and `cbuf`) by the average
+ *       of the 4 fine faces in each coarse face (div_free_restrict_op),
+ *       which keeps div B of the coarse image at round-off.
+ *   src_q, dst_q (int64) and child_id (uint8) are device arrays of nquads;
+ *   the dst_q must be distinct.  Results are those of the reference's
+ *   operators bit for bit (each product and sum rounded on its own). */
+int grb_restrict_to_coarse(grb_handle* h, const grb_grid* g, const grb_fields* fine,
+                           const grb_fields* cbuf, int64_t nquads, const int64_t* src_q,
+                           const int64_t* dst_q, const uint8_t* child_id,
+                           const int32_t* vars_lo, int32_t nlo, const int32_t* vars_ho,
+                           int32_t nho, void* stream);
+
 /* ---- scratch-free stage -------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (a host code whose GPU memory is owned up front by a pooling allocator, or

@@ -126,3 +126,16 @@ struct OracleNumerics {
 #define API(name) orc_##name
 #include "api_impl.hpp"
 #include "mlp_oracle.hpp"
+
+// FMR restriction into coarse buffers (amr_oracle.hpp).
+#include "amr_oracle.hpp"
+extern "C" void orc_restrict_cells(int n, int ngz, int nvars, const double* src, double* dst, int64_t nquads,
+                                   const int64_t* src_q, const int64_t* dst_q, const uint8_t* child,
+                                   const int* vlo, int nlo, const int* vhi, int nhi) {
+  orc_amr::restrict_cells(orc_amr::OrcOps{}, n, ngz, nvars, src, dst, nquads, src_q, dst_q, child, vlo, nlo, vhi,
+                          nhi);
+}
+extern "C" void orc_restrict_faces(int dir, int n, int ngz, const double* src, double* dst, int64_t nquads,
+                                   const int64_t* src_q, const int64_t* dst_q) {
+  orc_amr::restrict_faces(dir, n, ngz, src, dst, nquads, src_q, dst_q);
+}

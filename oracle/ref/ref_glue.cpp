@@ -220,3 +220,30 @@ struct RefNumerics {
 #define NUMERICS refglue::RefNumerics
 #define API(name) ref_##name
 #include "api_impl.hpp"
+
+// FMR restriction: the reference's own per-point operators
+// (include/grace/amr/ghostzone_kernels/pr_helpers.hh:187-322, with the
+// coefficient table of pr_ho_coeffs.hh), driven by the restated loops of
+// amr_oracle.hpp.
+#include <grace/amr/ghostzone_kernels/pr_helpers.hh>
+#include <grace/amr/ghostzone_kernels/pr_ho_coeffs.hh>
+#include "amr_oracle.hpp"
+namespace {
+struct RefOps {
+  std::vector<double> coeffs;
+  int n, ngz;
+  RefOps(int n_, int g_) : n(n_), ngz(g_) { grace::detail::fill_fifth_order_restriction_coefficients(coeffs); }
+  double lo(const orc_amr::Acc& u, int i, int j, int k) const { return grace::second_order_restrict_op{}(u, i, j, k); }
+  double hi(const orc_amr::Acc& u, int, int, int i, int j, int k, int hx, int hy, int hz) const {
+    Kokkos::View<double*, grace::default_space> cv(const_cast<double*>(coeffs.data()));
+    grace::lagrange_restrict_op<4> op(cv, n, n, n, ngz);
+    return op(u, i, j, k, hx, hy, hz);
+  }
+};
+}  // namespace
+extern "C" void ref_restrict_cells(int n, int ngz, int nvars, const double* src, double* dst, int64_t nquads,
+                                   const int64_t* src_q, const int64_t* dst_q, const uint8_t* child,
+                                   const int* vlo, int nlo, const int* vhi, int nhi) {
+  orc_amr::restrict_cells(RefOps(n, ngz), n, ngz, nvars, src, dst, nquads, src_q, dst_q, child, vlo, nlo, vhi,
+                          nhi);
+}

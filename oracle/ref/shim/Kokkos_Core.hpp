@@ -9,6 +9,9 @@
 #include <cstdint>
 #include <algorithm>
 #include <stdexcept>
+#include <array>
+#include <utility>
+#include <vector>
 #define KOKKOS_INLINE_FUNCTION inline
 #define KOKKOS_FORCEINLINE_FUNCTION inline
 #define KOKKOS_FUNCTION
@@ -29,6 +32,17 @@ template <class T, std::size_t N, class... P> struct View<T[N], P...> {
   explicit View(const char*) {}
   T& operator()(std::size_t i) { return d[i]; }
   const T& operator()(std::size_t i) const { return d[i]; }
+};
+// Pointer-backed 1-D view (View<T*, Space[, MemoryTraits]>) over storage the
+// checker owns, convertible to its const-element form.
+template <unsigned> struct MemoryTraits {};
+constexpr unsigned RandomAccess = 0;
+template <class T, class... P> struct View<T*, P...> {
+  T* p = nullptr;
+  View() = default;
+  explicit View(T* q) : p(q) {}
+  template <class U, class... Q> View(const View<U*, Q...>& o) : p(o.p) {}
+  T& operator()(std::size_t i) const { return p[i]; }
 };
 struct ALL_t {};
 inline ALL_t ALL() { return {}; }

@@ -35,12 +35,34 @@ def _bind(lib, pre):
         "kernels": (None, [C.c_int64, VP, C.c_int, VP]),
         "geom_sources": (None, [C.c_int64, VP, VP]),
         "fill_ghosts_brick": (None, [C.c_int] * 7 + [VP, VP, VP, VP, VP]),
+        "restrict_cells": (None, [C.c_int, C.c_int, C.c_int, VP, VP, C.c_int64, VP, VP, VP, VP, C.c_int, VP,
+                                  C.c_int]),
+        "restrict_faces": (None, [C.c_int, C.c_int, C.c_int, VP, VP, C.c_int64, VP, VP]),
     }
     for name, (res, args) in sig.items():
+        if not hasattr(lib, pre + name):  # the pinning build exports a subset
+            continue
         fn = getattr(lib, pre + name)
         fn.restype = res
         fn.argtypes = args
     return lib
+
+
+def restrict_cells(which, n, ngz, nvars, src, dst, src_q, dst_q, child, vlo, vhi):
+    """FMR restriction of cell variables into coarse buffers (amr_oracle.hpp)."""
+    L = lib(which)
+    q = lambda a, t: np.ascontiguousarray(a, dtype=t)
+    sq, dq, ch = q(src_q, np.int64), q(dst_q, np.int64), q(child, np.uint8)
+    vl, vh = q(vlo, np.int32), q(vhi, np.int32)
+    getattr(L, which + "_restrict_cells")(n, ngz, nvars, p(src), p(dst), len(sq), p(sq), p(dq), p(ch),
+                                          p(vl), len(vl), p(vh), len(vh))
+
+
+def restrict_faces(dir, n, ngz, src, dst, src_q, dst_q):
+    L = lib("orc")
+    q = lambda a: np.ascontiguousarray(a, dtype=np.int64)
+    sq, dq = q(src_q), q(dst_q)
+    L.orc_restrict_faces(dir, n, ngz, p(src), p(dst), len(sq), p(sq), p(dq))
 
 
 def build_oracle():
