@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--eager", action="store_true", help="launch the timed steps eagerly, not as a CUDA graph")
     ap.add_argument("--no-c2p", action="store_true")
-    ap.add_argument("--no-restrict", action="store_true", help="skip the FMR restriction measurement")
+    ap.add_argument("--no-restrict", action="store_true", help="skip the FMR restriction and prolongation measurements")
     ap.add_argument("--no-learned", action="store_true", help="c2p leg: plain bracket only")
     ap.add_argument("--c2p-only", action="store_true", help="run only the c2p micro-benchmark")
     ap.add_argument("--c2p-states", type=int, default=1 << 24, help="states of the c2p micro-benchmark")
@@ -403,6 +403,48 @@ def ours(args, rank, world, local_rank):
                             "restriction) and the three face-B arrays of every block; bytes = the fine "
                             "interior read once plus the coarse image written"}
 
+    # --- FMR prolongation into ghost zones (a separate measurement, not part
+    # of the step): all 26 ghost elements (6 faces, 12 edges, 8 corners) of
+    # every block filled from a coarse buffer, the 7 HRSC variables by the
+    # minmod slope-limited operator, the 16 others by the 5-point Lagrange
+    # one, face B by the divergence-preserving prolongation; the bench's
+    # state serves as the coarse buffers and a scratch copy as the fine blocks
+    prolong = None
+    if not args.no_restrict and args.mode == "tuned":
+        nq = su.nq
+        lo, hi = list(range(abi.N_HRSC)), list(range(abi.N_HRSC, abi.N_EVOL_VARS))
+        lists = []
+        for kind, ne in ((0, 6), (1, 12), (2, 8)):
+            fq = torch.arange(nq, dtype=torch.int64, device=dev).repeat_interleave(ne)
+            el = torch.arange(ne, dtype=torch.uint8, device=dev).repeat(nq)
+            hf = torch.zeros((nq * ne, 3, 2), dtype=torch.int8, device=dev)
+            lists.append((kind, fq, el, hf))
+        run = lambda: [g.prolong_to_ghosts(spp, state, k, fq, fq, el, hf, lo, hi) for k, fq, el, hf in lists]
+        for _ in range(2):
+            run()
+        torch.cuda.synchronize()
+        r0 = torch.cuda.Event(enable_timing=True)
+        r1 = torch.cuda.Event(enable_timing=True)
+        reps = 5
+        r0.record()
+        for _ in range(reps):
+            run()
+        r1.record()
+        torch.cuda.synchronize()
+        pms = r0.elapsed_time(r1) / reps
+        # algorithmic bytes: the fine ghost cells (and one face per ghost cell
+        # and array) written once, the coarse cells and faces covering them
+        # read once (1/8 and 1/4 as many)
+        NN = n + 2 * su.ngz
+        vg = NN ** 3 - n ** 3
+        pbytes = 8 * nq * (abi.N_EVOL_VARS * (vg + vg / 8) + 3 * (vg + vg / 4))
+        prolong = {"quads": nq, "ms": pms, "ghost_cells_per_s": nq * vg / (pms * 1e-3),
+                   "achieved_GBps": pbytes / (pms * 1e-3) / 1e9, "launches": 12,
+                   "note": "26 ghost elements of every block (3 calls, one per element kind): 23 state "
+                           "variables (7 slope-limited, 16 by the 5-point Lagrange prolongation) and the "
+                           "three face-B arrays; bytes = the fine ghost region written once plus the coarse "
+                           "data covering it read once"}
+
     # --- dominant kernel roofline (HBM), measured over the timed region
     peaks = {}
     try:
@@ -411,9 +453,10 @@ def ours(args, rank, world, local_rank):
         pass
     hbm = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    if restrict is not None:
-        restrict["hbm_frac"] = restrict["achieved_GBps"] / hbm
-        restrict["peak_source"] = peak_src
+    for leg in (restrict, prolong):
+        if leg is not None:
+            leg["hbm_frac"] = leg["achieved_GBps"] / hbm
+            leg["peak_source"] = peak_src
     top = max(kt.items(), key=lambda kv: kv[1][0])
     name, (kms, kcnt) = top
     # faces one flux launch (one direction) computes: the reference's full
@@ -467,7 +510,7 @@ def ours(args, rank, world, local_rank):
             "clocks": clk, "gpu_launches": launches,
             "kernel_ms": {k: round(v[0], 3) for k, v in kt.items() if v[1]},
             "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "c2p": c2p,
-            "mode": args.mode, "plain_form": plain, "tuning": tuning, "restrict": restrict,
+            "mode": args.mode, "plain_form": plain, "tuning": tuning, "restrict": restrict, "prolong": prolong,
         }
         print(json.dumps(line), flush=True)
     g.close()

@@ -117,4 +117,237 @@ __global__ void __launch_bounds__(128) k_restrict_faces(Geo G, Box box, const do
   dst[dst_q[iq] * sz + ((int64_t)(k + G.g) * N1 + (j + G.g)) * N0 + (i + G.g)] = __dmul_rn(0.25, val);
 }
 
+// ---------------------------------------------------------------------------
+// FMR prolongation into ghost zones (GRACE's prolong_op and
+// div_free_prolong_op, include/grace/amr/ghostzone_kernels/
+// prolongation_kernels.hh:46-399, with the index maps of index_helpers.hh
+// and the operators of pr_helpers.hh:73-185).  The ghost elements of one
+// kind (faces, edges or corners of fine quadrants whose neighbour is
+// coarser) are filled from each quadrant's coarse buffer: coarse cell
+// ngz + t covers fine cells ngz + 2t, ngz + 2t + 1, and the low coarse
+// ghosts start at ngz/2.
+
+// Along axis d of ghost element e of one kind: where its ghost region lies
+// (0 below the interior, 1 above it, 2 spanning it) and which of the
+// launch's three loop indices runs along that axis (the index maps of
+// compute_ghost_indices_{face,edge,corner}, index_helpers.hh:84-356).  A
+// face (e = 2 axis + side) runs its normal axis over loop index 0 and its
+// tangential axes over 1, 2; an edge (e = 4 axis + sides) its two fixed
+// axes over 0, 1 (the sides in bits 0, 1 of e) and its own axis over 2; a
+// corner axis d over d (the side in bit d of e).
+template <int kKind>
+__device__ __forceinline__ void ghost_axis(int e, int d, int& where, int& loop) {
+  if (kKind == GRB_ELEM_FACE) {
+    const int ax = e >> 1;
+    where = d == ax ? (e & 1) : 2;
+    loop = d == ax ? 0 : (d < ax ? d + 1 : d);
+  } else if (kKind == GRB_ELEM_EDGE) {
+    const int ax = e >> 2;
+    const int f1 = ax == 0 ? 1 : 0;
+    loop = d == ax ? 2 : (d == f1 ? 0 : 1);
+    where = d == ax ? 2 : ((e >> loop) & 1);
+  } else {
+    where = (e >> d) & 1;
+    loop = d;
+  }
+}
+__device__ __forceinline__ int ghost_idx(int where, int n, int g, int goff, int t) {
+  return where == 2 ? g + t : (where ? n + g + t : goff + t);
+}
+__device__ __forceinline__ int pick3(int l, int a, int b, int c) { return l == 0 ? a : (l == 1 ? b : c); }
+
+// The 5-point prolongation weights, lower fine half then upper.
+__constant__ double c_prolong5[10] = {-45.0 / 2048.0, 105.0 / 512.0, 945.0 / 1024.0, -63.0 / 512.0, 35.0 / 2048.0,
+                                      35.0 / 2048.0,  -63.0 / 512.0, 945.0 / 1024.0, 105.0 / 512.0, -45.0 / 2048.0};
+
+// Cell variables.  box: the kind's ghost extent (ngz, n | ngz, n | ngz) x
+// (nvars_in_list x nelems), variable fastest.  kHigh: the 5-point Lagrange
+// operator, else the minmod slope-limited one.
+template <int kKind, bool kHigh>
+__global__ void __launch_bounds__(128) k_prolong_cells(Geo G, Box box, RestrictVars V, FastDiv dnv,
+                                                       const double* __restrict__ cbuf, double* __restrict__ fine,
+                                                       const int64_t* __restrict__ fine_q,
+                                                       const int64_t* __restrict__ cbuf_q,
+                                                       const uint8_t* __restrict__ elem) {
+  int a, b, c;
+  int64_t t;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, a, b, c, t)) return;
+  const uint32_t iq = fast_div((uint32_t)t, dnv);
+  const int v = V.v[(uint32_t)t - iq * (uint32_t)V.n];
+  const int e = elem[iq];
+  int f[3], k[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int w, lp;
+    ghost_axis<kKind>(e, d, w, lp);
+    const int l = pick3(lp, a, b, c);
+    f[d] = ghost_idx(w, G.nx, G.g, 0, l);
+    k[d] = ghost_idx(w, G.nx / 2, G.g, G.g / 2, l >> 1);
+  }
+  const int N0 = G.NX, N1 = G.NY;
+  const double* u = cbuf + (cbuf_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
+  auto at = [&](int x, int y, int z) { return u[((int64_t)z * N1 + y) * N0 + x]; };
+  double r;
+  if (!kHigh) {
+    const double u0 = at(k[0], k[1], k[2]);
+    double acc = 0.0;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int dx = d == 0, dy = d == 1, dz = d == 2;
+      const double sl = __dsub_rn(u0, at(k[0] - dx, k[1] - dy, k[2] - dz));
+      const double sr = __dsub_rn(at(k[0] + dx, k[1] + dy, k[2] + dz), u0);
+      acc = __dadd_rn(acc, __dmul_rn((f[d] & 1) ? 0.25 : -0.25, lim_minmod(sl, sr)));
+    }
+    r = __dadd_rn(u0, acc);
+  } else {
+    const double* cx = c_prolong5 + 5 * (f[0] & 1);
+    const double* cy = c_prolong5 + 5 * (f[1] & 1);
+    const double* cz = c_prolong5 + 5 * (f[2] & 1);
+    double Sy[5];
+#pragma unroll
+    for (int dk = 0; dk < 5; ++dk) {
+      double col[5];
+#pragma unroll
+      for (int dj = 0; dj < 5; ++dj) {
+        double line[5];
+#pragma unroll
+        for (int di = 0; di < 5; ++di) line[di] = at(k[0] + di - 2, k[1] + dj - 2, k[2] + dk - 2);
+        col[dj] = contract5_rn(cx, line);
+      }
+      Sy[dk] = contract5_rn(cy, col);
+    }
+    r = contract5_rn(cz, Sy);
+  }
+  fine[(fine_q[iq] * GRB_N_EVOL_VARS + v) * G.cells + ((int64_t)f[2] * N1 + f[1]) * N0 + f[0]] = r;
+}
+
+// One block's face array staggered along d.
+struct FaceBlk {
+  double* p;
+  int N0, N1;
+  __device__ __forceinline__ double& operator()(int i, int j, int k) const {
+    return p[((int64_t)k * N1 + j) * N0 + i];
+  }
+};
+
+// Phase 1 at coarse point c / fine point f: the fine faces of array d lying
+// on the coarse face through c get the coarse value plus minmod slopes along
+// the face's two tangential axes (Toth & Roe 2002, eqs. 4-5).
+__device__ __forceinline__ void prolong_coarse_face(int d, const FaceBlk& F, const FaceBlk& C, const int c[3],
+                                                    const int f[3]) {
+  const int t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+  const double U0 = C(c[0], c[1], c[2]);
+  double sl[2];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int ax = h == 0 ? t1 : t2;
+    const int o0 = ax == 0, o1 = ax == 1, o2 = ax == 2;
+    const double dl = __dsub_rn(U0, C(c[0] - o0, c[1] - o1, c[2] - o2));
+    const double dr = __dsub_rn(C(c[0] + o0, c[1] + o1, c[2] + o2), U0);
+    sl[h] = __dmul_rn(0.25, lim_minmod(dl, dr));
+  }
+#pragma unroll
+  for (int p = 0; p < 2; ++p)
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+      int o[3] = {f[0], f[1], f[2]};
+      o[t1] += p;
+      o[t2] += q;
+      F(o[0], o[1], o[2]) = __dadd_rn(__dadd_rn(U0, p ? sl[0] : -sl[0]), q ? sl[1] : -sl[1]);
+    }
+}
+
+// Face B, one phase.  box: the kind's ghost extent halved x nelems; each
+// point is one coarse cell of the element.  have_fine[6 i + 2 axis + side]:
+// the neighbour across that side of element i's region holds fine data.
+// Phase 1 writes the fine faces on coarse faces, phase 2 (a separate launch,
+// as it reads phase 1's faces around each coarse cell) those inside coarse
+// cells (Toth & Roe 2002, eqs. 8-12).
+template <int kKind, int kPhase>
+__global__ void __launch_bounds__(128) k_prolong_faces(Geo G, Box box, double* __restrict__ bx,
+                                                       double* __restrict__ by, double* __restrict__ bz,
+                                                       const double* __restrict__ cbx, const double* __restrict__ cby,
+                                                       const double* __restrict__ cbz,
+                                                       const int64_t* __restrict__ fine_q,
+                                                       const int64_t* __restrict__ cbuf_q,
+                                                       const uint8_t* __restrict__ elem,
+                                                       const int8_t* __restrict__ have_fine) {
+  int a, b, c;
+  int64_t iq;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, a, b, c, iq)) return;
+  const int e = elem[iq];
+  const int n = G.nx, g = G.g;
+  int f[3], wh[3], l[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int lp;
+    ghost_axis<kKind>(e, d, wh[d], lp);
+    l[d] = pick3(lp, a, b, c);
+    f[d] = ghost_idx(wh[d], n, g, 0, 2 * l[d]);
+  }
+  const int N = G.NX;
+  const int64_t sz = (int64_t)(N + 1) * N * N;
+  const FaceBlk u{bx + fine_q[iq] * sz, N + 1, N}, v{by + fine_q[iq] * sz, N, N + 1}, w{bz + fine_q[iq] * sz, N, N};
+  if (kPhase == 1) {
+    const int64_t cq = cbuf_q[iq];
+    const FaceBlk C[3] = {{const_cast<double*>(cbx) + cq * sz, N + 1, N},
+                          {const_cast<double*>(cby) + cq * sz, N, N + 1},
+                          {const_cast<double*>(cbz) + cq * sz, N, N}};
+    const FaceBlk F[3] = {u, v, w};
+    const int8_t* hf = have_fine + 6 * iq;
+    int k[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) k[d] = ghost_idx(wh[d], n / 2, g, g / 2, l[d]);
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      const int first = wh[d] == 2 ? g : (wh[d] ? n + g : 0);
+      const int last = wh[d] == 2 ? n + g - 2 : (wh[d] ? n + 2 * g - 2 : g - 2);
+      if (!(f[d] == first && hf[2 * d])) prolong_coarse_face(d, F[d], C[d], k, f);
+      if (f[d] == last && !hf[2 * d + 1]) {
+        int k1[3] = {k[0], k[1], k[2]}, f1[3] = {f[0], f[1], f[2]};
+        k1[d] += 1;
+        f1[d] += 2;
+        prolong_coarse_face(d, F[d], C[d], k1, f1);
+      }
+    }
+  } else {
+    const int i = f[0], j = f[1], kk0 = f[2];
+    double Uxx = 0, Vyy = 0, Wzz = 0, Uxyz = 0, Vxyz = 0, Wxyz = 0;
+#pragma unroll
+    for (int ii = 0; ii < 2; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+        for (int kk = 0; kk < 2; ++kk) {
+          const bool sij = (ii ^ jj) == 0, sik = (ii ^ kk) == 0, sjk = (jj ^ kk) == 0, sijk = ((ii ^ jj ^ kk) & 1) == 1;
+          const double vu = v(i + ii, j + 2 * jj, kk0 + kk), wu = w(i + ii, j + jj, kk0 + 2 * kk);
+          const double uu = u(i + 2 * ii, j + jj, kk0 + kk);
+          Uxx = __dadd_rn(Uxx, __dadd_rn(sij ? vu : -vu, sik ? wu : -wu));
+          Vyy = __dadd_rn(Vyy, __dadd_rn(sij ? uu : -uu, sjk ? wu : -wu));
+          Wzz = __dadd_rn(Wzz, __dadd_rn(sik ? uu : -uu, sjk ? vu : -vu));
+          Uxyz = __dadd_rn(Uxyz, sijk ? uu : -uu);
+          Vxyz = __dadd_rn(Vxyz, sijk ? vu : -vu);
+          Wxyz = __dadd_rn(Wxyz, sijk ? wu : -wu);
+        }
+    Uxx = __dmul_rn(Uxx, 0.125);
+    Vyy = __dmul_rn(Vyy, 0.125);
+    Wzz = __dmul_rn(Wzz, 0.125);
+    Uxyz = __dmul_rn(Uxyz, 0.0625);
+    Vxyz = __dmul_rn(Vxyz, 0.0625);
+    Wxyz = __dmul_rn(Wxyz, 0.0625);
+#pragma unroll
+    for (int jj = 0; jj < 2; ++jj)
+#pragma unroll
+      for (int kk = 0; kk < 2; ++kk) {
+        const double sj = jj ? 1.0 : -1.0, sk = kk ? 1.0 : -1.0;
+        const double mu = __dmul_rn(0.5, __dadd_rn(u(i, j + jj, kk0 + kk), u(i + 2, j + jj, kk0 + kk)));
+        const double mv = __dmul_rn(0.5, __dadd_rn(v(i + jj, j, kk0 + kk), v(i + jj, j + 2, kk0 + kk)));
+        const double mw = __dmul_rn(0.5, __dadd_rn(w(i + jj, j + kk, kk0), w(i + jj, j + kk, kk0 + 2)));
+        u(i + 1, j + jj, kk0 + kk) = __dadd_rn(__dadd_rn(__dadd_rn(mu, Uxx), sk * Vxyz), sj * Wxyz);
+        v(i + jj, j + 1, kk0 + kk) = __dadd_rn(__dadd_rn(__dadd_rn(mv, Vyy), sj * Wxyz), sk * Uxyz);
+        w(i + jj, j + kk, kk0 + 1) = __dadd_rn(__dadd_rn(__dadd_rn(mw, Wzz), sk * Uxyz), sj * Vxyz);
+      }
+  }
+}
+
 }  // namespace grb

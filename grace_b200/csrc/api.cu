@@ -976,6 +976,30 @@ int grad_setup(grb_handle* h) {
 }
 }  // namespace
 
+// FMR prolongation launches of one element kind (grb_prolong_to_ghosts).
+template <int kKind>
+static void launch_prolong(const Geo& G, const int ext[3], const grb_fields* fine, const grb_fields* cbuf,
+                           int64_t nelems, const int64_t* fine_q, const int64_t* cbuf_q, const uint8_t* elem_id,
+                           const int8_t* have_fine, const RestrictVars* V, bool faces, cudaStream_t s) {
+  for (int pass = 0; pass < 2; ++pass) {
+    if (!V[pass].n) continue;
+    const Box b = box(0, 0, 0, ext[0], ext[1], ext[2], (int64_t)V[pass].n * nelems);
+    const FastDiv dv = make_fastdiv((uint32_t)V[pass].n);
+    if (pass == 0)
+      k_prolong_cells<kKind, false><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V[0], dv, cbuf->state, fine->state,
+                                                                         fine_q, cbuf_q, elem_id);
+    else
+      k_prolong_cells<kKind, true><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V[1], dv, cbuf->state, fine->state,
+                                                                        fine_q, cbuf_q, elem_id);
+  }
+  if (!faces) return;
+  const Box b = box(0, 0, 0, ext[0] / 2, ext[1] / 2, ext[2] / 2, nelems);
+  k_prolong_faces<kKind, 1><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, fine->bx, fine->by, fine->bz, cbuf->bx,
+                                                                 cbuf->by, cbuf->bz, fine_q, cbuf_q, elem_id, have_fine);
+  k_prolong_faces<kKind, 2><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, fine->bx, fine->by, fine->bz, cbuf->bx,
+                                                                 cbuf->by, cbuf->bz, fine_q, cbuf_q, elem_id, have_fine);
+}
+
 extern "C" {
 
 int grb_mlp_grad(grb_handle* h, int64_t n, const float* params, const float* feat, const float* target,
@@ -1458,6 +1482,48 @@ int grb_restrict_to_coarse(grb_handle* h, const grb_grid* g, const grb_fields* f
     if (d == 2) k_restrict_faces<2><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, fs[d], cs[d], src_q, dst_q);
     ++h->launches;
   }
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_prolong_to_ghosts(grb_handle* h, const grb_grid* g, const grb_fields* fine, const grb_fields* cbuf,
+                          int32_t elem_kind, int64_t nelems, const int64_t* fine_q, const int64_t* cbuf_q,
+                          const uint8_t* elem_id, const int8_t* have_fine, const int32_t* vars_lo, int32_t nlo,
+                          const int32_t* vars_ho, int32_t nho, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!g || !fine || !cbuf || nelems < 0 || elem_kind < GRB_ELEM_FACE || elem_kind > GRB_ELEM_CORNER ||
+      g->nx != g->ny || g->nx != g->nz || g->nx < 4 || g->nx % 2 || g->ngz < 4 || g->ngz % 2 || nlo < 0 ||
+      nho < 0 || nlo > GRB_N_EVOL_VARS || nho > GRB_N_EVOL_VARS || (nlo && !vars_lo) || (nho && !vars_ho) ||
+      !fine_q || !cbuf_q || !elem_id)
+    return fail(h, GRB_ERR_INVALID);
+  if (nelems == 0) return GRB_OK;
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, nelems);
+  const int n = g->nx, ng = g->ngz;
+  const int ext[3] = {ng, elem_kind == GRB_ELEM_FACE ? n : ng, elem_kind == GRB_ELEM_CORNER ? ng : n};
+  RestrictVars V[2] = {};
+  for (int pass = 0; pass < 2; ++pass) {
+    const int nl = pass == 0 ? nlo : nho;
+    const int32_t* vl = pass == 0 ? vars_lo : vars_ho;
+    if (!nl) continue;
+    if (!fine->state || !cbuf->state || (int64_t)nl * nelems >= (1ll << 32)) return fail(h, GRB_ERR_INVALID);
+    V[pass].n = nl;
+    for (int t = 0; t < nl; ++t) {
+      if (vl[t] < 0 || vl[t] >= GRB_N_EVOL_VARS) return fail(h, GRB_ERR_INVALID);
+      V[pass].v[t] = vl[t];
+    }
+  }
+  const bool faces = fine->bx || fine->by || fine->bz || cbuf->bx || cbuf->by || cbuf->bz;
+  if (faces && (!fine->bx || !fine->by || !fine->bz || !cbuf->bx || !cbuf->by || !cbuf->bz || !have_fine))
+    return fail(h, GRB_ERR_INVALID);
+  cudaStream_t s = (cudaStream_t)stream;
+  KScope ks(h, s, GRB_KIND_OTHER);
+  if (elem_kind == GRB_ELEM_FACE)
+    launch_prolong<GRB_ELEM_FACE>(G, ext, fine, cbuf, nelems, fine_q, cbuf_q, elem_id, have_fine, V, faces, s);
+  else if (elem_kind == GRB_ELEM_EDGE)
+    launch_prolong<GRB_ELEM_EDGE>(G, ext, fine, cbuf, nelems, fine_q, cbuf_q, elem_id, have_fine, V, faces, s);
+  else
+    launch_prolong<GRB_ELEM_CORNER>(G, ext, fine, cbuf, nelems, fine_q, cbuf_q, elem_id, have_fine, V, faces, s);
+  h->launches += (V[0].n > 0) + (V[1].n > 0) + 2 * faces;
   CK(cudaGetLastError());
   return GRB_OK;
 }

@@ -191,6 +191,30 @@ class GRMHDEquationsSystem:
             dst_q.data_ptr(), child_id.data_ptr() if child_id is not None else None, lo, len(vars_lo), hi,
             len(vars_ho), _stream_ptr(stream)), "grb_restrict_to_coarse")
 
+    def prolong_to_ghosts(self, fine, cbuf, elem_kind, fine_q, cbuf_q, elem_id, have_fine=None, vars_lo=(),
+                          vars_ho=(), faces=True, stream=None):
+        """FMR prolongation into the ghost elements of one kind
+        (grb_prolong_to_ghosts; elem_kind 0 faces, 1 edges, 2 corners).
+        fine, cbuf: Fields on the device (same block geometry); fine_q,
+        cbuf_q: int64 device tensors; elem_id: uint8 device tensor;
+        have_fine: int8 device tensor (nelems, 3, 2), needed with faces."""
+        g = self.blocks.c()
+        ff = abi.Fields(fine.state.data_ptr(), *(x.data_ptr() if faces else None for x in (fine.bx, fine.by, fine.bz)))
+        fc = abi.Fields(cbuf.state.data_ptr(), *(x.data_ptr() if faces else None for x in (cbuf.bx, cbuf.by, cbuf.bz)))
+        for t, dt in ((fine_q, torch.int64), (cbuf_q, torch.int64), (elem_id, torch.uint8)):
+            if t.dtype != dt or not t.is_cuda or not t.is_contiguous():
+                raise ValueError("fine_q / cbuf_q must be int64 and elem_id uint8 contiguous device tensors")
+        if faces and (have_fine is None or have_fine.dtype != torch.int8 or not have_fine.is_cuda
+                      or not have_fine.is_contiguous() or have_fine.numel() != 6 * fine_q.numel()):
+            raise ValueError("have_fine must be a contiguous int8 device tensor of shape (nelems, 3, 2)")
+        lo = (ctypes.c_int32 * max(1, len(vars_lo)))(*vars_lo)
+        hi = (ctypes.c_int32 * max(1, len(vars_ho)))(*vars_ho)
+        _lib.check(self.lib.grb_prolong_to_ghosts(
+            self.h, ctypes.byref(g), ctypes.byref(ff), ctypes.byref(fc), elem_kind, fine_q.numel(),
+            fine_q.data_ptr(), cbuf_q.data_ptr(), elem_id.data_ptr(),
+            have_fine.data_ptr() if (faces and have_fine is not None) else None, lo, len(vars_lo), hi,
+            len(vars_ho), _stream_ptr(stream)), "grb_prolong_to_ghosts")
+
     def set_static_metric(self, fields=None, stream=None):
         """Cowling: cache the metric derivatives of `fields` for the tuned
         update (grb_set_static_metric); None frees the cache."""

@@ -462,6 +462,43 @@ int grb_restrict_to_coarse(grb_handle* h, const grb_grid* g, const grb_fields* f
                            const int32_t* vars_lo, int32_t nlo, const int32_t* vars_ho,
                            int32_t nho, void* stream);
 
+/* ---- FMR: prolongation into ghost zones --------------------------------- */
+#define GRB_ELEM_FACE 0
+#define GRB_ELEM_EDGE 1
+#define GRB_ELEM_CORNER 2
+/* = the ghost-zone prolongation of GRACE's AMR, one task per element kind
+ *   (include/grace/amr/ghostzone_kernels/prolongation_task_factories.hh:
+ *   70-230, prolongation_kernels.hh:46-399): for each of the nelems ghost
+ *   elements of kind elem_kind (GRB_ELEM_FACE: face elem_id[i] in 0..5 =
+ *   2 axis + side; GRB_ELEM_EDGE: edge 0..11, 4 x its axis + the sides of
+ *   the two other axes in bits 0, 1; GRB_ELEM_CORNER: corner 0..7, bit d the
+ *   side along axis d), the ghost cells of block fine_q[i] of `fine` in that
+ *   element are filled from block cbuf_q[i] of the coarse buffers `cbuf`
+ *   (same block geometry; coarse cell ngz + t covers fine cells ngz + 2t,
+ *   ngz + 2t + 1, the low coarse ghosts start at ngz/2):
+ *     state variables vars_lo[0..nlo) by the minmod slope-limited operator
+ *       (slope_limited_prolong_op<minmod>, pr_helpers.hh:73-103);
+ *     state variables vars_ho[0..nho) by the 5-point Lagrange operator
+ *       (lagrange_prolong_op<4>, pr_helpers.hh:105-185, the coefficients of
+ *       fill_fifth_order_prolongation_coefficients);
+ *     face B (when the face arrays are given, all six) by the Toth-Roe
+ *       divergence-preserving prolongation (div_free_prolong_op): the fine
+ *       faces on coarse faces from the coarse face and its minmod slopes,
+ *       except the first face of an axis where have_fine[6 i + 2 axis + 0]
+ *       is set and with the last one where have_fine[6 i + 2 axis + 1] is
+ *       not (the neighbour on that side holds fine data), then the faces
+ *       inside coarse cells from those around them.
+ *   Blocks are cubic (nx = ny = nz, even, >= 4) with an even ngz >= 4.
+ *   fine_q, cbuf_q (int64), elem_id (uint8) and have_fine (int8, 6 per
+ *   element) are device arrays.  Results are those of the reference's
+ *   functors bit for bit (each product and sum rounded on its own); one
+ *   launch per variable list and two for face B. */
+int grb_prolong_to_ghosts(grb_handle* h, const grb_grid* g, const grb_fields* fine,
+                          const grb_fields* cbuf, int32_t elem_kind, int64_t nelems,
+                          const int64_t* fine_q, const int64_t* cbuf_q, const uint8_t* elem_id,
+                          const int8_t* have_fine, const int32_t* vars_lo, int32_t nlo,
+                          const int32_t* vars_ho, int32_t nho, void* stream);
+
 /* ---- scratch-free stage -------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (a host code whose GPU memory is owned up front by a pooling allocator, or

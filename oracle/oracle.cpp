@@ -139,3 +139,13 @@ extern "C" void orc_restrict_faces(int dir, int n, int ngz, const double* src, d
                                    const int64_t* src_q, const int64_t* dst_q) {
   orc_amr::restrict_faces(dir, n, ngz, src, dst, nquads, src_q, dst_q);
 }
+extern "C" void orc_prolong_cells(int kind, int n, int ngz, int nvars, double* fine, const double* cbuf,
+                                  int64_t nelems, const int64_t* fine_q, const int64_t* cbuf_q, const uint8_t* elem,
+                                  const int* vlo, int nlo, const int* vhi, int nhi) {
+  orc_amr::prolong_cells(kind, n, ngz, nvars, fine, cbuf, nelems, fine_q, cbuf_q, elem, vlo, nlo, vhi, nhi);
+}
+extern "C" void orc_prolong_faces(int kind, int n, int ngz, double* fx, double* fy, double* fz, const double* cx,
+                                  const double* cy, const double* cz, int64_t nelems, const int64_t* fine_q,
+                                  const int64_t* cbuf_q, const uint8_t* elem, const int8_t* have_fine) {
+  orc_amr::prolong_faces(kind, n, ngz, fx, fy, fz, cx, cy, cz, nelems, fine_q, cbuf_q, elem, have_fine);
+}

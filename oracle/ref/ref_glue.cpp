@@ -247,3 +247,103 @@ extern "C" void ref_restrict_cells(int n, int ngz, int nvars, const double* src,
   orc_amr::restrict_cells(RefOps(n, ngz), n, ngz, nvars, src, dst, nquads, src_q, dst_q, child, vlo, nlo, vhi,
                           nhi);
 }
+
+// FMR prolongation into ghost zones: the reference's own functors
+// (prolong_op and div_free_prolong_op of
+// include/grace/amr/ghostzone_kernels/prolongation_kernels.hh, with their
+// index_transformer_t and the operators slope_limited_prolong_op<minmod>,
+// lagrange_prolong_op<4> of pr_helpers.hh), each called over the iteration
+// range its task factory gives it (prolongation_task_factories.hh:150-230),
+// serially.
+#include <grace/amr/ghostzone_kernels/prolongation_kernels.hh>
+namespace {
+// LayoutLeft (N0, N1, N2, nv, nq) array of doubles, in the view shape the
+// functors index.
+struct Acc3 {
+  double* a;
+  size_t N0, N1;
+  double& operator()(size_t i, size_t j, size_t k) const { return a[(k * N1 + j) * N0 + i]; }
+};
+struct Acc4 {
+  double* a;
+  size_t N0, N1, N2, nv;
+  double& operator()(size_t i, size_t j, size_t k, size_t v) const { return a[((v * N2 + k) * N1 + j) * N0 + i]; }
+  size_t extent(int) const { return nv; }
+};
+struct Arr5 {
+  double* a;
+  size_t N0, N1, N2, nv;
+  double& operator()(size_t i, size_t j, size_t k, size_t v, size_t q) const {
+    return a[(((q * nv + v) * N2 + k) * N1 + j) * N0 + i];
+  }
+  Acc3 sub(int iv, int q) const { return Acc3{a + ((size_t)q * nv + iv) * N0 * N1 * N2, N0, N1}; }
+  Acc4 sub4(size_t q) const { return Acc4{a + q * nv * N0 * N1 * N2, N0, N1, N2, nv}; }
+};
+template <grace::amr::element_kind_t K>
+void ref_prolong_cells_k(int n, int ngz, int nvars, double* fine, const double* cbuf, int64_t nelems,
+                         const int64_t* fine_q, const int64_t* cbuf_q, const uint8_t* elem, const int* vlo, int nlo,
+                         const int* vhi, int nhi) {
+  const size_t N = n + 2 * ngz;
+  std::vector<size_t> q(fine_q, fine_q + nelems), c(cbuf_q, cbuf_q + nelems);
+  std::vector<uint8_t> e(elem, elem + nelems);
+  std::vector<size_t> lo(vlo, vlo + nlo), hi(vhi, vhi + nhi);
+  std::vector<double> co;
+  grace::detail::fill_fifth_order_prolongation_coefficients(co);
+  Arr5 F{fine, N, N, N, (size_t)nvars}, C{const_cast<double*>(cbuf), N, N, N, (size_t)nvars};
+  Kokkos::View<size_t*> Q(q.data()), Cq(c.data()), L(lo.data()), H(hi.data());
+  Kokkos::View<uint8_t*> E(e.data());
+  grace::amr::prolong_op<grace::slope_limited_prolong_op<grace::minmod>, K, Arr5> f_lo(F, C, Q, Cq, E, L, {}, n, ngz);
+  grace::lagrange_prolong_op<4> ho{Kokkos::View<double*, grace::default_space>(co.data())};
+  grace::amr::prolong_op<grace::lagrange_prolong_op<4>, K, Arr5> f_hi(F, C, Q, Cq, E, H, ho, n, ngz);
+  for (int pass = 0; pass < 2; ++pass) {
+    const auto r = grace::amr::get_iter_range<K>(ngz, n, pass == 0 ? nlo : nhi, nelems);
+    for (int64_t iq = 0; iq < r[4]; ++iq)
+      for (int64_t v = 0; v < r[3]; ++v)
+        for (int64_t k = 0; k < r[2]; ++k)
+          for (int64_t j = 0; j < r[1]; ++j)
+            for (int64_t i = 0; i < r[0]; ++i) {
+              if (pass == 0) f_lo(i, j, k, v, iq);
+              else f_hi(i, j, k, v, iq);
+            }
+  }
+}
+template <grace::amr::element_kind_t K>
+void ref_prolong_faces_k(int n, int ngz, double* fx, double* fy, double* fz, const double* cx, const double* cy,
+                         const double* cz, int64_t nelems, const int64_t* fine_q, const int64_t* cbuf_q,
+                         const uint8_t* elem, const int8_t* have_fine) {
+  const size_t N = n + 2 * ngz;
+  std::vector<size_t> q(fine_q, fine_q + nelems), c(cbuf_q, cbuf_q + nelems);
+  std::vector<uint8_t> e(elem, elem + nelems);
+  // have_fine_data(axis, side, element) from have_fine[element][axis][side]
+  std::vector<int8_t> hf(6 * nelems);
+  for (int64_t i = 0; i < nelems; ++i)
+    for (int a = 0; a < 3; ++a)
+      for (int sd = 0; sd < 2; ++sd) hf[a + 3 * (sd + 2 * i)] = have_fine[6 * i + 2 * a + sd];
+  Arr5 X{fx, N + 1, N, N, 1}, Y{fy, N, N + 1, N, 1}, Z{fz, N, N, N + 1, 1};
+  Arr5 CX{const_cast<double*>(cx), N + 1, N, N, 1}, CY{const_cast<double*>(cy), N, N + 1, N, 1},
+      CZ{const_cast<double*>(cz), N, N, N + 1, 1};
+  Kokkos::View<size_t*> Q(q.data()), Cq(c.data());
+  Kokkos::View<uint8_t*> E(e.data());
+  Kokkos::View<int8_t***> HF(hf.data(), 3, 2);
+  grace::amr::div_free_prolong_op<K, Arr5> op(X, Y, Z, CX, CY, CZ, Q, Cq, E, HF, n, ngz);
+  for (int64_t iq = 0; iq < nelems; ++iq) op(Kokkos::SerialTeam{(int)iq});
+}
+}  // namespace
+extern "C" void ref_prolong_cells(int kind, int n, int ngz, int nvars, double* fine, const double* cbuf,
+                                  int64_t nelems, const int64_t* fine_q, const int64_t* cbuf_q, const uint8_t* elem,
+                                  const int* vlo, int nlo, const int* vhi, int nhi) {
+  using namespace grace::amr;
+  if (kind == 0) ref_prolong_cells_k<FACE>(n, ngz, nvars, fine, cbuf, nelems, fine_q, cbuf_q, elem, vlo, nlo, vhi, nhi);
+  if (kind == 1) ref_prolong_cells_k<EDGE>(n, ngz, nvars, fine, cbuf, nelems, fine_q, cbuf_q, elem, vlo, nlo, vhi, nhi);
+  if (kind == 2)
+    ref_prolong_cells_k<CORNER>(n, ngz, nvars, fine, cbuf, nelems, fine_q, cbuf_q, elem, vlo, nlo, vhi, nhi);
+}
+extern "C" void ref_prolong_faces(int kind, int n, int ngz, double* fx, double* fy, double* fz, const double* cx,
+                                  const double* cy, const double* cz, int64_t nelems, const int64_t* fine_q,
+                                  const int64_t* cbuf_q, const uint8_t* elem, const int8_t* have_fine) {
+  using namespace grace::amr;
+  if (kind == 0) ref_prolong_faces_k<FACE>(n, ngz, fx, fy, fz, cx, cy, cz, nelems, fine_q, cbuf_q, elem, have_fine);
+  if (kind == 1) ref_prolong_faces_k<EDGE>(n, ngz, fx, fy, fz, cx, cy, cz, nelems, fine_q, cbuf_q, elem, have_fine);
+  if (kind == 2)
+    ref_prolong_faces_k<CORNER>(n, ngz, fx, fy, fz, cx, cy, cz, nelems, fine_q, cbuf_q, elem, have_fine);
+}

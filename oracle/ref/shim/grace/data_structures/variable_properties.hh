@@ -3,6 +3,7 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <array>
 namespace grace {
 enum bc_t { BC_NONE_SHIM = 0 };
 // the staggering names and array types the AMR helper headers mention
@@ -10,6 +11,9 @@ enum var_staggering_t : uint8_t {
   STAG_CENTER = 0, STAG_FACEX, STAG_FACEY, STAG_EDGEXY, STAG_FACEZ, STAG_EDGEXZ, STAG_EDGEYZ, STAG_CORNER,
   N_VAR_STAGGERINGS
 };
+inline std::array<int, 3> get_index_staggerings(var_staggering_t stag) {
+  return {stag & 1, (stag >> 1) & 1, (stag >> 2) & 1};
+}
 struct var_array_t {};
 struct staggered_variable_arrays_t {
   var_array_t face_staggered_fields_x, face_staggered_fields_y, face_staggered_fields_z;

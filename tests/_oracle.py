@@ -38,6 +38,8 @@ def _bind(lib, pre):
         "restrict_cells": (None, [C.c_int, C.c_int, C.c_int, VP, VP, C.c_int64, VP, VP, VP, VP, C.c_int, VP,
                                   C.c_int]),
         "restrict_faces": (None, [C.c_int, C.c_int, C.c_int, VP, VP, C.c_int64, VP, VP]),
+        "prolong_cells": (None, [C.c_int] * 4 + [VP, VP, C.c_int64, VP, VP, VP, VP, C.c_int, VP, C.c_int]),
+        "prolong_faces": (None, [C.c_int] * 3 + [VP] * 6 + [C.c_int64, VP, VP, VP, VP]),
     }
     for name, (res, args) in sig.items():
         if not hasattr(lib, pre + name):  # the pinning build exports a subset
@@ -63,6 +65,27 @@ def restrict_faces(dir, n, ngz, src, dst, src_q, dst_q):
     q = lambda a: np.ascontiguousarray(a, dtype=np.int64)
     sq, dq = q(src_q), q(dst_q)
     L.orc_restrict_faces(dir, n, ngz, p(src), p(dst), len(sq), p(sq), p(dq))
+
+
+def prolong_cells(which, kind, n, ngz, nvars, fine, cbuf, fine_q, cbuf_q, elem, vlo, vhi):
+    """FMR prolongation of cell variables into the ghost elements of one kind
+    (0 faces, 1 edges, 2 corners) from coarse buffers (amr_oracle.hpp)."""
+    L = lib(which)
+    q = lambda a, t: np.ascontiguousarray(a, dtype=t)
+    fq, cq, el = q(fine_q, np.int64), q(cbuf_q, np.int64), q(elem, np.uint8)
+    vl, vh = q(vlo, np.int32), q(vhi, np.int32)
+    getattr(L, which + "_prolong_cells")(kind, n, ngz, nvars, p(fine), p(cbuf), len(fq), p(fq), p(cq), p(el),
+                                         p(vl), len(vl), p(vh), len(vh))
+
+
+def prolong_faces(which, kind, n, ngz, fine, cbuf, fine_q, cbuf_q, elem, have_fine):
+    """Divergence-preserving prolongation of face B into the ghost elements of
+    one kind; fine, cbuf: (bx, by, bz) arrays; have_fine (nelems, 3, 2)."""
+    L = lib(which)
+    q = lambda a, t: np.ascontiguousarray(a, dtype=t)
+    fq, cq, el, hf = q(fine_q, np.int64), q(cbuf_q, np.int64), q(elem, np.uint8), q(have_fine, np.int8)
+    getattr(L, which + "_prolong_faces")(kind, n, ngz, p(fine[0]), p(fine[1]), p(fine[2]), p(cbuf[0]), p(cbuf[1]),
+                                         p(cbuf[2]), len(fq), p(fq), p(cq), p(el), p(hf))
 
 
 def build_oracle():

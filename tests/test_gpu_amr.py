@@ -1,7 +1,9 @@
-"""FMR restriction into coarse buffers on the GPU (grb_restrict_to_coarse)
+"""FMR restriction into coarse buffers (grb_restrict_to_coarse) and
+prolongation into ghost zones (grb_prolong_to_ghosts) on the GPU
 against the oracle (oracle/amr_oracle.hpp, itself pinned to the reference's
 operators): bit for bit, both variable lists, every Morton child position,
-the three face arrays; and div B of the restricted face field."""
+the three face arrays, every ghost element kind; and div B of the restricted
+and of the prolonged face fields."""
 import numpy as np
 import pytest
 import torch
@@ -68,3 +70,76 @@ def test_restricted_face_field_is_divergence_free():
     div = (cx[s, s, G + 1:G + h + 1] - cx[s, s, s]) + (cy[s, G + 1:G + h + 1, s] - cy[s, s, s]) + \
           (cz[G + 1:G + h + 1, s, s] - cz[s, s, s])
     assert np.max(np.abs(div)) < 1e-13
+
+
+NELEM = {0: 6, 1: 12, 2: 8}
+FSH = [(NN, NN, NN + 1), (NN, NN + 1, NN), (NN + 1, NN, NN)]
+
+
+@pytest.mark.parametrize("kind", [0, 1, 2])
+def test_prolong_to_ghosts_matches_oracle_bitwise(kind):
+    """grb_prolong_to_ghosts against the oracle (pinned to the reference's
+    prolong_op / div_free_prolong_op): every element of the kind on several
+    quadrants, both variable lists, face B with random fine-neighbour
+    flags, bit for bit."""
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(60 + kind)
+    nq, ncb = 6, 8
+    st0 = rng.standard_normal((nq, abi.N_EVOL_VARS, NN, NN, NN))
+    fb0 = [rng.standard_normal((nq,) + s) for s in FSH]
+    cst = rng.standard_normal((ncb, abi.N_EVOL_VARS, NN, NN, NN))
+    cfb = [rng.standard_normal((ncb,) + s) for s in FSH]
+    fq = np.repeat(np.arange(nq), NELEM[kind]).astype(np.int64)
+    el = np.tile(np.arange(NELEM[kind]), nq).astype(np.uint8)
+    perm = rng.permutation(len(fq))
+    fq, el = fq[perm], el[perm]
+    cq = rng.permutation(ncb)[:nq][fq].astype(np.int64)
+    hf = rng.integers(0, 2, size=(len(fq), 3, 2)).astype(np.int8)
+    vlo, vhi = [0, 5, 6, 13], [1, 2, 3, 4, 22]
+    g = GRMHDEquationsSystem(params.blast())
+    g.reserve(Blocks(N, N, N, G, nq, np.ones((nq, 3)), device=dev))
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    fine = Fields(T(st0), *[T(x) for x in fb0])
+    cb = Fields(T(cst), *[T(x) for x in cfb])
+    g.prolong_to_ghosts(fine, cb, kind, T(fq), T(cq), T(el), T(hf), vlo, vhi)
+    torch.cuda.synchronize()
+    ost = st0.copy()
+    _oracle.prolong_cells("orc", kind, N, G, abi.N_EVOL_VARS, ost, cst, fq, cq, el, vlo, vhi)
+    ofb = [x.copy() for x in fb0]
+    _oracle.prolong_faces("orc", kind, N, G, ofb, cfb, fq, cq, el, hf)
+    np.testing.assert_array_equal(fine.state.cpu().numpy(), ost)
+    for d in range(3):
+        np.testing.assert_array_equal((fine.bx, fine.by, fine.bz)[d].cpu().numpy(), ofb[d])
+    assert (ost != st0).any() and all((a != b).any() for a, b in zip(ofb, fb0))
+    assert g.status().device_flags == 0
+
+
+def test_prolonged_ghost_faces_are_divergence_free():
+    """Faces, edges and corners of a quadrant prolonged from a divergence-free
+    coarse face field (no fine neighbours): every fine ghost cell's div B at
+    round-off."""
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(9)
+    Ax = rng.standard_normal((NN + 1, NN + 1, NN))
+    Ay = rng.standard_normal((NN + 1, NN, NN + 1))
+    Az = rng.standard_normal((NN, NN + 1, NN + 1))
+    cbx = (Az[:, 1:, :] - Az[:, :-1, :]) - (Ay[1:] - Ay[:-1])
+    cby = (Ax[1:] - Ax[:-1]) - (Az[:, :, 1:] - Az[:, :, :-1])
+    cbz = (Ay[:, :, 1:] - Ay[:, :, :-1]) - (Ax[:, 1:, :] - Ax[:, :-1, :])
+    g = GRMHDEquationsSystem(params.blast())
+    g.reserve(Blocks(N, N, N, G, 1, np.ones((1, 3)), device=dev))
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    st = torch.zeros((1, abi.N_EVOL_VARS, NN, NN, NN), dtype=torch.float64, device=dev)
+    fine = Fields(st, *[torch.full((1,) + s, float("nan"), dtype=torch.float64, device=dev) for s in FSH])
+    cb = Fields(st.clone(), T(cbx[None]), T(cby[None]), T(cbz[None]))
+    for kind in (0, 1, 2):
+        el = torch.arange(NELEM[kind], dtype=torch.uint8, device=dev)
+        z = torch.zeros(NELEM[kind], dtype=torch.int64, device=dev)
+        hf = torch.zeros((NELEM[kind], 3, 2), dtype=torch.int8, device=dev)
+        g.prolong_to_ghosts(fine, cb, kind, z, z, el, hf)
+    bx, by, bz = (x[0].cpu().numpy() for x in (fine.bx, fine.by, fine.bz))
+    div = (bx[:, :, 1:] - bx[:, :, :-1]) + (by[:, 1:, :] - by[:, :-1, :]) + (bz[1:] - bz[:-1])
+    ghost = np.ones((NN, NN, NN), bool)
+    ghost[G:G + N, G:G + N, G:G + N] = False
+    assert np.isfinite(div[ghost]).all()
+    assert np.abs(div[ghost]).max() <= 1e-13 * max(np.abs(cbx).max(), np.abs(cby).max(), np.abs(cbz).max())
