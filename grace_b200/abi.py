@@ -169,6 +169,8 @@ PROTOTYPES = {
     "grb_restrict_to_coarse": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Fields),
                                          C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
                                          C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_void_p]),
+    "grb_accumulate_boundary_outflow": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.c_int64, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_double, C.c_double, C.c_void_p, C.c_void_p]),
     "grb_prolong_to_ghosts": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Fields),
                                         C.c_int32, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                         C.POINTER(C.c_int32), C.c_int32, C.POINTER(C.c_int32), C.c_int32,

@@ -42,6 +42,14 @@ struct RestrictVars {
   int n;
   int v[GRB_N_EVOL_VARS];
 };
+// V.v[i] by an unrolled select: a dynamic index into a kernel parameter
+// would copy the whole list to local memory.
+__device__ __forceinline__ int list_var(const RestrictVars& V, int i) {
+  int v = V.v[0];
+#pragma unroll
+  for (int t = 1; t < GRB_N_EVOL_VARS; ++t) v = i == t ? V.v[t] : v;
+  return v;
+}
 
 // Cell variables.  box: (n/2)^3 coarse cells x (nvars_in_list x nquads)
 // folded into the box's block index (variable fastest).  kHigh: the 5-point
@@ -56,7 +64,7 @@ __global__ void __launch_bounds__(128) k_restrict_cells(Geo G, Box box, Restrict
   int64_t t;
   if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, t)) return;
   const uint32_t iq = fast_div((uint32_t)t, dnv);
-  const int v = V.v[(uint32_t)t - iq * (uint32_t)V.n];
+  const int v = list_var(V, (int)((uint32_t)t - iq * (uint32_t)V.n));
   const int N0 = G.NX, N1 = G.NY;
   const double* u = src + (src_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
   auto at = [&](int x, int y, int z) { return u[((int64_t)z * N1 + y) * N0 + x]; };
@@ -160,9 +168,16 @@ __device__ __forceinline__ int pick3(int l, int a, int b, int c) { return l == 0
 __constant__ double c_prolong5[10] = {-45.0 / 2048.0, 105.0 / 512.0, 945.0 / 1024.0, -63.0 / 512.0, 35.0 / 2048.0,
                                       35.0 / 2048.0,  -63.0 / 512.0, 945.0 / 1024.0, 105.0 / 512.0, -45.0 / 2048.0};
 
-// Cell variables.  box: the kind's ghost extent (ngz, n | ngz, n | ngz) x
-// (nvars_in_list x nelems), variable fastest.  kHigh: the 5-point Lagrange
-// operator, else the minmod slope-limited one.
+// Cell variables, one thread per coarse cell of an element: it computes the
+// element's 8 fine cells inside that coarse cell.  box: the kind's ghost
+// extent halved, (ngz/2, n/2 | ngz/2, n/2 | ngz/2) x (nvars_in_list x
+// nelems), variable fastest.  kHigh: the 5-point Lagrange operator (its x
+// contractions shared by the children with the same x half, the y ones by
+// those with the same x and y halves: the reference's per-child sums
+// Sx[dj][dk], Sy[dk], result, each evaluated once), else the minmod
+// slope-limited one (the three limited slopes shared).  The two children
+// along x are adjacent doubles at an even fine index and leave as one
+// 16-byte store.
 template <int kKind, bool kHigh>
 __global__ void __launch_bounds__(128) k_prolong_cells(Geo G, Box box, RestrictVars V, FastDiv dnv,
                                                        const double* __restrict__ cbuf, double* __restrict__ fine,
@@ -173,7 +188,7 @@ __global__ void __launch_bounds__(128) k_prolong_cells(Geo G, Box box, RestrictV
   int64_t t;
   if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, a, b, c, t)) return;
   const uint32_t iq = fast_div((uint32_t)t, dnv);
-  const int v = V.v[(uint32_t)t - iq * (uint32_t)V.n];
+  const int v = list_var(V, (int)((uint32_t)t - iq * (uint32_t)V.n));
   const int e = elem[iq];
   int f[3], k[3];
 #pragma unroll
@@ -181,44 +196,68 @@ __global__ void __launch_bounds__(128) k_prolong_cells(Geo G, Box box, RestrictV
     int w, lp;
     ghost_axis<kKind>(e, d, w, lp);
     const int l = pick3(lp, a, b, c);
-    f[d] = ghost_idx(w, G.nx, G.g, 0, l);
-    k[d] = ghost_idx(w, G.nx / 2, G.g, G.g / 2, l >> 1);
+    f[d] = ghost_idx(w, G.nx, G.g, 0, 2 * l);  // the lower child; even
+    k[d] = ghost_idx(w, G.nx / 2, G.g, G.g / 2, l);
   }
   const int N0 = G.NX, N1 = G.NY;
   const double* u = cbuf + (cbuf_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
   auto at = [&](int x, int y, int z) { return u[((int64_t)z * N1 + y) * N0 + x]; };
-  double r;
+  double r[2][2][2];  // [pz][py][px]
   if (!kHigh) {
     const double u0 = at(k[0], k[1], k[2]);
-    double acc = 0.0;
+    double lim[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       const int dx = d == 0, dy = d == 1, dz = d == 2;
       const double sl = __dsub_rn(u0, at(k[0] - dx, k[1] - dy, k[2] - dz));
       const double sr = __dsub_rn(at(k[0] + dx, k[1] + dy, k[2] + dz), u0);
-      acc = __dadd_rn(acc, __dmul_rn((f[d] & 1) ? 0.25 : -0.25, lim_minmod(sl, sr)));
+      lim[d] = lim_minmod(sl, sr);
     }
-    r = __dadd_rn(u0, acc);
+#pragma unroll
+    for (int pz = 0; pz < 2; ++pz)
+#pragma unroll
+      for (int py = 0; py < 2; ++py)
+#pragma unroll
+        for (int px = 0; px < 2; ++px) {
+          double acc = 0.0;
+          acc = __dadd_rn(acc, __dmul_rn(px ? 0.25 : -0.25, lim[0]));
+          acc = __dadd_rn(acc, __dmul_rn(py ? 0.25 : -0.25, lim[1]));
+          acc = __dadd_rn(acc, __dmul_rn(pz ? 0.25 : -0.25, lim[2]));
+          r[pz][py][px] = __dadd_rn(u0, acc);
+        }
   } else {
-    const double* cx = c_prolong5 + 5 * (f[0] & 1);
-    const double* cy = c_prolong5 + 5 * (f[1] & 1);
-    const double* cz = c_prolong5 + 5 * (f[2] & 1);
-    double Sy[5];
+    double Sy[2][2][5];  // [px][py][dk]
 #pragma unroll
     for (int dk = 0; dk < 5; ++dk) {
-      double col[5];
+      double Sx[2][5];  // [px][dj]
 #pragma unroll
       for (int dj = 0; dj < 5; ++dj) {
         double line[5];
 #pragma unroll
         for (int di = 0; di < 5; ++di) line[di] = at(k[0] + di - 2, k[1] + dj - 2, k[2] + dk - 2);
-        col[dj] = contract5_rn(cx, line);
+        Sx[0][dj] = contract5_rn(c_prolong5, line);
+        Sx[1][dj] = contract5_rn(c_prolong5 + 5, line);
       }
-      Sy[dk] = contract5_rn(cy, col);
+#pragma unroll
+      for (int px = 0; px < 2; ++px) {
+        Sy[px][0][dk] = contract5_rn(c_prolong5, Sx[px]);
+        Sy[px][1][dk] = contract5_rn(c_prolong5 + 5, Sx[px]);
+      }
     }
-    r = contract5_rn(cz, Sy);
+#pragma unroll
+    for (int pz = 0; pz < 2; ++pz)
+#pragma unroll
+      for (int py = 0; py < 2; ++py)
+#pragma unroll
+        for (int px = 0; px < 2; ++px) r[pz][py][px] = contract5_rn(c_prolong5 + 5 * pz, Sy[px][py]);
   }
-  fine[(fine_q[iq] * GRB_N_EVOL_VARS + v) * G.cells + ((int64_t)f[2] * N1 + f[1]) * N0 + f[0]] = r;
+  double* o = fine + (fine_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
+#pragma unroll
+  for (int pz = 0; pz < 2; ++pz)
+#pragma unroll
+    for (int py = 0; py < 2; ++py)
+      *reinterpret_cast<double2*>(o + ((int64_t)(f[2] + pz) * N1 + (f[1] + py)) * N0 + f[0]) =
+          make_double2(r[pz][py][0], r[pz][py][1]);
 }
 
 // One block's face array staggered along d.

@@ -20,6 +20,7 @@
 
 #include "grace_b200.h"
 #include "amr.cuh"
+#include "outflow.cuh"
 #include "flux_tma.cuh"
 #include "mlp.cuh"
 #include "stage_kernels.cuh"
@@ -983,7 +984,7 @@ static void launch_prolong(const Geo& G, const int ext[3], const grb_fields* fin
                            const int8_t* have_fine, const RestrictVars* V, bool faces, cudaStream_t s) {
   for (int pass = 0; pass < 2; ++pass) {
     if (!V[pass].n) continue;
-    const Box b = box(0, 0, 0, ext[0], ext[1], ext[2], (int64_t)V[pass].n * nelems);
+    const Box b = box(0, 0, 0, ext[0] / 2, ext[1] / 2, ext[2] / 2, (int64_t)V[pass].n * nelems);
     const FastDiv dv = make_fastdiv((uint32_t)V[pass].n);
     if (pass == 0)
       k_prolong_cells<kKind, false><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V[0], dv, cbuf->state, fine->state,
@@ -1524,6 +1525,25 @@ int grb_prolong_to_ghosts(grb_handle* h, const grb_grid* g, const grb_fields* fi
   else
     launch_prolong<GRB_ELEM_CORNER>(G, ext, fine, cbuf, nelems, fine_q, cbuf_q, elem_id, have_fine, V, faces, s);
   h->launches += (V[0].n > 0) + (V[1].n > 0) + 2 * faces;
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_accumulate_boundary_outflow(grb_handle* h, const grb_grid* g, int64_t nfaces, const int64_t* quad,
+                                    const uint8_t* face, const double* dx, double dt, double dtfact,
+                                    double* outflow, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  int rc = check_grid(h, g);
+  if (rc) return fail(h, rc);
+  if (nfaces < 0 || nfaces > 0x7fffffff || !outflow || (nfaces && (!quad || !face || !dx)))
+    return fail(h, GRB_ERR_INVALID);
+  if (nfaces == 0) return GRB_OK;
+  if (!h->B.flux) return fail(h, GRB_ERR_NOT_RESERVED);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  cudaStream_t s = (cudaStream_t)stream;
+  KScope ks(h, s, GRB_KIND_OTHER);
+  k_boundary_outflow<<<(unsigned)nfaces, kOutflowThreads, 0, s>>>(G, h->B.flux, quad, face, dx, dt * dtfact, outflow);
+  ++h->launches;
   CK(cudaGetLastError());
   return GRB_OK;
 }

@@ -191,6 +191,20 @@ class GRMHDEquationsSystem:
             dst_q.data_ptr(), child_id.data_ptr() if child_id is not None else None, lo, len(vars_lo), hi,
             len(vars_ho), _stream_ptr(stream)), "grb_restrict_to_coarse")
 
+    def accumulate_boundary_outflow(self, quad, face, dx, dt, dtfact, outflow, stream=None):
+        """Add the substep's mass outflux through the listed outer-boundary
+        faces to the device scalar `outflow` (grb_accumulate_boundary_outflow).
+        quad: int64, face: uint8 device tensors; dx: float64 device tensor
+        (nq, 3) of cell spacings; outflow: float64 device tensor of one
+        element."""
+        for t, dt_ in ((quad, torch.int64), (face, torch.uint8), (dx, torch.float64), (outflow, torch.float64)):
+            if t.dtype != dt_ or not t.is_cuda or not t.is_contiguous():
+                raise ValueError("quad, face, dx and outflow must be contiguous device tensors of the documented types")
+        g = self.blocks.c()
+        _lib.check(self.lib.grb_accumulate_boundary_outflow(
+            self.h, ctypes.byref(g), quad.numel(), quad.data_ptr(), face.data_ptr(), dx.data_ptr(), float(dt),
+            float(dtfact), outflow.data_ptr(), _stream_ptr(stream)), "grb_accumulate_boundary_outflow")
+
     def prolong_to_ghosts(self, fine, cbuf, elem_kind, fine_q, cbuf_q, elem_id, have_fine=None, vars_lo=(),
                           vars_ho=(), faces=True, stream=None):
         """FMR prolongation into the ghost elements of one kind

@@ -68,6 +68,24 @@ class BrickSetup:
     def blocks(self, qr=None):
         return range(self.nq) if qr is None else range(*qr)
 
+    def outer_faces(self):
+        """(quad, face) of every block face on a non-periodic outer boundary
+        of the brick, face = 2 axis + side (side 1 upper): the list GRACE's
+        face iterator collects for the outflow diagnostic."""
+        quad, face = [], []
+        for q in range(self.nq):
+            qc = (q % self.nb[0], (q // self.nb[0]) % self.nb[1], q // (self.nb[0] * self.nb[1]))
+            for a in range(3):
+                if self.periodic[a]:
+                    continue
+                if qc[a] == 0:
+                    quad.append(q)
+                    face.append(2 * a)
+                if qc[a] == self.nb[a] - 1:
+                    quad.append(q)
+                    face.append(2 * a + 1)
+        return np.array(quad, np.int64), np.array(face, np.uint8)
+
     def cell_centres(self, qr=None):
         """(nq, 3, NZ, NY, NX) physical cell centres, ghosts included."""
         NX, NY, NZ = self.N

@@ -462,6 +462,26 @@ int grb_restrict_to_coarse(grb_handle* h, const grb_grid* g, const grb_fields* f
                            const int32_t* vars_lo, int32_t nlo, const int32_t* vars_ho,
                            int32_t nho, void* stream);
 
+/* ---- boundary mass outflux ------------------------------------------------ */
+/* = boundary_outflow_t::accumulate (include/grace/evolution/
+ *   boundary_outflow.hh:79-180, called from evolve.cpp:1704): for each of
+ *   the nfaces (quad[i], face[i]) on a non-periodic outer boundary (face =
+ *   2 axis + side, side 1 the upper face), adds
+ *     sign * dt * dtfact * dA * sum over the face's interior cells of the
+ *     DENS flux through the block's boundary face plane
+ *   to the device scalar *outflow (sign +1 on upper faces, -1 on lower;
+ *   dA the product of the two tangential spacings from dx, the (3, nq)
+ *   device array dx[d + 3 q] of getspacings()).  It reads the face fluxes
+ *   the last grb_advance_substep on this handle computed (after the FOFC
+ *   correction), so call it after each substep with that substep's dt and
+ *   dtfact.  quad (int64), face (uint8) are device arrays; one CTA per face,
+ *   summed into *outflow by one atomic add each, as the reference does.
+ *   Reading back, the MPI sum over ranks, the symmetry multiplier and the
+ *   reset (flush_to_host) stay with the caller. */
+int grb_accumulate_boundary_outflow(grb_handle* h, const grb_grid* g, int64_t nfaces,
+                                    const int64_t* quad, const uint8_t* face, const double* dx,
+                                    double dt, double dtfact, double* outflow, void* stream);
+
 /* ---- FMR: prolongation into ghost zones --------------------------------- */
 #define GRB_ELEM_FACE 0
 #define GRB_ELEM_EDGE 1
