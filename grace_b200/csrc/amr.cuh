@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(128) k_restrict_faces(Geo G, Box box, const do
 // axes over 0, 1 (the sides in bits 0, 1 of e) and its own axis over 2; a
 // corner axis d over d (the side in bit d of e).
 template <int kKind>
-__host__ __device__ __forceinline__ void ghost_axis(int e, int d, int& where, int& loop) {
+__device__ __forceinline__ void ghost_axis(int e, int d, int& where, int& loop) {
   if (kKind == GRB_ELEM_FACE) {
     const int ax = e >> 1;
     where = d == ax ? (e & 1) : 2;
@@ -159,7 +159,7 @@ __host__ __device__ __forceinline__ void ghost_axis(int e, int d, int& where, in
     loop = d;
   }
 }
-__host__ __device__ __forceinline__ int ghost_idx(int where, int n, int g, int goff, int t) {
+__device__ __forceinline__ int ghost_idx(int where, int n, int g, int goff, int t) {
   return where == 2 ? g + t : (where ? n + g + t : goff + t);
 }
 __device__ __forceinline__ int pick3(int l, int a, int b, int c) { return l == 0 ? a : (l == 1 ? b : c); }
@@ -258,93 +258,6 @@ __global__ void __launch_bounds__(128) k_prolong_cells(Geo G, Box box, RestrictV
     for (int py = 0; py < 2; ++py)
       *reinterpret_cast<double2*>(o + ((int64_t)(f[2] + pz) * N1 + (f[1] + py)) * N0 + f[0]) =
           make_double2(r[pz][py][0], r[pz][py][1]);
-}
-
-// Shared-memory footprint (doubles) of k_prolong_lag_smem for a coarse
-// region of r0 x r1 x r2 cells: the coarse data with its 2-cell halo, the
-// x contractions for both x halves, the y contractions for the 4 (x, y)
-// halves.
-__host__ __device__ inline int prolong_lag_smem_doubles(int r0, int r1, int r2) {
-  const int s1 = r1 + 4, s2 = r2 + 4;
-  return (r0 + 4) * s1 * s2 + 2 * r0 * s1 * s2 + 4 * r0 * r1 * s2;
-}
-
-// High-order list, one CTA per (element, variable): the element's coarse
-// region plus halo is staged in shared memory and the 5-point Lagrange
-// prolongation runs as three separable passes, each partial sum computed
-// once and shared by every fine cell that uses it (Sx along x for each x
-// half, Sy along y for each (x, y) half, the result along z), with the
-// reference's operands and order, so the fine values are those of
-// lagrange_prolong_op<4> bit for bit.  Grid: nelems x nvars_in_list CTAs,
-// variable fastest.
-template <int kKind>
-__global__ void __launch_bounds__(128) k_prolong_lag_smem(Geo G, RestrictVars V, const double* __restrict__ cbuf,
-                                                          double* __restrict__ fine,
-                                                          const int64_t* __restrict__ fine_q,
-                                                          const int64_t* __restrict__ cbuf_q,
-                                                          const uint8_t* __restrict__ elem) {
-  extern __shared__ double sm[];
-  const uint32_t iq = blockIdx.x / (uint32_t)V.n;
-  const int v = list_var(V, (int)(blockIdx.x - iq * (uint32_t)V.n));
-  const int e = elem[iq];
-  const int n = G.nx, g = G.g;
-  int r[3], k0[3], f0[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    int w, lp;
-    ghost_axis<kKind>(e, d, w, lp);
-    r[d] = w == 2 ? n / 2 : g / 2;
-    k0[d] = ghost_idx(w, n / 2, g, g / 2, 0) - 2;  // staged origin
-    f0[d] = ghost_idx(w, n, g, 0, 0);
-  }
-  const int s0 = r[0] + 4, s1 = r[1] + 4, s2 = r[2] + 4;
-  double* U = sm;                      // [z][y][x], s2 x s1 x s0
-  double* Sx = U + s0 * s1 * s2;       // [px][z][y][x], x < r0
-  double* Sy = Sx + 2 * r[0] * s1 * s2;  // [px][py][z][y][x], x < r0, y < r1
-  const int N0 = G.NX, N1 = G.NY;
-  const double* u = cbuf + (cbuf_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
-  const int nu = s0 * s1 * s2;
-  for (int t = threadIdx.x; t < nu; t += blockDim.x) {
-    const int x = t % s0, yz = t / s0, y = yz % s1, z = yz / s1;
-    U[t] = u[((int64_t)(k0[2] + z) * N1 + (k0[1] + y)) * N0 + (k0[0] + x)];
-  }
-  __syncthreads();
-  const int nx_ = 2 * r[0] * s1 * s2;
-  for (int t = threadIdx.x; t < nx_; t += blockDim.x) {
-    const int x = t % r[0], rest = t / r[0], yz = rest % (s1 * s2), px = rest / (s1 * s2);
-    const double* l = U + yz * s0 + x;
-    const double line[5] = {l[0], l[1], l[2], l[3], l[4]};
-    Sx[t] = contract5_rn(c_prolong5 + 5 * px, line);
-  }
-  __syncthreads();
-  const int ny_ = 4 * r[0] * r[1] * s2;
-  for (int t = threadIdx.x; t < ny_; t += blockDim.x) {
-    const int x = t % r[0], rest = t / r[0], y = rest % r[1], rest2 = rest / r[1], z = rest2 % s2, pp = rest2 / s2;
-    const int px = pp >> 1, py = pp & 1;
-    const double* l = Sx + ((px * s2 + z) * s1 + y) * r[0] + x;
-    const int st = r[0];
-    const double line[5] = {l[0], l[st], l[2 * st], l[3 * st], l[4 * st]};
-    Sy[t] = contract5_rn(c_prolong5 + 5 * py, line);
-  }
-  __syncthreads();
-  double* o = fine + (fine_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
-  const int no = 4 * r[0] * r[1] * r[2];
-  const int sy_p = r[0] * r[1] * s2;  // stride between (px, py) planes of Sy
-  for (int t = threadIdx.x; t < no; t += blockDim.x) {
-    const int x = t % r[0], rest = t / r[0], y = rest % r[1], rest2 = rest / r[1], z = rest2 % r[2],
-              pp = rest2 / r[2];
-    const int py = pp & 1, pz = pp >> 1;
-    double res[2];
-#pragma unroll
-    for (int px = 0; px < 2; ++px) {
-      const double* l = Sy + (px * 2 + py) * sy_p + (z * r[1] + y) * r[0] + x;
-      const int st = r[0] * r[1];
-      const double line[5] = {l[0], l[st], l[2 * st], l[3 * st], l[4 * st]};
-      res[px] = contract5_rn(c_prolong5 + 5 * pz, line);
-    }
-    *reinterpret_cast<double2*>(o + ((int64_t)(f0[2] + 2 * z + pz) * N1 + (f0[1] + 2 * y + py)) * N0 +
-                                f0[0] + 2 * x) = make_double2(res[0], res[1]);
-  }
 }
 
 // One block's face array staggered along d.

@@ -978,49 +978,12 @@ int grad_setup(grb_handle* h) {
 }  // namespace
 
 // FMR prolongation launches of one element kind (grb_prolong_to_ghosts).
-// The staged Lagrange kernel for the kind's largest element, when its shared
-// memory fits (set up once per device and size).
-template <int kKind>
-static bool prolong_lag_smem_ready(const Geo& G, size_t& bytes) {
-  const int ne = kKind == GRB_ELEM_FACE ? 6 : (kKind == GRB_ELEM_EDGE ? 12 : 8);
-  int most = 0;
-  for (int e = 0; e < ne; ++e) {
-    int r[3];
-    for (int d = 0; d < 3; ++d) {
-      int w, lp;
-      ghost_axis<kKind>(e, d, w, lp);
-      r[d] = w == 2 ? G.nx / 2 : G.g / 2;
-    }
-    const int m = prolong_lag_smem_doubles(r[0], r[1], r[2]);
-    most = m > most ? m : most;
-  }
-  bytes = sizeof(double) * (size_t)most;
-  if (bytes > 227 * 1024) return false;
-  static size_t attr[kMaxDevices] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
-  if (bytes > 48 * 1024 && bytes > attr[dev]) {
-    if (cudaFuncSetAttribute(k_prolong_lag_smem<kKind>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
-        cudaSuccess)
-      return false;
-    attr[dev] = bytes;
-  }
-  return true;
-}
-
 template <int kKind>
 static void launch_prolong(const Geo& G, const int ext[3], const grb_fields* fine, const grb_fields* cbuf,
                            int64_t nelems, const int64_t* fine_q, const int64_t* cbuf_q, const uint8_t* elem_id,
                            const int8_t* have_fine, const RestrictVars* V, bool faces, cudaStream_t s) {
-  size_t lag_bytes = 0;
-  if (V[1].n && (int64_t)V[1].n * nelems < (1ll << 31) && prolong_lag_smem_ready<kKind>(G, lag_bytes)) {
-    k_prolong_lag_smem<kKind><<<(unsigned)(V[1].n * nelems), 128, lag_bytes, s>>>(G, V[1], cbuf->state, fine->state,
-                                                                                 fine_q, cbuf_q, elem_id);
-  } else {
-    lag_bytes = 0;
-  }
   for (int pass = 0; pass < 2; ++pass) {
-    if (!V[pass].n || (pass == 1 && lag_bytes)) continue;
+    if (!V[pass].n) continue;
     const Box b = box(0, 0, 0, ext[0] / 2, ext[1] / 2, ext[2] / 2, (int64_t)V[pass].n * nelems);
     const FastDiv dv = make_fastdiv((uint32_t)V[pass].n);
     if (pass == 0)
