@@ -168,17 +168,13 @@ __device__ __forceinline__ int pick3(int l, int a, int b, int c) { return l == 0
 __constant__ double c_prolong5[10] = {-45.0 / 2048.0, 105.0 / 512.0, 945.0 / 1024.0, -63.0 / 512.0, 35.0 / 2048.0,
                                       35.0 / 2048.0,  -63.0 / 512.0, 945.0 / 1024.0, 105.0 / 512.0, -45.0 / 2048.0};
 
-// Cell variables, one thread per coarse cell of an element: it computes the
-// element's 8 fine cells inside that coarse cell.  box: the kind's ghost
-// extent halved, (ngz/2, n/2 | ngz/2, n/2 | ngz/2) x (nvars_in_list x
-// nelems), variable fastest.  kHigh: the 5-point Lagrange operator (its x
-// contractions shared by the children with the same x half, the y ones by
-// those with the same x and y halves: the reference's per-child sums
-// Sx[dj][dk], Sy[dk], result, each evaluated once), else the minmod
-// slope-limited one (the three limited slopes shared).  The two children
-// along x are adjacent doubles at an even fine index and leave as one
-// 16-byte store.
-template <int kKind, bool kHigh>
+// Low-order list, one thread per coarse cell of an element and variable:
+// the minmod slope-limited operator for the element's 8 fine cells inside
+// that coarse cell (the three limited slopes shared).  box: the kind's
+// ghost extent halved, (ngz/2, n/2 | ngz/2, n/2 | ngz/2) x (nvars_in_list x
+// nelems), variable fastest.  The two children along x are adjacent doubles
+// at an even fine index and leave as one 16-byte store.
+template <int kKind>
 __global__ void __launch_bounds__(128) k_prolong_cells(Geo G, Box box, RestrictVars V, FastDiv dnv,
                                                        const double* __restrict__ cbuf, double* __restrict__ fine,
                                                        const int64_t* __restrict__ fine_q,
@@ -202,62 +198,105 @@ __global__ void __launch_bounds__(128) k_prolong_cells(Geo G, Box box, RestrictV
   const int N0 = G.NX, N1 = G.NY;
   const double* u = cbuf + (cbuf_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
   auto at = [&](int x, int y, int z) { return u[((int64_t)z * N1 + y) * N0 + x]; };
-  double r[2][2][2];  // [pz][py][px]
-  if (!kHigh) {
-    const double u0 = at(k[0], k[1], k[2]);
-    double lim[3];
+  const double u0 = at(k[0], k[1], k[2]);
+  double lim[3];
 #pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      const int dx = d == 0, dy = d == 1, dz = d == 2;
-      const double sl = __dsub_rn(u0, at(k[0] - dx, k[1] - dy, k[2] - dz));
-      const double sr = __dsub_rn(at(k[0] + dx, k[1] + dy, k[2] + dz), u0);
-      lim[d] = lim_minmod(sl, sr);
-    }
-#pragma unroll
-    for (int pz = 0; pz < 2; ++pz)
-#pragma unroll
-      for (int py = 0; py < 2; ++py)
-#pragma unroll
-        for (int px = 0; px < 2; ++px) {
-          double acc = 0.0;
-          acc = __dadd_rn(acc, __dmul_rn(px ? 0.25 : -0.25, lim[0]));
-          acc = __dadd_rn(acc, __dmul_rn(py ? 0.25 : -0.25, lim[1]));
-          acc = __dadd_rn(acc, __dmul_rn(pz ? 0.25 : -0.25, lim[2]));
-          r[pz][py][px] = __dadd_rn(u0, acc);
-        }
-  } else {
-    double Sy[2][2][5];  // [px][py][dk]
-#pragma unroll
-    for (int dk = 0; dk < 5; ++dk) {
-      double Sx[2][5];  // [px][dj]
-#pragma unroll
-      for (int dj = 0; dj < 5; ++dj) {
-        double line[5];
-#pragma unroll
-        for (int di = 0; di < 5; ++di) line[di] = at(k[0] + di - 2, k[1] + dj - 2, k[2] + dk - 2);
-        Sx[0][dj] = contract5_rn(c_prolong5, line);
-        Sx[1][dj] = contract5_rn(c_prolong5 + 5, line);
-      }
-#pragma unroll
-      for (int px = 0; px < 2; ++px) {
-        Sy[px][0][dk] = contract5_rn(c_prolong5, Sx[px]);
-        Sy[px][1][dk] = contract5_rn(c_prolong5 + 5, Sx[px]);
-      }
-    }
-#pragma unroll
-    for (int pz = 0; pz < 2; ++pz)
-#pragma unroll
-      for (int py = 0; py < 2; ++py)
-#pragma unroll
-        for (int px = 0; px < 2; ++px) r[pz][py][px] = contract5_rn(c_prolong5 + 5 * pz, Sy[px][py]);
+  for (int d = 0; d < 3; ++d) {
+    const int dx = d == 0, dy = d == 1, dz = d == 2;
+    const double sl = __dsub_rn(u0, at(k[0] - dx, k[1] - dy, k[2] - dz));
+    const double sr = __dsub_rn(at(k[0] + dx, k[1] + dy, k[2] + dz), u0);
+    lim[d] = lim_minmod(sl, sr);
   }
   double* o = fine + (fine_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
 #pragma unroll
   for (int pz = 0; pz < 2; ++pz)
 #pragma unroll
-    for (int py = 0; py < 2; ++py)
+    for (int py = 0; py < 2; ++py) {
+      double r[2];
+#pragma unroll
+      for (int px = 0; px < 2; ++px) {
+        double acc = 0.0;
+        acc = __dadd_rn(acc, __dmul_rn(px ? 0.25 : -0.25, lim[0]));
+        acc = __dadd_rn(acc, __dmul_rn(py ? 0.25 : -0.25, lim[1]));
+        acc = __dadd_rn(acc, __dmul_rn(pz ? 0.25 : -0.25, lim[2]));
+        r[px] = __dadd_rn(u0, acc);
+      }
       *reinterpret_cast<double2*>(o + ((int64_t)(f[2] + pz) * N1 + (f[1] + py)) * N0 + f[0]) =
-          make_double2(r[pz][py][0], r[pz][py][1]);
+          make_double2(r[0], r[1]);
+    }
+}
+
+// High-order list, one thread per (x, y) column of an element's coarse
+// region and variable, walking the column along z: each z plane's x sums
+// (both x halves) and y sums (the 4 (x, y) halves) are computed once and the
+// last five planes' y sums kept in registers, from which every coarse cell
+// of the column gets its 8 fine cells (the z sum).  The operands and their
+// order are those of lagrange_prolong_op<4>, so the results are its bits;
+// against one thread per coarse cell it saves the loads and sums that
+// neighbouring cells along z share.  box: (the kind's largest number of
+// columns, 1, 1) x (nvars_in_list x nelems), variable fastest; threads past
+// the element's columns return.
+template <int kKind>
+__global__ void __launch_bounds__(128) k_prolong_lag_zcol(Geo G, Box box, RestrictVars V, FastDiv dnv,
+                                                          const double* __restrict__ cbuf, double* __restrict__ fine,
+                                                          const int64_t* __restrict__ fine_q,
+                                                          const int64_t* __restrict__ cbuf_q,
+                                                          const uint8_t* __restrict__ elem) {
+  int col, b_, c_;
+  int64_t t;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, col, b_, c_, t)) return;
+  const uint32_t iq = fast_div((uint32_t)t, dnv);
+  const int v = list_var(V, (int)((uint32_t)t - iq * (uint32_t)V.n));
+  const int e = elem[iq];
+  const int n = G.nx, g = G.g;
+  int r[3], k0[3], f0[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    int w, lp;
+    ghost_axis<kKind>(e, d, w, lp);
+    r[d] = w == 2 ? n / 2 : g / 2;
+    k0[d] = ghost_idx(w, n / 2, g, g / 2, 0);
+    f0[d] = ghost_idx(w, n, g, 0, 0);
+  }
+  if (col >= r[0] * r[1]) return;
+  const int x = col % r[0], y = col / r[0];
+  const int kx = k0[0] + x, ky = k0[1] + y;
+  const int N0 = G.NX, N1 = G.NY;
+  const double* u = cbuf + (cbuf_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
+  double* o = fine + (fine_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
+  double ring[4][5];  // [2 px + py][plane], plane 4 the newest
+  for (int zz = -2; zz < r[2] + 2; ++zz) {
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+      for (int q = 0; q < 4; ++q) ring[p][q] = ring[p][q + 1];
+    const double* plane = u + (int64_t)(k0[2] + zz) * N1 * N0;
+    double Sx[2][5];
+#pragma unroll
+    for (int dj = 0; dj < 5; ++dj) {
+      const double* l = plane + (int64_t)(ky + dj - 2) * N0 + kx - 2;
+      const double line[5] = {l[0], l[1], l[2], l[3], l[4]};
+      Sx[0][dj] = contract5_rn(c_prolong5, line);
+      Sx[1][dj] = contract5_rn(c_prolong5 + 5, line);
+    }
+#pragma unroll
+    for (int px = 0; px < 2; ++px) {
+      ring[2 * px][4] = contract5_rn(c_prolong5, Sx[px]);
+      ring[2 * px + 1][4] = contract5_rn(c_prolong5 + 5, Sx[px]);
+    }
+    if (zz >= 2) {
+      const int z = zz - 2;
+#pragma unroll
+      for (int pz = 0; pz < 2; ++pz)
+#pragma unroll
+        for (int py = 0; py < 2; ++py) {
+          const double lo = contract5_rn(c_prolong5 + 5 * pz, ring[py]);
+          const double hi = contract5_rn(c_prolong5 + 5 * pz, ring[2 + py]);
+          *reinterpret_cast<double2*>(o + ((int64_t)(f0[2] + 2 * z + pz) * N1 + (f0[1] + 2 * y + py)) * N0 + f0[0] +
+                                      2 * x) = make_double2(lo, hi);
+        }
+    }
+  }
 }
 
 // One block's face array staggered along d.

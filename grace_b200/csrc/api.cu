@@ -982,16 +982,27 @@ template <int kKind>
 static void launch_prolong(const Geo& G, const int ext[3], const grb_fields* fine, const grb_fields* cbuf,
                            int64_t nelems, const int64_t* fine_q, const int64_t* cbuf_q, const uint8_t* elem_id,
                            const int8_t* have_fine, const RestrictVars* V, bool faces, cudaStream_t s) {
-  for (int pass = 0; pass < 2; ++pass) {
-    if (!V[pass].n) continue;
-    const Box b = box(0, 0, 0, ext[0] / 2, ext[1] / 2, ext[2] / 2, (int64_t)V[pass].n * nelems);
-    const FastDiv dv = make_fastdiv((uint32_t)V[pass].n);
-    if (pass == 0)
-      k_prolong_cells<kKind, false><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V[0], dv, cbuf->state, fine->state,
-                                                                         fine_q, cbuf_q, elem_id);
-    else
-      k_prolong_cells<kKind, true><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V[1], dv, cbuf->state, fine->state,
-                                                                        fine_q, cbuf_q, elem_id);
+  if (V[0].n) {
+    const Box b = box(0, 0, 0, ext[0] / 2, ext[1] / 2, ext[2] / 2, (int64_t)V[0].n * nelems);
+    k_prolong_cells<kKind><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V[0], make_fastdiv((uint32_t)V[0].n),
+                                                                cbuf->state, fine->state, fine_q, cbuf_q, elem_id);
+  }
+  if (V[1].n) {
+    // the kind's largest element cross-section in (x, y), in coarse cells
+    const int ne = kKind == GRB_ELEM_FACE ? 6 : (kKind == GRB_ELEM_EDGE ? 12 : 8);
+    int cols = 0;
+    for (int e = 0; e < ne; ++e) {
+      int r[2];
+      for (int d = 0; d < 2; ++d) {
+        int w, lp;
+        ghost_axis<kKind>(e, d, w, lp);
+        r[d] = w == 2 ? G.nx / 2 : G.g / 2;
+      }
+      cols = r[0] * r[1] > cols ? r[0] * r[1] : cols;
+    }
+    const Box b = box(0, 0, 0, cols, 1, 1, (int64_t)V[1].n * nelems);
+    k_prolong_lag_zcol<kKind><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V[1], make_fastdiv((uint32_t)V[1].n),
+                                                                   cbuf->state, fine->state, fine_q, cbuf_q, elem_id);
   }
   if (!faces) return;
   const Box b = box(0, 0, 0, ext[0] / 2, ext[1] / 2, ext[2] / 2, nelems);
