@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(128) k_restrict_faces(Geo G, Box box, const do
 // axes over 0, 1 (the sides in bits 0, 1 of e) and its own axis over 2; a
 // corner axis d over d (the side in bit d of e).
 template <int kKind>
-__device__ __forceinline__ void ghost_axis(int e, int d, int& where, int& loop) {
+__host__ __device__ __forceinline__ void ghost_axis(int e, int d, int& where, int& loop) {
   if (kKind == GRB_ELEM_FACE) {
     const int ax = e >> 1;
     where = d == ax ? (e & 1) : 2;
@@ -159,7 +159,7 @@ __device__ __forceinline__ void ghost_axis(int e, int d, int& where, int& loop) 
     loop = d;
   }
 }
-__device__ __forceinline__ int ghost_idx(int where, int n, int g, int goff, int t) {
+__host__ __device__ __forceinline__ int ghost_idx(int where, int n, int g, int goff, int t) {
   return where == 2 ? g + t : (where ? n + g + t : goff + t);
 }
 __device__ __forceinline__ int pick3(int l, int a, int b, int c) { return l == 0 ? a : (l == 1 ? b : c); }

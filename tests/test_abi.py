@@ -30,6 +30,17 @@ def test_library_exports_every_declared_symbol():
     assert sorted(abi.PROTOTYPES) == names
 
 
+def test_library_imports_no_process_exit():
+    """No code path of the library ends the caller's process: every error
+    is a status code.  nvcc compiles a __device__-only helper that host code
+    calls into a host stub that calls exit(1) without a diagnostic, so an
+    imported exit() is that mistake."""
+    out = subprocess.run(["nm", "-D", "--undefined-only", _lib.load()._name], capture_output=True, text=True,
+                         check=True).stdout
+    imported = {ln.split()[-1].split("@")[0] for ln in out.splitlines() if ln.strip()}
+    assert not imported & {"exit", "_exit", "_Exit", "abort", "quick_exit"}
+
+
 def test_struct_layout_matches_header(tmp_path):
     src = tmp_path / "sz.c"
     src.write_text('''#include <stdio.h>
