@@ -102,6 +102,59 @@ __global__ void __launch_bounds__(128) k_restrict_cells(Geo G, Box box, Restrict
   dst[(dst_q[iq] * GRB_N_EVOL_VARS + v) * G.cells + ((int64_t)(k + G.g) * N1 + (j + G.g)) * N0 + (i + G.g)] = r;
 }
 
+// High-order list, one thread per (i, j) column of coarse cells and
+// variable, walking the column along z: each fine plane's contractions along
+// x and y (with the column's x and y stencils) are computed once and the
+// last five kept in registers; coarse cell k takes the z contraction of the
+// five planes of its stencil (fk + oz - 3 .. fk + oz + 1) when the walk has
+// reached the last of them.  Stencil windows never move back along z (the
+// edge and half-dependent offsets keep their ends non-decreasing), so one
+// pass over the fine planes ngz .. nz + ngz - 1 serves every cell.  The
+// operands and their order are those of k_restrict_cells<true>, bit for
+// bit.  box: (nx/2, ny/2, 1) x (nvars_in_list x nquads), variable fastest.
+__global__ void __launch_bounds__(128) k_restrict_lag_zcol(Geo G, Box box, RestrictVars V, FastDiv dnv,
+                                                           const double* __restrict__ src, double* __restrict__ dst,
+                                                           const int64_t* __restrict__ src_q,
+                                                           const int64_t* __restrict__ dst_q,
+                                                           const uint8_t* __restrict__ child) {
+  int i, j, k_;
+  int64_t t;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k_, t)) return;
+  const uint32_t iq = fast_div((uint32_t)t, dnv);
+  const int v = list_var(V, (int)((uint32_t)t - iq * (uint32_t)V.n));
+  const int N0 = G.NX, N1 = G.NY, g = G.g;
+  const double* u = src + (src_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
+  double* o = dst + (dst_q[iq] * GRB_N_EVOL_VARS + v) * G.cells;
+  const uint8_t cid = child[iq];
+  const int fi = 2 * i + g, fj = 2 * j + g, hz = (cid >> 2) & 1;
+  const int ox = lag4_offset(fi, G.nx, g, cid & 1), oy = lag4_offset(fj, G.ny, g, (cid >> 1) & 1);
+  const double* cx = c_restrict5 + 5 * ox;
+  const double* cy = c_restrict5 + 5 * oy;
+  const int x0 = fi + ox - 3, y0 = fj + oy - 3;
+  double ring[5];
+  int k = 0;
+  int oz = lag4_offset(g, G.nz, g, hz);
+  for (int z = g; z < G.nz + g; ++z) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ring[q] = ring[q + 1];
+    const double* plane = u + (int64_t)z * N1 * N0;
+    double col[5];
+#pragma unroll
+    for (int dj = 0; dj < 5; ++dj) {
+      const double* l = plane + (int64_t)(y0 + dj) * N0 + x0;
+      const double line[5] = {l[0], l[1], l[2], l[3], l[4]};
+      col[dj] = contract5_rn(cx, line);
+    }
+    ring[4] = contract5_rn(cy, col);
+    // every coarse cell whose stencil ends at this plane
+    while (k < G.nz / 2 && 2 * k + g + oz + 1 == z) {
+      o[((int64_t)(k + g) * N1 + (j + g)) * N0 + (i + g)] = contract5_rn(c_restrict5 + 5 * oz, ring);
+      ++k;
+      if (k < G.nz / 2) oz = lag4_offset(2 * k + g, G.nz, g, hz);
+    }
+  }
+}
+
 // Face B staggered along dir: box (n/2 + (dir == 0), n/2 + (dir == 1),
 // n/2 + (dir == 2)) x nquads.
 template <int dir>

@@ -1478,7 +1478,13 @@ int grb_restrict_to_coarse(grb_handle* h, const grb_grid* g, const grb_fields* f
     if (pass == 0)
       k_restrict_cells<false><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V, make_fastdiv((uint32_t)nl), fine->state,
                                                                    cbuf->state, src_q, dst_q, child_id);
-    else
+    else if (G.nz >= 6) {
+      // by z columns; with 4 cells along z the edge stencils' windows move
+      // back along z, so those blocks keep one thread per coarse cell
+      const Box bc = box(0, 0, 0, G.nx / 2, G.ny / 2, 1, (int64_t)nl * nquads);
+      k_restrict_lag_zcol<<<nblk(bc.count(), 128), 128, 0, s>>>(G, bc, V, make_fastdiv((uint32_t)nl), fine->state,
+                                                               cbuf->state, src_q, dst_q, child_id);
+    } else
       k_restrict_cells<true><<<nblk(b.count(), 128), 128, 0, s>>>(G, b, V, make_fastdiv((uint32_t)nl), fine->state,
                                                                   cbuf->state, src_q, dst_q, child_id);
     ++h->launches;

@@ -48,6 +48,30 @@ def test_restrict_to_coarse_matches_oracle_bitwise():
     assert g.status().device_flags == 0
 
 
+@pytest.mark.parametrize("n", [4, 6, 8])
+def test_restrict_small_blocks_match_oracle(n):
+    """The 5-point restriction on small blocks: with 4 cells along z one
+    thread per coarse cell, from 6 on the z-column walk, both bit for bit."""
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(40 + n)
+    nq = 8
+    M = n + 2 * G
+    st = rng.standard_normal((nq, abi.N_EVOL_VARS, M, M, M))
+    q = np.arange(nq, dtype=np.int64)
+    child = np.arange(nq).astype(np.uint8)
+    vlo, vhi = [0, 4], [1, 2, 3, 7, 20]
+    g = GRMHDEquationsSystem(params.blast())
+    g.reserve(Blocks(n, n, n, G, nq, np.ones((nq, 3)), device=dev))
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    fine = Fields(T(st), None, None, None)
+    cb = Fields(torch.zeros_like(fine.state), None, None, None)
+    g.restrict_to_coarse(fine, cb, T(q), T(q), T(child), vlo, vhi, faces=False)
+    torch.cuda.synchronize()
+    ost = np.zeros_like(st)
+    _oracle.restrict_cells("orc", n, G, abi.N_EVOL_VARS, st, ost, q, q, child, vlo, vhi)
+    np.testing.assert_array_equal(cb.state.cpu().numpy(), ost)
+
+
 def test_restricted_face_field_is_divergence_free():
     """A discretely divergence-free fine face field (curl of an edge vector
     potential) restricts to a divergence-free coarse one."""
