@@ -100,15 +100,18 @@ NELEM = {0: 6, 1: 12, 2: 8}
 FSH = [(NN, NN, NN + 1), (NN, NN + 1, NN), (NN + 1, NN, NN)]
 
 
+@pytest.mark.parametrize("n", [16, 8, 4])
 @pytest.mark.parametrize("kind", [0, 1, 2])
-def test_prolong_to_ghosts_matches_oracle_bitwise(kind):
+def test_prolong_to_ghosts_matches_oracle_bitwise(kind, n):
     """grb_prolong_to_ghosts against the oracle (pinned to the reference's
     prolong_op / div_free_prolong_op): every element of the kind on several
     quadrants, both variable lists, face B with random fine-neighbour
     flags, bit for bit."""
     dev = torch.device("cuda:0")
-    rng = np.random.default_rng(60 + kind)
+    rng = np.random.default_rng(60 + kind + n)
     nq, ncb = 6, 8
+    NN = n + 2 * G
+    FSH = [(NN, NN, NN + 1), (NN, NN + 1, NN), (NN + 1, NN, NN)]
     st0 = rng.standard_normal((nq, abi.N_EVOL_VARS, NN, NN, NN))
     fb0 = [rng.standard_normal((nq,) + s) for s in FSH]
     cst = rng.standard_normal((ncb, abi.N_EVOL_VARS, NN, NN, NN))
@@ -121,16 +124,16 @@ def test_prolong_to_ghosts_matches_oracle_bitwise(kind):
     hf = rng.integers(0, 2, size=(len(fq), 3, 2)).astype(np.int8)
     vlo, vhi = [0, 5, 6, 13], [1, 2, 3, 4, 22]
     g = GRMHDEquationsSystem(params.blast())
-    g.reserve(Blocks(N, N, N, G, nq, np.ones((nq, 3)), device=dev))
+    g.reserve(Blocks(n, n, n, G, nq, np.ones((nq, 3)), device=dev))
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     fine = Fields(T(st0), *[T(x) for x in fb0])
     cb = Fields(T(cst), *[T(x) for x in cfb])
     g.prolong_to_ghosts(fine, cb, kind, T(fq), T(cq), T(el), T(hf), vlo, vhi)
     torch.cuda.synchronize()
     ost = st0.copy()
-    _oracle.prolong_cells("orc", kind, N, G, abi.N_EVOL_VARS, ost, cst, fq, cq, el, vlo, vhi)
+    _oracle.prolong_cells("orc", kind, n, G, abi.N_EVOL_VARS, ost, cst, fq, cq, el, vlo, vhi)
     ofb = [x.copy() for x in fb0]
-    _oracle.prolong_faces("orc", kind, N, G, ofb, cfb, fq, cq, el, hf)
+    _oracle.prolong_faces("orc", kind, n, G, ofb, cfb, fq, cq, el, hf)
     np.testing.assert_array_equal(fine.state.cpu().numpy(), ost)
     for d in range(3):
         np.testing.assert_array_equal((fine.bx, fine.by, fine.bz)[d].cpu().numpy(), ofb[d])

@@ -26,10 +26,13 @@ def _elements(kind, nq, rng):
 
 
 @pytest.mark.skipif(not os.path.exists(_oracle.REF), reason="pinning build absent")
+@pytest.mark.parametrize("n", [16, 8, 4])
 @pytest.mark.parametrize("kind", [0, 1, 2])
-def test_prolong_cells_matches_reference_functor(kind):
-    rng = np.random.default_rng(40 + kind)
+def test_prolong_cells_matches_reference_functor(kind, n):
+    rng = np.random.default_rng(40 + kind + n)
     nvars, nq = 5, 2
+    NN = n + 2 * G
+    N = n
     cbuf = rng.standard_normal((nq, nvars, NN, NN, NN))
     fq, el = _elements(kind, nq, rng)
     cmap = rng.permutation(nq)
@@ -50,12 +53,16 @@ def test_prolong_cells_matches_reference_functor(kind):
 
 
 @pytest.mark.skipif(not os.path.exists(_oracle.REF), reason="pinning build absent")
+@pytest.mark.parametrize("n", [16, 8, 4])
 @pytest.mark.parametrize("kind", [0, 1, 2])
-def test_prolong_faces_matches_reference_functor(kind):
-    rng = np.random.default_rng(50 + kind)
+def test_prolong_faces_matches_reference_functor(kind, n):
+    rng = np.random.default_rng(50 + kind + n)
     nq = 2
-    cb = [rng.standard_normal((nq,) + s) for s in FACE_SHAPES]
-    init = [rng.standard_normal((nq,) + s) for s in FACE_SHAPES]  # "fine data" where flags say so
+    M = n + 2 * G
+    N = n
+    shapes = [(M, M, M + 1), (M, M + 1, M), (M + 1, M, M)]
+    cb = [rng.standard_normal((nq,) + s) for s in shapes]
+    init = [rng.standard_normal((nq,) + s) for s in shapes]  # "fine data" where flags say so
     fq, el = _elements(kind, nq, rng)
     cq = rng.permutation(nq)[fq]
     hf = rng.integers(0, 2, size=(len(fq), 3, 2)).astype(np.int8)
