@@ -188,6 +188,22 @@ def blast(nb=(16, 16, 16), n=(16, 16, 16), ngz=4, seed=SEED, qr=None, lo=(-6, -6
     return su, _fill(su, 4.0 / 3.0, rho, press, None, faces, qr)
 
 
+def blast_drifting(nb=(2, 2, 2), n=(8, 8, 8), lo=(-0.5, -0.5, -0.5), hi=(2.5, 2.5, 2.5), z=(0.3, -0.2, 0.1)):
+    """The blast wave moving with a uniform velocity (three-velocity times
+    W, z) on a sub-box whose low faces cut through the overdense core: mass
+    crosses every outer face, in through some and out through others, with
+    a net flux of the core's density.  For the outflow diagnostic."""
+    su, (st, bx, by, bz, aux) = blast(nb=nb, n=n, lo=lo, hi=hi)
+    rho, press, eps, s = aux[:, abi.RHO], aux[:, abi.PRESS], aux[:, abi.EPS], aux[:, abi.ENTROPY]
+    Bc = np.moveaxis(aux[:, abi.BX:abi.BZ + 1], 1, 0)
+    zz = np.empty((3,) + rho.shape)
+    for a in range(3):
+        zz[a] = z[a]
+    st[:, 0:7] = np.moveaxis(flat_prims_to_cons(rho, press, eps, zz, Bc, s), 0, 1)
+    aux[:, abi.ZVECX:abi.ZVECZ + 1] = np.moveaxis(zz, 0, 1)
+    return su, (st, bx, by, bz, aux)
+
+
 def balsara1(nb=(64, 1, 1), n=(16, 16, 16), ngz=4):
     """Balsara-1 shock tube: Gamma=2; left rho=1,p=1,B=(0.5,1,0); right
     rho=0.125,p=0.1,B=(0.5,-1,0); x in [-0.5,0.5], y,z in [-1/128,1/128]

@@ -64,6 +64,39 @@ int64_t API(scratch)(void* hh, int which, double* out) {
   if (out) std::memcpy(out, v->data(), v->size() * sizeof(double));
   return (int64_t)v->size();
 }
+// Mass outflux of the last substep through the listed outer-boundary faces
+// (boundary_outflow_t::accumulate, include/grace/evolution/
+// boundary_outflow.hh:79-180): per face (quad[f], face[f] = 2 axis + side)
+// the DENS face flux of the boundary plane summed over the face's interior
+// cells in the reference's order (first tangential index fastest), times
+// the outward sign, dt * dtfact and the face area from dx[3 q + d]; the
+// faces' contributions summed in list order.
+double API(boundary_outflow)(void* hh, int64_t nfaces, const int64_t* quad, const uint8_t* face,
+                             const double* dx, double dt, double dtfact) {
+  auto& st = static_cast<Handle*>(hh)->st;
+  const auto& d = st.d;
+  const int n[3] = {d.nx, d.ny, d.nz};
+  double total = 0.0;
+  for (int64_t f = 0; f < nfaces; ++f) {
+    const int64_t q = quad[f];
+    const int axis = face[f] / 2;
+    const double sgn = (face[f] & 1) ? 1.0 : -1.0;
+    const double* h = dx + 3 * q;
+    const double dA = axis == 0 ? h[1] * h[2] : axis == 1 ? h[0] * h[2] : h[0] * h[1];
+    const int plane = (face[f] & 1) ? n[axis] + d.g : d.g;
+    const int na = axis == 0 ? d.ny : d.nx, nb = axis == 2 ? d.ny : d.nz;
+    double sum = 0.0;
+    for (int lin = 0; lin < na * nb; ++lin) {
+      const int a = d.g + lin % na, b = d.g + lin / na;
+      const int i = axis == 0 ? plane : a;
+      const int j = axis == 1 ? plane : (axis == 0 ? a : b);
+      const int k = axis == 2 ? plane : b;
+      sum += st.F(i, j, k, 0, axis, q);
+    }
+    total += sgn * (dt * dtfact) * dA * sum;
+  }
+  return total;
+}
 void API(fofc_counts)(void* hh, int64_t* faces, int64_t* edges) {
   auto& st = static_cast<Handle*>(hh)->st;
   *faces = st.n_fofc_faces;

@@ -27,6 +27,7 @@ def _bind(lib, pre):
         "find_stable_timestep": (C.c_double, [VP, VP, VP, VP, C.c_double]),
         "linop": (None, [VP] + [VP] * 12 + [C.c_double, C.c_double]),
         "scratch": (C.c_int64, [VP, C.c_int, VP]),
+        "boundary_outflow": (C.c_double, [VP, C.c_int64, VP, VP, VP, C.c_double, C.c_double]),
         "fofc_counts": (None, [VP, P(C.c_int64), P(C.c_int64)]),
         "c2p_batch": (C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP, VP, VP, VP, C.c_int32, VP]),
         "prims_to_conservs": (C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP]),
@@ -213,6 +214,13 @@ class Stage:
         f, e = C.c_int64(), C.c_int64()
         getattr(self.L, self.pre + "fofc_counts")(self.h, C.byref(f), C.byref(e))
         return f.value, e.value
+
+    def boundary_outflow(self, quad, face, dx, dt, dtfact):
+        """Mass outflux of the last substep through the listed faces."""
+        q = np.ascontiguousarray(quad, dtype=np.int64)
+        f = np.ascontiguousarray(face, dtype=np.uint8)
+        d = np.ascontiguousarray(dx, dtype=np.float64)
+        return getattr(self.L, self.pre + "boundary_outflow")(self.h, len(q), p(q), p(f), p(d), dt, dtfact)
 
     def scratch(self, which):
         n = getattr(self.L, self.pre + "scratch")(self.h, which, None)

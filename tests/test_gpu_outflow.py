@@ -7,31 +7,17 @@ import numpy as np
 import pytest
 import torch
 
+import _oracle
 from grace_b200 import abi, params, workloads
 from grace_b200.host import Blocks, Fields, GRMHDEquationsSystem
 
 pytestmark = pytest.mark.gpu
 
 
-def _drifting_blast():
-    """The blast wave of 2^3 blocks of 8^3 cells on [-0.5, 2.5]^3, the low
-    faces cutting through the overdense core, moving with a uniform
-    three-velocity: mass crosses every outer face, in through some and out
-    through others, with a net flux of the core's density."""
-    su, f = workloads.blast(nb=(2, 2, 2), n=(8, 8, 8), lo=(-0.5,) * 3, hi=(2.5,) * 3)
-    st, bx, by, bz, aux = f
-    rho, press, eps, s = aux[:, abi.RHO], aux[:, abi.PRESS], aux[:, abi.EPS], aux[:, abi.ENTROPY]
-    Bc = np.moveaxis(aux[:, abi.BX:abi.BZ + 1], 1, 0)
-    z = np.empty((3,) + rho.shape)
-    z[0], z[1], z[2] = 0.3, -0.2, 0.1
-    st[:, 0:7] = np.moveaxis(workloads.flat_prims_to_cons(rho, press, eps, z, Bc, s), 0, 1)
-    return su, (st, bx, by, bz, aux)
-
-
 @pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
 def test_outflow_equals_mass_lost_by_the_update(mode):
     dev = torch.device("cuda:0")
-    su, f = _drifting_blast()
+    su, f = workloads.blast_drifting()
     P = params.blast()
     st, bx, by, bz, aux = f
     g = GRMHDEquationsSystem(P)
@@ -67,3 +53,44 @@ def test_outflow_equals_mass_lost_by_the_update(mode):
         total += flux_out
     assert abs(float(out) - total) <= 1e-15 * abs(total) + 1e-300
     assert g.status().device_flags == 0
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_outflow_matches_oracle(mode):
+    """One substep of the drifting blast wave on the GPU and in the oracle:
+    the accumulated outflux against the oracle's sum over its own face
+    fluxes (the restated accumulate), within 1e-11 relative."""
+    dev = torch.device("cuda:0")
+    su, f = workloads.blast_drifting()
+    P = params.blast()
+    st, bx, by, bz, aux = f
+    dt, dtfact = 0.25 * su.dx[0], 1.0
+    quad, face = su.outer_faces()
+    dxs = np.tile(su.dx, (su.nq, 1))
+    # oracle
+    S = _oracle.Stage(P, su.n[0], su.n[1], su.n[2], su.ngz, su.nq)
+    old = [x.copy() for x in (st, bx, by, bz)]
+    aux_h = aux.copy()
+    _oracle.fill_ghosts("orc", su, old)
+    S.compute_aux(su.idx().copy(), old, aux_h)
+    new = [x.copy() for x in old]
+    S.advance_substep(su.idx().copy(), dt, dtfact, new, old, aux_h)
+    want = S.boundary_outflow(quad, face, dxs, dt, dtfact)
+    # GPU
+    g = GRMHDEquationsSystem(P)
+    g.reserve(Blocks(su.n[0], su.n[1], su.n[2], su.ngz, su.nq, su.idx(), device=dev))
+    g.set_mode(mode)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    state = Fields(T(st), T(bx), T(by), T(bz))
+    aux_d = T(aux)
+    g.fill_ghosts_brick(state, su.nb, su.periodic)
+    g.compute_auxiliary_quantities(state, aux_d)
+    if mode == abi.MODE_TUNED:
+        g.set_tuning(1, 1, 1, 1)
+    out = torch.zeros(1, dtype=torch.float64, device=dev)
+    nw = state.clone()
+    g.advance_substep(0.0, dt, dtfact, nw, state, aux_d)
+    g.accumulate_boundary_outflow(T(quad), T(face), T(dxs), dt, dtfact, out)
+    torch.cuda.synchronize()
+    assert abs(want) > 0
+    assert abs(float(out) - want) <= 1e-11 * abs(want)
