@@ -9,9 +9,13 @@
 // (high-order list, stencils chosen per axis by the block edge and by the
 // quadrant's half of its parent, from its Morton child id), face B by the
 // average of the 4 fine faces inside each coarse face (divergence
-// preserving).  Every product and sum is rounded on its own (__dmul_rn,
-// __dadd_rn), as the reference writes them, so the results do not depend on
-// how the compiler would contract them.
+// preserving).  The second half of the file holds the prolongation into
+// ghost zones (the ghost-zone prolongation of prolongation_kernels.hh with
+// the operators of pr_helpers.hh:73-185): the face, edge and corner ghost
+// elements of fine quadrants filled from their coarse buffers.  Every
+// product and sum is rounded on its own (__dmul_rn, __dadd_rn), as the
+// reference writes them, so the results do not depend on how the compiler
+// would contract them.
 #pragma once
 #include "stage_kernels.cuh"
 
