@@ -1275,6 +1275,11 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
   const int64_t total = (int64_t)std::max({G.NX + 1, G.NY + 1, G.NZ + 1}) *
                         std::max({G.NX * G.NY, G.NY * G.NZ, G.NX * G.NZ});
   if (total > (1ll << 31) - 256) return fail(h, GRB_ERR_INVALID);
+  GhostDivs D;
+  for (int a = 0; a < 4; ++a) {
+    D.x[a] = make_fastdiv((uint32_t)(G.NX + (a == 1)));
+    D.y[a] = make_fastdiv((uint32_t)(G.NY + (a == 2)));
+  }
   const bool aligned = (((uintptr_t)f->state | (uintptr_t)bf[1] | (uintptr_t)bf[2]) & 15) == 0;
   if (aligned && ghost_runs(h, G, s)) {
     // 4-cell runs for the cells and the y, z face arrays; the x face array
@@ -1286,11 +1291,11 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
     k_ghost_runs<<<gr, 128, 0, s>>>(G, br, h->d_ghostruns, make_int3(o[0], o[1], o[2]), make_int3(c[0], c[1], c[2]),
                                     f->state, bf[1], bf[2]);
     const dim3 gx((unsigned)((total + 255) / 256), (unsigned)G.nq, 1u);
-    k_ghost<<<gx, 256, 0, s>>>(G, br, f->state, bf[0], bf[1], bf[2], 1);
+    k_ghost<<<gx, 256, 0, s>>>(G, br, D, f->state, bf[0], bf[1], bf[2], 1);
     h->launches += 2;
   } else {
     const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq, 4u);
-    k_ghost<<<grid, 256, 0, s>>>(G, br, f->state, bf[0], bf[1], bf[2]);
+    k_ghost<<<grid, 256, 0, s>>>(G, br, D, f->state, bf[0], bf[1], bf[2]);
     ++h->launches;
   }
   CK(cudaGetLastError());

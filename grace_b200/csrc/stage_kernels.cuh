@@ -854,11 +854,16 @@ __device__ __forceinline__ bool ghost_map(int x, int nin, int g, bool stag, bool
   }
   return false;
 }
+// Invariant divisors by the x and y extents of the four arrays (cells, x,
+// y, z faces), for the per-cell ghost kernel's index decoding.
+struct GhostDivs {
+  FastDiv x[4], y[4];
+};
 // One launch for the four arrays: blockIdx.z = 0 the cell-centred HRSC
 // variables, 1..3 the face array staggered along blockIdx.z - 1.  One
 // thread per cell of one block (blockIdx.y = q), x fastest; 32-bit index
 // arithmetic (q < 65536, a block's cells < 2^31).
-__global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, double* __restrict__ cells,
+__global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, GhostDivs D, double* __restrict__ cells,
                                               double* __restrict__ fx, double* __restrict__ fy,
                                               double* __restrict__ fz, int z0 = 0) {
   const int fd = (int)blockIdx.z + z0 - 1;
@@ -867,12 +872,17 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, double* __restri
   if (fd >= 0) n[fd] += 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n[0] * n[1] * n[2]) return;
+  // the array's divisors by select (a dynamic index into the parameter
+  // would copy it to local memory)
+  const FastDiv dx = fd < 0 ? D.x[0] : fd == 0 ? D.x[1] : fd == 1 ? D.x[2] : D.x[3];
+  const FastDiv dy = fd < 0 ? D.y[0] : fd == 0 ? D.y[1] : fd == 1 ? D.y[2] : D.y[3];
   double* a = fd < 0 ? cells : fd == 0 ? fx : fd == 1 ? fy : fz;
   const int nin[3] = {G.nx, G.ny, G.nz};
   const int nb[3] = {br.nbx, br.nby, br.nbz};
   const int qyz = q / br.nbx;
   const int qc[3] = {q - qyz * br.nbx, qyz % br.nby, qyz / br.nby};
-  const int c[3] = {t % n[0], (t / n[0]) % n[1], t / (n[0] * n[1])};
+  const uint32_t u1 = fast_div((uint32_t)t, dx), u2 = fast_div(u1, dy);
+  const int c[3] = {(int)((uint32_t)t - u1 * (uint32_t)n[0]), (int)(u1 - u2 * (uint32_t)n[1]), (int)u2};
   int sidx[3], off[3];
   bool ghost = false;
 #pragma unroll
