@@ -1283,15 +1283,15 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
   const bool aligned = (((uintptr_t)f->state | (uintptr_t)bf[1] | (uintptr_t)bf[2]) & 15) == 0;
   if (aligned && ghost_runs(h, G, s)) {
     // 4-cell runs for the cells and the y, z face arrays; the x face array
-    // (rows of NX+1) by the per-cell kernel
+    // (rows of NX+1) by rows
     const int* o = h->ghost_off;
     const int* c = h->ghost_cnt;
     const int mx = std::max({c[0], c[1], c[2]});
     const dim3 gr((unsigned)((mx + 127) / 128), (unsigned)G.nq, 3u);
     k_ghost_runs<<<gr, 128, 0, s>>>(G, br, h->d_ghostruns, make_int3(o[0], o[1], o[2]), make_int3(c[0], c[1], c[2]),
                                     f->state, bf[1], bf[2]);
-    const dim3 gx((unsigned)((total + 255) / 256), (unsigned)G.nq, 1u);
-    k_ghost<<<gx, 256, 0, s>>>(G, br, D, f->state, bf[0], bf[1], bf[2], 1);
+    const dim3 gx((unsigned)((G.NY * G.NZ + 127) / 128), (unsigned)G.nq, 1u);
+    k_ghost_xfaces<<<gx, 128, 0, s>>>(G, br, make_fastdiv((uint32_t)G.NY), bf[0]);
     h->launches += 2;
   } else {
     const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq, 4u);

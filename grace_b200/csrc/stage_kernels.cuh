@@ -865,8 +865,8 @@ struct GhostDivs {
 // arithmetic (q < 65536, a block's cells < 2^31).
 __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, GhostDivs D, double* __restrict__ cells,
                                               double* __restrict__ fx, double* __restrict__ fy,
-                                              double* __restrict__ fz, int z0 = 0) {
-  const int fd = (int)blockIdx.z + z0 - 1;
+                                              double* __restrict__ fz) {
+  const int fd = (int)blockIdx.z - 1;
   const int q = blockIdx.y;
   int n[3] = {G.NX, G.NY, G.NZ};
   if (fd >= 0) n[fd] += 1;
@@ -905,6 +905,52 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, GhostDivs D, dou
 #pragma unroll
   for (int v = 0; v < GRB_N_HRSC; ++v)
     if (v < nv) a[ld + v * vstride] = tmp[v];
+}
+
+// The x face array (rows of NX + 1 faces, staggered along x), one thread
+// per row of one block (blockIdx.y = q): a row whose y and z are interior
+// has 2 ngz ghost faces (x < ngz and x > nx + ngz), any other row is ghost
+// throughout.  Each thread loads up to 8 of its row's sources before it
+// stores them, so the copies of a row overlap; the source of every face is
+// the one k_ghost maps it to.
+__global__ void __launch_bounds__(128) k_ghost_xfaces(Geo G, Brick br, FastDiv dny, double* __restrict__ fx) {
+  const int N0 = G.NX + 1, N1 = G.NY;
+  const int row = blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= N1 * G.NZ) return;
+  const int q = blockIdx.y;
+  const int k = (int)fast_div((uint32_t)row, dny), j = row - k * N1;
+  const int nb[3] = {br.nbx, br.nby, br.nbz};
+  const int qyz = q / br.nbx;
+  const int qc[3] = {q - qyz * br.nbx, qyz % br.nby, qyz / br.nby};
+  int sy, oy, sz, oz;
+  const bool gy = ghost_map(j, G.ny, G.g, false, br.periodic[1] != 0, qc[1], nb[1], sy, oy);
+  const bool gz = ghost_map(k, G.nz, G.g, false, br.periodic[2] != 0, qc[2], nb[2], sz, oz);
+  const bool full = gy || gz;
+  const int cnt = full ? N0 : 2 * G.g;
+  const int64_t vst = (int64_t)N0 * N1 * G.NZ;
+  const int qyzs = (qc[1] + oy + nb[1]) % nb[1] + br.nby * ((qc[2] + oz + nb[2]) % nb[2]);
+  const int64_t drow = (int64_t)q * vst + (int64_t)N0 * (j + (int64_t)N1 * k);
+  const int64_t srow = (int64_t)N0 * (sy + (int64_t)N1 * sz);
+  for (int m0 = 0; m0 < cnt; m0 += 8) {
+    double v[8];
+    int xs[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int m = m0 + u;
+      xs[u] = -1;
+      if (m < cnt) {
+        const int x = full ? m : (m < G.g ? m : G.nx + G.g + 1 + (m - G.g));
+        int sx, ox;
+        ghost_map(x, G.nx, G.g, true, br.periodic[0] != 0, qc[0], nb[0], sx, ox);
+        const int qs = (qc[0] + ox + nb[0]) % nb[0] + br.nbx * qyzs;
+        v[u] = fx[(int64_t)qs * vst + srow + sx];
+        xs[u] = x;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (xs[u] >= 0) fx[drow + xs[u]] = v[u];
+  }
 }
 
 // The same fill in runs of 4 cells along x, for ghost width 4 and interior
