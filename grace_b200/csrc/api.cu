@@ -392,6 +392,16 @@ const double* static_metric(const grb_handle* h, const Geo& G, const double* idx
   return std::equal(key, key + 4, h->metder_key) ? h->d_metder : nullptr;
 }
 
+// Grid of the FOFC list kernel: three 128-thread CTAs per SM (its register
+// footprint) for a grid-stride loop over the listed faces.
+static unsigned fofc_list_grid() {
+  static int sms[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return 444;
+  if (!sms[dev] && cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) sms[dev] = 148;
+  return (unsigned)(3 * sms[dev]);
+}
+
 // The stage in tuned mode: only the faces the stage reads, FAST flux math,
 // tuned register caps.  Returns the number of kernels launched.
 int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, double dtfact,
@@ -430,6 +440,8 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
     cudaMemsetAsync(B.etag, 0, (size_t)nf, s);
     if (count_fofc) cudaMemsetAsync(B.counters, 0, 2 * sizeof(unsigned long long), s);
     const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, G.nq);
+    const bool listed = B.flist && fb.count() < (1ll << 30);
+    if (listed) cudaMemsetAsync(B.fcount, 0, sizeof(uint32_t), s);
     {
       KScope ks(h, s, GRB_KIND_FOFC_FLAG);
       launch_flag_tuned(h->var_flag, nblk(fb.count(), T), s, P, G, fb, dt, dtfact, nw->state, old->state,
@@ -438,7 +450,19 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
     }
     {
       KScope ks(h, s, GRB_KIND_FOFC_FIX);
-      k_fofc_faces<true><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by, old->bz, B);
+      if (listed) {
+        // the few tagged faces compacted first: the recompute kernel's
+        // register footprint then costs occupancy only where there is work
+        k_fofc_scan<<<nblk(fb.count(), 256), 256, 0, s>>>(G, fb, B);
+        k_fofc_faces_list<true><<<fofc_list_grid(), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by,
+                                                              old->bz, B);
+        k_fofc_faces<true, true><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by,
+                                                                   old->bz, B);
+        launches += 2;
+      } else {
+        k_fofc_faces<true><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by,
+                                                            old->bz, B);
+      }
       k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B);
       launches += 2;
     }
@@ -533,8 +557,11 @@ int grb_create(grb_handle** out, const grb_params* p) {
 static void free_scratch(grb_handle* h) {
   cudaFree(h->B.flux); cudaFree(h->B.eface); cudaFree(h->B.vbar); cudaFree(h->B.ecenter);
   cudaFree(h->B.emf); cudaFree(h->B.ftag); cudaFree(h->B.etag);
+  cudaFree(h->B.flist); cudaFree(h->B.fcount);
   h->B.flux = h->B.eface = h->B.vbar = h->B.ecenter = h->B.emf = nullptr;
   h->B.ftag = h->B.etag = nullptr;
+  h->B.flist = h->B.fcount = nullptr;
+  h->B.fcap = 0;
   h->reserved = false;
   h->cap_f = h->cap_c = 0;
 }
@@ -571,6 +598,12 @@ int grb_reserve(grb_handle* h, const grb_grid* g) {
     ok = al((void**)&h->B.eface, sizeof(double) * nf * 2 * 3) &&
          al((void**)&h->B.ecenter, sizeof(double) * nc * 3);
   if (ok && h->p.emf == GRB_EMF_UCT) ok = al((void**)&h->B.vbar, sizeof(double) * nf * 4 * 3);
+  if (ok && h->p.emf == GRB_EMF_GS && h->p.fofc_enable) {
+    // the compacted FOFC face list: up to 4 Mi faces a substep (more falls
+    // back to the full recompute launch)
+    h->B.fcap = (uint32_t)std::min<int64_t>(nf * 3, 1 << 22);
+    ok = al((void**)&h->B.flist, sizeof(uint32_t) * h->B.fcap) && al((void**)&h->B.fcount, sizeof(uint32_t));
+  }
   if (!ok) {
     free_scratch(h);
     cudaGetLastError();

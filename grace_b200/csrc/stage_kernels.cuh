@@ -24,6 +24,11 @@ struct StageBufs {
   int8_t* etag;     // FOFC edge tags
   unsigned long long* counters;  // [0] faces, [1] edges recomputed by FOFC
   uint32_t* flags;  // device status word
+  // compacted list of the tagged faces (tuned mode): entries t << 2 | dir
+  // (t the FOFC box index), *fcount of them, room for fcap
+  uint32_t* flist = nullptr;
+  uint32_t* fcount = nullptr;
+  uint32_t fcap = 0;
 };
 
 // ---- the Riemann problem at one face (grmhd.hh:774-970) -------------------
@@ -457,13 +462,17 @@ __global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box
 
 // correct_{x,y,z}_fluxes_fofc: donor + LLF on tagged faces.  The box is the
 // compaction range [g-1, n+g]^3; a face of direction d needs index_d >= g.
-template <bool FAST = false>
+// kListed: the tagged faces were compacted into B.flist by k_fofc_scan;
+// this launch is the fallback for a list that overflowed and returns at
+// once otherwise.
+template <bool FAST = false, bool kListed = false>
 __global__ void __launch_bounds__(128) k_fofc_faces(DevParams P, Geo G, Box box,
                                                      const double* __restrict__ st,
                                                      const double* __restrict__ aux,
                                                      const double* __restrict__ bx,
                                                      const double* __restrict__ by,
                                                      const double* __restrict__ bz, StageBufs B) {
+  if (kListed && *B.fcount <= B.fcap) return;
   int i, j, k;
   int64_t q;
   if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
@@ -485,6 +494,69 @@ __global__ void __launch_bounds__(128) k_fofc_faces(DevParams P, Geo G, Box box,
     ++cnt;
   }
   if (cnt) atomicAdd(&B.counters[0], (unsigned long long)cnt);
+}
+
+// The FOFC box's tagged faces compacted into B.flist (the faces
+// k_fofc_faces recomputes: face (i, j, k, d) of a box cell with index_d >=
+// ngz), warp-aggregated appends; entries past B.fcap are dropped and the
+// count still grows, which sends the launch that follows to the fallback.
+// Needs box.count() < 2^30.
+__global__ void __launch_bounds__(256) k_fofc_scan(Geo G, Box box, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  bool tg[3] = {false, false, false};
+  if (decode(box, t, i, j, k, q)) {
+    tg[0] = i >= G.g && B.ftag[emi(G, i, j, k, 0, q)];
+    tg[1] = j >= G.g && B.ftag[emi(G, i, j, k, 1, q)];
+    tg[2] = k >= G.g && B.ftag[emi(G, i, j, k, 2, q)];
+  }
+  const int nm = (int)tg[0] + (int)tg[1] + (int)tg[2];
+  const int lane = threadIdx.x & 31;
+  int incl = nm;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  uint32_t base = 0;
+  if (lane == 31 && total) base = atomicAdd(B.fcount, (uint32_t)total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  uint32_t at = base + (uint32_t)(incl - nm);
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    if (tg[d]) {
+      if (at < B.fcap) B.flist[at] = (uint32_t)t << 2 | (uint32_t)d;
+      ++at;
+    }
+}
+
+// k_fofc_faces over the compacted list: a grid-stride loop over the listed
+// faces, each recomputed as there (donor reconstruction, LLF); does nothing
+// when the list overflowed (the fallback launch covers that case).
+template <bool FAST = false>
+__global__ void __launch_bounds__(128) k_fofc_faces_list(DevParams P, Geo G, Box box,
+                                                          const double* __restrict__ st,
+                                                          const double* __restrict__ aux,
+                                                          const double* __restrict__ bx,
+                                                          const double* __restrict__ by,
+                                                          const double* __restrict__ bz, StageBufs B) {
+  const uint32_t n = *B.fcount;
+  if (n > B.fcap) return;
+  if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(&B.counters[0], (unsigned long long)n);
+  for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
+    const uint32_t w = B.flist[e];
+    const int dir = (int)(w & 3u);
+    int i, j, k;
+    int64_t q;
+    decode(box, (int64_t)(w >> 2), i, j, k, q);
+    double f[7], vb[4];
+    if (dir == 0) getflux<0, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bx, f, vb);
+    else if (dir == 1) getflux<1, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, by, f, vb);
+    else getflux<2, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bz, f, vb);
+    store_face(G, B, P.emf, dir, i, j, k, q, f, vb);
+  }
 }
 __global__ void __launch_bounds__(128) k_fofc_edges(Geo G, Box box, StageBufs B) {
   int i, j, k;
