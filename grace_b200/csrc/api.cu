@@ -456,9 +456,7 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
         k_fofc_scan<<<nblk(fb.count(), 256), 256, 0, s>>>(G, fb, B);
         k_fofc_faces_list<true><<<fofc_list_grid(), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by,
                                                               old->bz, B);
-        k_fofc_faces<true, true><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by,
-                                                                   old->bz, B);
-        launches += 2;
+        ++launches;
       } else {
         k_fofc_faces<true><<<nblk(fb.count(), T), T, 0, s>>>(P, G, fb, old->state, aux, old->bx, old->by,
                                                             old->bz, B);

@@ -462,17 +462,13 @@ __global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box
 
 // correct_{x,y,z}_fluxes_fofc: donor + LLF on tagged faces.  The box is the
 // compaction range [g-1, n+g]^3; a face of direction d needs index_d >= g.
-// kListed: the tagged faces were compacted into B.flist by k_fofc_scan;
-// this launch is the fallback for a list that overflowed and returns at
-// once otherwise.
-template <bool FAST = false, bool kListed = false>
+template <bool FAST = false>
 __global__ void __launch_bounds__(128) k_fofc_faces(DevParams P, Geo G, Box box,
                                                      const double* __restrict__ st,
                                                      const double* __restrict__ aux,
                                                      const double* __restrict__ bx,
                                                      const double* __restrict__ by,
                                                      const double* __restrict__ bz, StageBufs B) {
-  if (kListed && *B.fcount <= B.fcap) return;
   int i, j, k;
   int64_t q;
   if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
@@ -499,7 +495,7 @@ __global__ void __launch_bounds__(128) k_fofc_faces(DevParams P, Geo G, Box box,
 // The FOFC box's tagged faces compacted into B.flist (the faces
 // k_fofc_faces recomputes: face (i, j, k, d) of a box cell with index_d >=
 // ngz), warp-aggregated appends; entries past B.fcap are dropped and the
-// count still grows, which sends the launch that follows to the fallback.
+// count still grows, which sends k_fofc_faces_list to its whole-box loop.
 // Needs box.count() < 2^30.
 __global__ void __launch_bounds__(256) k_fofc_scan(Geo G, Box box, StageBufs B) {
   int i, j, k;
@@ -533,8 +529,9 @@ __global__ void __launch_bounds__(256) k_fofc_scan(Geo G, Box box, StageBufs B) 
 }
 
 // k_fofc_faces over the compacted list: a grid-stride loop over the listed
-// faces, each recomputed as there (donor reconstruction, LLF); does nothing
-// when the list overflowed (the fallback launch covers that case).
+// faces, each recomputed as there (donor reconstruction, LLF); when the
+// list overflowed, a grid-stride loop over the whole box instead, reading
+// the tags as k_fofc_faces does.
 template <bool FAST = false>
 __global__ void __launch_bounds__(128) k_fofc_faces_list(DevParams P, Geo G, Box box,
                                                           const double* __restrict__ st,
@@ -543,7 +540,33 @@ __global__ void __launch_bounds__(128) k_fofc_faces_list(DevParams P, Geo G, Box
                                                           const double* __restrict__ by,
                                                           const double* __restrict__ bz, StageBufs B) {
   const uint32_t n = *B.fcount;
-  if (n > B.fcap) return;
+  if (n > B.fcap) {
+    unsigned cnt = 0;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < box.count();
+         t += (int64_t)gridDim.x * blockDim.x) {
+      int i, j, k;
+      int64_t q;
+      decode(box, t, i, j, k, q);
+      double f[7], vb[4];
+      if (i >= G.g && B.ftag[emi(G, i, j, k, 0, q)]) {
+        getflux<0, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bx, f, vb);
+        store_face(G, B, P.emf, 0, i, j, k, q, f, vb);
+        ++cnt;
+      }
+      if (j >= G.g && B.ftag[emi(G, i, j, k, 1, q)]) {
+        getflux<1, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, by, f, vb);
+        store_face(G, B, P.emf, 1, i, j, k, q, f, vb);
+        ++cnt;
+      }
+      if (k >= G.g && B.ftag[emi(G, i, j, k, 2, q)]) {
+        getflux<2, FAST>(P, G, i, j, k, q, GRB_RECON_DONOR, true, st, aux, bz, f, vb);
+        store_face(G, B, P.emf, 2, i, j, k, q, f, vb);
+        ++cnt;
+      }
+    }
+    if (cnt) atomicAdd(&B.counters[0], (unsigned long long)cnt);
+    return;
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(&B.counters[0], (unsigned long long)n);
   for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) {
     const uint32_t w = B.flist[e];
