@@ -68,6 +68,9 @@ def parse():
     ap.add_argument("--c2p-states", type=int, default=1 << 24, help="states of the c2p micro-benchmark")
     ap.add_argument("--mode", default="tuned", choices=["tuned", "plain"])
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
+    ap.add_argument("--profile-step", action="store_true",
+                    help="after the warm-up, run one eager RK3 step between cudaProfilerStart/Stop and exit "
+                         "(for ncu --profile-from-start off)")
     ap.add_argument("--tuning", default="", help="kernel variants flux,fofc_flag,update,aux (grb_set_tuning) "
                     "instead of the autotuner, e.g. 1,1,0,2")
     return ap.parse_args()
@@ -118,70 +121,91 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def cpu_reference_run(nb_side, n, cfl, min_s=10.0, which="ref"):
-    """Time RK3 steps of the blast wave on the CPU with the reference numerics
-    (or the oracle port if the pinning build is absent).  Bounded sample:
-    the central nb_side^3 blocks of the full grid (same cell size).
-    Returns (zone-updates/s, cores, kind, sample description)."""
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import _oracle
-    from grace_b200 import params, workloads
-    lib = _oracle.lib(which)
-    kind = "reference"
-    if lib is None:
-        which, kind = "orc", "port"
-    half = 6.0 * nb_side / 16.0 * (n / 16.0) * 16.0 / n
-    su, f = workloads.blast(nb=(nb_side,) * 3, n=(n, n, n), lo=(-half,) * 3, hi=(half,) * 3)
-    P = params.blast()
-    st, bx, by, bz, aux = [x.copy() for x in f]
-    S = _oracle.Stage(P, n, n, n, su.ngz, su.nq, which)
-    state = [st, bx, by, bz]
-    _oracle.fill_ghosts(which, su, state)
-    S.compute_aux(su.idx().copy(), state, aux)
-    sp = [x.copy() for x in state]
-    spp = [x.copy() for x in state]
-    dt = cfl / su.idx()[0, 0]
+def _workload_config(nb, n):
+    """The bench line's config (both arms print the same one)."""
+    return {"workload": f"blast wave {nb * n}^3 ({nb ** 3} blocks of {n}^3), Gamma=4/3, "
+                        "WENO-Z+HLLE+GS CT+FOFC, SSP-RK3",
+            "blocks": nb ** 3, "cells_per_block": n ** 3, "ngz": 4,
+            "l2": "inputs larger than L2 (no flush)"}
+
+
+class CpuReference:
+    """RK3 steps of the blast wave on the CPU with the reference numerics
+    (oracle/_ref: GRACE's own per-cell functions compiled in place, driven by
+    the restated loops with OpenMP over blocks), or the oracle's port when
+    the pinning build is absent.  Bounded sample of the workload: the central
+    nb_side^3 blocks of the full grid (same cell size, same initial data),
+    with zero-gradient ghosts at the sample's faces."""
+
+    def __init__(self, nb_side, n, cfl):
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import _oracle
+        from grace_b200 import params, workloads
+        self.o = _oracle
+        self.which, self.kind = "ref", "reference"
+        if _oracle.lib("ref") is None:
+            self.which, self.kind = "orc", "port"
+        half = 6.0 * nb_side / 16.0 * (n / 16.0) * 16.0 / n
+        self.su, f = workloads.blast(nb=(nb_side,) * 3, n=(n, n, n), lo=(-half,) * 3, hi=(half,) * 3)
+        P = params.blast()
+        st, bx, by, bz, self.aux = [x.copy() for x in f]
+        self.S = _oracle.Stage(P, n, n, n, self.su.ngz, self.su.nq, self.which)
+        self.state = [st, bx, by, bz]
+        _oracle.fill_ghosts(self.which, self.su, self.state)
+        self.S.compute_aux(self.su.idx().copy(), self.state, self.aux)
+        self.sp = [x.copy() for x in self.state]
+        self.spp = [x.copy() for x in self.state]
+        self.dt = cfl / self.su.idx()[0, 0]
+        self.zones_per_step = self.su.nq * n ** 3 * 3
+        self.cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        self.nb_side, self.n = nb_side, n
+
+    def step(self):
+        self.o.rk3_step(self.S, self.su, self.dt, self.state, self.sp, self.spp, self.aux, self.which)
+
+    def sample(self):
+        return (f"each step: one RK3 step of the blast wave on the central {self.nb_side}^3 blocks of "
+                f"{self.n}^3 cells of the same grid (same cell size and initial data), {self.kind} numerics, "
+                f"OpenMP over blocks on {self.cores} threads")
+
+
+def cpu_reference_run(nb_side, n, cfl, min_s=10.0):
+    """zone-updates/s of RK3 steps on the CPU sample (at least one step and
+    min_s seconds); returns (rate, cores, kind, sample description)."""
+    R = CpuReference(nb_side, n, cfl)
     done = 0
     t0 = time.perf_counter()
     while done < 1 or time.perf_counter() - t0 < min_s:
-        _oracle.rk3_step(S, su, dt, state, sp, spp, aux, which)
+        R.step()
         done += 1
     el = time.perf_counter() - t0
-    zu = su.nq * n ** 3 * 3 * done
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    sample = (f"{done} RK3 step(s) of the blast wave on the central {nb_side}^3 blocks of "
-              f"{n}^3 cells (same cell size), {kind} numerics, OpenMP over blocks")
-    return zu / el, cores, kind, sample
+    return R.zones_per_step * done / el, R.cores, R.kind, R.sample().replace("each step: one", f"{done}")
 
 
 def reference_arm(args, rank):
+    """The CPU reference on the host cores, rank 0 only: W warm-up and K
+    timed steps, each one RK3 step of the bounded sample (the central 8^3 of
+    the 16^3 blocks: an eighth of the workload, ~3 s per step on 16
+    threads), so that the whole run takes a couple of minutes."""
     if rank != 0:
         return
-    nb_side = 4
-    vals = []
-    cpu = None
+    R = CpuReference(8 if args.nb >= 8 else args.nb, args.n, args.cfl)
     for _ in range(args.warmup):
-        cpu_reference_run(nb_side, args.n, args.cfl, min_s=0.0)
+        R.step()
+    t0 = time.perf_counter()
     for _ in range(args.steps):
-        v, cores, kind, sample = cpu_reference_run(nb_side, args.n, args.cfl, min_s=10.0)
-        vals.append(v)
-        cpu = (cores, kind, sample)
-    value = statistics.median(vals)
-    nb, n = args.nb, args.n
-    zones = nb ** 3 * n ** 3 * 3  # zone-updates of one RK3 step of the full workload
+        R.step()
+    el = time.perf_counter() - t0
+    value = R.zones_per_step * args.steps / el
     line = {
         "impl": "reference", "metric": "GRMHD zone-updates/s per RK stage", "value": value,
         "unit": "zone-updates/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": zones / value * 1e3,
+        "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded blast-wave initial data)",
-        "config": {"workload": f"blast wave {nb * n}^3 ({nb ** 3} blocks of {n}^3), Gamma=4/3, "
-                               "WENO-Z+HLLE+GS CT+FOFC, SSP-RK3",
-                   "blocks": nb ** 3, "cells_per_block": n ** 3, "ngz": 4,
-                   "sample": f"timed on the central {nb_side}^3 blocks (same cell size); ms_per_step is "
-                             "the full workload's step at that rate"},
-        "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": cpu[0], "kind": cpu[1],
-                         "sample": cpu[2]},
+        "config": _workload_config(args.nb, args.n),
+        "cpu_baseline": {"value": value, "unit": "zone-updates/s", "cores": R.cores, "kind": R.kind,
+                         "sample": R.sample()},
         "e2e": {"value": value, "unit": "zone-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -216,6 +240,10 @@ def ours(args, rank, world, local_rank):
     su = workloads.BrickSetup((nb,) * 3, (n,) * 3, (-6,) * 3, (6,) * 3, 4, (False,) * 3)
     blocks = Blocks(n, n, n, 4, su.nq, su.idx(), device=dev)
     P = params.blast()
+    if args.mode == "tuned":
+        # aux pass and linop on the cells the next stage reads (the stage's
+        # own ghost exchange refills the rest every substep)
+        P.ranges = abi.RANGES_NEXT_STAGE
     g = GRMHDEquationsSystem(P)
     g.reserve(blocks)
     state, aux = build_blast_on_device(blocks, su, nb, n, dev, torch, Fields)
@@ -261,6 +289,19 @@ def ours(args, rank, world, local_rank):
     dt_pass = {"separate_step_ms": step_ms(False), "fused_step_ms": step_ms(True)}
     fused = dt_pass["fused_step_ms"] < dt_pass["separate_step_ms"]
     dt_pass["used"] = "fused" if fused else "separate"
+    if args.profile_step:
+        # one eager step between profiler start and stop (for ncu
+        # --profile-from-start off): the launch list of exactly one step
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        g.rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd, fused_dt=fused)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        if rank == 0:
+            print(json.dumps({"profile_step": True, "blocks": su.nq, "cells_per_block": n ** 3,
+                              "zone_updates": su.nq * n ** 3 * 3, "tuning": tuning}), flush=True)
+        g.close()
+        return
     graph, per_step = None, None
     if not args.eager:
         graph, per_step = g.capture_rk3_step(dt, state, sp, spp, aux, bc, next_dt=nd, fused_dt=fused)
@@ -488,7 +529,7 @@ def ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
-        v, cores, kind, sample = cpu_reference_run(4, n, args.cfl, min_s=10.0)
+        v, cores, kind, sample = cpu_reference_run(8 if nb >= 8 else nb, n, args.cfl, min_s=10.0)
         cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": kind, "sample": sample}
 
     if rank == 0:
@@ -497,10 +538,8 @@ def ours(args, rank, world, local_rank):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded blast-wave initial data)",
-            "config": {"workload": f"blast wave {nb * n}^3 ({su.nq} blocks of {n}^3), Gamma=4/3, "
-                                   "WENO-Z+HLLE+GS CT+FOFC, SSP-RK3",
-                       "blocks": su.nq, "cells_per_block": n ** 3, "ngz": 4,
-                       "l2": "inputs larger than L2 (no flush)", "parallelism": f"replicas x{world}",
+            "config": _workload_config(nb, n),
+            "run": {"parallelism": f"replicas x{world}",
                        "launch": "cuda_graph" if graph is not None else "eager",
                        "step": "3 x (advance_substep + ghost fill + aux) + linops; the last aux pass "
                                "also reduces the next stable dt (dt itself held fixed)",

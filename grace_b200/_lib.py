@@ -10,27 +10,31 @@ from . import abi
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libgrace_b200.so")
-_lib = None
+# the same sources with every multiply and add rounded on its own
+# (nvcc -fmad=false), for parity tests that need the oracle's rounding
+EXACT_LIB_PATH = os.path.join(_HERE, "libgrace_b200_exact.so")
+_libs = {}
 
 
 class LibraryMissing(RuntimeError):
     pass
 
 
-def load():
-    """Load and bind libgrace_b200.so (every symbol of include/grace_b200.h)."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    if not os.path.exists(LIB_PATH):
+def load(variant="default"):
+    """Load and bind libgrace_b200.so, or with variant="exact" its -fmad=false
+    build (every symbol of include/grace_b200.h)."""
+    if variant in _libs:
+        return _libs[variant]
+    path = {"default": LIB_PATH, "exact": EXACT_LIB_PATH}[variant]
+    if not os.path.exists(path):
         raise LibraryMissing(
-            f"{LIB_PATH} is missing; build it with `python -m grace_b200.build`")
-    lib = ctypes.CDLL(LIB_PATH)
+            f"{path} is missing; build it with `python -m grace_b200.build`")
+    lib = ctypes.CDLL(path)
     for name, (res, args) in abi.PROTOTYPES.items():
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    _lib = lib
+    _libs[variant] = lib
     return lib
 
 

@@ -26,6 +26,7 @@ EOS_IDEAL_GAS, EOS_HYBRID_PWPOLY = 0, 1
 RECON_WENOZ, RECON_MC2, RECON_MINMOD, RECON_DONOR = 0, 1, 2, 3
 RIEMANN_HLL, RIEMANN_LLF = 0, 1
 EMF_GS, EMF_UCT = 0, 1
+RANGES_FULL, RANGES_NEXT_STAGE = 0, 1
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOT_RESERVED, ERR_NO_MODEL = 0, -1, -2, -3, -4, -5
 STATIC_SCRATCH_BYTES = 64 << 20
@@ -68,6 +69,7 @@ class Params(C.Structure):
         ("fofc_enable", C.c_int32), ("dmp_enable", C.c_int32),
         ("dmp_M", C.c_double),
         ("recon", C.c_int32), ("riemann", C.c_int32), ("emf", C.c_int32),
+        ("ranges", C.c_int32),
     ]
 
 
@@ -157,7 +159,9 @@ PROTOTYPES = {
                                C.c_void_p, C.c_void_p]),
     "grb_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "grb_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
+    "grb_set_fofc_list_capacity": (C.c_int, [C.c_void_p, C.c_int64]),
     "grb_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
+    "grb_measure_fp64_peak": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "grb_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),
                                    C.c_int32]),
     "grb_advance_substep_static": (C.c_int, [C.POINTER(Params), C.POINTER(Grid), C.c_double,

@@ -13,7 +13,6 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include <random>
 #include <new>
 #include <vector>
@@ -69,6 +68,7 @@ struct grb_handle {
   int auxlist_key[4] = {0, 0, 0, 0};      // nx, ny, nz, ngz it was built for
   float tune_aux_queue_ms = 0.f;
   bool mlp_ready = false;
+  uint32_t fcap_alloc = 0;  // entries allocated for the compacted FOFC face list
 };
 
 namespace {
@@ -129,6 +129,7 @@ bool valid_params(const grb_params* p) {
   if (p->recon < GRB_RECON_WENOZ || p->recon > GRB_RECON_DONOR) return false;
   if (p->riemann != GRB_RIEMANN_HLL && p->riemann != GRB_RIEMANN_LLF) return false;
   if (p->emf != GRB_EMF_GS && p->emf != GRB_EMF_UCT) return false;
+  if (p->ranges != GRB_RANGES_FULL && p->ranges != GRB_RANGES_NEXT_STAGE) return false;
   // flag_fofc_cells asserts on UCT (evolve.cpp:479-481)
   if (p->fofc_enable && p->emf == GRB_EMF_UCT) return false;
   return true;
@@ -384,6 +385,12 @@ void launch_linop_box(cudaStream_t s, const LinBox& L, int nv, int64_t nq, doubl
   k_linop_box<<<grid, 256, 0, s>>>(L, nv, a, x, y, b, c);
 }
 
+// Aux pass and linop on the next stage's cells only (tuned mode with
+// GRB_RANGES_NEXT_STAGE); otherwise every cell, the drop-in contract.
+inline bool trimmed(const grb_handle* h) {
+  return h->mode == GRB_MODE_TUNED && h->p.ranges == GRB_RANGES_NEXT_STAGE;
+}
+
 // The static-metric cache when it was built for this geometry and these
 // spacings and covers these blocks, else null.
 const double* static_metric(const grb_handle* h, const Geo& G, const double* idx) {
@@ -403,7 +410,8 @@ static unsigned fofc_list_grid() {
 }
 
 // The stage in tuned mode: only the faces the stage reads, FAST flux math,
-// tuned register caps.  Returns the number of kernels launched.
+// tuned register caps.  Returns the number of kernels launched, or -1 when
+// a scratch reset could not be enqueued.
 int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, double dtfact,
                 const grb_fields* nw, const grb_fields* old, const double* aux, cudaStream_t s,
                 StageBufs B, bool count_fofc) {
@@ -436,12 +444,13 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
   }
   if (P.fofc && P.emf == GRB_EMF_GS) {
     const int64_t nf = G.fcells * G.nq * 3;
-    cudaMemsetAsync(B.ftag, 0, (size_t)nf, s);
-    cudaMemsetAsync(B.etag, 0, (size_t)nf, s);
-    if (count_fofc) cudaMemsetAsync(B.counters, 0, 2 * sizeof(unsigned long long), s);
+    if (cudaMemsetAsync(B.ftag, 0, (size_t)nf, s) != cudaSuccess ||
+        cudaMemsetAsync(B.etag, 0, (size_t)nf, s) != cudaSuccess ||
+        (count_fofc && cudaMemsetAsync(B.counters, 0, 2 * sizeof(unsigned long long), s) != cudaSuccess))
+      return -1;
     const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, G.nq);
     const bool listed = B.flist && fb.count() < (1ll << 30);
-    if (listed) cudaMemsetAsync(B.fcount, 0, sizeof(uint32_t), s);
+    if (listed && cudaMemsetAsync(B.fcount, 0, sizeof(uint32_t), s) != cudaSuccess) return -1;
     {
       KScope ks(h, s, GRB_KIND_FOFC_FLAG);
       launch_flag_tuned(h->var_flag, nblk(fb.count(), T), s, P, G, fb, dt, dtfact, nw->state, old->state,
@@ -502,6 +511,7 @@ void grb_params_defaults(grb_params* p, int32_t eos_kind) {
   p->rusanov_use_c_limit = 0.0;
   p->fofc_enable = 1; p->dmp_enable = 1; p->dmp_M = 1.2;
   p->recon = GRB_RECON_WENOZ; p->riemann = GRB_RIEMANN_HLL; p->emf = GRB_EMF_GS;
+  p->ranges = GRB_RANGES_FULL;
 }
 
 int grb_eos_setup_pwpoly(grb_eos_params* e, int32_t n, double kappa_0, const double* gammas,
@@ -559,7 +569,7 @@ static void free_scratch(grb_handle* h) {
   h->B.flux = h->B.eface = h->B.vbar = h->B.ecenter = h->B.emf = nullptr;
   h->B.ftag = h->B.etag = nullptr;
   h->B.flist = h->B.fcount = nullptr;
-  h->B.fcap = 0;
+  h->B.fcap = h->fcap_alloc = 0;
   h->reserved = false;
   h->cap_f = h->cap_c = 0;
 }
@@ -599,7 +609,7 @@ int grb_reserve(grb_handle* h, const grb_grid* g) {
   if (ok && h->p.emf == GRB_EMF_GS && h->p.fofc_enable) {
     // the compacted FOFC face list: up to 4 Mi faces a substep (more falls
     // back to the full recompute launch)
-    h->B.fcap = (uint32_t)std::min<int64_t>(nf * 3, 1 << 22);
+    h->B.fcap = h->fcap_alloc = (uint32_t)std::min<int64_t>(nf * 3, 1 << 22);
     ok = al((void**)&h->B.flist, sizeof(uint32_t) * h->B.fcap) && al((void**)&h->B.fcount, sizeof(uint32_t));
   }
   if (!ok) {
@@ -660,7 +670,9 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt, d
   const int gz = G.g, T = 128;
   StageBufs B = h->B;
   if (h->mode == GRB_MODE_TUNED) {
-    h->launches += stage_tuned(h, G, g, dt, dtfact, nw, old, aux, s, B, true);
+    const int nl = stage_tuned(h, G, g, dt, dtfact, nw, old, aux, s, B, true);
+    if (nl < 0) return fail(h, GRB_ERR_CUDA);
+    h->launches += nl;
     CK(cudaGetLastError());
     return GRB_OK;
   }
@@ -792,7 +804,7 @@ int grb_compute_auxiliary_quantities_dt(grb_handle* h, const grb_grid* g, const 
     ++h->launches;
   }
   if (h->mode == GRB_MODE_TUNED) {
-    const Box tb = tuned_aux_box(h, G, s);
+    const Box tb = trimmed(h) ? tuned_aux_box(h, G, s) : b;
     launch_aux_tuned(h->var_aux, nblk(tb.count(), 128), s, h->dp, G, tb, st->state, st->bx, st->by, st->bz, aux,
                      g->idx, g->coords, h->B, dt_out ? &dta : nullptr, h->d_queue);
   } else if (dt_out) {
@@ -850,7 +862,7 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A, const
   const double* x[4] = {Bf->state, Bf->bx, Bf->by, Bf->bz};
   const double* y[4] = {Cf ? Cf->state : nullptr, Cf ? Cf->bx : nullptr, Cf ? Cf->by : nullptr, Cf ? Cf->bz : nullptr};
   KScope ks(h, s, GRB_KIND_LINOP);
-  if (h->mode == GRB_MODE_TUNED) {
+  if (trimmed(h)) {
     // The Cowling metric and curvature are static, and the next stage reads
     // the combination only on the HRSC variables of cells [g-2, n+g+2) (the
     // FOFC flag window) and on the faces the CT update advances before the
@@ -1601,6 +1613,13 @@ int grb_accumulate_boundary_outflow(grb_handle* h, const grb_grid* g, int64_t nf
   return GRB_OK;
 }
 
+int grb_set_fofc_list_capacity(grb_handle* h, int64_t faces) {
+  if (!h || faces < 0) return fail(h, GRB_ERR_INVALID);
+  if (!h->reserved) return fail(h, GRB_ERR_NOT_RESERVED);
+  h->B.fcap = (uint32_t)std::min<int64_t>(faces, h->fcap_alloc);
+  return GRB_OK;
+}
+
 int grb_set_mode(grb_handle* h, int32_t mode) {
   if (!h || (mode != GRB_MODE_PLAIN && mode != GRB_MODE_TUNED)) return GRB_ERR_INVALID;
   h->mode = mode;
@@ -1679,7 +1698,7 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
   const Box fbx = box(lo[0], lo[1], lo[2], n[0], n[1], n[2], nt);
   const Box fb = box(gz - 1, gz - 1, gz - 1, G.nx + 2, G.ny + 2, G.nz + 2, nt);
   const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, nt);
-  Box ab = tuned_aux_box(h, G, s);
+  Box ab = trimmed(h) ? tuned_aux_box(h, G, s) : box(0, 0, 0, G.NX, G.NY, G.NZ, nt);
   ab.nq = nt;
   int best[4] = {0, 0, 0, 0};
   for (int fam = 0; fam < 4; ++fam) {
@@ -1745,6 +1764,56 @@ int grb_set_tuning(grb_handle* h, const int32_t* variant) {
   return GRB_OK;
 }
 
+// FP64 throughput probe: kFmaChains independent fused multiply-add chains
+// per thread, iters steps each; the final values feed a store that never
+// happens (their sum is never negative), so nothing is optimised away.
+constexpr int kFmaChains = 8;
+__global__ void __launch_bounds__(256) k_fp64_peak(int iters, double b, double c, double* __restrict__ sink) {
+  double a[kFmaChains];
+#pragma unroll
+  for (int u = 0; u < kFmaChains; ++u) a[u] = 1.0 + 1e-9 * (threadIdx.x + 37 * u);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int u = 0; u < kFmaChains; ++u) a[u] = fma(a[u], b, c);
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int u = 0; u < kFmaChains; ++u) s += a[u];
+  if (s < 0.0) sink[blockIdx.x] = s;
+}
+
+int grb_measure_fp64_peak(double* tflops, double* ms_out, void* stream) {
+  if (!tflops) return GRB_ERR_INVALID;
+  grb_handle* h = nullptr;
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0, sms = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const unsigned grid = (unsigned)(sms * 8);
+  const int iters = 1 << 14;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  k_fp64_peak<<<grid, 256, 0, s>>>(iters / 16, 0.9999999, 1e-7, nullptr);  // warm-up
+  float best = 1e30f;
+  for (int r = 0; r < 5; ++r) {
+    cudaEventRecord(e0, s);
+    k_fp64_peak<<<grid, 256, 0, s>>>(iters, 0.9999999, 1e-7, nullptr);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    best = t < best ? t : best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  CK(cudaGetLastError());
+  const double flops = 2.0 * kFmaChains * (double)iters * grid * 256.0;
+  *tflops = flops / (best * 1e-3) / 1e12;
+  if (ms_out) *ms_out = best;
+  return GRB_OK;
+}
+
 int grb_set_kernel_timing(grb_handle* h, int32_t enable) {
   if (!h) return GRB_ERR_INVALID;
   h->timing = enable != 0;
@@ -1792,8 +1861,6 @@ int grb_kernel_times(grb_handle* h, double* ms, int64_t* counts, int32_t nkinds)
 // ---------------------------------------------------------------------------
 namespace {
 static __device__ __align__(256) unsigned char g_static_scratch[GRB_STATIC_SCRATCH_BYTES];
-std::mutex g_static_mu;
-void* g_static_addr[256] = {};  // device address of g_static_scratch, per device ordinal
 
 // cell-centred E = -vtilde x B with B including sqrt(gamma)
 // (auxiliaries.cpp:131-162), for the blocks of one chunk
@@ -1859,20 +1926,14 @@ extern "C" int grb_advance_substep_static(const grb_params* p, const grb_grid* g
                  g->nx, g->ny, g->nz, g->ngz, L.per_block, (size_t)GRB_STATIC_SCRATCH_BYTES - header);
     return GRB_ERR_INVALID;
   }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return GRB_ERR_CUDA;
-  unsigned char* base = nullptr;
-  {
-    // Set-up, once per device with that device current: the host-side name
-    // g_static_scratch is only a stand-in, the kernels need its device address.
-    std::lock_guard<std::mutex> lk(g_static_mu);
-    if (!g_static_addr[dev]) {
-      void* ptr = nullptr;
-      if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || !ptr) return GRB_ERR_CUDA;
-      g_static_addr[dev] = ptr;
-    }
-    base = static_cast<unsigned char*>(g_static_addr[dev]);
-  }
+  // The host-side name g_static_scratch is only a stand-in: the kernels need
+  // the array's device address on the current device.  It is looked up on
+  // every call (cheap, allocates nothing), so it stays right after a device
+  // reset reloads the module.  On a device's first call this also loads the
+  // module there, which is why that first call belongs before any capture.
+  void* ptr = nullptr;
+  if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || !ptr) return GRB_ERR_CUDA;
+  unsigned char* base = static_cast<unsigned char*>(ptr);
   const DevParams P = to_dev(*p);
   cudaStream_t s = (cudaStream_t)stream;
   const int64_t chunk = (int64_t)((GRB_STATIC_SCRATCH_BYTES - header) / L.per_block);

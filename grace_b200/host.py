@@ -94,8 +94,10 @@ class Blocks:
 class GRMHDEquationsSystem:
     """grmhd_equations_system_t<eos_t> + the evolve.cpp drivers, on the GPU."""
 
-    def __init__(self, params):
-        self.lib = _lib.load()
+    def __init__(self, params, variant="default"):
+        """variant "exact": the -fmad=false build of the library (parity
+        tests); the default build otherwise."""
+        self.lib = _lib.load(variant)
         self.params = params
         h = ctypes.c_void_p()
         _lib.check(self.lib.grb_create(ctypes.byref(h), ctypes.byref(params)), "grb_create")
@@ -378,6 +380,11 @@ class GRMHDEquationsSystem:
         """Pick tuned-mode candidates (indices 0..2) without timing."""
         v = (ctypes.c_int32 * 4)(flux, flag, update, aux)
         _lib.check(self.lib.grb_set_tuning(self.h, v), "grb_set_tuning")
+
+    def set_fofc_list_capacity(self, faces):
+        """Capacity of the compacted FOFC face list of the tuned stage
+        (grb_set_fofc_list_capacity); 0 forces the whole-box recompute."""
+        _lib.check(self.lib.grb_set_fofc_list_capacity(self.h, int(faces)), "grb_set_fofc_list_capacity")
 
     def set_kernel_timing(self, on):
         _lib.check(self.lib.grb_set_kernel_timing(self.h, 1 if on else 0), "grb_set_kernel_timing")

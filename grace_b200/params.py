@@ -44,6 +44,7 @@ def defaults(eos_kind=abi.EOS_IDEAL_GAS):
     p.recon = abi.RECON_WENOZ
     p.riemann = abi.RIEMANN_HLL
     p.emf = abi.EMF_GS
+    p.ranges = abi.RANGES_FULL  # aux / linop write every cell (the drop-in contract)
     return p
 
 

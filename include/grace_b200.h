@@ -96,6 +96,20 @@ enum grb_recon_kind { GRB_RECON_WENOZ = 0, GRB_RECON_MC2 = 1,
                       GRB_RECON_MINMOD = 2, GRB_RECON_DONOR = 3 };
 enum grb_riemann_kind { GRB_RIEMANN_HLL = 0, GRB_RIEMANN_LLF = 1 };
 enum grb_emf_kind { GRB_EMF_GS = 0, GRB_EMF_UCT = 1 };
+/* What grb_compute_auxiliary_quantities(_dt) and grb_linop_apply write in
+ * GRB_MODE_TUNED.  GRB_RANGES_FULL (the default, the drop-in contract):
+ * every cell of every block, ghosts included, as compute_auxiliary_quantities
+ * (auxiliaries.cpp:111-130) and linop_apply (tstep_utils.hh:54-229) do, so
+ * any consumer of aux or of the combined state (regrid, output, diagnostics)
+ * sees complete arrays.  GRB_RANGES_NEXT_STAGE: only what the next
+ * advance_substep reads before the caller's ghost exchange refills the rest
+ * (aux: the cells with at least two indices in [ngz-1, n+ngz+1) and the
+ * cells of [ngz-2, n+ngz+2)^3, GS EMF only; linop: the 7 evolved HRSC
+ * variables on the cells with y, z in [ngz-2, n+ngz+2) and the faces with
+ * interior y, z, the Cowling metric being static); the other aux ghost
+ * cells, their c2p rewrites of the state, and the metric and outer planes
+ * of a linop target keep their previous values.  GRB_MODE_PLAIN ignores it. */
+enum grb_ranges_kind { GRB_RANGES_FULL = 0, GRB_RANGES_NEXT_STAGE = 1 };
 
 #define GRB_MAX_PIECES 8
 
@@ -136,6 +150,9 @@ typedef struct grb_params {
   double dmp_M;
   /* scheme selection */
   int32_t recon, riemann, emf;
+  /* cells the aux pass and linop_apply cover in GRB_MODE_TUNED
+   * (grb_ranges_kind); the plain mode always covers every cell */
+  int32_t ranges;
 } grb_params;
 
 /* Block geometry shared by all blocks of a call. */
@@ -212,11 +229,13 @@ int grb_set_static_metric(grb_handle* h, const grb_grid* g, const grb_fields* st
  *   (src/evolution/auxiliaries.cpp:81-180): c2p on every cell including
  *   ghosts, conservative rewrites, C2P_ERR sticky-OR, BDIV, and (GS) the
  *   cell-centred E used by the next stage's EMF.
- *   GRB_MODE_TUNED with the GS EMF covers only the cells the next
- *   advance_substep reads before the ghost exchange refills the rest: those
- *   with at least two indices in [ngz-1, n+ngz+1), and [ngz-2, n+ngz+2)^3
- *   (14 % fewer cells for 16^3 blocks with 4 ghosts); aux and the
- *   conservative rewrites of the other ghost cells are left as they were. */
+ *   Only with GRB_MODE_TUNED, the GS EMF and params.ranges =
+ *   GRB_RANGES_NEXT_STAGE: just the cells the next advance_substep reads
+ *   before the ghost exchange refills the rest, those with at least two
+ *   indices in [ngz-1, n+ngz+1), and [ngz-2, n+ngz+2)^3 (14 % fewer cells
+ *   for 16^3 blocks with 4 ghosts); aux and the conservative rewrites of the
+ *   other 1,936 ghost cells of a 16^3 block are then left as they were.
+ *   With the default GRB_RANGES_FULL every cell is written in both modes. */
 int grb_compute_auxiliary_quantities(grb_handle* h, const grb_grid* g,
                                      const grb_fields* state, double* aux,
                                      void* stream);
@@ -243,11 +262,14 @@ int grb_reset_c2p_diagnostics(grb_handle* h, const grb_grid* g, double* aux,
                               void* stream);
 /* = grace::linop_apply (include/grace/utils/tstep_utils.hh:54-229):
  *   A = b*B (C == NULL) or A = b*B + c*C on cells and faces, all 23 vars.
- *   GRB_MODE_TUNED combines only what the next advance_substep reads before
- *   the ghost exchange: the 7 evolved HRSC variables on the cells with
- *   y, z in [ngz-2, n+ngz+2) (all x) and the faces with y, z in the
- *   interior (all x) (the metric is static in Cowling); the caller's ghost exchange must refill A's ghost zones before
- *   anything else reads them, as evolve_impl does after every stage. */
+ *   Only with GRB_MODE_TUNED and params.ranges = GRB_RANGES_NEXT_STAGE: just
+ *   what the next advance_substep reads before the ghost exchange, the 7
+ *   evolved HRSC variables on the cells with y, z in [ngz-2, n+ngz+2) (all
+ *   x) and the faces with y, z in the interior (all x) (the metric is static
+ *   in Cowling); A's metric, curvature and outer planes keep their previous
+ *   values, and the caller's ghost exchange must refill A's ghost zones
+ *   before anything else reads them, as evolve_impl does after every stage.
+ *   With the default GRB_RANGES_FULL all 23 variables everywhere. */
 int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A,
                     const grb_fields* B, const grb_fields* C, double b,
                     double c, void* stream);
@@ -353,11 +375,12 @@ int grb_mlp_grad(grb_handle* h, int64_t n, const float* params,
 /* GRB_MODE_PLAIN: one thread per face / edge / cell over the reference's own
  * launch ranges (compute_fluxes computes faces over the full transverse
  * ghost range, evolve.cpp:908-922; linop_apply combines all 23 variables).
- * GRB_MODE_TUNED: only the faces the stage reads, one reciprocal per face
- * for the HLL fluxes, division-free WENO-Z weights, the register-cap
- * variant picked by grb_autotune, and linop on the evolved variables only
- * (the Cowling metric is static).  Results agree with the plain mode to
- * rounding. */
+ * GRB_MODE_TUNED: only the faces the stage reads (internal scratch), one
+ * reciprocal per face for the HLL fluxes, division-free WENO-Z weights, the
+ * register-cap variant picked by grb_autotune, fewer divisions in the c2p.
+ * Results agree with the plain mode to rounding.  Which cells the aux pass
+ * and linop_apply write is chosen separately, by params.ranges
+ * (grb_ranges_kind). */
 enum grb_mode { GRB_MODE_PLAIN = 0, GRB_MODE_TUNED = 1 };
 int grb_set_mode(grb_handle* h, int32_t mode);
 /* Times the register-cap variants of the flux, FOFC-flag, update and aux
@@ -379,6 +402,16 @@ int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms);
  * tiles from a device counter — at 1, 4, 5 CTAs/SM). */
 int grb_set_tuning(grb_handle* h, const int32_t* variant);
 
+/* Capacity, in faces, of the compacted list through which GRB_MODE_TUNED
+ * stages recompute the FOFC-tagged faces: at most what grb_reserve
+ * allocated (min(4 Mi, the grid's faces); the default).  A substep that
+ * tags more faces than this recomputes them in a loop over the whole FOFC
+ * box instead, with the same results; 0 sends every substep there (so that
+ * tests can reach that path).  Calls after it on this handle use the new
+ * capacity until the next grb_reserve of another geometry.
+ * GRB_ERR_NOT_RESERVED before grb_reserve. */
+int grb_set_fofc_list_capacity(grb_handle* h, int64_t faces);
+
 /* ---- measurement helpers -------------------------------------------------- */
 /* Kernel kinds for grb_kernel_times. */
 enum grb_kernel_kind {
@@ -391,6 +424,12 @@ enum grb_kernel_kind {
  * returns the summed milliseconds and launch-group counts per kind
  * (arrays of GRB_KIND_COUNT) and resets the accumulators. */
 int grb_set_kernel_timing(grb_handle* h, int32_t enable);
+/* No counterpart in the reference: the current device's FP64 throughput,
+ * the denominator of the FP64 roofline.  Times (CUDA events, best of 5 on
+ * the stream) a kernel of independent fused multiply-add chains, 8 CTAs of
+ * 256 threads per SM; *tflops = 2 x FMAs / time in TFLOP/s, *ms (or NULL)
+ * the launch time.  Synchronises the stream. */
+int grb_measure_fp64_peak(double* tflops, double* ms, void* stream);
 int grb_kernel_times(grb_handle* h, double* ms, int64_t* counts, int32_t nkinds);
 
 /* ---- harness-side helper (outside the reference's hot path) -------------- */
@@ -530,9 +569,11 @@ int grb_prolong_to_ghosts(grb_handle* h, const grb_grid* g, const grb_fields* fi
  * chunks that fit the array, so any nq works; a single block whose scratch
  * (~30 doubles per face-grid point + 3 per cell) exceeds the array is
  * rejected with GRB_ERR_INVALID and a message on stderr.  Every GPU that
- * loads the library holds the array until exit.  The first call on a device
- * looks up the array's device address (once per device, with that device
- * current); make that first call before any stream capture.  All calls share
+ * loads the library holds the array until exit.  Each call looks up the
+ * array's device address on the current device (cudaGetSymbolAddress, no
+ * allocation), so the address stays right after a device reset; the first
+ * call on a device also loads the library's kernels there, so make that
+ * first call before any stream capture.  All calls share
  * the one array, which keeps the last call's contents (what must start at
  * zero is cleared by each call), so calls that overlap on the GPU — from
  * two streams or two threads — race and corrupt each other's results.

@@ -91,10 +91,15 @@ def prolong_faces(which, kind, n, ngz, fine, cbuf, fine_q, cbuf_q, elem, have_fi
 
 def build_oracle():
     """Build liboracle.so (and the pinning build when the GRACE sources are
-    present) with oracle/Makefile."""
-    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all"], check=True)
-    if os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    present; oracle/Makefile knows where) with oracle/Makefile."""
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "all", "ref-if-present"], check=True)
+
+
+def ref_dir():
+    """The GRACE source tree the pinning build compiles (oracle/Makefile's
+    REF: GRACE_REF_DIR or its default)."""
+    return subprocess.run(["make", "-s", "--no-print-directory", "-C", os.path.join(ROOT, "oracle"), "print-ref"],
+                          check=True, capture_output=True, text=True).stdout.strip()
 
 
 _cache = {}

@@ -38,8 +38,26 @@ def _beta_low(x, y, z):
     return np.stack([sum(G[j][k] * b[k] for k in range(3)) for j in range(3)])
 
 
-def curved_setup(nb=(2, 2, 2), n=(8, 8, 8), emf=abi.EMF_GS, fofc=1):
-    P = params.hybrid_pwpoly(100.0, [2.0], [], gamma_th=1.8, emf=emf, fofc_enable=fofc,
+def cold_pwpoly(e, rho):
+    """Cold pressure and specific energy of the piecewise polytrope in the
+    EOS parameters e (piece i for pw_rho[i] < rho <= pw_rho[i+1], the last
+    piece above; piecewise_polytropic_eos.hh:51-190)."""
+    n = e.n_pieces
+    i = np.zeros(rho.shape, dtype=int)
+    for k in range(1, n):
+        i = np.where(rho > e.pw_rho[k], k, i)
+    K = np.asarray(e.pw_kappa[:n])[i]
+    G = np.asarray(e.pw_gamma[:n])[i]
+    E = np.asarray(e.pw_eps[:n])[i]
+    pc = K * rho ** G
+    return pc, E + pc / (rho * (G - 1.0))
+
+
+def curved_setup(nb=(2, 2, 2), n=(8, 8, 8), emf=abi.EMF_GS, fofc=1, pieces=None):
+    """pieces: (kappa_0, gammas, rhos) of a piecewise-polytropic cold part
+    (default: one piece, K = 100, Gamma = 2)."""
+    kappa, gammas, rhos = pieces if pieces is not None else (100.0, [2.0], [])
+    P = params.hybrid_pwpoly(kappa, gammas, rhos, gamma_th=1.8, emf=emf, fofc_enable=fofc,
                              max_sigma=1.0e4)
     su = BrickSetup(nb, n, (3.0, -1.0, -1.0), (5.0, 1.0, 1.0), 4, (False, False, False))
     state, bx, by, bz, aux = su.empty()
@@ -64,8 +82,9 @@ def curved_setup(nb=(2, 2, 2), n=(8, 8, 8), emf=abi.EMF_GS, fofc=1):
     q2 = ((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / sig ** 2
     rho = 1e-3 * np.exp(-q2) + 1e-7
     eth = np.full_like(rho, 1e-4 / 0.8)
-    press = 100.0 * rho ** 2 + 0.8 * rho * eth
-    eps = 100.0 * rho + eth
+    pc, ec = cold_pwpoly(P.eos, rho)
+    press = pc + 0.8 * rho * eth
+    eps = ec + eth
     zv = 0.1 * np.exp(-0.5 * q2) * np.stack([-y, x - c[0], 0.3 * np.ones_like(x)])
     # densitized face fields from A_z on z-edges (cell corners in x-y)
     dx = su.dx

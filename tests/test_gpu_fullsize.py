@@ -39,7 +39,9 @@ def test_blast_256cubed_two_steps_properties():
     dev = torch.device("cuda:0")
     su0 = workloads.BrickSetup((NB,) * 3, (N,) * 3, (-6, -6, -6), (6, 6, 6), G, (True, True, True))
     blocks = Blocks(N, N, N, G, su0.nq, su0.idx(), device=dev)
-    g = GRMHDEquationsSystem(params.blast())
+    P = params.blast()
+    P.ranges = abi.RANGES_NEXT_STAGE  # the benchmark's aux and linop ranges
+    g = GRMHDEquationsSystem(P)
     g.reserve(blocks)
     _, state, aux = _device_blast(blocks, dev)
     bc = lambda fl: g.fill_ghosts_brick(fl, su0.nb, su0.periodic)

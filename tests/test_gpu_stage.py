@@ -25,10 +25,16 @@ def _setup(name):
     return P, su, f, cfl / su.idx()[0, 0]
 
 
-def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN, tuning=None, static_metric=False):
+def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN, tuning=None, static_metric=False,
+             ranges=abi.RANGES_NEXT_STAGE):
+    """nsteps SSP-RK3 steps on the GPU.  Tuned runs use the aux and linop
+    ranges of the benchmark (the next stage's cells only) unless `ranges`
+    says otherwise."""
     dev = torch.device("cuda:0")
     st, bx, by, bz, aux = f
     blocks = Blocks(su.n[0], su.n[1], su.n[2], su.ngz, su.nq, su.idx(), device=dev)
+    P = abi.Params.from_buffer_copy(P)
+    P.ranges = ranges
     g = GRMHDEquationsSystem(P)
     g.reserve(blocks)
     g.set_mode(mode)
@@ -52,10 +58,11 @@ def _gpu_run(P, su, f, dt, nsteps, mode=abi.MODE_PLAIN, tuning=None, static_metr
     return [x.cpu().numpy() for x in (state.state, state.bx, state.by, state.bz)], aux_d.cpu().numpy(), g
 
 
-def _aux_sel(P, su, mode):
+def _aux_sel(P, su, mode, ranges=abi.RANGES_NEXT_STAGE):
     """Index of the aux cells maintained by this mode (all cells, or the
-    tuned pass's list with the GS EMF), for arrays (nq, NZ, NY, NX)."""
-    if mode == abi.MODE_TUNED and P.emf == abi.EMF_GS:
+    tuned pass's list with the GS EMF and the next stage's ranges), for
+    arrays (nq, NZ, NY, NX)."""
+    if mode == abi.MODE_TUNED and P.emf == abi.EMF_GS and ranges == abi.RANGES_NEXT_STAGE:
         return (slice(None), tuned_aux_mask(su))
     return (slice(None),)
 

@@ -1,7 +1,9 @@
 """Two ranks over gloo (CPU): the blast wave on a 4x2x2 brick split into two
 x-slabs of blocks, each rank advancing its own blocks with the oracle and
 exchanging x-halos between stages, reproduces the single-rank RK3 step bit
-for bit.  Covers the host-side partitioning logic of N>1 runs."""
+for bit, with outflow and with periodic x boundaries (with two ranks both
+x-neighbours are the same rank).  Covers the host-side partitioning logic
+of N>1 runs."""
 import os
 import socket
 
@@ -11,7 +13,7 @@ import torch.multiprocessing as mp
 
 import _oracle
 from grace_b200 import abi, params, workloads
-from grace_b200.distributed import exchange_x_halos, split_columns
+from _slab import exchange_x_halos, split_columns
 
 
 def _free_port():
@@ -27,9 +29,17 @@ N = 8
 G = 4
 
 
-def _single():
+def _periodic(su, periodic_x):
+    """The same brick with periodic x boundaries when asked."""
+    if not periodic_x:
+        return su
+    return workloads.BrickSetup(su.nb, su.n, su.lo, su.hi, su.ngz, (True, False, False))
+
+
+def _single(periodic_x=False):
     P = params.blast()
     su, f = workloads.blast(nb=NB, n=(N,) * 3)
+    su = _periodic(su, periodic_x)
     st, bx, by, bz, aux = [x.copy() for x in f]
     S = _oracle.Stage(P, N, N, N, G, su.nq)
     state = [st, bx, by, bz]
@@ -48,7 +58,7 @@ def _view(a, nbx):
     return a.reshape(NB[2], NB[1], nbx, nv, *sh[-3:])
 
 
-def _worker(rank, world, port, out_q):
+def _worker(rank, world, port, out_q, periodic_x=False):
     import torch.distributed as dist
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
@@ -72,7 +82,7 @@ def _worker(rank, world, port, out_q):
                 (_view(fields[2], nbl), False), (_view(fields[3], nbl), False)]
         hrsc = arrs[0][0].copy()
         arrs[0] = (hrsc, False)
-        exchange_x_halos(arrs, G, N, nbl, False, dist, rank, world)
+        exchange_x_halos(arrs, G, N, nbl, periodic_x, dist, rank, world)
         # the exchanged x-slabs span the neighbour's full y, z extent (its
         # own y and z ghosts included), so edges and corners are right too
         _view(fields[0], nbl)[:, :, :, :abi.N_HRSC] = hrsc
@@ -100,12 +110,13 @@ def _worker(rank, world, port, out_q):
     dist.destroy_process_group()
 
 
-def test_two_rank_slab_split_matches_single_rank():
-    ref = _single()
+@pytest.mark.parametrize("periodic_x", [False, True])
+def test_two_rank_slab_split_matches_single_rank(periodic_x):
+    ref = _single(periodic_x)
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q, periodic_x)) for r in range(2)]
     for p in procs:
         p.start()
     got = [q.get(timeout=120) for _ in range(2)]
@@ -118,3 +129,22 @@ def test_two_rank_slab_split_matches_single_rank():
         b = ref[0][qs][:, :7, g:-g, g:-g, g:-g]
         bad = [int(np.sum(a[:, v] != b[:, v])) for v in range(7)]
         assert sum(bad) == 0, (rank, bad)
+
+
+def test_one_rank_periodic_wrap_matches_brick_fill():
+    """world == 1 with periodic x: the rank wraps its own edge columns (no
+    message), and the x-ghosts equal the oracle's periodic brick fill."""
+    su, f = workloads.blast(nb=NB, n=(N,) * 3)
+    ref = [x.copy() for x in f[:4]]
+    _oracle.fill_ghosts("orc", _periodic(su, True), ref)
+    got = [x.copy() for x in f[:4]]
+    _oracle.fill_ghosts("orc", su, got)  # outflow everywhere first
+    arrs = [(_view(got[0], NB[0])[:, :, :, :abi.N_HRSC], False), (_view(got[1], NB[0]), True),
+            (_view(got[2], NB[0]), False), (_view(got[3], NB[0]), False)]
+    hrsc = arrs[0][0].copy()
+    arrs[0] = (hrsc, False)
+    exchange_x_halos(arrs, G, N, NB[0], True, None, 0, 1)
+    _view(got[0], NB[0])[:, :, :, :abi.N_HRSC] = hrsc
+    assert np.array_equal(got[0][:, :abi.N_HRSC], ref[0][:, :abi.N_HRSC])
+    for a, b in zip(got[1:], ref[1:]):
+        assert np.array_equal(a, b)

@@ -7,8 +7,11 @@ exports a variant of the stage whose scratch lives in a fixed file-scope
 device array.  This test calls it through the C ABI on two consecutive
 stages and checks the new state against the handle-based
 grb_advance_substep on the same inputs (same kernels: within the 1e-10
-stage tolerance, in practice bit for bit).  The grid has more blocks than
-one pass over the static array holds, so the chunked path is exercised.
+stage tolerance, in practice bit for bit), with the Gardiner-Stone EMF and
+FOFC and with the UCT EMF (whose chunks hold the face velocities instead of
+the face and cell-centred E).  The grid has more blocks than one pass over
+the static array holds, so the chunked path is exercised.  One 16^3 block
+(the benchmark's block size) is also compared with the CPU oracle.
 The file sorts last so that a run stopping at the first failure has run
 every other test before it.
 """
@@ -18,6 +21,7 @@ import numpy as np
 import pytest
 import torch
 
+import _oracle
 from grace_b200 import _lib, abi, params, workloads
 from grace_b200.host import Blocks, Fields, GRMHDEquationsSystem
 from parity import cons_rel_err, interior
@@ -36,14 +40,19 @@ def _static_stage(lib, P, blocks, dt, dtfact, new, old, aux):
                                           ctypes.c_void_p(aux.data_ptr()), s)
 
 
-def test_static_scratch_stage_matches_handle_stage():
+@pytest.mark.parametrize("emf", [abi.EMF_GS, abi.EMF_UCT])
+def test_static_scratch_stage_matches_handle_stage(emf):
     lib = _lib.load()
     dev = torch.device("cuda:0")
     P = params.blast()
-    P.max_sigma = 100.0  # keeps FOFC busy on this setup (see test_gpu_stage)
+    if emf == abi.EMF_GS:
+        P.max_sigma = 100.0  # keeps FOFC busy on this setup (see test_gpu_stage)
+    else:
+        P.emf, P.fofc_enable = abi.EMF_UCT, 0  # FOFC needs the GS EMF
     su, (st, bx, by, bz, aux) = workloads.blast(nb=(4, 4, 4), n=(8, 8, 8))
-    # 64 blocks of 8^3 need ~83 MB of scratch: more than one pass of the array
-    per_block = 8 * (17 ** 3) * (21 + 6 + 3) + 8 * 16 ** 3 * 3
+    # 64 blocks of 8^3 need ~83 MB (GS) / ~92 MB (UCT) of scratch: more than
+    # one pass of the array
+    per_block = 8 * (17 ** 3) * ((21 + 6 + 3) if emf == abi.EMF_GS else (21 + 12 + 3))
     assert su.nq * per_block > abi.STATIC_SCRATCH_BYTES
     blocks = Blocks(8, 8, 8, 4, su.nq, su.idx(), device=dev)
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -75,6 +84,40 @@ def test_static_scratch_stage_matches_handle_stage():
             ref.fill_ghosts_brick(f, su.nb, su.periodic)
             ref.compute_auxiliary_quantities(f, au)
         a_old, b_old = a_new, b_new
+
+
+def test_static_scratch_stage_on_a_16cubed_block_matches_oracle():
+    """One substep of one 16^3 block of the blast wave (GS + FOFC) through the
+    scratch-free entry point, twice in a row on the same inputs (the array
+    keeps the first call's contents: the second must not depend on them),
+    against the CPU oracle's advance_substep."""
+    lib = _lib.load()
+    dev = torch.device("cuda:0")
+    P = params.blast()
+    P.max_sigma = 100.0
+    su, f = workloads.blast(nb=(1, 1, 1), n=(16, 16, 16), lo=(-1.5,) * 3, hi=(1.5,) * 3)
+    old = [x.copy() for x in f[:4]]
+    aux = f[4].copy()
+    S = _oracle.Stage(P, 16, 16, 16, 4, 1)
+    _oracle.fill_ghosts("orc", su, old)
+    S.compute_aux(su.idx().copy(), old, aux)
+    dt = 0.25 / su.idx()[0, 0]
+    new_h = [x.copy() for x in old]
+    S.advance_substep(su.idx().copy(), dt, 1.0, new_h, old, aux)
+    assert S.fofc_counts()[0] > 0
+    blocks = Blocks(16, 16, 16, 4, 1, su.idx(), device=dev)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    o = Fields(*[T(x) for x in old])
+    aux_d = T(aux)
+    for _ in range(2):
+        n = o.clone()
+        assert _static_stage(lib, P, blocks, dt, 1.0, n, o, aux_d) == abi.OK
+        torch.cuda.synchronize()
+        e = cons_rel_err(interior(n.state.cpu().numpy()[:, :7], 4), interior(new_h[0][:, :7], 4))
+        assert e.max() < TOL, e
+        for x, y in zip((n.bx, n.by, n.bz), new_h[1:]):
+            d = np.max(np.abs(x.cpu().numpy() - y)) / max(np.max(np.abs(y)), 1e-300)
+            assert d < TOL
 
 
 def test_static_scratch_rejects_oversized_blocks():
