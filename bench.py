@@ -486,6 +486,17 @@ def ours(args, rank, world, local_rank):
                            "three face-B arrays; bytes = the fine ghost region written once plus the coarse "
                            "data covering it read once"}
 
+    # --- FP64 throughput of this GPU (the FP64 roofline's denominator)
+    import ctypes
+    from grace_b200 import _lib
+    fp64_tf, fp64_ms = ctypes.c_double(), ctypes.c_double()
+    _lib.check(_lib.load().grb_measure_fp64_peak(ctypes.byref(fp64_tf), ctypes.byref(fp64_ms),
+                                                 ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)),
+               "grb_measure_fp64_peak")
+    fp64_peak = {"tflops": fp64_tf.value, "launch_ms": fp64_ms.value,
+                 "how": "grb_measure_fp64_peak: 8 independent FMA chains per thread, 8 CTAs x 256 threads per "
+                        "SM, best of 5, CUDA events"}
+
     # --- dominant kernel roofline (HBM), measured over the timed region
     peaks = {}
     try:
@@ -548,7 +559,7 @@ def ours(args, rank, world, local_rank):
                        else "metric differentiated every stage"},
             "clocks": clk, "gpu_launches": launches,
             "kernel_ms": {k: round(v[0], 3) for k, v in kt.items() if v[1]},
-            "roofline": roof, "e2e": e2e, "cpu_baseline": cpu, "c2p": c2p,
+            "roofline": roof, "fp64_peak": fp64_peak, "e2e": e2e, "cpu_baseline": cpu, "c2p": c2p,
             "mode": args.mode, "plain_form": plain, "tuning": tuning, "restrict": restrict, "prolong": prolong,
         }
         print(json.dumps(line), flush=True)

@@ -171,9 +171,10 @@ def test_pwpoly_three_pieces_c2p_matches_oracle(mode):
                              max_sigma=2.0e3)
     rng = np.random.default_rng(21)
     n = 20000
-    cons, _ = workloads.c2p_states(n, seed=21)
-    # rescale the densities into [1e-7, 1e-3] keeping each state's shape
-    s = 10 ** rng.uniform(-7, -3, n) / np.maximum(cons[0], 1e-300)
+    cons, prims = workloads.c2p_states(n, seed=21)
+    # rescale the rest-mass densities into [1e-7, 1e-3] (log-uniform)
+    # keeping each state's velocity, specific energy and magnetisation
+    s = 10 ** rng.uniform(-7, -3, n) / prims[abi.P_RHO]
     cons[:7] *= s[None]
     cons[7:10] *= np.sqrt(s)[None]
     dev = torch.device("cuda:0")
