@@ -42,11 +42,21 @@ ALGO_BYTES = {
     # per interior cell: 21 face fluxes, 9 aux, 16 metric/curvature, 7 cons RMW
     "update": 8 * (21 + 9 + 16 + 14),
 }
-# DRAM bytes per face of the tuned flux kernel, measured by ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum = 129.5 MB for one launch of
-# 64 blocks x 19x18x18 faces, cold L2; profiles/flux_tuned_blast64blocks_ncu_full.md),
-# scaled to a full launch by the faces it computes
-FLUX_DRAM_BYTES_PER_FACE = 129.51e6 / (64 * 19 * 18 * 18)
+# Per-item counts of the tuned step measured by ncu on 64 blocks of the same
+# workload (profiles/step_dram_fp64_blast64blocks.md: one RK3 step between
+# cudaProfilerStart/Stop, every launch, cold L2 per kernel), scaled to a full
+# launch by the items it computes:
+#   the TMA-staged flux kernel (mean of the three directions), per face:
+FLUX_DRAM_BYTES_PER_FACE = 312.1      # dram__bytes_read.sum + dram__bytes_write.sum
+FLUX_FP64_FLOP_PER_FACE = 2234.7      # dadd + dmul + 2 dfma (thread instructions)
+FLUX_FP64_INST_PER_FACE = 1684.0      # dadd + dmul + dfma
+#   the whole RK3 step (54 launches), per zone-update:
+STEP_DRAM_BYTES_PER_ZU = 4661.4
+STEP_FP64_FLOP_PER_ZU = 15871.2
+STEP_FP64_INST_PER_ZU = 11460.3
+# algorithmic FP64 bytes per zone-update: 66 doubles on RK3 stage 1, 76 on
+# stages 2 and 3 (they also read the u^n combination), 581 B averaged
+ALGO_BYTES_PER_ZU = 581.0
 
 
 def parse():
@@ -529,8 +539,34 @@ def ours(args, rank, world, local_rank):
         roof = {"bound": "hbm", "kernel": name, "achieved": ach, "peak": hbm, "unit": "GB/s",
                 "frac": ach / hbm, "peak_source": peak_src, "traffic": traffic,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "items_per_launch": items[name],
-                "launch_ms": per_launch_ms,
-                "note": "FP64 arithmetic, not HBM, binds this kernel (see profiles/)"}
+                "launch_ms": per_launch_ms}
+        if name == "flux" and args.mode == "tuned":
+            # the FP64 roofline of the same launches: flops and FP64
+            # instructions per face from ncu, time from the events above,
+            # against the FMA throughput measured on this GPU (2 flops or 1
+            # instruction per lane per clock)
+            fl = FLUX_FP64_FLOP_PER_FACE * items[name] / (per_launch_ms * 1e-3) / 1e12
+            ins = FLUX_FP64_INST_PER_FACE * items[name] / (per_launch_ms * 1e-3) / 1e12
+            roof["fp64"] = {"achieved": fl, "peak": fp64_peak["tflops"], "unit": "TFLOP/s",
+                            "frac": fl / fp64_peak["tflops"],
+                            "issue_frac": ins / (fp64_peak["tflops"] / 2.0),
+                            "flop_per_face": FLUX_FP64_FLOP_PER_FACE, "inst_per_face": FLUX_FP64_INST_PER_FACE,
+                            "peak_source": "measured (grb_measure_fp64_peak)"}
+            roof["binding"] = (f"FP64 pipe: its FP64 instructions issue at {roof['fp64']['issue_frac']:.0%} of the "
+                               f"measured FMA rate ({roof['fp64']['frac']:.0%} in flops: DADD/DMUL count one flop "
+                               f"an issue), HBM at {ach / hbm:.0%}")
+        # the whole step against both rooflines
+        zu_s = value / world
+        roof_step = {
+            "algorithmic_bytes_per_zone_update": ALGO_BYTES_PER_ZU,
+            "dram_bytes_per_zone_update": STEP_DRAM_BYTES_PER_ZU,
+            "fp64_flop_per_zone_update": STEP_FP64_FLOP_PER_ZU,
+            "hbm_frac_algorithmic": ALGO_BYTES_PER_ZU * zu_s / 1e9 / hbm,
+            "hbm_frac_dram": STEP_DRAM_BYTES_PER_ZU * zu_s / 1e9 / hbm,
+            "fp64_frac": STEP_FP64_FLOP_PER_ZU * zu_s / 1e12 / fp64_peak["tflops"],
+            "fp64_issue_frac": STEP_FP64_INST_PER_ZU * zu_s / 1e12 / (fp64_peak["tflops"] / 2.0),
+            "source": "per-zone-update counts of one tuned RK3 step on 64 blocks (ncu), rates of this run"}
+        roof["step"] = roof_step
 
     # --- c2p micro-benchmark (2^24 states): plain, then with the learned
     # bracket trained on the GPU from 2^20 other seeded states
