@@ -93,6 +93,17 @@ class Status(C.Structure):
                 ("launches", C.c_int64)]
 
 
+class Reflux(C.Structure):
+    _fields_ = [("nfaces", C.c_int64), ("face_coarse_q", C.c_void_p), ("face_coarse_id", C.c_void_p),
+                ("face_fine_q", C.c_void_p),
+                ("nsame_faces", C.c_int64), ("same_face_q", C.c_void_p), ("same_face_id", C.c_void_p),
+                ("same_level_flux_average", C.c_int32),
+                ("nedges", C.c_int64), ("edge_nsides", C.c_void_p), ("edge_id", C.c_void_p),
+                ("edge_is_fine", C.c_void_p), ("edge_q", C.c_void_p), ("edge_off", C.c_void_p),
+                ("nsame_edges", C.c_int64), ("same_edge_nsides", C.c_void_p), ("same_edge_id", C.c_void_p),
+                ("same_edge_q", C.c_void_p)]
+
+
 class C2PDiag(C.Structure):
     _fields_ = [("iters", C.c_void_p), ("guess_used", C.c_void_p), ("mu", C.c_void_p),
                 ("bracket", C.c_void_p)]
@@ -160,6 +171,7 @@ PROTOTYPES = {
     "grb_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
     "grb_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "grb_set_fofc_list_capacity": (C.c_int, [C.c_void_p, C.c_int64]),
+    "grb_set_reflux": (C.c_int, [C.c_void_p, C.POINTER(Reflux)]),
     "grb_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "grb_measure_fp64_peak": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "grb_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),

@@ -21,6 +21,7 @@
 #include "amr.cuh"
 #include "outflow.cuh"
 #include "flux_tma.cuh"
+#include "reflux.cuh"
 #include "mlp.cuh"
 #include "stage_kernels.cuh"
 
@@ -69,6 +70,13 @@ struct grb_handle {
   float tune_aux_queue_ms = 0.f;
   bool mlp_ready = false;
   uint32_t fcap_alloc = 0;  // entries allocated for the compacted FOFC face list
+  // refluxing (grb_set_reflux): the caller's descriptor lists and the edge
+  // accumulation buffers
+  bool reflux = false;
+  bool reflux_flux_same = false;
+  RefluxDev rf{};
+  double* d_refacc = nullptr;
+  size_t refacc_bytes = 0;
 };
 
 namespace {
@@ -399,6 +407,40 @@ const double* static_metric(const grb_handle* h, const Geo& G, const double* idx
   return std::equal(key, key + 4, h->metder_key) ? h->d_metder : nullptr;
 }
 
+// Refluxing of the stage (grb_set_reflux): the fluxes after FOFC, the edge
+// EMFs after the update.  Returns the kernels launched.
+int reflux_fluxes(grb_handle* h, const Geo& G, cudaStream_t s, const StageBufs& B) {
+  if (!h->reflux) return 0;
+  const RefluxDev& R = h->rf;
+  const int64_t n2 = (int64_t)G.nx * G.nx * GRB_N_HRSC;
+  int l = 0;
+  if (R.nfaces) { k_reflux_faces<<<nblk(n2 * R.nfaces, 128), 128, 0, s>>>(G, R, B.flux); ++l; }
+  if (R.nsame && h->reflux_flux_same) {
+    k_reflux_same_faces<<<nblk(n2 * R.nsame, 128), 128, 0, s>>>(G, R, B.flux);
+    ++l;
+  }
+  return l;
+}
+int reflux_emfs(grb_handle* h, const Geo& G, cudaStream_t s, const StageBufs& B) {
+  if (!h->reflux) return 0;
+  const RefluxDev& R = h->rf;
+  const int64_t n = G.nx;
+  int l = 0;
+  if (R.nfaces) { k_reflux_emf_faces<<<nblk(n / 2 * (n / 2) * R.nfaces, 128), 128, 0, s>>>(G, R, B.emf); ++l; }
+  if (R.nsame) { k_reflux_emf_same_faces<<<nblk(n * n * R.nsame, 128), 128, 0, s>>>(G, R, B.emf); ++l; }
+  if (R.nedges) {
+    k_reflux_emf_edges_compute<<<nblk(n * R.nedges, 128), 128, 0, s>>>(G, R, B.emf);
+    k_reflux_emf_edges_apply<<<nblk(n * R.nedges, 128), 128, 0, s>>>(G, R, B.emf);
+    l += 2;
+  }
+  if (R.nsame_edges) {
+    k_reflux_emf_same_edges_compute<<<nblk(n * R.nsame_edges, 128), 128, 0, s>>>(G, R, B.emf);
+    k_reflux_emf_same_edges_apply<<<nblk(n * R.nsame_edges, 128), 128, 0, s>>>(G, R, B.emf);
+    l += 2;
+  }
+  return l;
+}
+
 // Grid of the FOFC list kernel: three 128-thread CTAs per SM (its register
 // footprint) for a grid-stride loop over the listed faces.
 static unsigned fofc_list_grid() {
@@ -474,12 +516,20 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
       launches += 2;
     }
   }
+  if (h->reflux) {
+    KScope ks(h, s, GRB_KIND_OTHER);
+    launches += reflux_fluxes(h, G, s, B);
+  }
   const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, G.nq);
   {
     KScope ks(h, s, GRB_KIND_UPDATE);
     launch_update_tuned(h->var_update, nblk(ub.count(), T), s, P, G, ub, dt, dtfact, nw->state, old->state,
                         aux, g->idx, B, static_metric(h, G, g->idx));
     ++launches;
+  }
+  if (h->reflux) {
+    KScope ks(h, s, GRB_KIND_OTHER);
+    launches += reflux_emfs(h, G, s, B);
   }
   {
     KScope ks(h, s, GRB_KIND_CT);
@@ -588,6 +638,7 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_ghostruns);
   cudaFree(h->d_stage_io);
   cudaFree(h->d_metder);
+  cudaFree(h->d_refacc);
   delete h;
   return GRB_OK;
 }
@@ -715,10 +766,18 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt, d
     k_fofc_edges<<<nblk(fb.count(), T), T, 0, s>>>(G, fb, B); ++h->launches;
     }
   }
+  if (h->reflux) {
+    KScope ks(h, s, GRB_KIND_OTHER);
+    h->launches += reflux_fluxes(h, G, s, B);
+  }
   const Box ub = box(gz, gz, gz, G.nx, G.ny, G.nz, G.nq);
   {
   KScope ks(h, s, GRB_KIND_UPDATE);
   k_update<1><<<nblk(ub.count(), T), T, 0, s>>>(P, G, ub, dt, dtfact, nw->state, old->state, aux, g->idx, B); ++h->launches;
+  }
+  if (h->reflux) {
+    KScope ks(h, s, GRB_KIND_OTHER);
+    h->launches += reflux_emfs(h, G, s, B);
   }
   {
   KScope ks(h, s, GRB_KIND_CT);
@@ -1610,6 +1669,52 @@ int grb_accumulate_boundary_outflow(grb_handle* h, const grb_grid* g, int64_t nf
   k_boundary_outflow<<<(unsigned)nfaces, kOutflowThreads, 0, s>>>(G, h->B.flux, quad, face, dx, dt * dtfact, outflow);
   ++h->launches;
   CK(cudaGetLastError());
+  return GRB_OK;
+}
+
+int grb_set_reflux(grb_handle* h, const grb_reflux* r) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!r || (r->nfaces == 0 && r->nsame_faces == 0 && r->nedges == 0 && r->nsame_edges == 0)) {
+    h->reflux = false;
+    h->rf = RefluxDev{};
+    return GRB_OK;
+  }
+  if (!h->reserved) return fail(h, GRB_ERR_NOT_RESERVED);
+  const Geo& G = h->geo;
+  if (G.nx != G.ny || G.nx != G.nz || G.nx % 2 || r->nfaces < 0 || r->nsame_faces < 0 || r->nedges < 0 ||
+      r->nsame_edges < 0)
+    return fail(h, GRB_ERR_INVALID);
+  if ((r->nfaces && (!r->face_coarse_q || !r->face_coarse_id || !r->face_fine_q)) ||
+      (r->nsame_faces && (!r->same_face_q || !r->same_face_id)) ||
+      (r->nedges && (!r->edge_nsides || !r->edge_id || !r->edge_is_fine || !r->edge_q || !r->edge_off)) ||
+      (r->nsame_edges && (!r->same_edge_nsides || !r->same_edge_id || !r->same_edge_q)))
+    return fail(h, GRB_ERR_INVALID);
+  const size_t need = sizeof(double) * (size_t)G.nx * (2 * (size_t)r->nedges + (size_t)r->nsame_edges);
+  if (need > h->refacc_bytes) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(nullptr, &cs) == cudaSuccess && cs != cudaStreamCaptureStatusNone)
+      return fail(h, GRB_ERR_INVALID);
+    cudaFree(h->d_refacc);
+    h->d_refacc = nullptr;
+    h->refacc_bytes = 0;
+    if (cudaMalloc(&h->d_refacc, need) != cudaSuccess) {
+      cudaGetLastError();
+      return fail(h, GRB_ERR_NOMEM);
+    }
+    h->refacc_bytes = need;
+  }
+  RefluxDev R{};
+  R.nfaces = r->nfaces; R.face_cq = r->face_coarse_q; R.face_cid = r->face_coarse_id; R.face_fq = r->face_fine_q;
+  R.nsame = r->nsame_faces; R.same_q = r->same_face_q; R.same_id = r->same_face_id;
+  R.nedges = r->nedges; R.edge_ns = r->edge_nsides; R.edge_id = r->edge_id; R.edge_fine = r->edge_is_fine;
+  R.edge_q = r->edge_q; R.edge_off = r->edge_off;
+  R.nsame_edges = r->nsame_edges; R.sedge_ns = r->same_edge_nsides; R.sedge_id = r->same_edge_id;
+  R.sedge_q = r->same_edge_q;
+  R.acc_edges = h->d_refacc;
+  R.acc_same_edges = h->d_refacc + (size_t)G.nx * 2 * (size_t)r->nedges;
+  h->rf = R;
+  h->reflux_flux_same = r->same_level_flux_average != 0;
+  h->reflux = true;
   return GRB_OK;
 }
 

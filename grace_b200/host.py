@@ -381,6 +381,26 @@ class GRMHDEquationsSystem:
         v = (ctypes.c_int32 * 4)(flux, flag, update, aux)
         _lib.check(self.lib.grb_set_tuning(self.h, v), "grb_set_tuning")
 
+    def set_reflux(self, lists=None, same_level_flux_average=False):
+        """Reflux descriptor lists (grb_set_reflux): a dict of numpy arrays in
+        the grb_reflux layout (grace_b200.fmr.Hierarchy.reflux_lists), copied
+        to the device and kept by this object; None turns refluxing off."""
+        if lists is None:
+            _lib.check(self.lib.grb_set_reflux(self.h, None), "grb_set_reflux")
+            self._reflux = None
+            return
+        dev = self.blocks.device
+        d = {k: torch.from_numpy(v.copy()).to(dev) for k, v in lists.items()}
+        self._reflux = d  # the library reads these arrays on every substep
+        P = lambda k: d[k].data_ptr() if d[k].numel() else None
+        r = abi.Reflux(len(d["face_coarse_q"]), P("face_coarse_q"), P("face_coarse_id"), P("face_fine_q"),
+                       len(d["same_face_q"]) // 2, P("same_face_q"), P("same_face_id"),
+                       1 if same_level_flux_average else 0,
+                       len(d["edge_nsides"]), P("edge_nsides"), P("edge_id"), P("edge_is_fine"), P("edge_q"),
+                       P("edge_off"),
+                       len(d["same_edge_nsides"]), P("same_edge_nsides"), P("same_edge_id"), P("same_edge_q"))
+        _lib.check(self.lib.grb_set_reflux(self.h, ctypes.byref(r)), "grb_set_reflux")
+
     def set_fofc_list_capacity(self, faces):
         """Capacity of the compacted FOFC face list of the tuned stage
         (grb_set_fofc_list_capacity); 0 forces the whole-box recompute."""

@@ -262,3 +262,44 @@ def c2p_states(n, seed=SEED, kappa=100.0, gamma=2.0, gamma_th=1.8):
     prims[abi.P_TEMP], prims[abi.P_ENT] = T, s
     prims[abi.P_BX:abi.P_BZ + 1] = B
     return cons, prims
+
+
+def fmr_blast(hier, bx0=0.1, r0=0.8, gamma=4.0 / 3.0, flow=0.0):
+    """The blast wave (Gamma=4/3, rho=1e-4 / p=5e-4 outside, rho=1e-2 / p=1
+    inside r<r0, uniform Bx) on the leaves of a static FMR hierarchy
+    (grace_b200.fmr.Hierarchy), with a smooth 1e-3 relative pressure ripple
+    instead of cell noise so that every level samples the same field; flow:
+    amplitude of a smooth shearing velocity (W v = flow x (sin 0.7y,
+    sin 0.9z, sin 1.1x)) that makes the EMFs nonzero from the first
+    substep.  Returns (state, bx, by, bz, aux) in the library layout."""
+    NN = hier.n + 2 * hier.ngz
+    nq = hier.nq
+    state = np.zeros((nq, abi.N_EVOL_VARS, NN, NN, NN))
+    bx = np.full((nq, NN, NN, NN + 1), bx0)
+    by = np.zeros((nq, NN, NN + 1, NN))
+    bz = np.zeros((nq, NN + 1, NN, NN))
+    aux = np.zeros((nq, abi.N_AUX_VARS, NN, NN, NN))
+    state[:, abi.GXX] = state[:, abi.GYY] = state[:, abi.GZZ] = 1.0
+    state[:, abi.ALP] = 1.0
+    X = hier.cell_centres()
+    r = np.sqrt(np.sum(X * X, axis=1))
+    inside = r < r0
+    rho = np.where(inside, 1e-2, 1e-4)
+    press = np.where(inside, 1.0, 5e-4) * (1.0 + 1e-3 * np.sin(1.3 * X[:, 0]) * np.cos(0.7 * X[:, 1] + 0.4 * X[:, 2]))
+    eps = press / ((gamma - 1.0) * rho)
+    s = np.log(eps) / (gamma - 1.0) - np.log(rho)
+    z = np.zeros((3,) + rho.shape)
+    if flow:
+        z[0] = flow * np.sin(0.7 * X[:, 1])
+        z[1] = flow * np.sin(0.9 * X[:, 2])
+        z[2] = flow * np.sin(1.1 * X[:, 0])
+    Bc = np.zeros((3,) + rho.shape)
+    Bc[0] = bx0
+    cons = flat_prims_to_cons(rho, press, eps, z, Bc, s)
+    aux[:, abi.ZVECX:abi.ZVECZ + 1] = np.moveaxis(z, 0, 1)
+    state[:, 0:7] = np.moveaxis(cons, 0, 1)
+    aux[:, abi.RHO], aux[:, abi.PRESS], aux[:, abi.EPS] = rho, press, eps
+    aux[:, abi.TEMP] = eps * (gamma - 1.0)
+    aux[:, abi.ENTROPY] = s
+    aux[:, abi.BX] = bx0
+    return state, bx, by, bz, aux

@@ -558,6 +558,68 @@ int grb_prolong_to_ghosts(grb_handle* h, const grb_grid* g, const grb_fields* fi
                           const int8_t* have_fine, const int32_t* vars_lo, int32_t nlo,
                           const int32_t* vars_ho, int32_t nho, void* stream);
 
+/* ---- reflux at coarse-fine interfaces ------------------------------------ */
+/* The reflux descriptors of the caller's AMR hierarchy on this rank: what
+ * GRACE's ghost layer builds from the p4est face and edge iterators
+ * (include/grace/amr/amr_ghosts.hh:190-330, src/amr/ghost_helpers/
+ * iterate_faces.cpp:150-280, iterate_edges.cpp:330-407), here as device
+ * arrays of block indices.  Blocks are cubic.  Face ids are 2 axis + side
+ * (side 1 the upper face); edge ids are p4est's (4 axis + s_a + 2 s_b, with
+ * s_a, s_b the sides along the edge's two other axes in x, y, z order). */
+typedef struct grb_reflux {
+  /* hanging faces: face face_coarse_id[i] of block face_coarse_q[i] is
+   * covered by the four blocks face_fine_q[4 i + c] of the next finer level,
+   * c = a + 2 b with a, b the halves along the face's other two axes (x
+   * before y before z); each touches it with its opposite face */
+  int64_t nfaces;
+  const int64_t* face_coarse_q;
+  const uint8_t* face_coarse_id;
+  const int64_t* face_fine_q;
+  /* faces between blocks of the same level: blocks same_face_q[2 i + s]
+   * meet with their faces same_face_id[2 i + s], s = 0, 1 */
+  int64_t nsame_faces;
+  const int64_t* same_face_q;
+  const uint8_t* same_face_id;
+  /* average the fluxes of same-level faces too (the reference's
+   * GRACE_SAME_LEVEL_FACE_AVERAGE build option); EMFs always are */
+  int32_t same_level_flux_average;
+  /* hanging edges (blocks of two levels along one edge, and the two middle
+   * lines of each hanging face): edge_nsides[i] <= 4 sides; side s has the
+   * edge id edge_id[4 i + s] in its block(s), edge_is_fine[4 i + s] set
+   * when it holds the two finer blocks edge_q[8 i + 2 s + c] (c the lower,
+   * upper half along the edge), else one coarser block edge_q[8 i + 2 s]
+   * whose edge cell other axes move to the block's middle where
+   * edge_off[8 i + 2 s + 0 / 1] is set (middle lines of a hanging face) */
+  int64_t nedges;
+  const uint8_t* edge_nsides;
+  const uint8_t* edge_id;
+  const uint8_t* edge_is_fine;
+  const int64_t* edge_q;
+  const uint8_t* edge_off;
+  /* edges between blocks of one level: same_edge_nsides[i] <= 4 sides, side
+   * s is edge same_edge_id[4 i + s] of block same_edge_q[4 i + s] */
+  int64_t nsame_edges;
+  const uint8_t* same_edge_nsides;
+  const uint8_t* same_edge_id;
+  const int64_t* same_edge_q;
+} grb_reflux;
+/* = the refluxing of advance_substep (src/evolution/evolve.cpp:1690-1705,
+ *   src/evolution/refluxing.cpp:528-1170, the local branches): from now on
+ *   every grb_advance_substep on this handle, after FOFC and before the flux
+ *   divergence, replaces the coarse flux on each hanging face by the area
+ *   average of the fine fluxes (and averages same-level faces' fluxes if
+ *   asked), and after the update, before the CT update, makes the edge EMFs
+ *   of every interface agree (hanging faces' inner lines from the fine
+ *   EMFs, same-level faces' inner lines by the mean of both sides, hanging
+ *   and same-level edges by the rule of the reference: the fine, or the
+ *   first, side in edge-id order).  The arrays are the caller's and are read
+ *   by every later substep (keep them alive and unchanged, or set again);
+ *   the handle allocates its edge accumulation buffers here (call before any
+ *   stream capture).  r = NULL, or all counts 0, turns refluxing off.
+ *   Requires grb_reserve and cubic blocks.  The MPI exchange of remote
+ *   sides stays with the caller. */
+int grb_set_reflux(grb_handle* h, const grb_reflux* r);
+
 /* ---- scratch-free stage -------------------------------------------------- */
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
  * (a host code whose GPU memory is owned up front by a pooling allocator, or

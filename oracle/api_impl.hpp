@@ -44,6 +44,21 @@ int API(compute_aux)(void* hh, const double* idx, const double* coords, double* 
   st.compute_aux(mk(s, bx, by, bz), aux);
   return st.fatal;
 }
+// Reflux descriptor lists (the layout of grb_reflux, host arrays, copied).
+void API(set_reflux)(void* hh, int64_t nfaces, const int64_t* fcq, const uint8_t* fcid, const int64_t* ffq,
+                     int64_t nsame, const int64_t* sq, const uint8_t* sid, int32_t flux_same, int64_t nedges,
+                     const uint8_t* ens, const uint8_t* eid, const uint8_t* efine, const int64_t* eq,
+                     const uint8_t* eoff, int64_t nsedges, const uint8_t* sens, const uint8_t* seid,
+                     const int64_t* seq) {
+  auto& r = static_cast<Handle*>(hh)->st.rf;
+  auto cp = [](auto& v, const auto* p, int64_t n) { v.assign(p, p + (p ? n : 0)); };
+  cp(r.face_cq, fcq, nfaces); cp(r.face_cid, fcid, nfaces); cp(r.face_fq, ffq, 4 * nfaces);
+  cp(r.same_q, sq, 2 * nsame); cp(r.same_id, sid, 2 * nsame);
+  r.flux_same = flux_same != 0;
+  cp(r.edge_ns, ens, nedges); cp(r.edge_id, eid, 4 * nedges); cp(r.edge_fine, efine, 4 * nedges);
+  cp(r.edge_q, eq, 8 * nedges); cp(r.edge_off, eoff, 8 * nedges);
+  cp(r.sedge_ns, sens, nsedges); cp(r.sedge_id, seid, 4 * nsedges); cp(r.sedge_q, seq, 4 * nsedges);
+}
 void API(reset_diag)(void* hh, double* aux) { static_cast<Handle*>(hh)->st.reset_diag(aux); }
 double API(find_stable_timestep)(void* hh, double* s, const double* aux, const double* dx, double cfl) {
   return static_cast<Handle*>(hh)->st.find_stable_timestep(mk(s, nullptr, nullptr, nullptr), aux, dx, cfl);

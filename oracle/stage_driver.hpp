@@ -58,6 +58,12 @@ struct Stage {
   std::vector<int8_t> ftag, etag;
   int fatal = 0;
   int64_t n_fofc_faces = 0, n_fofc_edges = 0;
+  // reflux descriptors (grb_reflux, host copies); empty: no refluxing
+  struct Reflux {
+    std::vector<int64_t> face_cq, face_fq, same_q, edge_q, sedge_q;
+    std::vector<uint8_t> face_cid, same_id, edge_ns, edge_id, edge_fine, edge_off, sedge_ns, sedge_id;
+    bool flux_same = false;
+  } rf;
 
   Stage(const grb_params& p, const Dims& dd) : P(p), eos(N::make_eos(p.eos)), d(dd) {
     flux.assign(d.fcells() * 7 * 3 * d.nq, 0.0);
@@ -500,8 +506,174 @@ struct Stage {
           }
   }
 
-  // advance_substep (evolve.cpp:1671-1717); reflux is a no-op without
-  // coarse-fine faces.
+  // ---- refluxing (refluxing.cpp:528-1170, local branches) --------------
+  static int odir(int axis, int which) { return which == 0 ? (axis == 0 ? 1 : 0) : (axis == 2 ? 1 : 2); }
+  // reflux_correct_fluxes: the coarse flux on a hanging face := 0.25 x the
+  // sum of the 4 fine fluxes (loop order x, y, z); same-level faces (the
+  // GRACE_SAME_LEVEL_FACE_AVERAGE option): the mean of the two sides.
+  void reflux_fluxes() {
+    const int n = d.nx, g = d.g;
+    const int64_t nf = (int64_t)rf.face_cq.size();
+    for (int64_t iq = 0; iq < nf; ++iq)
+      for (int v = 0; v < 7; ++v)
+        for (int j = 0; j < n; ++j)
+          for (int i = 0; i < n; ++i) {
+            const int face = rf.face_cid[iq], dir = face / 2;
+            int c[3], f[3];
+            c[dir] = (face & 1) ? g + n : g;
+            c[odir(dir, 0)] = g + i;
+            c[odir(dir, 1)] = g + j;
+            const int child = (2 * i >= n) + 2 * (2 * j >= n);
+            const int64_t qf = rf.face_fq[4 * iq + child];
+            f[dir] = (face & 1) ? g : g + n;
+            f[odir(dir, 0)] = g + (2 * i) % n;
+            f[odir(dir, 1)] = g + (2 * j) % n;
+            double s = 0.0;
+            for (int ii = 0; ii <= (dir != 0); ++ii)
+              for (int jj = 0; jj <= (dir != 1); ++jj)
+                for (int kk = 0; kk <= (dir != 2); ++kk) s += F(f[0] + ii, f[1] + jj, f[2] + kk, v, dir, qf);
+            s *= 0.25;
+            F(c[0], c[1], c[2], v, dir, rf.face_cq[iq]) = s;
+          }
+    if (!rf.flux_same) return;
+    const int64_t ns = (int64_t)rf.same_q.size() / 2;
+    for (int64_t iq = 0; iq < ns; ++iq)
+      for (int v = 0; v < 7; ++v)
+        for (int j = 0; j < n; ++j)
+          for (int i = 0; i < n; ++i) {
+            double* at[2];
+            double s = 0.0;
+            for (int is = 0; is < 2; ++is) {
+              const int fid = rf.same_id[2 * iq + is], fdir = fid / 2;
+              int c[3];
+              c[fdir] = (fid & 1) ? n + g : g;
+              c[odir(fdir, 0)] = g + i;
+              c[odir(fdir, 1)] = g + j;
+              at[is] = &F(c[0], c[1], c[2], v, fdir, rf.same_q[2 * iq + is]);
+              s += *at[is];
+            }
+            s *= 0.5;
+            *at[0] = s;
+            *at[1] = s;
+          }
+  }
+  double& edge_em(int eid, int i, bool off_i, bool off_j, int64_t q) {
+    const int n = d.nx, g = d.g, edir = eid / 4;
+    int c[3];
+    c[edir] = g + i;
+    c[odir(edir, 0)] = off_i ? n / 2 + g : ((eid & 1) ? n + g : g);
+    c[odir(edir, 1)] = off_j ? n / 2 + g : (((eid >> 1) & 1) ? n + g : g);
+    return EM(c[0], c[1], c[2], edir, q);
+  }
+  // reflux_correct_emfs: hanging faces' inner lines, same-level faces'
+  // inner lines, hanging edges, same-level edges, in that order
+  void reflux_emfs() {
+    const int n = d.nx, g = d.g, h = n / 2;
+    const int64_t nf = (int64_t)rf.face_cq.size();
+    for (int64_t iq = 0; iq < nf; ++iq)
+      for (int j = 0; j < h; ++j)
+        for (int i = 0; i < h; ++i) {
+          const int face = rf.face_cid[iq];
+          const int fdir = face / 2, idir = odir(fdir, 0), jdir = odir(fdir, 1), side = face & 1;
+          for (int ch = 0; ch < 4; ++ch) {
+            const int64_t qf = rf.face_fq[4 * iq + ch];
+            int f[3], c[3];
+            f[fdir] = side ? g : n + g;
+            f[idir] = 2 * i + g;
+            f[jdir] = 2 * j + g;
+            const double ei = 0.5 * (EM(f[0], f[1], f[2], idir, qf) +
+                                     EM(f[0] + (idir == 0), f[1] + (idir == 1), f[2] + (idir == 2), idir, qf));
+            const double ej = 0.5 * (EM(f[0], f[1], f[2], jdir, qf) +
+                                     EM(f[0] + (jdir == 0), f[1] + (jdir == 1), f[2] + (jdir == 2), jdir, qf));
+            c[fdir] = side ? n + g : g;
+            c[idir] = i + ((ch & 1) ? h : 0) + g;
+            c[jdir] = j + ((ch & 2) ? h : 0) + g;
+            if (c[jdir] != h + g && c[jdir] != g) EM(c[0], c[1], c[2], idir, rf.face_cq[iq]) = ei;
+            if (c[idir] != h + g && c[idir] != g) EM(c[0], c[1], c[2], jdir, rf.face_cq[iq]) = ej;
+          }
+        }
+    const int64_t ns = (int64_t)rf.same_q.size() / 2;
+    for (int64_t iq = 0; iq < ns; ++iq)
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) {
+          double s0 = 0.0, s1 = 0.0;
+          double *a0[2], *a1[2];
+          bool w0[2], w1[2];
+          for (int is = 0; is < 2; ++is) {
+            const int fid = rf.same_id[2 * iq + is], fdir = fid / 2, idir = odir(fdir, 0), jdir = odir(fdir, 1);
+            const int64_t q = rf.same_q[2 * iq + is];
+            int c[3];
+            c[fdir] = (fid & 1) ? n + g : g;
+            c[idir] = g + i;
+            c[jdir] = g + j;
+            a0[is] = &EM(c[0], c[1], c[2], idir, q);
+            a1[is] = &EM(c[0], c[1], c[2], jdir, q);
+            w0[is] = c[jdir] > g;
+            w1[is] = c[idir] > g;
+            s0 += *a0[is];
+            s1 += *a1[is];
+          }
+          s0 *= 0.5;
+          s1 *= 0.5;
+          for (int is = 0; is < 2; ++is) {
+            if (w0[is]) *a0[is] = s0;
+            if (w1[is]) *a1[is] = s1;
+          }
+        }
+    // hanging edges: the fine side of smallest edge id gives every side's value
+    const int64_t ne = (int64_t)rf.edge_ns.size();
+    std::vector<double> acc((size_t)ne * 2 * n);
+    for (int64_t iq = 0; iq < ne; ++iq)
+      for (int i = 0; i < n; ++i) {
+        int best = 256;
+        double v0 = 0.0, v1 = 0.0;
+        for (int s = 0; s < rf.edge_ns[iq]; ++s) {
+          if (!rf.edge_fine[4 * iq + s]) continue;
+          const int eid = rf.edge_id[4 * iq + s];
+          if (eid >= best) continue;
+          best = eid;
+          v0 = edge_em(eid, i, false, false, rf.edge_q[8 * iq + 2 * s]);
+          v1 = edge_em(eid, i, false, false, rf.edge_q[8 * iq + 2 * s + 1]);
+        }
+        acc[(2 * iq) * n + i] = v0;
+        acc[(2 * iq + 1) * n + i] = v1;
+      }
+    for (int64_t iq = 0; iq < ne; ++iq)
+      for (int i = 0; i < n; ++i)
+        for (int s = 0; s < rf.edge_ns[iq]; ++s) {
+          const int eid = rf.edge_id[4 * iq + s];
+          const double* a = acc.data() + 2 * iq * n;
+          if (!rf.edge_fine[4 * iq + s]) {
+            const int ch = (2 * i) >= n, k = (2 * i) % n;
+            edge_em(eid, i, rf.edge_off[8 * iq + 2 * s] != 0, rf.edge_off[8 * iq + 2 * s + 1] != 0,
+                    rf.edge_q[8 * iq + 2 * s]) = 0.5 * (a[ch * n + k] + a[ch * n + k + 1]);
+          } else {
+            for (int ch = 0; ch < 2; ++ch) edge_em(eid, i, false, false, rf.edge_q[8 * iq + 2 * s + ch]) = a[ch * n + i];
+          }
+        }
+    // same-level edges: the side of smallest edge id
+    const int64_t nse = (int64_t)rf.sedge_ns.size();
+    std::vector<double> sacc((size_t)nse * n);
+    for (int64_t iq = 0; iq < nse; ++iq)
+      for (int i = 0; i < n; ++i) {
+        int best = 256;
+        double v = 0.0;
+        for (int s = 0; s < rf.sedge_ns[iq]; ++s) {
+          const int eid = rf.sedge_id[4 * iq + s];
+          if (eid >= best) continue;
+          best = eid;
+          v = edge_em(eid, i, false, false, rf.sedge_q[4 * iq + s]);
+        }
+        sacc[iq * n + i] = v;
+      }
+    for (int64_t iq = 0; iq < nse; ++iq)
+      for (int i = 0; i < n; ++i)
+        for (int s = 0; s < rf.sedge_ns[iq]; ++s)
+          edge_em(rf.sedge_id[4 * iq + s], i, false, false, rf.sedge_q[4 * iq + s]) = sacc[iq * n + i];
+  }
+
+  // advance_substep (evolve.cpp:1671-1717), with refluxing when descriptor
+  // lists are set
   void advance_substep(double dt, double dtfact, const Fields& nw, const Fields& old,
                        const double* aux) {
     compute_fluxes(old, aux);
@@ -510,7 +682,9 @@ struct Stage {
       flag_fofc(dt, dtfact, nw, old);
       apply_fofc(old, aux);
     }
+    reflux_fluxes();
     add_fluxes_and_sources(dt, dtfact, nw, old, aux);
+    reflux_emfs();
     update_ct(dt, dtfact, nw);
   }
 

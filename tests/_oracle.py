@@ -29,6 +29,8 @@ def _bind(lib, pre):
         "scratch": (C.c_int64, [VP, C.c_int, VP]),
         "boundary_outflow": (C.c_double, [VP, C.c_int64, VP, VP, VP, C.c_double, C.c_double]),
         "fofc_counts": (None, [VP, P(C.c_int64), P(C.c_int64)]),
+        "set_reflux": (None, [VP, C.c_int64, VP, VP, VP, C.c_int64, VP, VP, C.c_int32, C.c_int64, VP, VP, VP, VP, VP,
+                              C.c_int64, VP, VP, VP]),
         "c2p_batch": (C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP, VP, VP, VP, C.c_int32, VP]),
         "prims_to_conservs": (C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP]),
         "eos_press_eps_csnd2_temp_rho": (C.c_int, [P(abi.Params), C.c_int64, VP, VP, VP, VP, VP]),
@@ -214,6 +216,17 @@ class Stage:
     def linop(self, A, B, Cf, b, c):
         Cp = [p(x) for x in Cf] if Cf is not None else [None] * 4
         getattr(self.L, self.pre + "linop")(self.h, *[p(x) for x in A], *[p(x) for x in B], *Cp, b, c)
+
+    def set_reflux(self, r, flux_same=False):
+        """Reflux descriptor lists (the dict of grace_b200.fmr.Hierarchy.reflux_lists)."""
+        self._rf = {k: np.ascontiguousarray(v) for k, v in r.items()}  # kept alive
+        x = self._rf
+        getattr(self.L, self.pre + "set_reflux")(
+            self.h, len(x["face_coarse_q"]), p(x["face_coarse_q"]), p(x["face_coarse_id"]), p(x["face_fine_q"]),
+            len(x["same_face_q"]) // 2, p(x["same_face_q"]), p(x["same_face_id"]), 1 if flux_same else 0,
+            len(x["edge_nsides"]), p(x["edge_nsides"]), p(x["edge_id"]), p(x["edge_is_fine"]), p(x["edge_q"]),
+            p(x["edge_off"]), len(x["same_edge_nsides"]), p(x["same_edge_nsides"]), p(x["same_edge_id"]),
+            p(x["same_edge_q"]))
 
     def fofc_counts(self):
         f, e = C.c_int64(), C.c_int64()
