@@ -265,146 +265,187 @@ class Hierarchy:
                 "edge_off": u8(e_off),
                 "same_edge_nsides": u8(se_ns), "same_edge_id": u8(se_id), "same_edge_q": a64(se_q)}
 
-    # ---- composite ghost fill (host harness) ---------------------------------
-    def _maps(self):
-        """Per block: for every cell of the ghosted block a gather recipe
-        (source block, flat source cell indices, weight), built once."""
-        if hasattr(self, "_cell_maps"):
-            return self._cell_maps, self._face_maps
+    # ---- composite ghost fill ------------------------------------------------
+    def _lookup(self, P):
+        """Vectorised leaf_at over finest-lattice points P (m, 3) already
+        inside the domain: (level, qindex) arrays."""
+        lev = np.full(len(P), -1, dtype=np.int64)
+        qi = np.full(len(P), -1, dtype=np.int64)
+        for l in range(self.L, -1, -1):
+            mine = [(b, q) for q, (ll, b) in enumerate(self.leaves) if ll == l]
+            if not mine:
+                continue
+            E = self.E(l)
+            nbl = [self.nb0[a] * 2 ** l for a in range(3)]
+            key_of = lambda b: (b[2] * nbl[1] + b[1]) * nbl[0] + b[0]
+            keys = np.array([key_of(b) for b, _ in mine], dtype=np.int64)
+            qs = np.array([q for _, q in mine], dtype=np.int64)
+            order = np.argsort(keys)
+            keys, qs = keys[order], qs[order]
+            todo = lev < 0
+            B = P[todo] // E
+            k = (B[:, 2] * nbl[1] + B[:, 1]) * nbl[0] + B[:, 0]
+            pos = np.clip(np.searchsorted(keys, k), 0, len(keys) - 1)
+            hit = keys[pos] == k
+            idx = np.flatnonzero(todo)[hit]
+            lev[idx] = l
+            qi[idx] = qs[pos[hit]]
+        assert np.all(lev >= 0)
+        return lev, qi
+
+    def _domain(self, P):
+        """Wrap periodic axes, clamp the others into the domain (a ghost
+        cell outside a non-periodic boundary takes the data of the nearest
+        leaf cell: zero-gradient)."""
+        P = P.copy()
+        for a in range(3):
+            if self.periodic[a]:
+                P[:, a] %= self.N[a]
+            else:
+                P[:, a] = np.clip(P[:, a], 0, self.N[a] - 1)
+        return P
+
+    def gather_maps(self):
+        """Ghost-fill gather maps: for the cells (key "cells") and the face
+        arrays staggered along x, y, z (keys 0, 1, 2), arrays dst (m,) of flat
+        indices into one variable of the block arrays (q x cells per block +
+        local), src (m, 8) of flat source indices and w (m, 8) of weights
+        (unused slots weight 0 on the first source).  A ghost cell takes the
+        leaf data at its place: a copy from a same-level cell, the containing
+        coarser cell, or the mean of the 8 finer cells; a ghost face a copy,
+        the coarser face it lies on (or the linear interpolation between the
+        two coarser faces around it), or the mean of the 4 finer faces."""
+        if hasattr(self, "_gmaps"):
+            return self._gmaps
         n, g = self.n, self.ngz
         NN = n + 2 * g
-        self._cell_maps = []
-        self._face_maps = [[], [], []]
-        r = np.arange(NN)
-        for q, (l, b) in enumerate(self.leaves):
-            E = self.E(l)
-            s = E // n  # finest cells per cell of this level
-            K, J, I = np.meshgrid(r, r, r, indexing="ij")
-            ghost = (I < g) | (I >= n + g) | (J < g) | (J >= n + g) | (K < g) | (K >= n + g)
-            cells = []
-            for k, j, i in zip(K[ghost], J[ghost], I[ghost]):
-                # finest-lattice centre of this cell
-                p = [(b[0] * n + i - g) * s + s // 2, (b[1] * n + j - g) * s + s // 2, (b[2] * n + k - g) * s + s // 2]
-                t = self.leaf_at(p)
-                if t is None:
-                    cells.append((i, j, k, None))
-                    continue
-                cells.append((i, j, k, self._cell_source(t, p, s)))
-            self._cell_maps.append(cells)
-            for d in range(3):
-                shp = [NN, NN, NN]
-                shp[2 - d] += 1
-                KK, JJ, II = np.meshgrid(*[np.arange(x) for x in shp], indexing="ij")
-                idx = [II, JJ, KK]
-                gh = np.zeros(KK.shape, bool)
+        lv = np.array([l for l, _ in self.leaves], dtype=np.int64)
+        bb = np.array([b for _, b in self.leaves], dtype=np.int64)
+        out = {}
+        for arr in ("cells", 0, 1, 2):
+            shp = [NN, NN, NN]
+            if arr != "cells":
+                shp[arr] += 1  # extent along the staggered axis (x, y, z order)
+            per = shp[0] * shp[1] * shp[2]
+            K, J, I = np.meshgrid(np.arange(shp[2]), np.arange(shp[1]), np.arange(shp[0]), indexing="ij")
+            c = [I.ravel(), J.ravel(), K.ravel()]
+            gh = np.zeros(per, bool)
+            for a in range(3):
+                hi = n + g + (1 if arr == a else 0)
+                gh |= (c[a] < g) | (c[a] >= hi)
+            loc = np.flatnonzero(gh)
+            cl = [x[loc] for x in c]
+            Q = np.repeat(np.arange(self.nq), len(loc))
+            s = (np.array([self.E(l) for l in lv]) // n)[Q]
+            P = np.empty((len(Q), 3), dtype=np.int64)
+            for a in range(3):
+                ca = np.tile(cl[a], self.nq)
+                if arr == a:
+                    P[:, a] = (bb[Q, a] * n + ca - g) * s
+                else:
+                    P[:, a] = (bb[Q, a] * n + ca - g) * s + s // 2
+            dst = Q * per + np.tile(loc, self.nq)
+            if arr == "cells":
+                W = self._domain(P)
+                tl, tq = self._lookup(W)
+                st = (np.array([self.E(l) for l in range(self.L + 1)]) // n)[tl]
+                base_b = bb[tq]
+                src = np.zeros((len(Q), 8), dtype=np.int64)
+                w = np.zeros((len(Q), 8))
+                finer = st < s
+                li = lambda pts, a: pts[:, a] // st - base_b[:, a] * n + g
+                flat = lambda i, j, k: tq * per + (k * NN + j) * NN + i
+                f0 = flat(li(W, 0), li(W, 1), li(W, 2))
+                src[:] = f0[:, None]
+                w[:, 0] = np.where(finer, 0.125, 1.0)
+                for t_ in range(1, 8):
+                    off = np.array([t_ & 1, (t_ >> 1) & 1, t_ >> 2])
+                    Pc = W - (s // 2)[:, None] + off[None, :] * st[:, None]
+                    Pb = W - (s // 2)[:, None]
+                    f = flat(li(Pc, 0), li(Pc, 1), li(Pc, 2))
+                    src[finer, t_] = f[finer]
+                    w[finer, t_] = 0.125
+                # the finer case's first source is the (0,0,0) finer cell
+                fb = flat(li(Pb, 0), li(Pb, 1), li(Pb, 2))
+                src[finer, 0] = fb[finer]
+            else:
+                d = arr
+                W = P.copy()
+                top = np.zeros(len(W), bool)
                 for a in range(3):
-                    hi = n + g + (1 if a == d else 0)
-                    gh |= (idx[a] < g) | (idx[a] >= hi)
-                faces = []
-                for k, j, i in zip(KK[gh], JJ[gh], II[gh]):
-                    c = (i, j, k)
-                    p = [(b[a] * n + c[a] - g) * s + (0 if a == d else s // 2) for a in range(3)]
-                    faces.append((i, j, k, self._face_source(d, p, s)))
-                self._face_maps[d].append(faces)
-        return self._cell_maps, self._face_maps
+                    if self.periodic[a]:
+                        W[:, a] %= self.N[a]
+                    elif a == d:
+                        top = W[:, a] >= self.N[a]
+                        W[:, a] = np.clip(W[:, a], 0, self.N[a])
+                    else:
+                        W[:, a] = np.clip(W[:, a], 0, self.N[a] - 1)
+                Wl = W.copy()
+                Wl[top, d] -= 1  # the cell below a face on the upper boundary
+                tl, tq = self._lookup(Wl)
+                st = (np.array([self.E(l) for l in range(self.L + 1)]) // n)[tl]
+                base_b = bb[tq]
+                fd = W[:, d] - base_b[:, d] * n * st
+                lo_f = fd // st
+                frac = (fd - lo_f * st) / st
+                o1, o2 = ODIR[d]
 
-    def _cell_source(self, t, p, s):
-        lt, bt = t
-        n, g = self.n, self.ngz
-        st = self.E(lt) // n
-        w = self.wrap(p)
-        qs = self.index[t]
-        if st == s:
-            return qs, [tuple(w[a] // st - bt[a] * n + g for a in range(3))], 1.0
-        if st > s:  # coarser: the containing cell
-            return qs, [tuple(w[a] // st - bt[a] * n + g for a in range(3))], 1.0
-        # finer: the 8 cells of the finer level inside this cell
-        base = [w[a] - s // 2 for a in range(3)]
-        cs = []
-        for dz in (0, 1):
-            for dy in (0, 1):
-                for dx_ in (0, 1):
-                    off = (dx_, dy, dz)
-                    cs.append(tuple((base[a] + off[a] * st) // st - bt[a] * n + g for a in range(3)))
-        return qs, cs, 0.125
+                def flatf(i3):
+                    ext = list(shp)
+                    return tq * per + (i3[2] * ext[1] + i3[1]) * ext[0] + i3[0]
 
-    def _face_source(self, d, p, s):
-        """Face of axis d at finest-lattice point p (on the face plane)."""
-        n, g = self.n, self.ngz
-        # the leaf owning the cell on the upper side of the face (or lower
-        # side at the domain's upper end)
-        t = self.leaf_at(p)
-        if t is None:
-            pm = list(p)
-            pm[d] -= 1
-            t = self.leaf_at(pm)
-            if t is None:
-                return None
-        lt, bt = t
-        st = self.E(lt) // n
-        w = self.wrap(p)
-        if w is None:
-            pm = list(p)
-            pm[d] -= 1
-            w = list(self.wrap(pm))
-            w[d] += 1
-        qs = self.index[t]
-        local = lambda x, a: x // st - bt[a] * n + g
-        if st == s:
-            return qs, [tuple(local(w[a], a) if a != d else (w[a] - bt[a] * n * st) // st + g for a in range(3))], [1.0]
-        if st > s:  # coarser: on a coarse face plane take it, else interpolate between the two
-            fd = (w[d] - bt[d] * n * st)
-            lo_f = fd // st
-            frac = (fd - lo_f * st) / st
-            c = [local(w[a], a) if a != d else lo_f + g for a in range(3)]
-            if frac == 0:
-                return qs, [tuple(c)], [1.0]
-            c2 = list(c)
-            c2[d] += 1
-            return qs, [tuple(c), tuple(c2)], [1.0 - frac, frac]
-        # finer: the 4 finer faces inside this face
-        o1, o2 = ODIR[d]
-        base = list(w)
-        base[o1] -= s // 2
-        base[o2] -= s // 2
-        cs = []
-        for b2 in (0, 1):
-            for b1 in (0, 1):
-                pp = list(base)
-                pp[o1] += b1 * st
-                pp[o2] += b2 * st
-                cs.append(tuple(local(pp[a], a) if a != d else (pp[a] - bt[a] * n * st) // st + g for a in range(3)))
-        return qs, cs, [0.25] * 4
+                i3 = [None] * 3
+                i3[d] = lo_f + g
+                for a in (o1, o2):
+                    i3[a] = W[:, a] // st - base_b[:, a] * n + g
+                f0 = flatf(i3)
+                src = np.repeat(f0[:, None], 8, axis=1)
+                w = np.zeros((len(Q), 8))
+                w[:, 0] = 1.0
+                interp = (st > s) & (frac > 0)
+                j3 = list(i3)
+                j3[d] = lo_f + g + 1
+                f1 = flatf(j3)
+                w[interp, 0] = 1.0 - frac[interp]
+                src[interp, 1] = f1[interp]
+                w[interp, 1] = frac[interp]
+                finer = st < s
+                for t_ in range(4):
+                    k3 = [None] * 3
+                    k3[d] = lo_f + g
+                    for u, a in enumerate((o1, o2)):
+                        pa = W[:, a] - s // 2 + (((t_ >> u) & 1) * st)
+                        k3[a] = pa // st - base_b[:, a] * n + g
+                    fk = flatf(k3)
+                    src[finer, t_] = fk[finer]
+                    w[finer, t_] = 0.25
+            out[arr] = (dst, src, w)
+        self._gmaps = out
+        return out
 
     def fill_ghosts(self, state, bx, by, bz, nvars=abi.N_HRSC):
         """Composite ghost fill of the first nvars state variables and face B
-        (host numpy arrays in the library layout), in place.  Sources are
-        read from the interiors (the fill reads the arrays as they were)."""
-        cm, fm = self._maps()
-        src = state.copy()
-        for q, cells in enumerate(cm):
-            for i, j, k, rec in cells:
-                if rec is None:
-                    continue
-                qs, cs, w = rec
-                acc = 0.0
-                for (ci, cj, ck) in cs:
-                    acc = acc + src[qs, :nvars, ck, cj, ci]
-                state[q, :nvars, k, j, i] = acc * w if len(cs) > 1 else acc
+        (host numpy arrays in the library layout), in place, with the maps of
+        gather_maps: each value is w0 v0 + w1 v1 + ... + w7 v7 accumulated in
+        slot order, one product and one sum rounded at a time (the device
+        fill, grb_fill_ghosts_gather, gives the same bits).  Sources are
+        interior cells and faces only."""
+        M = self.gather_maps()
+        NN = self.n + 2 * self.ngz
+        per = NN ** 3
+        dst, src, w = M["cells"]
+        S = state.reshape(self.nq, state.shape[1], per)
+        for v in range(nvars):
+            sv = np.ascontiguousarray(S[:, v, :]).reshape(-1)
+            acc = w[:, 0] * sv[src[:, 0]]
+            for t_ in range(1, 8):
+                acc = acc + w[:, t_] * sv[src[:, t_]]
+            sv[dst] = acc
+            S[:, v, :] = sv.reshape(self.nq, per)
         for d, arr in enumerate((bx, by, bz)):
-            srcb = arr.copy()
-            for q, faces in enumerate(fm[d]):
-                for i, j, k, rec in faces:
-                    if rec is None:
-                        continue
-                    qs, cs, ws = rec
-                    if len(cs) == 1:
-                        arr[q, k, j, i] = srcb[qs, cs[0][2], cs[0][1], cs[0][0]]
-                    elif len(cs) == 2:
-                        arr[q, k, j, i] = ws[0] * srcb[qs, cs[0][2], cs[0][1], cs[0][0]] + \
-                            ws[1] * srcb[qs, cs[1][2], cs[1][1], cs[1][0]]
-                    else:
-                        s_ = 0.0
-                        for c in cs:
-                            s_ += srcb[qs, c[2], c[1], c[0]]
-                        arr[q, k, j, i] = 0.25 * s_
+            dst, src, w = M[d]
+            flat = arr.reshape(-1)
+            acc = w[:, 0] * flat[src[:, 0]]
+            for t_ in range(1, 8):
+                acc = acc + w[:, t_] * flat[src[:, t_]]
+            flat[dst] = acc

@@ -303,3 +303,170 @@ def fmr_blast(hier, bx0=0.1, r0=0.8, gamma=4.0 / 3.0, flow=0.0):
     aux[:, abi.ENTROPY] = s
     aux[:, abi.BX] = bx0
     return state, bx, by, bz, aux
+
+
+# ---------------------------------------------------------------------------
+# Magnetised TOV star in the Cowling approximation
+def tov_solution(kappa=100.0, gamma=2.0, rho_c=1.28e-3, dr=2e-3, p_floor_rel=1e-12):
+    """Static spherical star of the polytrope P = kappa rho^gamma (TOV
+    equations in the areal radius r, fourth-order Runge-Kutta, mass m,
+    pressure P, log lapse nu, isotropic radius), matched at the surface to
+    Schwarzschild's exterior in isotropic coordinates.  Returns a dict of
+    the tables (areal r, isotropic radius riso, m, P, nu) and the star's
+    mass M, areal radius R and isotropic radius Riso."""
+    gm1 = gamma - 1.0
+
+    def energy(P):
+        P = max(P, 0.0)
+        rho = (P / kappa) ** (1.0 / gamma)
+        return rho + P / gm1
+
+    def rhs(r, y):
+        m, P, nu, lri = y
+        e = energy(P)
+        den = r * (r - 2.0 * m)
+        dnu = (m + 4.0 * np.pi * r ** 3 * P) / den
+        return np.array([4.0 * np.pi * r * r * e, -(e + P) * dnu, dnu, 1.0 / (r * np.sqrt(1.0 - 2.0 * m / r))])
+
+    Pc = kappa * rho_c ** gamma
+    ec = energy(Pc)
+    r = dr
+    # series start: m = 4/3 pi e_c r^3, P ~ P_c, nu ~ 0, riso ~ r
+    y = np.array([4.0 / 3.0 * np.pi * ec * r ** 3, Pc, 0.0, np.log(r)])
+    rs, ys = [0.0, r], [np.array([0.0, Pc, 0.0, -np.inf]), y.copy()]
+    pf = p_floor_rel * Pc
+    while True:
+        k1 = rhs(r, y)
+        k2 = rhs(r + 0.5 * dr, y + 0.5 * dr * k1)
+        k3 = rhs(r + 0.5 * dr, y + 0.5 * dr * k2)
+        k4 = rhs(r + dr, y + dr * k3)
+        yn = y + dr / 6.0 * (k1 + 2 * k2 + 2 * k3 + k4)
+        if yn[1] <= pf:
+            lam = (pf - y[1]) / (yn[1] - y[1])
+            R = r + lam * dr
+            ysurf = y + lam * (yn - y)
+            rs.append(R)
+            ysurf[1] = 0.0
+            ys.append(ysurf)
+            break
+        r += dr
+        y = yn
+        rs.append(r)
+        ys.append(y.copy())
+    rs = np.asarray(rs)
+    Y = np.stack(ys)
+    M = Y[-1, 0]
+    # exterior matching: nu(R) = 1/2 ln(1 - 2M/R), riso(R) from Schwarzschild
+    nu = Y[:, 2] + (0.5 * np.log(1.0 - 2.0 * M / R) - Y[-1, 2])
+    Riso = 0.5 * (R - M + np.sqrt(R * (R - 2.0 * M)))
+    riso = np.exp(Y[:, 3] - Y[-1, 3]) * Riso
+    riso[0] = 0.0
+    return {"r": rs, "riso": riso, "m": Y[:, 0], "P": np.maximum(Y[:, 1], 0.0), "nu": nu, "M": M, "R": R,
+            "Riso": Riso, "kappa": kappa, "gamma": gamma}
+
+
+def tov_metric(sol, ri):
+    """Conformal factor psi^4 and lapse at isotropic radii ri (arrays)."""
+    M, Riso = sol["M"], sol["Riso"]
+    inside = ri < Riso
+    rr = np.interp(ri, sol["riso"], sol["r"])
+    # r / riso -> its central limit at the centre
+    c0 = sol["r"][1] / sol["riso"][1]
+    ratio = np.where(ri > 0, rr / np.maximum(ri, 1e-300), c0)
+    psi4_in = ratio ** 2
+    alp_in = np.exp(np.interp(ri, sol["riso"], sol["nu"]))
+    h = M / (2.0 * np.maximum(ri, 1e-300))
+    psi4_out = (1.0 + h) ** 4
+    alp_out = (1.0 - h) / (1.0 + h)
+    return np.where(inside, psi4_in, psi4_out), np.where(inside, alp_in, alp_out)
+
+
+def tov_pressure(sol, ri):
+    return np.where(ri < sol["Riso"], np.interp(ri, sol["riso"], sol["P"]), 0.0)
+
+
+def magnetised_tov(hier, kappa=100.0, gamma=2.0, rho_c=1.28e-3, gamma_th=1.8, rho_atm=1e-10,
+                   eps_th=1e-10, bmax=1e-4, p_cut=0.04, a_n=2.0, noise=1e-3, seed=SEED):
+    """The magnetised polytropic neutron star in Cowling (the TOV solution
+    above: K=100, Gamma=2, rho_c=1.28e-3, ~1.4 solar masses) on the leaves
+    of a static FMR hierarchy: conformally flat metric psi^4 delta_ij, the
+    lapse, zero shift and extrinsic curvature (static); rest-mass density
+    with seeded relative noise (counter hash of each cell's level and
+    integer position), cold pressure and energy of the polytrope plus a tiny
+    thermal part (hybrid EOS with Gamma_th); atmosphere rho_atm outside; an
+    interior poloidal field from A = A_b max(P - p_cut P_c, 0)^a_n (-y, x, 0)
+    (the form of GRACE's Avec_poloidal_id_t), taken as the discrete curl on
+    each block's edges (div B = 0 to round-off) and scaled so that
+    max |B| = bmax.  Returns ((state, bx, by, bz, aux), tov solution)."""
+    sol = tov_solution(kappa, gamma, rho_c)
+    NN = hier.n + 2 * hier.ngz
+    nq = hier.nq
+    g = hier.ngz
+    state = np.zeros((nq, abi.N_EVOL_VARS, NN, NN, NN))
+    aux = np.zeros((nq, abi.N_AUX_VARS, NN, NN, NN))
+    X = hier.cell_centres()
+    ri = np.sqrt(np.sum(X * X, axis=1))
+    psi4, alp = tov_metric(sol, ri)
+    state[:, abi.GXX] = state[:, abi.GYY] = state[:, abi.GZZ] = psi4
+    state[:, abi.ALP] = alp
+    Pc = kappa * rho_c ** gamma
+    P = tov_pressure(sol, ri)
+    rho = np.maximum((P / kappa) ** (1.0 / gamma), rho_atm)
+    # seeded noise per cell, independent of the block order
+    key = np.zeros((nq, 3, NN, NN, NN), dtype=np.int64)
+    r = np.arange(NN)
+    for q, (l, b) in enumerate(hier.leaves):
+        key[q, 0] = b[0] * hier.n + r[None, None, :] + (l << 20)
+        key[q, 1] = b[1] * hier.n + r[None, :, None]
+        key[q, 2] = b[2] * hier.n + r[:, None, None]
+    u = _counter_uniform(np.moveaxis(key, 1, -1).reshape(-1, 3) + 64, seed, np.array([1 << 22, 1 << 22])).reshape(rho.shape)
+    rho = np.where(P > 0, rho * (1.0 + noise * u), rho)
+    Pcold = kappa * rho ** gamma
+    ecold = kappa * rho ** (gamma - 1.0) / (gamma - 1.0)
+    press = Pcold + (gamma_th - 1.0) * rho * eps_th
+    eps = ecold + eps_th
+    # face B (densitized: sqrt(gamma) B^i) as the discrete curl of the edge
+    # potential, block by block
+    bx = np.zeros((nq, NN, NN, NN + 1))
+    by = np.zeros((nq, NN, NN + 1, NN))
+    bz = np.zeros((nq, NN + 1, NN, NN))
+    Afun = lambda Pv: np.maximum(Pv - p_cut * Pc, 0.0) ** a_n
+    f = np.arange(NN + 1)
+    c = np.arange(NN)
+    for q, (l, b) in enumerate(hier.leaves):
+        d = hier.dx(l)
+        o = hier.lo + np.asarray(b) * hier.n * d
+        xf, yf, zf = o[0] + (f - g) * d[0], o[1] + (f - g) * d[1], o[2] + (f - g) * d[2]
+        xc, yc, zc = o[0] + (c - g + 0.5) * d[0], o[1] + (c - g + 0.5) * d[1], o[2] + (c - g + 0.5) * d[2]
+        # A_x on x-edges (xc, yf, zf), A_y on y-edges (xf, yc, zf); array order (z, y, x)
+        Zx, Yx, Xx = np.meshgrid(zf, yf, xc, indexing="ij")
+        Ax = -Yx * Afun(tov_pressure(sol, np.sqrt(Xx ** 2 + Yx ** 2 + Zx ** 2)))
+        Zy, Yy, Xy = np.meshgrid(zf, yc, xf, indexing="ij")
+        Ay = Xy * Afun(tov_pressure(sol, np.sqrt(Xy ** 2 + Yy ** 2 + Zy ** 2)))
+        # Bx(x face, yc, zc) = -dAy/dz ; By(xc, y face, zc) = dAx/dz ;
+        # Bz(xc, yc, z face) = dAy/dx - dAx/dy
+        bx[q] = -(Ay[1:, :, :] - Ay[:-1, :, :]) / d[2]
+        by[q] = (Ax[1:, :, :] - Ax[:-1, :, :]) / d[2]
+        bz[q] = (Ay[:, :, 1:] - Ay[:, :, :-1]) / d[0] - (Ax[:, 1:, :] - Ax[:, :-1, :]) / d[1]
+    sq = psi4 ** 1.5  # sqrt(gamma) = psi^6
+    Bc = np.stack([0.5 * (bx[..., :-1] + bx[..., 1:]), 0.5 * (by[:, :, :-1, :] + by[:, :, 1:, :]),
+                   0.5 * (bz[:, :-1] + bz[:, 1:])]) / sq[None]
+    bmag = np.sqrt(psi4 * np.sum(Bc * Bc, axis=0))
+    scale = bmax / max(float(np.max(bmag)), 1e-300)
+    bx *= scale
+    by *= scale
+    bz *= scale
+    Bc *= scale
+    # conserved variables of a static fluid (v = 0, W = 1)
+    b2 = psi4 * np.sum(Bc * Bc, axis=0)
+    gmth = gamma_th - 1.0
+    s = np.log(eps_th * rho ** (-gmth)) / gmth
+    D = sq * rho
+    state[:, abi.DENS] = D
+    state[:, abi.TAU] = sq * (rho * eps + 0.5 * b2)
+    state[:, abi.ENTROPYSTAR] = D * s
+    aux[:, abi.RHO], aux[:, abi.PRESS], aux[:, abi.EPS] = rho, press, eps
+    aux[:, abi.TEMP] = eps_th * gmth
+    aux[:, abi.ENTROPY] = s
+    aux[:, abi.BX:abi.BZ + 1] = np.moveaxis(Bc, 0, 1)
+    return (state, bx, by, bz, aux), sol
