@@ -104,6 +104,10 @@ class Reflux(C.Structure):
                 ("same_edge_q", C.c_void_p)]
 
 
+class Gather(C.Structure):
+    _fields_ = [("n", C.c_int64), ("dst", C.c_void_p), ("src", C.c_void_p), ("w", C.c_void_p)]
+
+
 class C2PDiag(C.Structure):
     _fields_ = [("iters", C.c_void_p), ("guess_used", C.c_void_p), ("mu", C.c_void_p),
                 ("bracket", C.c_void_p)]
@@ -172,6 +176,8 @@ PROTOTYPES = {
     "grb_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "grb_set_fofc_list_capacity": (C.c_int, [C.c_void_p, C.c_int64]),
     "grb_set_reflux": (C.c_int, [C.c_void_p, C.POINTER(Reflux)]),
+    "grb_fill_ghosts_gather": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Gather),
+                                         C.c_int32, C.POINTER(Gather), C.c_void_p]),
     "grb_set_kernel_timing": (C.c_int, [C.c_void_p, C.c_int32]),
     "grb_measure_fp64_peak": (C.c_int, [C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p]),
     "grb_kernel_times": (C.c_int, [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_int64),

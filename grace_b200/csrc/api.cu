@@ -1672,6 +1672,38 @@ int grb_accumulate_boundary_outflow(grb_handle* h, const grb_grid* g, int64_t nf
   return GRB_OK;
 }
 
+int grb_fill_ghosts_gather(grb_handle* h, const grb_grid* g, const grb_fields* f, const grb_gather* cells,
+                           int32_t nvars, const grb_gather* faces, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!g || !f || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->nq < 1 || g->ngz < 1 || nvars < 0 ||
+      nvars > GRB_N_EVOL_VARS)
+    return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  cudaStream_t s = (cudaStream_t)stream;
+  KScope ks(h, s, GRB_KIND_GHOST);
+  auto ok = [](const grb_gather* m) { return m->n >= 0 && (m->n == 0 || (m->dst && m->src && m->w)); };
+  if (cells && nvars > 0 && cells->n > 0) {
+    if (!ok(cells) || !f->state) return fail(h, GRB_ERR_INVALID);
+    k_ghost_gather<<<nblk(cells->n * nvars, 256), 256, 0, s>>>(cells->n, nvars, G.cells, G.cells * GRB_N_EVOL_VARS,
+                                                               cells->dst, cells->src, cells->w, f->state);
+    ++h->launches;
+  }
+  if (faces) {
+    double* arr[3] = {f->bx, f->by, f->bz};
+    const int64_t per[3] = {(int64_t)(G.NX + 1) * G.NY * G.NZ, (int64_t)G.NX * (G.NY + 1) * G.NZ,
+                            (int64_t)G.NX * G.NY * (G.NZ + 1)};
+    for (int d = 0; d < 3; ++d) {
+      const grb_gather& m = faces[d];
+      if (m.n <= 0) continue;
+      if (!ok(&m) || !arr[d]) return fail(h, GRB_ERR_INVALID);
+      k_ghost_gather<<<nblk(m.n, 256), 256, 0, s>>>(m.n, 1, per[d], per[d], m.dst, m.src, m.w, arr[d]);
+      ++h->launches;
+    }
+  }
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
 int grb_set_reflux(grb_handle* h, const grb_reflux* r) {
   if (!h) return GRB_ERR_INVALID;
   if (!r || (r->nfaces == 0 && r->nsame_faces == 0 && r->nedges == 0 && r->nsame_edges == 0)) {

@@ -57,13 +57,44 @@ class Hierarchy:
             for by in range(self.nb0[1]):
                 for bx in range(self.nb0[0]):
                     walk(0, (bx, by, bz))
-        leaves.sort(key=lambda t: (t[0], t[1][2], t[1][1], t[1][0]))
+        # finest-cell lattice: a level-l block spans E(l) finest cells
+        self.N = tuple(self.nb0[a] * self.n * 2 ** self.L for a in range(3))
+        self._set_leaves(leaves)
+        self._balance()
+        self._check_balance()
+
+    def _set_leaves(self, leaves):
+        leaves = sorted(leaves, key=lambda t: (t[0], t[1][2], t[1][1], t[1][0]))
         self.leaves = leaves
         self.index = {t: q for q, t in enumerate(leaves)}
         self.nq = len(leaves)
-        # finest-cell lattice: a level-l block spans E(l) finest cells
-        self.N = tuple(self.nb0[a] * self.n * 2 ** self.L for a in range(3))
-        self._check_balance()
+
+    def _balance(self):
+        """Refine leaves until every face, edge and corner neighbour is at
+        most one level finer (p4est's 2:1 balance)."""
+        while True:
+            split = set()
+            for l, b in self.leaves:
+                E = self.E(l)
+                for d in itertools.product((-1, 0, 1), repeat=3):
+                    if d == (0, 0, 0):
+                        continue
+                    # probe the neighbour region at the finest spacing along its boundary
+                    for u in range(0, E, max(1, E // 4)):
+                        p = [b[a] * E + (E if d[a] > 0 else (-1 if d[a] < 0 else u)) for a in range(3)]
+                        t = self.leaf_at(p)
+                        if t is not None and t[0] - l > 1:
+                            split.add((l, b))
+                            break
+                    if (l, b) in split:
+                        break
+            if not split:
+                return
+            leaves = [t for t in self.leaves if t not in split]
+            for l, b in split:
+                for c in itertools.product((0, 1), repeat=3):
+                    leaves.append((l + 1, (2 * b[0] + c[2], 2 * b[1] + c[1], 2 * b[2] + c[0])))
+            self._set_leaves(leaves)
 
     # ---- geometry ---------------------------------------------------------
     def E(self, l):
@@ -133,10 +164,11 @@ class Hierarchy:
             for d in itertools.product((-1, 0, 1), repeat=3):
                 if d == (0, 0, 0):
                     continue
-                p = [b[a] * E + (E if d[a] > 0 else (-1 if d[a] < 0 else E // 2)) for a in range(3)]
-                t = self.leaf_at(p)
-                if t is not None:
-                    assert abs(t[0] - l) <= 1, f"hierarchy not 2:1 balanced at level {l} block {b}"
+                for u in range(0, E, max(1, E // 4)):
+                    p = [b[a] * E + (E if d[a] > 0 else (-1 if d[a] < 0 else u)) for a in range(3)]
+                    t = self.leaf_at(p)
+                    if t is not None:
+                        assert abs(t[0] - l) <= 1, f"hierarchy not 2:1 balanced at level {l} block {b}"
 
     # ---- reflux descriptors -------------------------------------------------
     def reflux_lists(self):
@@ -271,17 +303,20 @@ class Hierarchy:
         inside the domain: (level, qindex) arrays."""
         lev = np.full(len(P), -1, dtype=np.int64)
         qi = np.full(len(P), -1, dtype=np.int64)
+        if not hasattr(self, "_level_keys"):
+            self._level_keys = {}
+            for l in range(self.L + 1):
+                nbl = [self.nb0[a] * 2 ** l for a in range(3)]
+                mine = [(b, q) for q, (ll, b) in enumerate(self.leaves) if ll == l]
+                keys = np.array([(b[2] * nbl[1] + b[1]) * nbl[0] + b[0] for b, _ in mine], dtype=np.int64)
+                qs = np.array([q for _, q in mine], dtype=np.int64)
+                order = np.argsort(keys)
+                self._level_keys[l] = (keys[order], qs[order], nbl)
         for l in range(self.L, -1, -1):
-            mine = [(b, q) for q, (ll, b) in enumerate(self.leaves) if ll == l]
-            if not mine:
+            keys, qs, nbl = self._level_keys[l]
+            if len(keys) == 0:
                 continue
             E = self.E(l)
-            nbl = [self.nb0[a] * 2 ** l for a in range(3)]
-            key_of = lambda b: (b[2] * nbl[1] + b[1]) * nbl[0] + b[0]
-            keys = np.array([key_of(b) for b, _ in mine], dtype=np.int64)
-            qs = np.array([q for _, q in mine], dtype=np.int64)
-            order = np.argsort(keys)
-            keys, qs = keys[order], qs[order]
             todo = lev < 0
             B = P[todo] // E
             k = (B[:, 2] * nbl[1] + B[:, 1]) * nbl[0] + B[:, 0]

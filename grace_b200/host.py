@@ -17,6 +17,7 @@ ERROR() macro would abort the run.
 import ctypes
 from dataclasses import dataclass
 
+import numpy as np
 import torch
 
 from . import _lib, abi
@@ -380,6 +381,25 @@ class GRMHDEquationsSystem:
         """Pick tuned-mode candidates (indices 0..2) without timing."""
         v = (ctypes.c_int32 * 4)(flux, flag, update, aux)
         _lib.check(self.lib.grb_set_tuning(self.h, v), "grb_set_tuning")
+
+    def fill_ghosts_gather(self, fields, maps, nvars=abi.N_HRSC, stream=None):
+        """Ghost fill by gather maps (grb_fill_ghosts_gather).  maps: the dict
+        of grace_b200.fmr.Hierarchy.gather_maps (numpy), uploaded on first use
+        and kept by this object."""
+        key = id(maps)
+        if getattr(self, "_gmaps_key", None) != key:
+            dev = self.blocks.device
+            up = lambda t: tuple(torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in t)
+            self._gmaps = {k: up(v) for k, v in maps.items()}
+            self._gmaps_key = key
+        G = self._gmaps
+        mk = lambda t: abi.Gather(t[0].numel(), t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr())
+        cells = mk(G["cells"])
+        faces = (abi.Gather * 3)(mk(G[0]), mk(G[1]), mk(G[2]))
+        g = self.blocks.c()
+        f = fields.c()
+        _lib.check(self.lib.grb_fill_ghosts_gather(self.h, ctypes.byref(g), ctypes.byref(f), ctypes.byref(cells),
+                                                   nvars, faces, _stream_ptr(stream)), "grb_fill_ghosts_gather")
 
     def set_reflux(self, lists=None, same_level_flux_average=False):
         """Reflux descriptor lists (grb_set_reflux): a dict of numpy arrays in

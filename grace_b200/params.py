@@ -129,3 +129,17 @@ def c2p_bench():
     W and sigma ceilings above the sampled ranges."""
     return hybrid_pwpoly(100.0, [2.0], [], gamma_th=1.8, c2p_tol=1e-12, max_w=60.0,
                          max_sigma=2.0e3)
+
+
+def tov():
+    """Magnetised TOV star: hybrid EOS (cold polytrope K=100, Gamma=2;
+    thermal Gamma_th=1.8), WENO-Z + HLLE + Gardiner-Stone + FOFC; atmosphere
+    floor 1e-12 below the 1e-10 atmosphere of the initial data."""
+    return hybrid_pwpoly(100.0, [2.0], [], gamma_th=1.8, emf=abi.EMF_GS, fofc_enable=1, rho_fl=1e-12)
+
+
+def torus():
+    """Fishbone-Moncrief torus: ideal gas Gamma=4/3, WENO-Z + HLLE +
+    Gardiner-Stone + FOFC; atmosphere floor 1e-9 below the 1e-8 atmosphere
+    of the initial data."""
+    return ideal_gas(4.0 / 3.0, emf=abi.EMF_GS, fofc_enable=1, rho_fl=1e-9)

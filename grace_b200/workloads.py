@@ -470,3 +470,294 @@ def magnetised_tov(hier, kappa=100.0, gamma=2.0, rho_c=1.28e-3, gamma_th=1.8, rh
     aux[:, abi.ENTROPY] = s
     aux[:, abi.BX:abi.BZ + 1] = np.moveaxis(Bc, 0, 1)
     return (state, bx, by, bz, aux), sol
+
+
+def tov_hierarchy(n=16):
+    """The FMR hierarchy of the magnetised TOV star: the cube +-48 (M_sun
+    units) in 4^3 base blocks of n^3 cells, refined where a block comes
+    within 26, 14, 8, 3.5 of the centre (levels 0..3), five levels, outflow
+    boundaries: 32 / 224 / 224 / 224 / 256 blocks on levels 0..4 (uneven
+    per-level counts), finest spacing 0.09375 at n = 16."""
+    from . import fmr
+    radii = (26.0, 14.0, 8.0, 3.5)
+    half, nb0 = 48.0, 4
+
+    def refine(l, b):
+        if l >= len(radii):
+            return False
+        size = 2 * half / nb0 / 2 ** l
+        lo = -half + np.asarray(b) * size
+        hi = lo + size
+        d = np.sqrt(np.sum(np.maximum(0.0, np.maximum(lo, -hi)) ** 2))
+        return d < radii[l]
+
+    return fmr.Hierarchy((nb0,) * 3, n, (-half,) * 3, (half,) * 3, refine, len(radii), periodic=(False,) * 3)
+
+
+# ---------------------------------------------------------------------------
+# General 3+1 metric helpers and the Fishbone-Moncrief torus in Kerr-Schild
+def sym3(g6):
+    """(6, ...) symmetric components xx, xy, xz, yy, yz, zz -> (3, 3, ...)."""
+    xx, xy, xz, yy, yz, zz = g6
+    return np.array([[xx, xy, xz], [xy, yy, yz], [xz, yz, zz]])
+
+
+def curved_prims_to_cons(g6, beta, alp, rho, press, eps, z, B, s):
+    """Densitized conserved variables (7, ...) DENS, S_i, TAU, YESTAR (0),
+    ENTROPYSTAR from primitives on a 3+1 metric (g6 the spatial metric's 6
+    components, beta^i, alpha): z^i = W v^i, B^i (not densitized).  The
+    usual ideal-MHD expressions: b^0 = W B.v / alpha, b^2 = (B^2 +
+    alpha^2 (b^0)^2) / W^2, D = rho W, S_i = (rho h + b^2) W^2 v_i -
+    alpha b^0 b_i, tau = (rho h + b^2) W^2 - (P + b^2/2) - alpha^2 (b^0)^2 - D,
+    all times sqrt(gamma)."""
+    G = sym3(g6)
+    det = (G[0, 0] * (G[1, 1] * G[2, 2] - G[1, 2] ** 2) - G[0, 1] * (G[0, 1] * G[2, 2] - G[0, 2] * G[1, 2]) +
+           G[0, 2] * (G[0, 1] * G[1, 2] - G[0, 2] * G[1, 1]))
+    sq = np.sqrt(det)
+    zl = np.einsum("ij...,j...->i...", G, z)
+    W = np.sqrt(1.0 + np.sum(z * zl, axis=0))
+    v = z / W
+    vl = zl / W
+    Bl = np.einsum("ij...,j...->i...", G, B)
+    Bv = np.sum(B * vl, axis=0)
+    B2 = np.sum(B * Bl, axis=0)
+    b0 = W * Bv / alp
+    b2 = (B2 + alp * alp * b0 * b0) / (W * W)
+    # b_i = gamma_ij b^j + beta_i b^0 with b^j = (B^j + alpha b^0 W (v^j - beta^j/alpha)) / W
+    bu = (B + alp * b0 * W * (v - beta / alp)) / W
+    betal = np.einsum("ij...,j...->i...", G, beta)
+    bl = np.einsum("ij...,j...->i...", G, bu) + betal * b0
+    rhoh = rho * (1.0 + eps) + press
+    D = rho * W
+    out = np.zeros((7,) + rho.shape)
+    out[0] = sq * D
+    out[1:4] = sq * ((rhoh + b2) * W * W * vl - alp * b0 * bl)
+    out[4] = sq * ((rhoh + b2) * W * W - (press + 0.5 * b2) - alp * alp * b0 * b0 - D)
+    out[6] = sq * D * s
+    return out, sq, b2
+
+
+def kerr_schild(x, y, z, a, r_reg=0.5):
+    """Cartesian Kerr-Schild (M = 1): spatial metric g6, shift beta^i, lapse,
+    and the Boyer-Lindquist radius r (at least r_reg)."""
+    R2 = x * x + y * y + z * z
+    r2 = 0.5 * (R2 - a * a + np.sqrt((R2 - a * a) ** 2 + 4.0 * a * a * z * z))
+    # regularised well inside the horizon (r_+ = 1 + sqrt(1 - a^2)): the
+    # excised region needs finite values, not the ring singularity
+    r2 = np.maximum(r2, r_reg * r_reg)
+    r = np.sqrt(r2)
+    H = r2 * r / (r2 * r2 + a * a * z * z)
+    l = np.stack([(r * x + a * y) / (r2 + a * a), (r * y - a * x) / (r2 + a * a), z / r])
+    g6 = np.stack([1.0 + 2 * H * l[0] * l[0], 2 * H * l[0] * l[1], 2 * H * l[0] * l[2],
+                   1.0 + 2 * H * l[1] * l[1], 2 * H * l[1] * l[2], 1.0 + 2 * H * l[2] * l[2]])
+    beta = 2 * H * l / (1.0 + 2 * H)
+    alp = 1.0 / np.sqrt(1.0 + 2 * H)
+    return g6, beta, alp, r
+
+
+def kerr_schild_curvature(x, y, z, a, h=1e-5):
+    """Extrinsic curvature K_ij of the stationary Kerr-Schild slice,
+    K_ij = (D_i beta_j + D_j beta_i) / (2 alpha), with the derivatives of
+    the metric and of beta_j = gamma_jk beta^k by central differences of the
+    analytic fields (step h).  Returns the 6 components (xx, xy, xz, yy,
+    yz, zz)."""
+    P = (x, y, z)
+
+    def at(d, sgn):
+        q = [x, y, z]
+        q = [q[k] + (sgn * h if k == d else 0.0) for k in range(3)]
+        g6, beta, alp, _ = kerr_schild(q[0], q[1], q[2], a)
+        G = sym3(g6)
+        return G, np.einsum("ij...,j...->i...", G, beta)
+
+    g6, beta, alp, _ = kerr_schild(*P, a)
+    G = sym3(g6)
+    Gi = np.linalg.inv(np.moveaxis(G, (0, 1), (-2, -1)))
+    Gi = np.moveaxis(Gi, (-2, -1), (0, 1))
+    dG, dbl = [], []
+    for d in range(3):
+        Gp, blp = at(d, +1)
+        Gm, blm = at(d, -1)
+        dG.append((Gp - Gm) / (2 * h))
+        dbl.append((blp - blm) / (2 * h))
+    dG = np.stack(dG)      # [d][i][j]: d_d g_ij
+    dbl = np.stack(dbl)    # [d][j]: d_d beta_j
+    betal = np.einsum("ij...,j...->i...", G, beta)
+    # Gamma_kij (lowered first index) = (d_i g_kj + d_j g_ki - d_k g_ij) / 2
+    Gam_l = 0.5 * (np.einsum("ikj...->kij...", dG) + np.einsum("jki...->kij...", dG) - dG)
+    Gam = np.einsum("lk...,kij...->lij...", Gi, Gam_l)
+    Dbl = dbl - np.einsum("kij...,k...->ij...", Gam, betal)  # D_i beta_j
+    K = (Dbl + np.einsum("ij...->ji...", Dbl)) / (2.0 * alp)
+    return np.stack([K[0, 0], K[0, 1], K[0, 2], K[1, 1], K[1, 2], K[2, 2]])
+
+
+def fm_torus(hier, a=0.9375, r_in=6.0, r_pmax=12.0, gamma=4.0 / 3.0, kappa=1e-3, rho_atm=1e-8,
+             beta_p=100.0, a_cut=0.2, noise=2e-2, seed=SEED):
+    """Fishbone-Moncrief torus in the fixed Kerr-Schild metric on the leaves
+    of a static FMR hierarchy, written from the configuration text (the
+    reference's own torus initial data is not part of its sources): the
+    torus of constant specific angular momentum set by r_pmax, inner edge
+    r_in, polytrope P = kappa rho^gamma with rho normalised to 1 at its
+    maximum, the orbital velocity transformed from Boyer-Lindquist to
+    Cartesian Kerr-Schild; atmosphere rho_atm (at rest in the Kerr-Schild
+    frame, pressure of the same polytrope); a poloidal field from
+    A = A_b max(rho/rho_max - a_cut, 0) (-y, x, 0) as the discrete curl on
+    each block's edges, scaled so that max P / max(b^2/2) = beta_p; seeded
+    relative pressure noise.  Returns (state, bx, by, bz, aux)."""
+    def lnh_bl(r, th, l):
+        sth, cth = np.sin(th), np.cos(th)
+        DD = r * r - 2 * r + a * a
+        AA = (r * r + a * a) ** 2 - DD * a * a * sth * sth
+        SS = r * r + a * a * cth * cth
+        t = np.sqrt(1.0 + 4.0 * l * l * SS * SS * DD / (AA * AA * sth * sth))
+        return 0.5 * np.log((1.0 + t) / (SS * DD / AA)) - 0.5 * t - 2.0 * a * r * l / AA
+
+    # Fishbone-Moncrief angular momentum of the pressure maximum
+    rp = r_pmax
+    sr = np.sqrt(rp)
+    l = (((a * a - 2 * a * sr + rp * rp) * ((-2 * a * rp * (a * a - 2 * a * sr + rp * rp)) /
+         np.sqrt(2 * a * sr + (rp - 3) * rp) + ((a + (rp - 2) * sr) * (rp ** 3 + a * a * (2 + rp))) /
+         np.sqrt(1 + 2 * a / rp ** 1.5 - 3 / rp))) / (rp ** 3 * np.sqrt(2 * a * sr + (rp - 3) * rp) *
+                                                      (a * a + (rp - 2) * rp)))
+    lnh_in = lnh_bl(r_in, 0.5 * np.pi, l)
+    # rho_max at the pressure maximum (equator, r_pmax)
+    hmax = np.exp(lnh_bl(r_pmax, 0.5 * np.pi, l) - lnh_in)
+    rho_max = ((hmax - 1) * (gamma - 1) / (kappa * gamma)) ** (1 / (gamma - 1))
+
+    def fluid(x, y, z):
+        g6, beta, alp, r = kerr_schild(x, y, z, a)
+        th = np.arccos(np.clip(z / np.maximum(r, 1e-300), -1, 1))
+        sth = np.maximum(np.sin(th), 1e-12)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            lnh = np.where(r >= r_in, lnh_bl(np.maximum(r, r_in), th, l) - lnh_in, -1.0)
+        inside = (r >= r_in) & (lnh > 0)
+        h = np.exp(np.where(inside, lnh, 0.0))
+        rho = np.where(inside, ((h - 1) * (gamma - 1) / (kappa * gamma)) ** (1 / (gamma - 1)) / rho_max, rho_atm)
+        # u^phi in Boyer-Lindquist (= Kerr-Schild's when u^r = 0)
+        rr = np.maximum(r, r_in)
+        DD = rr * rr - 2 * rr + a * a
+        AA = (rr * rr + a * a) ** 2 - DD * a * a * sth * sth
+        SS = rr * rr + a * a * np.cos(th) ** 2
+        em2chi = SS * SS * DD / (AA * AA * sth * sth)
+        up1 = np.sqrt((-1 + np.sqrt(1 + 4 * l * l * em2chi)) / 2)
+        uphi = 2 * a * rr * np.sqrt(1 + up1 * up1) / np.sqrt(AA * SS * DD) + np.sqrt(SS / AA) * up1 / sth
+        uphi = np.where(inside, uphi, 0.0)
+        # Cartesian KS: u^x = -y u^phi, u^y = x u^phi; u^t from u.u = -1
+        ui = np.stack([-y * uphi, x * uphi, np.zeros_like(x)])
+        G = sym3(g6)
+        uil = np.einsum("ij...,j...->i...", G, ui)
+        # g_tt = -alp^2 + beta.beta, g_ti = beta_i: solve for u^t > 0
+        betal = np.einsum("ij...,j...->i...", G, beta)
+        gtt = -alp * alp + np.sum(beta * betal, axis=0)
+        A_ = gtt
+        B_ = 2 * np.sum(betal * ui, axis=0)
+        C_ = np.sum(ui * uil, axis=0) + 1.0
+        with np.errstate(invalid="ignore"):
+            ut = (-B_ - np.sqrt(B_ * B_ - 4 * A_ * C_)) / (2 * A_)
+        # z^i = u^i + u^t beta^i in the torus; the atmosphere at rest for the
+        # normal observers (z = 0, regular in the ergoregion too)
+        zv = np.where(inside[None], ui + ut * beta, 0.0)
+        rho = np.maximum(rho, rho_atm)
+        return g6, beta, alp, r, rho, zv
+
+    NN = hier.n + 2 * hier.ngz
+    nq = hier.nq
+    g = hier.ngz
+    X = hier.cell_centres()
+    x, y, zc = X[:, 0], X[:, 1], X[:, 2]
+    g6, beta, alp, r, rho, zv = fluid(x, y, zc)
+    Kc = kerr_schild_curvature(x, y, zc, a)
+    press = kappa * (rho * rho_max) ** gamma / rho_max  # normalised units: P / rho_max
+    key = np.zeros((nq, 3, NN, NN, NN), dtype=np.int64)
+    rr_ = np.arange(NN)
+    for q, (lv, b) in enumerate(hier.leaves):
+        key[q, 0] = b[0] * hier.n + rr_[None, None, :] + (lv << 20)
+        key[q, 1] = b[1] * hier.n + rr_[:, None] * 0 + rr_[None, :, None]
+        key[q, 2] = b[2] * hier.n + rr_[:, None, None]
+    u = _counter_uniform(np.moveaxis(key, 1, -1).reshape(-1, 3) + 64, seed, np.array([1 << 22, 1 << 22])).reshape(rho.shape)
+    press = press * (1.0 + noise * u)
+    eps = press / ((gamma - 1.0) * rho)
+    s = np.log(eps) / (gamma - 1.0) - np.log(rho)
+    # field: discrete curl of A = f(rho(x)) (-y, x, 0) on each block's edges
+    bx = np.zeros((nq, NN, NN, NN + 1))
+    by = np.zeros((nq, NN, NN + 1, NN))
+    bz = np.zeros((nq, NN + 1, NN, NN))
+    def rho_only(xx, yy, zz):
+        # the torus density alone (the vector potential's profile)
+        R2 = xx * xx + yy * yy + zz * zz
+        r = np.sqrt(0.5 * (R2 - a * a + np.sqrt((R2 - a * a) ** 2 + 4.0 * a * a * zz * zz)))
+        th = np.arccos(np.clip(zz / np.maximum(r, 1e-300), -1, 1))
+        with np.errstate(invalid="ignore", divide="ignore"):
+            lnh = np.where(r >= r_in, lnh_bl(np.maximum(r, r_in), th, l) - lnh_in, -1.0)
+        h = np.exp(np.where((r >= r_in) & (lnh > 0), lnh, 0.0))
+        return ((h - 1) * (gamma - 1) / (kappa * gamma)) ** (1 / (gamma - 1)) / rho_max
+
+    fA = lambda xx, yy, zz: np.maximum(rho_only(xx, yy, zz) - a_cut, 0.0)
+    f_ = np.arange(NN + 1)
+    c_ = np.arange(NN)
+    for q, (lv, b) in enumerate(hier.leaves):
+        d = hier.dx(lv)
+        o = hier.lo + np.asarray(b) * hier.n * d
+        xf, yf, zf = o[0] + (f_ - g) * d[0], o[1] + (f_ - g) * d[1], o[2] + (f_ - g) * d[2]
+        xc, yc, zcc = o[0] + (c_ - g + 0.5) * d[0], o[1] + (c_ - g + 0.5) * d[1], o[2] + (c_ - g + 0.5) * d[2]
+        Zx, Yx, Xx = np.meshgrid(zf, yf, xc, indexing="ij")
+        Ax = -Yx * fA(Xx, Yx, Zx)
+        Zy, Yy, Xy = np.meshgrid(zf, yc, xf, indexing="ij")
+        Ay = Xy * fA(Xy, Yy, Zy)
+        bx[q] = -(Ay[1:, :, :] - Ay[:-1, :, :]) / d[2]
+        by[q] = (Ax[1:, :, :] - Ax[:-1, :, :]) / d[2]
+        bz[q] = (Ay[:, :, 1:] - Ay[:, :, :-1]) / d[0] - (Ax[:, 1:, :] - Ax[:, :-1, :]) / d[1]
+    G = sym3(g6)
+    det = (G[0, 0] * (G[1, 1] * G[2, 2] - G[1, 2] ** 2) - G[0, 1] * (G[0, 1] * G[2, 2] - G[0, 2] * G[1, 2]) +
+           G[0, 2] * (G[0, 1] * G[1, 2] - G[0, 2] * G[1, 1]))
+    sq = np.sqrt(det)
+    Bc = np.stack([0.5 * (bx[..., :-1] + bx[..., 1:]), 0.5 * (by[:, :, :-1, :] + by[:, :, 1:, :]),
+                   0.5 * (bz[:, :-1] + bz[:, 1:])]) / sq[None]
+    _, _, b2 = curved_prims_to_cons(g6, beta, alp, rho, press, eps, zv, Bc, s)
+    scale = np.sqrt(float(np.max(press)) / (beta_p * 0.5 * max(float(np.max(b2)), 1e-300)))
+    for arr in (bx, by, bz, Bc):
+        arr *= scale
+    cons, sq, b2 = curved_prims_to_cons(g6, beta, alp, rho, press, eps, zv, Bc, s)
+    state = np.zeros((nq, abi.N_EVOL_VARS, NN, NN, NN))
+    aux = np.zeros((nq, abi.N_AUX_VARS, NN, NN, NN))
+    state[:, 0:7] = np.moveaxis(cons, 0, 1)
+    for k in range(6):
+        state[:, abi.GXX + k] = g6[k]
+        state[:, abi.KXX + k] = Kc[k]
+    state[:, abi.ALP] = alp
+    for k in range(3):
+        state[:, abi.BETAX + k] = beta[k]
+    aux[:, abi.RHO], aux[:, abi.PRESS], aux[:, abi.EPS] = rho, press, eps
+    aux[:, abi.TEMP] = eps * (gamma - 1.0)
+    aux[:, abi.ENTROPY] = s
+    aux[:, abi.ZVECX:abi.ZVECZ + 1] = np.moveaxis(zv, 0, 1)
+    aux[:, abi.BX:abi.BZ + 1] = np.moveaxis(Bc, 0, 1)
+    return state, bx, by, bz, aux
+
+
+def torus_hierarchy(n=16):
+    """The FMR hierarchy of the torus: the cube +-40 (units of M) in 4^3
+    base blocks of n^3 cells, four levels, refined where a block comes
+    within 10, 5, 2.5 of the torus' pressure-maximum ring (cylindrical radius
+    12 in the equatorial plane) or within 3, 2, 1.5 of the black hole
+    (levels 0..2), then 2:1 balanced; outflow boundaries; uneven per-level
+    counts."""
+    from . import fmr
+    half, nb0 = 40.0, 4
+    ring, hole = (10.0, 5.0, 2.5), (3.0, 2.0, 1.5)
+
+    def refine(l, b):
+        if l >= len(ring):
+            return False
+        size = 2 * half / nb0 / 2 ** l
+        lo = -half + np.asarray(b) * size
+        hi = lo + size
+        # distance from the box to the origin and to the ring R = 12, z = 0
+        d0 = np.sqrt(np.sum(np.maximum(0.0, np.maximum(lo, -hi)) ** 2))
+        # sample the box for the ring distance (boxes are few)
+        t = np.linspace(0, 1, 9)
+        X, Y, Z = np.meshgrid(lo[0] + t * size, lo[1] + t * size, lo[2] + t * size, indexing="ij")
+        dr = np.sqrt((np.sqrt(X ** 2 + Y ** 2) - 12.0) ** 2 + Z ** 2).min()
+        return dr < ring[l] or d0 < hole[l]
+
+    return fmr.Hierarchy((nb0,) * 3, n, (-half,) * 3, (half,) * 3, refine, len(ring), periodic=(False,) * 3)

@@ -558,6 +558,28 @@ int grb_prolong_to_ghosts(grb_handle* h, const grb_grid* g, const grb_fields* fi
                           const int8_t* have_fine, const int32_t* vars_lo, int32_t nlo,
                           const int32_t* vars_ho, int32_t nho, void* stream);
 
+/* ---- ghost fill by gather maps (harness-side helper) --------------------- */
+/* One gather map: entry e sets a[dst[e]] = sum over t < 8 of w[8 e + t] *
+ * a[src[8 e + t]] (accumulated in slot order, each product and sum rounded
+ * on its own), the flat indices counting the cells of one variable of the
+ * array: block q's local cell c at q * (cells of one variable of a block) +
+ * c.  Unused slots carry weight 0. */
+typedef struct grb_gather {
+  int64_t n;
+  const int64_t* dst;  /* [n] device */
+  const int64_t* src;  /* [n][8] device */
+  const double* w;     /* [n][8] device */
+} grb_gather;
+/* No counterpart in the reference (its ghost exchange is the host's): fills
+ * the ghost zones of f by precomputed gather maps, cells for the first nvars
+ * state variables and faces[0..2] for the face-B arrays staggered along x, y,
+ * z (NULL entries skipped).  Stands in, for multi-level block lists on one
+ * rank, for the host's same-level copies, restriction and prolongation: the
+ * maps encode where each ghost value comes from (grace_b200.fmr builds them
+ * for a static hierarchy).  The sources must be interior cells and faces. */
+int grb_fill_ghosts_gather(grb_handle* h, const grb_grid* g, const grb_fields* f, const grb_gather* cells,
+                           int32_t nvars, const grb_gather* faces, void* stream);
+
 /* ---- reflux at coarse-fine interfaces ------------------------------------ */
 /* The reflux descriptors of the caller's AMR hierarchy on this rank: what
  * GRACE's ghost layer builds from the p4est face and edge iterators

@@ -1,0 +1,125 @@
+"""The FMR configurations on the GPU against the oracle: the magnetised TOV
+star on its five-level hierarchy (grace_b200.workloads.tov_hierarchy,
+32/224/224/224/256 blocks per level) and the Fishbone-Moncrief torus in
+Kerr-Schild on its four-level one (torus_hierarchy, 32/224/184/576), with
+8^3 blocks here (the benchmark runs 16^3), through one SSP-RK3 step of the
+stage with refluxing (grb_set_reflux) and the gather-map ghost fill between
+stages (grb_fill_ghosts_gather); the oracle runs the same step with the
+same descriptor lists and the host fill of the same maps.  The device
+gather fill itself matches the host fill bit for bit."""
+import numpy as np
+import pytest
+import torch
+
+import _oracle
+from grace_b200 import abi, params, workloads
+from grace_b200.host import Blocks, Fields, GRMHDEquationsSystem
+from parity import cons_rel_err, interior
+
+pytestmark = pytest.mark.gpu
+
+STEP_TOL = 1e-10
+
+
+def _oracle_rk3(S, H, idx, dt, state, aux):
+    bc = lambda f: H.fill_ghosts(*f)
+    sp = [x.copy() for x in state]
+    spp = [x.copy() for x in state]
+    S.reset_diag(aux)
+    S.advance_substep(idx, dt, 1.0, sp, state, aux)
+    bc(sp)
+    S.compute_aux(idx, sp, aux)
+    S.linop(spp, state, sp, 0.75, 0.25)
+    S.advance_substep(idx, dt, 0.25, spp, sp, aux)
+    bc(spp)
+    S.compute_aux(idx, spp, aux)
+    S.linop(state, state, spp, 1.0 / 3, 2.0 / 3.0)
+    S.advance_substep(idx, dt, 2.0 / 3.0, state, spp, aux)
+    bc(state)
+    S.compute_aux(idx, state, aux)
+
+
+def _case(name):
+    if name == "tov":
+        H = workloads.tov_hierarchy(8)
+        (st, bx, by, bz, aux), _ = workloads.magnetised_tov(H)
+        return H, params.tov(), (st, bx, by, bz, aux)
+    H = workloads.torus_hierarchy(8)
+    return H, params.torus(), workloads.fm_torus(H)
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+@pytest.mark.parametrize("name", ["tov", "torus"])
+def test_fmr_config_rk3_step_matches_oracle(name, mode):
+    H, P, (st, bx, by, bz, aux) = _case(name)
+    H.fill_ghosts(st, bx, by, bz)
+    R = H.reflux_lists()
+    maps = H.gather_maps()
+    idx = H.idx()
+    dt = 0.25 / idx[:, 0].max()
+    # oracle
+    ost = [x.copy() for x in (st, bx, by, bz)]
+    oaux = aux.copy()
+    S = _oracle.Stage(P, H.n, H.n, H.n, H.ngz, H.nq)
+    S.set_reflux(R)
+    S.compute_aux(idx.copy(), ost, oaux)
+    _oracle_rk3(S, H, idx.copy(), dt, ost, oaux)
+    # GPU
+    dev = torch.device("cuda:0")
+    Pg = abi.Params.from_buffer_copy(P)
+    if mode == abi.MODE_TUNED:
+        Pg.ranges = abi.RANGES_NEXT_STAGE
+    g = GRMHDEquationsSystem(Pg)
+    g.reserve(Blocks(H.n, H.n, H.n, H.ngz, H.nq, idx, device=dev))
+    g.set_mode(mode)
+    g.set_reflux(R)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    state = Fields(T(st), T(bx), T(by), T(bz))
+    aux_d = T(aux)
+    bc = lambda f: g.fill_ghosts_gather(f, maps)
+    g.compute_auxiliary_quantities(state, aux_d)
+    sp, spp = state.clone(), state.clone()
+    if mode == abi.MODE_TUNED:
+        g.set_static_metric(state)
+        g.set_tuning(1, 1, 1, 1)
+    g.rk3_step(dt, state, sp, spp, aux_d, bc)
+    torch.cuda.synchronize()
+    gs = [x.cpu().numpy() for x in (state.state, state.bx, state.by, state.bz)]
+    e = cons_rel_err(interior(gs[0][:, :7], H.ngz), interior(ost[0][:, :7], H.ngz))
+    assert e.max() < STEP_TOL, e
+    for a, b in zip(gs[1:], ost[1:]):
+        assert np.max(np.abs(a - b)) < STEP_TOL * np.max(np.abs(b))
+    ga = aux_d.cpu().numpy()
+    gi, oi = interior(ga, H.ngz), interior(oaux, H.ngz)
+    for v in (abi.RHO, abi.PRESS):
+        r = np.max(np.abs(gi[:, v] - oi[:, v]) / np.abs(oi[:, v]))
+        assert r < STEP_TOL, (v, r)
+    np.testing.assert_array_equal(gi[:, abi.C2P_ERR], oi[:, abi.C2P_ERR])
+    # div B stays at round-off in every block
+    bmax = max(np.max(np.abs(x)) for x in gs[1:])
+    dx = H.spacings()
+    assert np.max(np.abs(gi[:, abi.BDIV]) * dx[:, 0, None, None, None]) < 1e-12 * bmax
+    assert g.status().device_flags == 0
+
+
+def test_gather_fill_matches_host_fill():
+    """grb_fill_ghosts_gather on random data equals the host fill of the
+    same maps bit for bit (both accumulate the 8 slots in order, each
+    product and sum rounded on its own)."""
+    H = workloads.tov_hierarchy(8)
+    rng = np.random.default_rng(3)
+    NN = H.n + 2 * H.ngz
+    st = rng.standard_normal((H.nq, abi.N_EVOL_VARS, NN, NN, NN))
+    bx = rng.standard_normal((H.nq, NN, NN, NN + 1))
+    by = rng.standard_normal((H.nq, NN, NN + 1, NN))
+    bz = rng.standard_normal((H.nq, NN + 1, NN, NN))
+    dev = torch.device("cuda:0")
+    g = GRMHDEquationsSystem(params.tov())
+    g.reserve(Blocks(H.n, H.n, H.n, H.ngz, H.nq, H.idx(), device=dev))
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    f = Fields(T(st), T(bx), T(by), T(bz))
+    g.fill_ghosts_gather(f, H.gather_maps())
+    torch.cuda.synchronize()
+    H.fill_ghosts(st, bx, by, bz)
+    for a, b in zip((f.state, f.bx, f.by, f.bz), (st, bx, by, bz)):
+        assert np.array_equal(a.cpu().numpy(), b)

@@ -84,3 +84,27 @@ def test_balsara1_density_l1_at_t_end(mode):
     assert l1 <= 1e-8, l1
     # the shock tube evolved: the density range spans the fan
     assert rr.max() > 0.9 and rr.min() < 0.2
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_balsara1_configured_size_density_l1_against_reference_fixture(mode):
+    """Balsara-1 at its configured size, 1024 x 16 x 16 cells (64 blocks of
+    16^3), to t = 0.4 on the GPU against the reference's own numerics run to
+    the same time (tests/golden/balsara1024_ref.npz, made by
+    tests/golden/make_balsara1024.py with the pinning build: 1006 steps; the
+    reference's density does not vary across the periodic y, z directions,
+    to the bit, so one x-line stands for the whole field): the same step
+    count and density L1 difference <= 1e-8 relative."""
+    import os
+    fx = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "balsara1024_ref.npz"))
+    assert float(fx["transverse_spread"]) == 0.0
+    P = params.balsara1()
+    su, f = workloads.balsara1(nb=(64, 1, 1), n=(16, 16, 16))
+    ag, ng = _run_gpu(P, su, f, mode)
+    assert ng == int(fx["steps"])
+    g = su.ngz
+    rg = ag[:, abi.RHO, g:-g, g:-g, g:-g]                    # (64, nz, ny, nx)
+    line = fx["rho_line"].reshape(64, 1, 1, 16)
+    l1 = np.sum(np.abs(rg - line)) / np.sum(np.abs(np.broadcast_to(line, rg.shape)))
+    print(f"Balsara-1 1024x16x16 t=0.4: {ng} steps, density L1 rel {l1:.3e}")
+    assert l1 <= 1e-8, l1
