@@ -77,6 +77,10 @@ def parse():
     ap.add_argument("--c2p-only", action="store_true", help="run only the c2p micro-benchmark")
     ap.add_argument("--c2p-states", type=int, default=1 << 24, help="states of the c2p micro-benchmark")
     ap.add_argument("--mode", default="tuned", choices=["tuned", "plain"])
+    ap.add_argument("--config", default="blast", choices=["blast", "tov", "torus"],
+                    help="blast: the 256^3 blast wave (the headline); tov, torus: the magnetised TOV star and the "
+                         "Fishbone-Moncrief torus on their FMR hierarchies (16^3 blocks, refluxing, gather-map "
+                         "ghost fill)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
     ap.add_argument("--profile-step", action="store_true",
                     help="after the warm-up, run one eager RK3 step between cudaProfilerStart/Stop and exit "
@@ -238,6 +242,80 @@ def build_blast_on_device(blocks, su, nb, n, dev, torch, fields_cls, chunk=256):
     return st, aux
 
 
+def make_workload(args, dev):
+    """The timed workload: blocks, parameters, a device-field builder, the
+    ghost fill between stages, the bench line's config and data strings and
+    the CPU-reference sample."""
+    import torch
+    from grace_b200 import abi, params, workloads
+    from grace_b200.host import Blocks, Fields
+    nb, n = args.nb, args.n
+    if args.config == "blast":
+        su = workloads.BrickSetup((nb,) * 3, (n,) * 3, (-6,) * 3, (6,) * 3, 4, (False,) * 3)
+        blocks = Blocks(n, n, n, 4, su.nq, su.idx(), device=dev)
+        return {"blocks": blocks, "params": params.blast(), "idx": su.idx(),
+                "fields": lambda g: build_blast_on_device(blocks, su, nb, n, dev, torch, Fields),
+                "bc": lambda g: (lambda f: g.fill_ghosts_brick(f, su.nb, su.periodic)),
+                "config": _workload_config(nb, n), "data": "synthetic (seeded blast-wave initial data)",
+                "cpu": lambda: cpu_reference_run(8 if nb >= 8 else nb, n, args.cfl, min_s=10.0)}
+    if args.config == "tov":
+        H = workloads.tov_hierarchy(n)
+        (f, _), P = workloads.magnetised_tov(H), params.tov()
+        desc = (f"magnetised TOV star (K=100, Gamma=2, rho_c=1.28e-3; hybrid EOS Gamma_th=1.8; poloidal field "
+                f"max|B|=1e-4) in Cowling, +-48, {H.nq} blocks of {n}^3 on 5 FMR levels "
+                f"({'/'.join(str(c) for c in H.level_counts())}), WENO-Z+HLLE+GS CT+FOFC, refluxing, SSP-RK3")
+        data = "synthetic (TOV solution of the polytrope with seeded 1e-3 density noise)"
+    else:
+        H = workloads.torus_hierarchy(n)
+        f, P = workloads.fm_torus(H), params.torus()
+        desc = (f"Fishbone-Moncrief torus (a=0.9375, r_in=6, r_pmax=12, Gamma=4/3, beta=100) in fixed Kerr-Schild, "
+                f"+-40, {H.nq} blocks of {n}^3 on 4 FMR levels ({'/'.join(str(c) for c in H.level_counts())}), "
+                "WENO-Z+HLLE+GS CT+FOFC, refluxing, SSP-RK3")
+        data = "synthetic (Fishbone-Moncrief equilibrium with seeded 2% pressure noise)"
+    st, bx, by, bz, aux = f
+    H.fill_ghosts(st, bx, by, bz)
+    maps, R = H.gather_maps(), H.reflux_lists()
+    blocks = Blocks(n, n, n, H.ngz, H.nq, H.idx(), device=dev)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+    def fields(g):
+        g.set_reflux(R)
+        return Fields(T(st), T(bx), T(by), T(bz)), T(aux)
+
+    def cpu():
+        # one RK3 step of the whole hierarchy with the reference numerics
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import _oracle
+        which, kind = ("ref", "reference") if _oracle.lib("ref") is not None else ("orc", "port")
+        S = _oracle.Stage(P, n, n, n, H.ngz, H.nq, which)
+        S.set_reflux(R)
+        idx = H.idx()
+        state = [x.copy() for x in (st, bx, by, bz)]
+        a = aux.copy()
+        S.compute_aux(idx.copy(), state, a)
+        sp, spp = [x.copy() for x in state], [x.copy() for x in state]
+        dt = args.cfl / idx[:, 0].max()
+        t0 = time.perf_counter()
+        S.reset_diag(a)
+        for st_out, st_in, fac, comb in ((sp, state, 1.0, None), (spp, sp, 0.25, (0.75, 0.25)),
+                                         (state, spp, 2.0 / 3.0, (1.0 / 3.0, 2.0 / 3.0))):
+            if comb is not None:
+                S.linop(st_out, state, st_in, *comb)
+            S.advance_substep(idx.copy(), dt, fac, st_out, st_in, a)
+            H.fill_ghosts(*st_out)
+            S.compute_aux(idx.copy(), st_out, a)
+        el = time.perf_counter() - t0
+        cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+        return (H.nq * n ** 3 * 3 / el, cores, kind,
+                f"one RK3 step of the whole hierarchy ({H.nq} blocks) with refluxing and the host ghost fill, "
+                f"{kind} numerics, OpenMP over blocks on {cores} threads")
+
+    return {"blocks": blocks, "params": P, "idx": H.idx(), "fields": fields,
+            "bc": lambda g: (lambda fl: g.fill_ghosts_gather(fl, maps)),
+            "config": {"workload": desc, "blocks": H.nq, "cells_per_block": n ** 3, "ngz": H.ngz,
+                       "l2": "inputs larger than L2 (no flush)"}, "data": data, "cpu": cpu}
+
+
 def ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -247,21 +325,21 @@ def ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     nb, n = args.nb, args.n
-    su = workloads.BrickSetup((nb,) * 3, (n,) * 3, (-6,) * 3, (6,) * 3, 4, (False,) * 3)
-    blocks = Blocks(n, n, n, 4, su.nq, su.idx(), device=dev)
-    P = params.blast()
+    W = make_workload(args, dev)
+    blocks, P, nq = W["blocks"], W["params"], W["blocks"].nq
     if args.mode == "tuned":
         # aux pass and linop on the cells the next stage reads (the stage's
         # own ghost exchange refills the rest every substep)
         P.ranges = abi.RANGES_NEXT_STAGE
     g = GRMHDEquationsSystem(P)
     g.reserve(blocks)
-    state, aux = build_blast_on_device(blocks, su, nb, n, dev, torch, Fields)
-    bc = lambda f: g.fill_ghosts_brick(f, su.nb, su.periodic)
+    state, aux = W["fields"](g)
+    bc = W["bc"](g)
     bc(state)
     g.compute_auxiliary_quantities(state, aux)
     sp, spp = state.clone(), state.clone()
-    dt = args.cfl / su.idx()[0, 0]
+    idx_h = W["idx"]
+    dt = args.cfl / idx_h[:, 0].max()
     tuning = None
     if args.mode == "tuned":
         g.set_mode(abi.MODE_TUNED)
@@ -279,7 +357,7 @@ def ours(args, rank, world, local_rank):
 
     # each step also reduces the next stable time step (find_stable_timestep,
     # fused into the last aux pass); the bench keeps dt fixed
-    dx_d = torch.from_numpy(np.ascontiguousarray(1.0 / su.idx())).to(dev)
+    dx_d = torch.from_numpy(np.ascontiguousarray(1.0 / idx_h)).to(dev)
     dt_next = torch.zeros(1, dtype=torch.float64, device=dev)
     nd = (dx_d, args.cfl, dt_next)
     # warm-up: eager steps (one with the dt reduction fused into the last aux
@@ -308,8 +386,8 @@ def ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
         if rank == 0:
-            print(json.dumps({"profile_step": True, "blocks": su.nq, "cells_per_block": n ** 3,
-                              "zone_updates": su.nq * n ** 3 * 3, "tuning": tuning}), flush=True)
+            print(json.dumps({"profile_step": True, "blocks": nq, "cells_per_block": n ** 3,
+                              "zone_updates": nq * n ** 3 * 3, "tuning": tuning}), flush=True)
         g.close()
         return
     graph, per_step = None, None
@@ -351,7 +429,7 @@ def ours(args, rank, world, local_rank):
         t = torch.tensor([ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    zu_rank = su.nq * n ** 3 * 3 * args.steps
+    zu_rank = nq * n ** 3 * 3 * args.steps
     value = zu_rank * world / (ms * 1e-3)
 
     # --- the plain per-item form on the same state, for the speed-up ratio
@@ -368,7 +446,7 @@ def ours(args, rank, world, local_rank):
             g.rk3_step(dt, state, sp, spp, aux, bc)
         p1.record()
         torch.cuda.synchronize()
-        pv = su.nq * n ** 3 * 3 * psteps / (p0.elapsed_time(p1) * 1e-3)
+        pv = nq * n ** 3 * 3 * psteps / (p0.elapsed_time(p1) * 1e-3)
         plain = {"value": pv, "steps": psteps, "speedup_tuned_over_plain": (value / world) / pv}
         g.set_mode(abi.MODE_TUNED)
 
@@ -410,9 +488,9 @@ def ours(args, rank, world, local_rank):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
         nx = ny = nz = n
-        nbytes = 8 * su.nq * (abi.N_HRSC * nx * ny * nz + (nx + 1) * ny * nz + nx * (ny + 1) * nz +
+        nbytes = 8 * nq * (abi.N_HRSC * nx * ny * nz + (nx + 1) * ny * nz + nx * (ny + 1) * nz +
                               nx * ny * (nz + 1))
-        e2e = {"value": su.nq * n ** 3 * 3 * ksteps * world / (ems * 1e-3), "unit": "zone-updates/s",
+        e2e = {"value": nq * n ** 3 * 3 * ksteps * world / (ems * 1e-3), "unit": "zone-updates/s",
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ksteps,
                "note": "interior of the evolved variables (7 HRSC + face B) copied between packed pinned host "
                        "arrays and the device every step (grb_copy_evolved_packed: one DMA copy per array "
@@ -425,8 +503,7 @@ def ours(args, rank, world, local_rank):
     # variables by the 8-cell average, the 16 metric and curvature variables
     # by the 5-point Lagrange operator, and the three face-B arrays
     restrict = None
-    if not args.no_restrict and args.mode == "tuned":
-        nq = su.nq
+    if not args.no_restrict and args.mode == "tuned" and args.config == "blast":
         qs = torch.arange(nq, dtype=torch.int64, device=dev)
         ch = (qs % 8).to(torch.uint8)
         lo, hi = list(range(abi.N_HRSC)), list(range(abi.N_HRSC, abi.N_EVOL_VARS))
@@ -461,8 +538,7 @@ def ours(args, rank, world, local_rank):
     # one, face B by the divergence-preserving prolongation; the bench's
     # state serves as the coarse buffers and a scratch copy as the fine blocks
     prolong = None
-    if not args.no_restrict and args.mode == "tuned":
-        nq = su.nq
+    if not args.no_restrict and args.mode == "tuned" and args.config == "blast":
         lo, hi = list(range(abi.N_HRSC)), list(range(abi.N_HRSC, abi.N_EVOL_VARS))
         lists = []
         for kind, ne in ((0, 6), (1, 12), (2, 8)):
@@ -486,7 +562,7 @@ def ours(args, rank, world, local_rank):
         # algorithmic bytes: the fine ghost cells (and one face per ghost cell
         # and array) written once, the coarse cells and faces covering them
         # read once (1/8 and 1/4 as many)
-        NN = n + 2 * su.ngz
+        NN = n + 2 * 4
         vg = NN ** 3 - n ** 3
         pbytes = 8 * nq * (abi.N_EVOL_VARS * (vg + vg / 8) + 3 * (vg + vg / 4))
         prolong = {"quads": nq, "ms": pms, "ghost_cells_per_s": nq * vg / (pms * 1e-3),
@@ -526,9 +602,9 @@ def ours(args, rank, world, local_rank):
     # reads in the tuned form (GS: n+2 transverse, UCT: n+6)
     tr = (n + 8) if args.mode != "tuned" else ((n + 2) if P.emf == abi.EMF_GS else (n + 6))
     items = {
-        "flux": su.nq * (n + 3) * tr ** 2,
-        "aux": su.nq * (n + 8) ** 3,
-        "update": su.nq * n ** 3,
+        "flux": nq * (n + 3) * tr ** 2,
+        "aux": nq * (n + 8) ** 3,
+        "update": nq * n ** 3,
     }
     roof = None
     if name in ALGO_BYTES and kcnt:
@@ -571,12 +647,12 @@ def ours(args, rank, world, local_rank):
     # --- c2p micro-benchmark (2^24 states): plain, then with the learned
     # bracket trained on the GPU from 2^20 other seeded states
     c2p = None
-    if not args.no_c2p and rank == 0:
+    if not args.no_c2p and rank == 0 and args.config == "blast":
         c2p = c2p_bench(dev, learned=not args.no_learned)
 
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
-        v, cores, kind, sample = cpu_reference_run(8 if nb >= 8 else nb, n, args.cfl, min_s=10.0)
+        v, cores, kind, sample = W["cpu"]()
         cpu = {"value": v, "unit": "zone-updates/s", "cores": cores, "kind": kind, "sample": sample}
 
     if rank == 0:
@@ -584,8 +660,8 @@ def ours(args, rank, world, local_rank):
             "metric": "GRMHD zone-updates/s per RK stage", "value": value, "unit": "zone-updates/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded blast-wave initial data)",
-            "config": _workload_config(nb, n),
+            "data": W["data"],
+            "config": W["config"],
             "run": {"parallelism": f"replicas x{world}",
                        "launch": "cuda_graph" if graph is not None else "eager",
                        "step": "3 x (advance_substep + ghost fill + aux) + linops; the last aux pass "
