@@ -105,7 +105,8 @@ class Reflux(C.Structure):
 
 
 class Gather(C.Structure):
-    _fields_ = [("n", C.c_int64), ("dst", C.c_void_p), ("src", C.c_void_p), ("w", C.c_void_p)]
+    _fields_ = [("n", C.c_int64), ("cnt", C.c_void_p), ("dst", C.c_void_p), ("src", C.c_void_p),
+                ("w", C.c_void_p)]
 
 
 class C2PDiag(C.Structure):

@@ -485,25 +485,22 @@ __global__ void __launch_bounds__(128) k_prolong_faces(Geo G, Box box, double* _
   }
 }
 
-// Ghost fill by gather maps (grb_fill_ghosts_gather): entry e of a map
-// writes sum_t w[8 e + t] * a[src[8 e + t]] into a[dst[e]] for each of nv
-// variables, the flat indices counting one variable of the array (block q
-// at q * per + local, per the cells of one variable of a block); the sum is
-// accumulated in slot order with every product and sum rounded on its own.
-// Sources are never destinations (interior cells and faces only).
-__global__ void __launch_bounds__(256) k_ghost_gather(int64_t n, int nv, int64_t per, int64_t qstride,
+// Ghost fill by gather maps (grb_fill_ghosts_gather): entry e writes
+// sum over its cnt[e] used slots k of w[k n + e] * a[src[k n + e] + v vs]
+// into a[dst[e] + v vs] for variable v = blockIdx.y (vs the offset between
+// variables), accumulated in slot order with every product and sum rounded
+// on its own.  Sources are never destinations (interior cells and faces).
+__global__ void __launch_bounds__(256) k_ghost_gather(int64_t n, int64_t vstride, const int8_t* __restrict__ cnt,
                                                       const int64_t* __restrict__ dst,
                                                       const int64_t* __restrict__ src,
                                                       const double* __restrict__ w, double* __restrict__ a) {
-  const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n * nv) return;
-  const int64_t e = t % n;
-  const int v = (int)(t / n);
-  auto at = [&](int64_t f) { return (f / per) * qstride + (int64_t)v * per + f % per; };
-  double acc = __dmul_rn(w[8 * e], a[at(src[8 * e])]);
-#pragma unroll
-  for (int k = 1; k < 8; ++k) acc = __dadd_rn(acc, __dmul_rn(w[8 * e + k], a[at(src[8 * e + k])]));
-  a[at(dst[e])] = acc;
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n) return;
+  const int64_t vo = (int64_t)blockIdx.y * vstride;
+  const int c = cnt[e];
+  double acc = __dmul_rn(w[e], a[src[e] + vo]);
+  for (int k = 1; k < c; ++k) acc = __dadd_rn(acc, __dmul_rn(w[k * n + e], a[src[k * n + e] + vo]));
+  a[dst[e] + vo] = acc;
 }
 
 }  // namespace grb

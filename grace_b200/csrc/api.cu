@@ -70,6 +70,10 @@ struct grb_handle {
   float tune_aux_queue_ms = 0.f;
   bool mlp_ready = false;
   uint32_t fcap_alloc = 0;  // entries allocated for the compacted FOFC face list
+  // the tuned batch c2p's deferred entropy backups: records and their count
+  C2PDeferred* d_defer = nullptr;
+  int64_t defer_cap = 0;
+  unsigned long long* d_ndefer = nullptr;
   // refluxing (grb_set_reflux): the caller's descriptor lists and the edge
   // accumulation buffers
   bool reflux = false;
@@ -639,6 +643,8 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_stage_io);
   cudaFree(h->d_metder);
   cudaFree(h->d_refacc);
+  cudaFree(h->d_defer);
+  cudaFree(h->d_ndefer);
   delete h;
   return GRB_OK;
 }
@@ -963,15 +969,42 @@ int launch_c2p(grb_handle* h, int64_t n, const double* cons, const double* metri
   if (n > (int64_t)kC2PThreads * 0x7fffffff) return fail(h, GRB_ERR_INVALID);
   const unsigned nb = nblk(n, kC2PThreads);
   const bool fast = h->mode == GRB_MODE_TUNED;
-  if (learned && fast)
-    k_c2p_batch<true, true><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d,
-                                                       h->d_mlp_pack, h->d_flags);
-  else if (learned)
+  if (fast) {
+    // tuned mode: the entropy backups deferred to a second, compacted pass
+    if (n > h->defer_cap) {
+      cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+      if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+        return fail(h, GRB_ERR_INVALID);  // the first call of a size must come before any capture
+      cudaFree(h->d_defer);
+      h->d_defer = nullptr;
+      h->defer_cap = 0;
+      if (!h->d_ndefer && cudaMalloc(&h->d_ndefer, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, GRB_ERR_NOMEM);
+      }
+      if (cudaMalloc(&h->d_defer, sizeof(C2PDeferred) * (size_t)n) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(h, GRB_ERR_NOMEM);
+      }
+      h->defer_cap = n;
+    }
+    CK(cudaMemsetAsync(h->d_ndefer, 0, sizeof(unsigned long long), s));
+    if (learned)
+      k_c2p_batch_front<true, true><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d,
+                                                              h->d_mlp_pack, h->d_flags, h->d_defer, h->d_ndefer);
+    else
+      k_c2p_batch_front<false, true><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d,
+                                                               nullptr, h->d_flags, h->d_defer, h->d_ndefer);
+    const unsigned gb = (unsigned)std::min<int64_t>(nb, 148 * 16);
+    k_c2p_batch_backup<true><<<gb, kC2PThreads, 0, s>>>(h->dp, n, metric, prims, cons_out, err, h->d_flags,
+                                                       h->d_defer, h->d_ndefer);
+    h->launches += 2;
+    CK(cudaGetLastError());
+    return GRB_OK;
+  }
+  if (learned)
     k_c2p_batch<true><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, h->d_mlp_pack,
                                                  h->d_flags);
-  else if (fast)
-    k_c2p_batch<false, true><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, nullptr,
-                                                        h->d_flags);
   else
     k_c2p_batch<false><<<nb, kC2PThreads, 0, s>>>(h->dp, n, cons, metric, prims, cons_out, err, d, nullptr,
                                                   h->d_flags);
@@ -1681,22 +1714,24 @@ int grb_fill_ghosts_gather(grb_handle* h, const grb_grid* g, const grb_fields* f
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   cudaStream_t s = (cudaStream_t)stream;
   KScope ks(h, s, GRB_KIND_GHOST);
-  auto ok = [](const grb_gather* m) { return m->n >= 0 && (m->n == 0 || (m->dst && m->src && m->w)); };
+  auto ok = [](const grb_gather* m) {
+    return m->n >= 0 && m->n < (1ll << 40) && (m->n == 0 || (m->cnt && m->dst && m->src && m->w));
+  };
   if (cells && nvars > 0 && cells->n > 0) {
     if (!ok(cells) || !f->state) return fail(h, GRB_ERR_INVALID);
-    k_ghost_gather<<<nblk(cells->n * nvars, 256), 256, 0, s>>>(cells->n, nvars, G.cells, G.cells * GRB_N_EVOL_VARS,
-                                                               cells->dst, cells->src, cells->w, f->state);
+    const dim3 gr(nblk(cells->n, 256), (unsigned)nvars);
+    k_ghost_gather<<<gr, 256, 0, s>>>(cells->n, G.cells, cells->cnt, cells->dst, cells->src, cells->w, f->state);
     ++h->launches;
   }
   if (faces) {
     double* arr[3] = {f->bx, f->by, f->bz};
     const int64_t per[3] = {(int64_t)(G.NX + 1) * G.NY * G.NZ, (int64_t)G.NX * (G.NY + 1) * G.NZ,
-                            (int64_t)G.NX * G.NY * (G.NZ + 1)};
+                            (int64_t)G.NX * G.NY * (G.NZ + 1)};  // one variable of a block
     for (int d = 0; d < 3; ++d) {
       const grb_gather& m = faces[d];
       if (m.n <= 0) continue;
       if (!ok(&m) || !arr[d]) return fail(h, GRB_ERR_INVALID);
-      k_ghost_gather<<<nblk(m.n, 256), 256, 0, s>>>(m.n, 1, per[d], per[d], m.dst, m.src, m.w, arr[d]);
+      k_ghost_gather<<<nblk(m.n, 256), 256, 0, s>>>(m.n, per[d], m.cnt, m.dst, m.src, m.w, arr[d]);
       ++h->launches;
     }
   }

@@ -525,24 +525,37 @@ struct C2POut {
   double W, iW;  // Lorentz factor of the final primitives (tuned mode)
 };
 
-// conservs_to_prims (c2p.cpp:188-414).  c: densitized cons with densitized
-// cell-centred B (in), re-densitized consistent cons (out).
+// conservs_to_prims (c2p.cpp:188-414), in three parts so that a batch can
+// defer the entropy backup of the states that need it to a second pass
+// (c2p_front: up to the decision to distrust the Kastaun result;
+// c2p_backup: the entropy-based solve; c2p_back: signals, atmosphere,
+// temperature floor, limit_primitives, prims_to_cons).  c2p() runs the three
+// in sequence: the reference's order of operations.  c: densitized cons
+// with densitized cell-centred B (in), re-densitized consistent cons (out).
 // FAST (tuned mode): multiplications by 1/sqrt(gamma) and 1/D where the
 // reference divides repeatedly by the same value, the FAST master function,
 // and W, b^mu, b^2 formed once per set of primitives (WB) instead of in
 // each of the beta test, limit_primitives and prims_to_cons; equal to the
 // reference's operations up to rounding.  kAllCons false (tuned mode):
 // the returned cons hold only what the reset flags in o.err ask for.
-template <bool FAST = false, bool kAllCons = true>
-GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P, double r_sph,
-                  bool dry_run, double alp_bh_thresh, const Guess& gs) {
-  C2POut o{0u, 0u, 0, false, false, 0.0, 0.0, 0.0};
-  const double ialp = FAST ? 1.0 / m.alp : 0.0;
-  WB wb{};
-  bool wb_ok = false;  // wb belongs to the current z and B
+struct C2PState {
+  C2POut o;
+  uint32_t ret;
+  bool failed, lenient, ran, backup, done;
+  WB wb;
+  bool wb_ok;  // wb belongs to the current z and B
+};
+
+template <bool FAST = false>
+GRB_HD C2PState c2p_front(double c[10], double pr[13], const Met& m, const DevParams& P, bool dry_run,
+                          double alp_bh_thresh, const Guess& gs) {
+  C2PState F{};
+  F.o = C2POut{0u, 0u, 0, false, false, 0.0, 0.0, 0.0};
+  F.wb_ok = false;
+  F.failed = false;
+  F.ret = 0;
   const DevEos& e = P.eos;
-  bool failed = false;
-  uint32_t ret = 0;
+  C2POut& o = F.o;
   o.err = ERR_RESET_ENTROPY;
   const double isg = FAST ? 1.0 / m.sqrtg : 0.0;
 #pragma unroll
@@ -551,13 +564,14 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
   if (c[0] < 0) {
     reset_atmo(c, pr, m, P, o.err);
     o.floored = true;
-    return o;
+    F.done = true;
+    return F;
   }
   const double iD0 = FAST ? 1.0 / c[0] : 0.0;
   pr[GRB_P_YE] = FAST ? c[5] * iD0 : c[5] / c[0];
   if (pr[GRB_P_YE] > e.yemax) { pr[GRB_P_YE] = e.yemax; o.err |= ERR_RESET_YE; }
   if (pr[GRB_P_YE] < 0.0) { pr[GRB_P_YE] = 0.0; o.err |= ERR_RESET_YE; }
-  const bool lenient = m.alp < alp_bh_thresh;
+  F.lenient = m.alp < alp_bh_thresh;
   {  // limit_conservatives (c2p.cpp:117-157)
     double lo, hi;
     eos_eps_range(e, lo, hi, c[0]);
@@ -576,66 +590,88 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
       o.floored = true;
     }
   }
-  if (o.floored && dry_run) return o;
+  if (o.floored && dry_run) {
+    F.done = true;
+    return F;
+  }
   if (c[0] >= P.rho_fl * (1 + P.atmo_tol)) {
+    F.ran = true;
     Guess g2 = gs;
     if (o.floored) g2.has_mu0 = false;  // limit_conservatives changed the state
-    const double res = kastaun_invert<FAST>(e, m, c, pr, ret, o.iters, g2, o.guess_used, o.mu);
-    failed = (fabs(res) > P.tol) || (ret & SIG_RHO_HIGH) || (ret & SIG_EPS_HIGH) || !isfinite(res);
+    const double res = kastaun_invert<FAST>(e, m, c, pr, F.ret, o.iters, g2, o.guess_used, o.mu);
+    F.failed = (fabs(res) > P.tol) || (F.ret & SIG_RHO_HIGH) || (F.ret & SIG_EPS_HIGH) || !isfinite(res);
+    if (dry_run) return F;  // no backup in a dry run: beta is not needed
     double beta;
     if (FAST) {
-      wb = wb_of(m, pr);
-      wb_ok = true;
-      beta = 2.0 * pr[GRB_P_PRESS] / fmax(wb.b2, 1e-50);
+      F.wb = wb_of(m, pr);
+      F.wb_ok = true;
+      beta = 2.0 * pr[GRB_P_PRESS] / fmax(F.wb.b2, 1e-50);
     } else {
       const double W = lorentz(m.g, pr + GRB_P_ZX);
       double b[4], b2;
       comoving_b(m.alp, m.beta, m.g, pr + GRB_P_BX, pr + GRB_P_ZX, W, b, b2);
       beta = 2.0 * pr[GRB_P_PRESS] / fmax(b2, 1e-50);
     }
-    const bool distrust = failed || (ret & SIG_EPS_LOW) || (beta <= P.beta_fallback);
-    if (distrust && P.use_ent_backup && !dry_run) {
-      double save[13];
+    const bool distrust = F.failed || (F.ret & SIG_EPS_LOW) || (beta <= P.beta_fallback);
+    F.backup = distrust && P.use_ent_backup && !dry_run;
+  } else {
+    F.failed = true;
+  }
+  return F;
+}
+
+// The entropy-based backup of a distrusted Kastaun result (c2p.cpp:262-290).
+GRB_HD void c2p_backup(C2PState& F, double c[10], double pr[13], const Met& m, const DevParams& P) {
+  double save[13];
 #pragma unroll
-      for (int v = 0; v < 13; ++v) save[v] = pr[v];
-      uint32_t bret = 0;
-      const double rb = entropy_invert(e, m, c, pr, bret);
-      const bool ok = (fabs(rb) <= P.tol) && isfinite(rb) && (pr[GRB_P_EPS] < e.eps_max);
-      if (ok) {
-        ret = bret;
-        failed = false;
-        o.err |= ERR_ENT_BACKUP;
-        wb_ok = false;
-      } else if (!failed) {
+  for (int v = 0; v < 13; ++v) save[v] = pr[v];
+  uint32_t bret = 0;
+  const double rb = entropy_invert(P.eos, m, c, pr, bret);
+  const bool ok = (fabs(rb) <= P.tol) && isfinite(rb) && (pr[GRB_P_EPS] < P.eos.eps_max);
+  if (ok) {
+    F.ret = bret;
+    F.failed = false;
+    F.o.err |= ERR_ENT_BACKUP;
+    F.wb_ok = false;
+  } else if (!F.failed) {
 #pragma unroll
-        for (int v = 0; v < 13; ++v) pr[v] = save[v];
-      } else {
-        wb_ok = false;
-      }
-    }
+    for (int v = 0; v < 13; ++v) pr[v] = save[v];
+  } else {
+    F.wb_ok = false;
+  }
+}
+
+// kDry: a dry run (the FOFC flag's), which needs only o.floored: the final
+// prims_to_cons is skipped.
+template <bool FAST = false, bool kAllCons = true, bool kDry = false>
+GRB_HD void c2p_back(C2PState& F, double c[10], double pr[13], const Met& m, const DevParams& P, double r_sph) {
+  const DevEos& e = P.eos;
+  C2POut& o = F.o;
+  WB& wb = F.wb;
+  const double ialp = FAST ? 1.0 / m.alp : 0.0;
+  if (F.ran) {
+    const uint32_t ret = F.ret;
     if (ret & (SIG_EPS_HIGH | SIG_RHO_LOW | SIG_RHO_HIGH | SIG_VEL_HIGH)) o.floored = true;
     if (e.kind == GRB_EOS_IDEAL_GAS && (ret & SIG_EPS_LOW)) o.floored = true;
-    handle_sig(ret, lenient, o.err, o.fatal);
-  } else {
-    failed = true;
+    handle_sig(ret, F.lenient, o.err, o.fatal);
   }
   const bool excise = P.excise_by_radius ? (r_sph <= P.r_ex) : (m.alp <= P.alp_ex);
-  if (failed || excise || pr[GRB_P_RHO] < (1. + P.atmo_tol) * P.rho_fl) {
+  if (F.failed || excise || pr[GRB_P_RHO] < (1. + P.atmo_tol) * P.rho_fl) {
     reset_atmo(c, pr, m, P, o.err);
     o.floored = true;
-    wb_ok = false;
+    F.wb_ok = false;
   } else if (pr[GRB_P_TEMP] < P.temp_fl) {
     pr[GRB_P_TEMP] = P.temp_fl;
     double cs2;
     uint32_t q = 0;
     pr[GRB_P_PRESS] = eos_PT(e, pr[GRB_P_EPS], cs2, &pr[GRB_P_ENT], pr[GRB_P_TEMP], pr[GRB_P_RHO], q);
-    handle_eos_sig(q, lenient, o.err, o.fatal);
+    handle_eos_sig(q, F.lenient, o.err, o.fatal);
     o.err |= ERR_RESET_TAU | ERR_RESET_STILDE | ERR_RESET_ENTROPY | ERR_T_FLOORED;
     if (e.kind == GRB_EOS_IDEAL_GAS) o.floored = true;
   } else {  // limit_primitives (c2p.cpp:63-115)
     uint32_t s2 = 0;
     const double z2max = P.max_w * P.max_w - 1.;
-    if (FAST && !wb_ok) { wb = wb_of(m, pr); wb_ok = true; }
+    if (FAST && !F.wb_ok) { wb = wb_of(m, pr); F.wb_ok = true; }
     const double z2 = FAST ? wb.z2 : sqs(m.g, pr + GRB_P_ZX);
     if (z2 >= z2max) {
       const double zn = 0.99 * sqrt(z2max / z2);
@@ -659,18 +695,37 @@ GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P,
       pr[GRB_P_PRESS] = eos_PT(e, pr[GRB_P_EPS], cs2, &pr[GRB_P_ENT], pr[GRB_P_TEMP], pr[GRB_P_RHO], q);
       s2 |= SIG_SIGMA_HIGH;
     }
-    handle_sig(s2, lenient, o.err, o.fatal);
+    handle_sig(s2, F.lenient, o.err, o.fatal);
     if (s2 & (SIG_VEL_HIGH | SIG_SIGMA_HIGH)) o.floored = true;
   }
+  if (kDry) return;
   if (FAST) {
-    if (!wb_ok) wb = wb_of(m, pr);
+    if (!F.wb_ok) wb = wb_of(m, pr);
     prims_to_cons_wb(pr, c, m, wb, ialp, kAllCons ? ~0u : o.err);
     o.W = wb.W;
     o.iW = wb.iW;
   } else {
     prims_to_cons(pr, c, m);
   }
-  return o;
+}
+
+template <bool FAST = false, bool kAllCons = true>
+GRB_HD C2POut c2p(double c[10], double pr[13], const Met& m, const DevParams& P, double r_sph,
+                  bool dry_run, double alp_bh_thresh, const Guess& gs) {
+  C2PState F = c2p_front<FAST>(c, pr, m, P, dry_run, alp_bh_thresh, gs);
+  if (F.done) return F.o;
+  if (F.backup) c2p_backup(F, c, pr, m, P);
+  c2p_back<FAST, kAllCons>(F, c, pr, m, P, r_sph);
+  return F.o;
+}
+// The FOFC flag's dry run (c2p.cpp:188-414 with the dry-run flag): whether
+// the state would be floored; no entropy backup, no final prims_to_cons.
+template <bool FAST = false>
+GRB_HD bool c2p_floored(double c[10], double pr[13], const Met& m, const DevParams& P, double r_sph) {
+  C2PState F = c2p_front<FAST>(c, pr, m, P, true, 1e30, no_guess());
+  if (F.done) return F.o.floored;
+  c2p_back<FAST, true, true>(F, c, pr, m, P, r_sph);
+  return F.o.floored;
 }
 
 }  // namespace grb

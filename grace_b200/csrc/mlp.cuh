@@ -398,6 +398,137 @@ __global__ void __launch_bounds__(kC2PThreads) k_c2p_batch(DevParams P, int64_t 
   }
 }
 
+// ---- batched c2p with the entropy backup deferred ------------------------------
+// The states whose Kastaun result is distrusted (failed, eps too low, or
+// beta = 2P/b^2 <= beta_fallback) take the entropy-based backup solve.  In
+// a batch of mixed states nearly every warp holds some, so a one-pass
+// kernel runs both solves on every warp.  k_c2p_batch_front runs each
+// state up to that decision and finishes the trusted ones; the distrusted
+// ones are appended (warp-aggregated) to a list with their intermediate
+// state, and k_c2p_batch_backup runs the backup and the rest of the policy
+// on the listed states only, every warp of it busy with backups.  Each
+// state sees the same operations in the same order as in c2p(): only the
+// order in which states are processed changes.
+struct C2PDeferred {
+  double c[10];
+  double pr[13];
+  C2PState F;
+  int64_t t;
+};
+
+template <bool kLearned, bool kFast>
+__global__ void __launch_bounds__(kC2PThreads) k_c2p_batch_front(DevParams P, int64_t n,
+                                                                const double* __restrict__ cons,
+                                                                const double* __restrict__ metric,
+                                                                double* __restrict__ prims,
+                                                                double* __restrict__ cons_out,
+                                                                uint32_t* __restrict__ err, C2PDiagDev diag,
+                                                                const MlpSmem* __restrict__ net, uint32_t* flags,
+                                                                C2PDeferred* __restrict__ defer,
+                                                                unsigned long long* __restrict__ ndefer) {
+  __shared__ __align__(16) unsigned char smraw[kLearned ? sizeof(C2PLearnedSmem) : 16];
+  C2PLearnedSmem& S = *reinterpret_cast<C2PLearnedSmem*>(smraw);
+  if (kLearned) {
+    const uint4* src = reinterpret_cast<const uint4*>(net);
+    uint4* dst = reinterpret_cast<uint4*>(&S.net);
+    for (int w = threadIdx.x; w < (int)(sizeof(MlpSmem) / 16); w += kC2PThreads) dst[w] = src[w];
+    __syncthreads();
+  }
+  const int64_t t = (int64_t)blockIdx.x * kC2PThreads + threadIdx.x;
+  const bool active = t < n;
+  const int64_t ts = active ? t : 0;
+  const Met m = batch_metric(metric, n, ts);
+  double c[10], pr[13];
+#pragma unroll
+  for (int v = 0; v < 10; ++v) c[v] = active ? cons[v * n + t] : 0.0;
+  Guess gs = no_guess();
+  if (kLearned) {
+    float f[kMlpIn];
+    __nv_bfloat16 x[kMlpK0];
+    const double mu0 = active ? plain_mu0(P.eos, m, c) : 0.0;
+    if (active) mlp_features(c, m, mu0, f);
+    else {
+#pragma unroll
+      for (int k = 0; k < kMlpIn; ++k) f[k] = S.net.nrm.fmu[k];
+    }
+    mlp_inputs(S.net.nrm, f, x);
+    const float out = mlp_warp32(S.net, S.xs[threadIdx.x >> 5], x);
+    gs = mlp_bracket(S.net.nrm, out, mu0);
+  }
+  C2PState F{};
+  if (active) F = c2p_front<kFast>(c, pr, m, P, false, P.alp_bh_thresh, gs);
+  const bool later = active && !F.done && F.backup;
+  // one slot per deferred lane, one atomic per warp
+  const unsigned mask = __ballot_sync(0xffffffffu, later);
+  unsigned long long base = 0;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0 && mask) base = atomicAdd(ndefer, (unsigned long long)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  if (!active) return;
+  if (diag.iters) diag.iters[t] = F.o.iters;
+  if (diag.guess_used) diag.guess_used[t] = F.o.guess_used ? 1 : 0;
+  if (diag.mu) diag.mu[t] = F.o.mu;
+  if (diag.bracket) {
+    diag.bracket[t] = gs.valid ? gs.lo : 0.0;
+    diag.bracket[n + t] = gs.valid ? gs.hi : 0.0;
+  }
+  if (later) {
+    C2PDeferred& d = defer[base + __popc(mask & ((1u << lane) - 1u))];
+#pragma unroll
+    for (int v = 0; v < 10; ++v) d.c[v] = c[v];
+#pragma unroll
+    for (int v = 0; v < 13; ++v) d.pr[v] = pr[v];
+    d.F = F;
+    d.t = t;
+    return;
+  }
+  if (!F.done) c2p_back<kFast>(F, c, pr, m, P, 0.0);
+  if (F.o.fatal) atomicOr(flags, F.o.fatal);
+  pr[GRB_P_CS2] = 0.0;
+#pragma unroll
+  for (int v = 0; v < 13; ++v) prims[v * n + t] = pr[v];
+  if (cons_out) {
+#pragma unroll
+    for (int v = 0; v < 10; ++v) cons_out[v * n + t] = c[v];
+  }
+  if (err) err[t] = F.o.err;
+}
+
+// The listed states: the entropy backup and the rest of the policy
+// (grid-stride over the count the front kernel left).
+template <bool kFast>
+__global__ void __launch_bounds__(kC2PThreads) k_c2p_batch_backup(DevParams P, int64_t n,
+                                                                 const double* __restrict__ metric,
+                                                                 double* __restrict__ prims,
+                                                                 double* __restrict__ cons_out,
+                                                                 uint32_t* __restrict__ err, uint32_t* flags,
+                                                                 const C2PDeferred* __restrict__ defer,
+                                                                 const unsigned long long* __restrict__ ndefer) {
+  const int64_t nd = (int64_t)*ndefer;
+  for (int64_t e = (int64_t)blockIdx.x * kC2PThreads + threadIdx.x; e < nd; e += (int64_t)gridDim.x * kC2PThreads) {
+    const C2PDeferred& d = defer[e];
+    double c[10], pr[13];
+#pragma unroll
+    for (int v = 0; v < 10; ++v) c[v] = d.c[v];
+#pragma unroll
+    for (int v = 0; v < 13; ++v) pr[v] = d.pr[v];
+    C2PState F = d.F;
+    const int64_t t = d.t;
+    const Met m = batch_metric(metric, n, t);
+    c2p_backup(F, c, pr, m, P);
+    c2p_back<kFast>(F, c, pr, m, P, 0.0);
+    if (F.o.fatal) atomicOr(flags, F.o.fatal);
+    pr[GRB_P_CS2] = 0.0;
+#pragma unroll
+    for (int v = 0; v < 13; ++v) prims[v * n + t] = pr[v];
+    if (cons_out) {
+#pragma unroll
+      for (int v = 0; v < 10; ++v) cons_out[v * n + t] = c[v];
+    }
+    if (err) err[t] = F.o.err;
+  }
+}
+
 // ---- training data ----------------------------------------------------------
 // Raw features [6][n] and target y = asinh(log(mu0 / mu) / L0) [n] (NaN where
 // the plain c2p did not reach the Kastaun solve) from the states and the

@@ -445,8 +445,7 @@ __global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box
   if (!dmp) {  // the c2p dry run only matters when the DMP test passed
     const Met m = cell_met(G, os, i, j, k, q);
     double pr[13];
-    const Guess none = no_guess();
-    floored = c2p<kFast>(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), true, 1e30, none).floored;
+    floored = c2p_floored<kFast>(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q));
   }
   if (floored || dmp) {
     int8_t* T = B.ftag;

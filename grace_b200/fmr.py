@@ -341,11 +341,11 @@ class Hierarchy:
         return P
 
     def gather_maps(self):
-        """Ghost-fill gather maps: for the cells (key "cells") and the face
-        arrays staggered along x, y, z (keys 0, 1, 2), arrays dst (m,) of flat
-        indices into one variable of the block arrays (q x cells per block +
-        local), src (m, 8) of flat source indices and w (m, 8) of weights
-        (unused slots weight 0 on the first source).  A ghost cell takes the
+        """Ghost-fill gather maps for the cells (key "cells") and the face
+        arrays staggered along x, y, z (keys 0, 1, 2), each a dict in the
+        format of grb_gather: cnt (m,) used slots, dst (m,) element offsets of
+        variable 0, src (8, m) and w (8, m) slot-major, vstride the offset
+        between variables.  A ghost cell takes the
         leaf data at its place: a copy from a same-level cell, the containing
         coarser cell, or the mean of the 8 finer cells; a ghost face a copy,
         the coarser face it lies on (or the linear interpolation between the
@@ -454,33 +454,48 @@ class Hierarchy:
                     fk = flatf(k3)
                     src[finer, t_] = fk[finer]
                     w[finer, t_] = 0.25
-            out[arr] = (dst, src, w)
+            out[arr] = self._pack(arr, dst, src, w, per)
         self._gmaps = out
         return out
+
+    @staticmethod
+    def _pack(arr, dst, src, w, per):
+        """The maps in the library's format (grb_gather): element offsets of
+        variable 0 of the target array (the state holds N_EVOL_VARS
+        variables per block), slot-major sources and weights, the number of
+        used slots per entry."""
+        def off(f):
+            if arr != "cells":
+                return f
+            return (f // per) * (abi.N_EVOL_VARS * per) + f % per
+        cnt = np.maximum(1, np.sum(w != 0.0, axis=1)).astype(np.int8)
+        # used slots first (they are, by construction), unused ones weight 0
+        return {"cnt": cnt, "dst": off(dst), "src": np.ascontiguousarray(off(src).T),
+                "w": np.ascontiguousarray(w.T), "vstride": per}
+
+    @staticmethod
+    def _apply(flat, m, v):
+        """One map on variable v of a flat array: w0 v0 + w1 v1 + ... over
+        the used slots, accumulated in slot order, one product and one sum
+        rounded at a time (as grb_fill_ghosts_gather does)."""
+        o = v * m["vstride"]
+        src, w, cnt = m["src"], m["w"], m["cnt"]
+        acc = w[0] * flat[src[0] + o]
+        for k in range(1, 8):
+            use = cnt > k
+            if not np.any(use):
+                break
+            acc = np.where(use, acc + w[k] * flat[np.where(use, src[k], src[0]) + o], acc)
+        flat[m["dst"] + o] = acc
 
     def fill_ghosts(self, state, bx, by, bz, nvars=abi.N_HRSC):
         """Composite ghost fill of the first nvars state variables and face B
         (host numpy arrays in the library layout), in place, with the maps of
-        gather_maps: each value is w0 v0 + w1 v1 + ... + w7 v7 accumulated in
-        slot order, one product and one sum rounded at a time (the device
-        fill, grb_fill_ghosts_gather, gives the same bits).  Sources are
-        interior cells and faces only."""
+        gather_maps (the device fill, grb_fill_ghosts_gather, gives the same
+        bits).  Sources are interior cells and faces only."""
         M = self.gather_maps()
-        NN = self.n + 2 * self.ngz
-        per = NN ** 3
-        dst, src, w = M["cells"]
-        S = state.reshape(self.nq, state.shape[1], per)
+        flat = state.reshape(-1)
         for v in range(nvars):
-            sv = np.ascontiguousarray(S[:, v, :]).reshape(-1)
-            acc = w[:, 0] * sv[src[:, 0]]
-            for t_ in range(1, 8):
-                acc = acc + w[:, t_] * sv[src[:, t_]]
-            sv[dst] = acc
-            S[:, v, :] = sv.reshape(self.nq, per)
+            self._apply(flat, M["cells"], v)
         for d, arr in enumerate((bx, by, bz)):
-            dst, src, w = M[d]
-            flat = arr.reshape(-1)
-            acc = w[:, 0] * flat[src[:, 0]]
-            for t_ in range(1, 8):
-                acc = acc + w[:, t_] * flat[src[:, t_]]
-            flat[dst] = acc
+            self._apply(arr.reshape(-1), M[d], 0)

@@ -389,11 +389,12 @@ class GRMHDEquationsSystem:
         key = id(maps)
         if getattr(self, "_gmaps_key", None) != key:
             dev = self.blocks.device
-            up = lambda t: tuple(torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in t)
+            up = lambda m: {k: torch.from_numpy(np.ascontiguousarray(m[k])).to(dev) for k in ("cnt", "dst", "src", "w")}
             self._gmaps = {k: up(v) for k, v in maps.items()}
             self._gmaps_key = key
         G = self._gmaps
-        mk = lambda t: abi.Gather(t[0].numel(), t[0].data_ptr(), t[1].data_ptr(), t[2].data_ptr())
+        mk = lambda t: abi.Gather(t["dst"].numel(), t["cnt"].data_ptr(), t["dst"].data_ptr(), t["src"].data_ptr(),
+                                  t["w"].data_ptr())
         cells = mk(G["cells"])
         faces = (abi.Gather * 3)(mk(G[0]), mk(G[1]), mk(G[2]))
         g = self.blocks.c()

@@ -284,7 +284,12 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A,
  *          state, the plain bracket when the learned one misses the root);
  *          GRB_ERR_NO_MODEL without a model.
  * GRB_MODE_TUNED evaluates the c2p with the tuned-mode arithmetic (the same
- * functions up to rounding: fewer divisions, W and b^2 formed once). */
+ * functions up to rounding: fewer divisions, W and b^2 formed once) and
+ * defers the entropy-based backup solves to a second pass over the states
+ * that need them (compacted, so its warps are uniform; each state's
+ * operations and their order unchanged).  The handle keeps one record per
+ * state for that pass: the first tuned call with a larger n allocates it
+ * (make it before any stream capture). */
 int grb_c2p_batch(grb_handle* h, int64_t n, const double* cons,
                   const double* metric, double* prims, double* cons_out,
                   uint32_t* err, int32_t use_learned, void* stream);
@@ -559,16 +564,17 @@ int grb_prolong_to_ghosts(grb_handle* h, const grb_grid* g, const grb_fields* fi
                           const int32_t* vars_ho, int32_t nho, void* stream);
 
 /* ---- ghost fill by gather maps (harness-side helper) --------------------- */
-/* One gather map: entry e sets a[dst[e]] = sum over t < 8 of w[8 e + t] *
- * a[src[8 e + t]] (accumulated in slot order, each product and sum rounded
- * on its own), the flat indices counting the cells of one variable of the
- * array: block q's local cell c at q * (cells of one variable of a block) +
- * c.  Unused slots carry weight 0. */
+/* One gather map: entry e sets, for each variable v, a[dst[e] + v vs] =
+ * the sum over its cnt[e] (1..8) slots k of w[k n + e] * a[src[k n + e] +
+ * v vs] (accumulated in slot order, each product and sum rounded on its
+ * own); dst and src are element offsets of variable 0 in the array, vs the
+ * cells of one variable of a block. */
 typedef struct grb_gather {
   int64_t n;
+  const int8_t* cnt;   /* [n] device */
   const int64_t* dst;  /* [n] device */
-  const int64_t* src;  /* [n][8] device */
-  const double* w;     /* [n][8] device */
+  const int64_t* src;  /* [8][n] device, slot-major */
+  const double* w;     /* [8][n] device, slot-major */
 } grb_gather;
 /* No counterpart in the reference (its ghost exchange is the host's): fills
  * the ghost zones of f by precomputed gather maps, cells for the first nvars

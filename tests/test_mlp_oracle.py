@@ -181,3 +181,31 @@ def test_oracle_bracket_changes_iterations_not_results():
     pr2, _, e2, it2, gu2, _, _ = _oracle.c2p_batch_guess(P, cons, lo2, hi2)
     assert not gu2.any()
     assert np.array_equal(pr2, pr0) and np.array_equal(it2, it0)
+
+
+def test_plain_solver_window_exceeds_flat_1e12():
+    """The acceptance bound of a learned bracket against the plain c2p.
+    Brent stops within 2 eps |mu| + 1e-15 of the root in mu
+    (kastaun_c2p.hh:372, rootfinding.hh:73-231): an absolute window, so a
+    state with small mu (hot or magnetised) has a relative window up to
+    1e-15 / mu in mu, and W = (1 - v^2)^(-1/2) amplifies it by ~W^2 in the
+    primitives.  The plain solver itself, started from any other valid
+    bracket around the root, moves the primitives of about 17 % of the c2p
+    workload's states by more than 1e-12 (up to ~1e-9 at W ~ 50), with every
+    state within 1e-12 x max(1, W^2): a flat 1e-12 is not a property of the
+    plain path, the W^2-scaled bound is, and the learned bracket is held to
+    that bound (same error bits, residual <= 1e-12 max(1, W^2))."""
+    from parity import prim_tol, state_residual
+    P = params.c2p_bench()
+    n = 1 << 16
+    cons, _ = workloads.c2p_states(n, seed=5)
+    z = np.zeros(n)
+    pr0, _, err0, _, _, mu0, _ = _oracle.c2p_batch_guess(P, cons, z, z)
+    assert np.all(mu0 > 0)
+    # the same plain solve from the bracket [0.9 mu, mu0]: same function,
+    # same tolerance, another start
+    pr1, _, err1, _, used, mu1, _ = _oracle.c2p_batch_guess(P, cons, 0.9 * mu0, np.full(n, 1e300))
+    assert used.mean() == 1.0 and np.array_equal(err0, err1)
+    r = state_residual(pr1, pr0)
+    assert 0.05 < np.mean(r > 1e-12) < 0.5 and r.max() > 1e-10
+    assert np.all(r <= prim_tol(pr0))
