@@ -68,6 +68,7 @@ struct grb_handle {
   uint32_t auxlist_n = 0;
   int auxlist_key[4] = {0, 0, 0, 0};      // nx, ny, nz, ngz it was built for
   float tune_aux_queue_ms = 0.f;
+  float tune_aux_defer_ms = 0.f;
   bool mlp_ready = false;
   uint32_t fcap_alloc = 0;  // entries allocated for the compacted FOFC face list
   // the tuned batch c2p's deferred entropy backups: records and their count
@@ -338,12 +339,40 @@ void launch_aux_queue(cudaStream_t s, const DevParams& P, const Geo& G, const Bo
   k_aux_queue<MINB, kDt, true><<<grid, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, dta);
 }
 
+// The aux pass with the entropy backups deferred to a second kernel over
+// the listed cells (when the handle holds the list).
+template <int MINB, bool kDt>
+void launch_aux_deferred(unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b, double* st,
+                         const double* bx, const double* by, const double* bz, double* aux, const double* idx,
+                         const double* crd, const StageBufs& B, const DtArgs& dta) {
+  cudaMemsetAsync(B.nadefer, 0, sizeof(unsigned long long), s);
+  k_aux_front<MINB, kDt, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, dta);
+  k_aux_backup<MINB, kDt, true><<<std::min(nb, 148u * 8u), 128, 0, s>>>(P, G, st, bx, by, bz, aux, idx, crd, B,
+                                                                       dta);
+}
+
 // Aux candidates: 0..2 one thread per cell at kMinB[v] CTAs/SM; 3..5 the
-// work-queue form at kMinB[v - 3].
+// work-queue form at kMinB[v - 3]; 6..8 the deferred-backup form at
+// kMinB[v - 6].
 void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                       double* st, const double* bx, const double* by, const double* bz, double* aux,
                       const double* idx, const double* crd, const StageBufs& B,
                       const DtArgs* dta = nullptr, unsigned long long* queue = nullptr) {
+  if (v >= 6 && B.adefer) {
+    const DtArgs d0{nullptr, 0.0, nullptr};
+    const int m = v - 6;
+    if (dta) {
+      if (m == 1) launch_aux_deferred<4, true>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+      else if (m == 2) launch_aux_deferred<5, true>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+      else launch_aux_deferred<1, true>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+    } else {
+      if (m == 1) launch_aux_deferred<4, false>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, d0);
+      else if (m == 2) launch_aux_deferred<5, false>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, d0);
+      else launch_aux_deferred<1, false>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, d0);
+    }
+    return;
+  }
+  if (v >= 6) v -= 6;
   if (v >= 3 && queue) {
     const DtArgs d0{nullptr, 0.0, nullptr};
     const int m = v - 3;
@@ -395,6 +424,32 @@ void launch_linop_box(cudaStream_t s, const LinBox& L, int nv, int64_t nq, doubl
                       const double* y, double b, double c) {
   const dim3 grid((unsigned)((L.ny * L.N0 + 255) / 256), (unsigned)(L.nz * nv), (unsigned)nq);
   k_linop_box<<<grid, 256, 0, s>>>(L, nv, a, x, y, b, c);
+}
+
+// The deferred aux pass's cell list: one record per aux cell of the grid, at
+// most 2^24 (cells past the capacity finish in place).  Not inside a
+// stream capture.
+bool ensure_aux_defer(grb_handle* h, int64_t cells) {
+  const int64_t cap = std::min<int64_t>(cells, 1ll << 24);
+  if (h->B.adefer && h->B.adefer_cap >= cap) return true;
+  cudaFree(h->B.adefer);
+  h->B.adefer = nullptr;
+  h->B.adefer_cap = 0;
+  if (!h->B.nadefer && cudaMalloc(&h->B.nadefer, sizeof(unsigned long long)) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (cudaMalloc(&h->B.adefer, sizeof(AuxDeferred) * (size_t)cap) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  h->B.adefer_cap = cap;
+  return true;
+}
+void free_aux_defer(grb_handle* h) {
+  cudaFree(h->B.adefer);
+  h->B.adefer = nullptr;
+  h->B.adefer_cap = 0;
 }
 
 // Aux pass and linop on the next stage's cells only (tuned mode with
@@ -643,6 +698,8 @@ int grb_destroy(grb_handle* h) {
   cudaFree(h->d_stage_io);
   cudaFree(h->d_metder);
   cudaFree(h->d_refacc);
+  cudaFree(h->B.adefer);
+  cudaFree(h->B.nadefer);
   cudaFree(h->d_defer);
   cudaFree(h->d_ndefer);
   delete h;
@@ -1808,31 +1865,61 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
   if (rc) return fail(h, rc);
   if (!nw || !old || !aux) return fail(h, GRB_ERR_INVALID);
   cudaStream_t s = (cudaStream_t)stream;
+  // a sample of nt blocks spread evenly over the grid (block k*nq/nt), so
+  // that the candidates see every level of a hierarchy, not only its first
   const int64_t nt = g->nq < 96 ? g->nq : 96;
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, nt);
-  const size_t cs = sizeof(double) * G.cells * nt;
-  const size_t fx = sizeof(double) * (size_t)(G.NX + 1) * G.NY * G.NZ * nt;
-  const size_t fy = sizeof(double) * (size_t)G.NX * (G.NY + 1) * G.NZ * nt;
-  const size_t fz = sizeof(double) * (size_t)G.NX * G.NY * (G.NZ + 1) * nt;
+  const size_t c1 = sizeof(double) * G.cells;  // one variable of one block
+  const size_t cs = c1 * nt;
+  const size_t f1[3] = {sizeof(double) * (size_t)(G.NX + 1) * G.NY * G.NZ,
+                        sizeof(double) * (size_t)G.NX * (G.NY + 1) * G.NZ,
+                        sizeof(double) * (size_t)G.NX * G.NY * (G.NZ + 1)};
+  const size_t fsz[3] = {f1[0] * nt, f1[1] * nt, f1[2] * nt};
   double *ns = nullptr, *os = nullptr, *ax = nullptr, *b3[6] = {nullptr};
+  double *pns = nullptr, *pax = nullptr, *pb3[3] = {nullptr}, *sidx = nullptr, *scrd = nullptr;
   bool ok = cudaMalloc(&ns, cs * GRB_N_EVOL_VARS) == cudaSuccess &&
             cudaMalloc(&os, cs * GRB_N_EVOL_VARS) == cudaSuccess &&
-            cudaMalloc(&ax, cs * GRB_N_AUX_VARS) == cudaSuccess;
-  const size_t fsz[3] = {fx, fy, fz};
+            cudaMalloc(&ax, cs * GRB_N_AUX_VARS) == cudaSuccess &&
+            cudaMalloc(&pns, cs * GRB_N_EVOL_VARS) == cudaSuccess &&
+            cudaMalloc(&pax, cs * GRB_N_AUX_VARS) == cudaSuccess &&
+            cudaMalloc(&sidx, sizeof(double) * 3 * nt) == cudaSuccess &&
+            (!g->coords || cudaMalloc(&scrd, sizeof(double) * 3 * nt) == cudaSuccess);
   for (int a = 0; a < 6 && ok; ++a) ok = cudaMalloc(&b3[a], fsz[a % 3]) == cudaSuccess;
+  for (int a = 0; a < 3 && ok; ++a) ok = cudaMalloc(&pb3[a], fsz[a]) == cudaSuccess;
   auto cleanup = [&]() {
-    cudaFree(ns); cudaFree(os); cudaFree(ax);
+    cudaFree(ns); cudaFree(os); cudaFree(ax); cudaFree(pns); cudaFree(pax); cudaFree(sidx); cudaFree(scrd);
     for (int a = 0; a < 6; ++a) cudaFree(b3[a]);
+    for (int a = 0; a < 3; ++a) cudaFree(pb3[a]);
   };
   if (!ok) { cleanup(); cudaGetLastError(); return fail(h, GRB_ERR_NOMEM); }
-  cudaMemcpyAsync(ns, nw->state, cs * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
-  cudaMemcpyAsync(os, old->state, cs * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
-  cudaMemcpyAsync(ax, aux, cs * GRB_N_AUX_VARS, cudaMemcpyDeviceToDevice, s);
   const double* srcb[6] = {nw->bx, nw->by, nw->bz, old->bx, old->by, old->bz};
-  for (int a = 0; a < 6; ++a) cudaMemcpyAsync(b3[a], srcb[a], fsz[a % 3], cudaMemcpyDeviceToDevice, s);
+  for (int64_t k = 0; k < nt; ++k) {
+    const int64_t q = k * g->nq / nt;
+    cudaMemcpyAsync(ns + k * G.cells * GRB_N_EVOL_VARS, nw->state + q * G.cells * GRB_N_EVOL_VARS,
+                    c1 * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(os + k * G.cells * GRB_N_EVOL_VARS, old->state + q * G.cells * GRB_N_EVOL_VARS,
+                    c1 * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(ax + k * G.cells * GRB_N_AUX_VARS, aux + q * G.cells * GRB_N_AUX_VARS, c1 * GRB_N_AUX_VARS,
+                    cudaMemcpyDeviceToDevice, s);
+    for (int a = 0; a < 6; ++a) {
+      const size_t e = f1[a % 3] / sizeof(double);
+      cudaMemcpyAsync(b3[a] + k * e, srcb[a] + q * e, f1[a % 3], cudaMemcpyDeviceToDevice, s);
+    }
+    cudaMemcpyAsync(sidx + 3 * k, g->idx + 3 * q, 3 * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (scrd) cudaMemcpyAsync(scrd + 3 * k, g->coords + 3 * q, 3 * sizeof(double), cudaMemcpyDeviceToDevice, s);
+  }
+  // pristine copies of what the candidates modify
+  cudaMemcpyAsync(pns, ns, cs * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
+  cudaMemcpyAsync(pax, ax, cs * GRB_N_AUX_VARS, cudaMemcpyDeviceToDevice, s);
+  for (int a = 0; a < 3; ++a) cudaMemcpyAsync(pb3[a], b3[a], fsz[a], cudaMemcpyDeviceToDevice, s);
   grb_fields fn{ns, b3[0], b3[1], b3[2]}, fo{os, b3[3], b3[4], b3[5]};
   grb_grid gs = *g;
   gs.nq = nt;
+  gs.idx = sidx;
+  gs.coords = scrd;
+  // the static-metric cache of the first nt blocks stands in for the
+  // sample's (the timing reads it the same way; the values do not matter)
+  const double* md = static_metric(h, make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq), g->idx);
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -1843,9 +1930,9 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
   // restore the copies before every launch so that each candidate sees the
   // same input (the update and aux kernels modify their arrays)
   auto restore = [&]() {
-    cudaMemcpyAsync(ns, nw->state, cs * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
-    cudaMemcpyAsync(ax, aux, cs * GRB_N_AUX_VARS, cudaMemcpyDeviceToDevice, s);
-    for (int a = 0; a < 3; ++a) cudaMemcpyAsync(b3[a], srcb[a], fsz[a], cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(ns, pns, cs * GRB_N_EVOL_VARS, cudaMemcpyDeviceToDevice, s);
+    cudaMemcpyAsync(ax, pax, cs * GRB_N_AUX_VARS, cudaMemcpyDeviceToDevice, s);
+    for (int a = 0; a < 3; ++a) cudaMemcpyAsync(b3[a], pb3[a], fsz[a], cudaMemcpyDeviceToDevice, s);
   };
   auto time_it = [&](auto&& fn_launch) {
     restore();
@@ -1884,7 +1971,7 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
                                             fo.by, fo.bz, gs.idx, gs.coords, B); });
       else if (fam == 2)
         t = time_it([&] { launch_update_tuned(v, nblk(ub.count(), 128), s, P, G, ub, 1e-12, 1.0, ns, os, ax,
-                                              gs.idx, B, static_metric(h, G, gs.idx)); });
+                                              gs.idx, B, md); });
       else
         t = time_it([&] { launch_aux_tuned(v, nblk(ab.count(), 128), s, P, G, ab, ns, fn.bx, fn.by, fn.bz,
                                            ax, gs.idx, gs.coords, B); });
@@ -1897,7 +1984,22 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
     launch_aux_tuned(best[3] + 3, nblk(ab.count(), 128), s, P, G, ab, ns, fn.bx, fn.by, fn.bz, ax, gs.idx,
                      gs.coords, B, nullptr, h->d_queue);
   });
-  if (h->tune_aux_queue_ms < h->tune_ms[3][best[3]]) best[3] += 3;
+  // and the deferred-backup form of the same cap (its list allocated for the
+  // whole grid's aux cells, and freed again if another form wins)
+  const Box abig = trimmed(h) ? tuned_aux_box(h, make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq), s)
+                              : box(0, 0, 0, G.NX, G.NY, G.NZ, g->nq);
+  float defer_ms = 1e30f;
+  if (ensure_aux_defer(h, abig.count())) {
+    B = h->B;
+    defer_ms = time_it([&] {
+      launch_aux_tuned(best[3] + 6, nblk(ab.count(), 128), s, P, G, ab, ns, fn.bx, fn.by, fn.bz, ax, gs.idx,
+                       gs.coords, B);
+    });
+  }
+  h->tune_aux_defer_ms = defer_ms;
+  if (h->tune_aux_queue_ms < h->tune_ms[3][best[3]] && h->tune_aux_queue_ms <= defer_ms) best[3] += 3;
+  else if (defer_ms < h->tune_ms[3][best[3]]) best[3] += 6;
+  if (best[3] < 6) free_aux_defer(h);
   h->var_flux = best[0];
   h->var_flag = best[1];
   h->var_update = best[2];
@@ -1917,7 +2019,7 @@ int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   variant[0] = kFluxMinB[h->var_flux] + (kFluxTma[h->var_flux] ? 100 : 0);
   variant[1] = kMinB[h->var_flag];
   variant[2] = h->d_metder ? kMinBCached[h->var_update] : kMinB[h->var_update];
-  variant[3] = kMinB[h->var_aux % 3] + (h->var_aux >= 3 ? 100 : 0);
+  variant[3] = kMinB[h->var_aux % 3] + 100 * (h->var_aux / 3);
   if (ms)
     for (int f = 0; f < 4; ++f)
       for (int v = 0; v < kNumVar; ++v) ms[f * kNumVar + v] = h->tune_ms[f][v];
@@ -1927,7 +2029,15 @@ int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
 int grb_set_tuning(grb_handle* h, const int32_t* variant) {
   if (!h || !variant) return GRB_ERR_INVALID;
   for (int f = 0; f < 4; ++f)
-    if (variant[f] < 0 || variant[f] >= (f == 3 ? 2 * kNumVar : kNumVar)) return fail(h, GRB_ERR_INVALID);
+    if (variant[f] < 0 || variant[f] >= (f == 3 ? 3 * kNumVar : kNumVar)) return fail(h, GRB_ERR_INVALID);
+  if (variant[3] >= 2 * kNumVar) {
+    // the deferred-backup aux pass: its list, for the reserved grid
+    if (!h->reserved) return fail(h, GRB_ERR_NOT_RESERVED);
+    const Box ab = h->p.ranges == GRB_RANGES_NEXT_STAGE && h->dp.emf == GRB_EMF_GS
+                       ? tuned_aux_box(h, h->geo, nullptr)
+                       : box(0, 0, 0, h->geo.NX, h->geo.NY, h->geo.NZ, h->geo.nq);
+    if (!ensure_aux_defer(h, ab.count())) return fail(h, GRB_ERR_NOMEM);
+  }
   h->var_flux = variant[0];
   h->var_flag = variant[1];
   h->var_update = variant[2];

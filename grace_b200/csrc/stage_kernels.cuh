@@ -24,6 +24,10 @@ struct StageBufs {
   int8_t* etag;     // FOFC edge tags
   unsigned long long* counters;  // [0] faces, [1] edges recomputed by FOFC
   uint32_t* flags;  // device status word
+  // the deferred aux pass's list of cells (AuxDeferred records) and count
+  void* adefer = nullptr;
+  unsigned long long* nadefer = nullptr;
+  int64_t adefer_cap = 0;
   // compacted list of the tagged faces (tuned mode): entries t << 2 | dir
   // (t the FOFC box index), *fcount of them, room for fcap
   uint32_t* flist = nullptr;
@@ -772,38 +776,51 @@ __global__ void __launch_bounds__(128) k_dt(DevParams P, Geo G, Box box, const d
 // ---- aux: c2p on every cell + resets + C2P_ERR + BDIV + cell-centred E -----
 // kDt: also the time-step reduction over the interior cells, from the
 // primitives just computed (the aux pass that ends an RK step).
-// One cell of the aux pass; returns the cell's dt candidate (kDt, interior
-// cells) or +inf.
+// One cell of the aux pass in three parts: aux_load (the cell's densitized
+// cons and cell-centred B, the metric, aux B), the c2p (in one piece, or
+// deferred at the entropy backup), aux_finish (prims, resets, C2P_ERR,
+// BDIV, the cell-centred E, the dt candidate of an interior cell (kDt) or
+// +inf).
+struct AuxIn {
+  double c[10];
+  double bf[6];  // bx0, bx1, by0, by1, bz0, bz1
+};
+__device__ __forceinline__ Met aux_load(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
+                                        const double* __restrict__ st, const double* __restrict__ bx,
+                                        const double* __restrict__ by, const double* __restrict__ bz,
+                                        double* __restrict__ aux, bool write_b, bool kFast, AuxIn& A) {
+  const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
+  const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
+  A.bf[0] = bx[bxi(G, i, j, k, q)]; A.bf[1] = bx[bxi(G, i + 1, j, k, q)];
+  A.bf[2] = by[byi(G, i, j, k, q)]; A.bf[3] = by[byi(G, i, j + 1, k, q)];
+  A.bf[4] = bz[bzi(G, i, j, k, q)]; A.bf[5] = bz[bzi(G, i, j, k + 1, q)];
+#pragma unroll
+  for (int v = 0; v < 7; ++v) A.c[v] = st[c0 + G.cells * v];
+  A.c[7] = 0.5 * (A.bf[0] + A.bf[1]);
+  A.c[8] = 0.5 * (A.bf[2] + A.bf[3]);
+  A.c[9] = 0.5 * (A.bf[4] + A.bf[5]);
+  const Met m = cell_met(G, st, i, j, k, q);
+  if (write_b) {
+    const double isg = kFast ? 1.0 / m.sqrtg : 0.0;
+    aux[a0 + G.cells * GRB_BX] = kFast ? A.c[7] * isg : A.c[7] / m.sqrtg;
+    aux[a0 + G.cells * GRB_BY] = kFast ? A.c[8] * isg : A.c[8] / m.sqrtg;
+    aux[a0 + G.cells * GRB_BZ] = kFast ? A.c[9] * isg : A.c[9] / m.sqrtg;
+  }
+  (void)P;
+  return m;
+}
+// After the c2p: c, pr the c2p's output; A the cell's inputs (A.c its
+// cons before the c2p).
 template <bool kDt, bool kFast>
-__device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
-                                           double* __restrict__ st, const double* __restrict__ bx,
-                                           const double* __restrict__ by, const double* __restrict__ bz,
-                                           double* __restrict__ aux, const double* __restrict__ idx,
-                                           const double* __restrict__ coords, const StageBufs& B,
-                                           const DtArgs& dta) {
+__device__ __forceinline__ double aux_finish(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
+                                             double* __restrict__ st, double* __restrict__ aux,
+                                             const double* __restrict__ idx, const Met& m, const AuxIn& A,
+                                             const double c[10], const double pr[13], const C2POut& o,
+                                             const StageBufs& B, const DtArgs& dta) {
   double dtc = INFINITY;
   const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
   const int64_t c0 = cvar(G, i, j, k, 0, GRB_N_EVOL_VARS, q);
   const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
-  const double bx0 = bx[bxi(G, i, j, k, q)], bx1 = bx[bxi(G, i + 1, j, k, q)];
-  const double by0 = by[byi(G, i, j, k, q)], by1 = by[byi(G, i, j + 1, k, q)];
-  const double bz0 = bz[bzi(G, i, j, k, q)], bz1 = bz[bzi(G, i, j, k + 1, q)];
-  double c[10], orig[7];
-#pragma unroll
-  for (int v = 0; v < 7; ++v) { c[v] = st[c0 + G.cells * v]; orig[v] = c[v]; }
-  c[7] = 0.5 * (bx0 + bx1);
-  c[8] = 0.5 * (by0 + by1);
-  c[9] = 0.5 * (bz0 + bz1);
-  const Met m = cell_met(G, st, i, j, k, q);
-  const double isg = kFast ? 1.0 / m.sqrtg : 0.0;
-  aux[a0 + G.cells * GRB_BX] = kFast ? c[7] * isg : c[7] / m.sqrtg;
-  aux[a0 + G.cells * GRB_BY] = kFast ? c[8] * isg : c[8] / m.sqrtg;
-  aux[a0 + G.cells * GRB_BZ] = kFast ? c[9] * isg : c[9] / m.sqrtg;
-  const double cbx = c[7], cby = c[8], cbz = c[9];
-  double pr[13];
-  const Guess none = no_guess();
-  const C2POut o =
-      c2p<kFast, !kFast>(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), false, P.alp_bh_thresh, none);
   if (o.fatal) atomicOr(B.flags, o.fatal);
   aux[a0 + G.cells * GRB_RHO] = pr[GRB_P_RHO];
   aux[a0 + G.cells * GRB_EPS] = pr[GRB_P_EPS];
@@ -815,7 +832,7 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
   aux[a0 + G.cells * GRB_ZVECY] = pr[GRB_P_ZY];
   aux[a0 + G.cells * GRB_ZVECZ] = pr[GRB_P_ZZ];
   if (o.err & ERR_RESET_DENS) {
-    aux[a0 + G.cells * GRB_C2P_DENS_ERR] += orig[GRB_DENS] - c[0];
+    aux[a0 + G.cells * GRB_C2P_DENS_ERR] += A.c[GRB_DENS] - c[0];
     st[c0] = c[0];
   }
   if (o.err & ERR_RESET_STILDE)
@@ -828,10 +845,12 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
     aux[a0 + G.cells * GRB_C2P_ERR] = (double)(prev | (uint64_t)o.err);
   }
   {
-    const double dv = (bx1 - bx0) * ix[0] + (by1 - by0) * ix[1] + (bz1 - bz0) * ix[2];
+    const double isg = kFast ? 1.0 / m.sqrtg : 0.0;
+    const double dv = (A.bf[1] - A.bf[0]) * ix[0] + (A.bf[3] - A.bf[2]) * ix[1] + (A.bf[5] - A.bf[4]) * ix[2];
     aux[a0 + G.cells * GRB_BDIV] = kFast ? dv * isg : dv / m.sqrtg;
   }
   if (P.emf == GRB_EMF_GS) {
+    const double cbx = A.c[7], cby = A.c[8], cbz = A.c[9];
     // tuned mode: 1/W of the final primitives from the c2p
     const double W = kFast ? o.W : sqrt(1. + sqs(m.g, pr + GRB_P_ZX));
     double vt[3];
@@ -846,6 +865,40 @@ __device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int
     dtc = dta.cfl / max_eigenspeed(P.eos, m, pr) * dta.dx[3 * q];
   return dtc;
 }
+
+template <bool kDt, bool kFast>
+__device__ __forceinline__ double aux_cell(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
+                                           double* __restrict__ st, const double* __restrict__ bx,
+                                           const double* __restrict__ by, const double* __restrict__ bz,
+                                           double* __restrict__ aux, const double* __restrict__ idx,
+                                           const double* __restrict__ coords, const StageBufs& B,
+                                           const DtArgs& dta) {
+  AuxIn A;
+  const Met m = aux_load(P, G, i, j, k, q, st, bx, by, bz, aux, true, kFast, A);
+  double c[10], pr[13];
+#pragma unroll
+  for (int v = 0; v < 10; ++v) c[v] = A.c[v];
+  const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
+  const Guess none = no_guess();
+  const C2POut o =
+      c2p<kFast, !kFast>(c, pr, m, P, cell_r(G, coords, ix, i, j, k, q), false, P.alp_bh_thresh, none);
+  return aux_finish<kDt, kFast>(P, G, i, j, k, q, st, aux, idx, m, A, c, pr, o, B, dta);
+}
+
+// The aux pass with the entropy backups deferred (tuned candidate, for
+// blocks where many cells take the backup: a cold atmosphere, magnetised
+// regions): k_aux_front runs each cell up to the decision to distrust its
+// Kastaun result and finishes the trusted ones; the distrusted ones go to
+// a list (up to B.adefer_cap; beyond it a cell finishes in place), and
+// k_aux_backup runs the backup and the rest for the listed cells.  Every
+// cell's operations and their order are those of aux_cell.
+struct AuxDeferred {
+  double c[10];
+  double pr[13];
+  C2PState F;
+  int32_t i, j, k;
+  int64_t q;
+};
 
 // One thread per cell over the box.
 template <int MINB = 1, bool kDt = false, bool kFast = false>
@@ -897,6 +950,89 @@ __global__ void __launch_bounds__(128, MINB) k_aux_queue(DevParams P, Geo G, Box
       if (kDt) dt_reduce(dtc, dta.out);
     }
   }
+}
+
+template <int MINB = 1, bool kDt = false, bool kFast = false>
+__global__ void __launch_bounds__(128, MINB) k_aux_front(DevParams P, Geo G, Box box, double* __restrict__ st,
+                                                    const double* __restrict__ bx,
+                                                    const double* __restrict__ by,
+                                                    const double* __restrict__ bz,
+                                                    double* __restrict__ aux,
+                                                    const double* __restrict__ idx,
+                                                    const double* __restrict__ coords, StageBufs B,
+                                                    DtArgs dta = DtArgs{nullptr, 0.0, nullptr}) {
+  int i = 0, j = 0, k = 0;
+  int64_t q = 0;
+  double dtc = INFINITY;
+  const bool active = decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q);
+  AuxIn A;
+  Met m;
+  double c[10], pr[13];
+  C2PState F{};
+  double r = 0.0;
+  if (active) {
+    m = aux_load(P, G, i, j, k, q, st, bx, by, bz, aux, true, kFast, A);
+#pragma unroll
+    for (int v = 0; v < 10; ++v) c[v] = A.c[v];
+    const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
+    r = cell_r(G, coords, ix, i, j, k, q);
+    F = c2p_front<kFast>(c, pr, m, P, false, P.alp_bh_thresh, no_guess());
+  }
+  const bool later = active && !F.done && F.backup;
+  const unsigned mask = __ballot_sync(0xffffffffu, later);
+  unsigned long long base = 0;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0 && mask) base = atomicAdd(B.nadefer, (unsigned long long)__popc(mask));
+  base = __shfl_sync(0xffffffffu, base, 0);
+  const unsigned long long slot = base + __popc(mask & ((1u << lane) - 1u));
+  if (active) {
+    if (later && slot < (unsigned long long)B.adefer_cap) {
+      AuxDeferred& d = static_cast<AuxDeferred*>(B.adefer)[slot];
+#pragma unroll
+      for (int v = 0; v < 10; ++v) d.c[v] = c[v];
+#pragma unroll
+      for (int v = 0; v < 13; ++v) d.pr[v] = pr[v];
+      d.F = F;
+      d.i = i; d.j = j; d.k = k; d.q = q;
+    } else {
+      if (!F.done) {
+        if (F.backup) c2p_backup(F, c, pr, m, P);
+        c2p_back<kFast, !kFast>(F, c, pr, m, P, r);
+      }
+      dtc = aux_finish<kDt, kFast>(P, G, i, j, k, q, st, aux, idx, m, A, c, pr, F.o, B, dta);
+    }
+  }
+  if (kDt) dt_reduce(dtc, dta.out);
+}
+template <int MINB = 1, bool kDt = false, bool kFast = false>
+__global__ void __launch_bounds__(128, MINB) k_aux_backup(DevParams P, Geo G, double* __restrict__ st,
+                                                     const double* __restrict__ bx,
+                                                     const double* __restrict__ by,
+                                                     const double* __restrict__ bz,
+                                                     double* __restrict__ aux,
+                                                     const double* __restrict__ idx,
+                                                     const double* __restrict__ coords, StageBufs B,
+                                                     DtArgs dta = DtArgs{nullptr, 0.0, nullptr}) {
+  const int64_t nd = (int64_t)min(*B.nadefer, (unsigned long long)B.adefer_cap);
+  double dtc = INFINITY;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < nd; e += (int64_t)gridDim.x * blockDim.x) {
+    const AuxDeferred& d = static_cast<const AuxDeferred*>(B.adefer)[e];
+    const int i = d.i, j = d.j, k = d.k;
+    const int64_t q = d.q;
+    AuxIn A;
+    const Met m = aux_load(P, G, i, j, k, q, st, bx, by, bz, aux, false, kFast, A);
+    double c[10], pr[13];
+#pragma unroll
+    for (int v = 0; v < 10; ++v) c[v] = d.c[v];
+#pragma unroll
+    for (int v = 0; v < 13; ++v) pr[v] = d.pr[v];
+    C2PState F = d.F;
+    const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
+    c2p_backup(F, c, pr, m, P);
+    c2p_back<kFast, !kFast>(F, c, pr, m, P, cell_r(G, coords, ix, i, j, k, q));
+    dtc = fmin(dtc, aux_finish<kDt, kFast>(P, G, i, j, k, q, st, aux, idx, m, A, c, pr, F.o, B, dta));
+  }
+  if (kDt) dt_reduce(dtc, dta.out);
 }
 
 // reset_c2p_diagnostics (evolve.cpp:154-161)

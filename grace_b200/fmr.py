@@ -328,16 +328,18 @@ class Hierarchy:
         assert np.all(lev >= 0)
         return lev, qi
 
-    def _domain(self, P):
-        """Wrap periodic axes, clamp the others into the domain (a ghost
-        cell outside a non-periodic boundary takes the data of the nearest
-        leaf cell: zero-gradient)."""
+    def _domain(self, P, s):
+        """Wrap periodic axes; on the others move a point outside the domain
+        to the nearest cell centre of its own spacing s inside it (a ghost
+        cell beyond a non-periodic boundary takes the data of the nearest
+        leaf region of its size: zero-gradient), so that the region of size
+        s around it stays inside the domain."""
         P = P.copy()
         for a in range(3):
             if self.periodic[a]:
                 P[:, a] %= self.N[a]
             else:
-                P[:, a] = np.clip(P[:, a], 0, self.N[a] - 1)
+                P[:, a] = np.clip(P[:, a], s // 2, self.N[a] - s // 2)
         return P
 
     def gather_maps(self):
@@ -381,7 +383,7 @@ class Hierarchy:
                     P[:, a] = (bb[Q, a] * n + ca - g) * s + s // 2
             dst = Q * per + np.tile(loc, self.nq)
             if arr == "cells":
-                W = self._domain(P)
+                W = self._domain(P, s)
                 tl, tq = self._lookup(W)
                 st = (np.array([self.E(l) for l in range(self.L + 1)]) // n)[tl]
                 base_b = bb[tq]
@@ -414,7 +416,7 @@ class Hierarchy:
                         top = W[:, a] >= self.N[a]
                         W[:, a] = np.clip(W[:, a], 0, self.N[a])
                     else:
-                        W[:, a] = np.clip(W[:, a], 0, self.N[a] - 1)
+                        W[:, a] = np.clip(W[:, a], s // 2, self.N[a] - s // 2)
                 Wl = W.copy()
                 Wl[top, d] -= 1  # the cell below a face on the upper boundary
                 tl, tq = self._lookup(Wl)

@@ -386,14 +386,16 @@ def tov_pressure(sol, ri):
 
 
 def magnetised_tov(hier, kappa=100.0, gamma=2.0, rho_c=1.28e-3, gamma_th=1.8, rho_atm=1e-10,
-                   eps_th=1e-10, bmax=1e-4, p_cut=0.04, a_n=2.0, noise=1e-3, seed=SEED):
+                   eps_th=1e-4, bmax=1e-4, p_cut=0.04, a_n=2.0, noise=1e-3, seed=SEED):
     """The magnetised polytropic neutron star in Cowling (the TOV solution
     above: K=100, Gamma=2, rho_c=1.28e-3, ~1.4 solar masses) on the leaves
     of a static FMR hierarchy: conformally flat metric psi^4 delta_ij, the
     lapse, zero shift and extrinsic curvature (static); rest-mass density
     with seeded relative noise (counter hash of each cell's level and
-    integer position), cold pressure and energy of the polytrope plus a tiny
-    thermal part (hybrid EOS with Gamma_th); atmosphere rho_atm outside; an
+    integer position), cold pressure and energy of the polytrope plus a
+    small uniform specific thermal energy eps_th (hybrid EOS with Gamma_th;
+    1e-4 keeps the entropy, a logarithm of eps - eps_cold, well conditioned
+    next to eps_cold ~ 0.1 at the centre); atmosphere rho_atm outside; an
     interior poloidal field from A = A_b max(P - p_cut P_c, 0)^a_n (-y, x, 0)
     (the form of GRACE's Avec_poloidal_id_t), taken as the discrete curl on
     each block's edges (div B = 0 to round-off) and scaled so that

@@ -389,22 +389,28 @@ int grb_mlp_grad(grb_handle* h, int64_t n, const float* params,
 enum grb_mode { GRB_MODE_PLAIN = 0, GRB_MODE_TUNED = 1 };
 int grb_set_mode(grb_handle* h, int32_t mode);
 /* Times the register-cap variants of the flux, FOFC-flag, update and aux
- * kernels on device copies of the first blocks of the grid (the arrays
- * passed in are only read) and keeps the fastest for the tuned mode.
- * Allocates and frees temporary copies; synchronises the stream. */
+ * kernels on device copies of up to 96 blocks spread evenly over the grid
+ * (block k nq / 96: every level of a hierarchy ordered by level is
+ * represented; the arrays passed in are only read) and keeps the fastest
+ * for the tuned mode.  Allocates and frees temporary copies; synchronises
+ * the stream. */
 int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* new_state,
                  const grb_fields* old_state, const double* aux, void* stream);
 /* variant[4]: chosen minimum-CTAs-per-SM of flux, flag, update, aux (flux:
  * plus 100 when the TMA-staged shared-memory kernel was chosen; update: of
  * the kernel that reads the static-metric cache when one is set; aux: plus
- * 100 when the work-queue form was chosen);
+ * 100 for the work-queue form, plus 200 for the deferred-backup form);
  * ms[12] (or NULL): timed milliseconds of the 3 candidates per family. */
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms);
 /* Choose the tuned-mode candidates without timing: variant[4] = candidate
  * index 0..2 of flux, flag, update, aux (flux: 0 global-load kernel, 1 and 2
  * TMA-staged kernel at 4 and 5 CTAs/SM; others: 1, 4, 5 CTAs/SM; aux also
  * 3..5: the work-queue form — one wave of CTAs pulling chunks of 128-cell
- * tiles from a device counter — at 1, 4, 5 CTAs/SM). */
+ * tiles from a device counter — at 1, 4, 5 CTAs/SM, and 6..8: the
+ * deferred-backup form — the cells whose Kastaun result is distrusted
+ * listed and finished by a second kernel running their entropy backups
+ * together — at 1, 4, 5 CTAs/SM, its list allocated here for the reserved
+ * grid: call before any stream capture). */
 int grb_set_tuning(grb_handle* h, const int32_t* variant);
 
 /* Capacity, in faces, of the compacted list through which GRB_MODE_TUNED

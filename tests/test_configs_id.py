@@ -90,3 +90,14 @@ def test_gather_maps_copy_same_level_ghosts_exactly(which):
     assert same.mean() > 0.5
     flat, ref = st.reshape(-1), before.reshape(-1)
     assert np.array_equal(flat[m["dst"][same]], ref[m["src"][0][same]])
+
+
+@pytest.mark.parametrize("which", ["tov", "torus"])
+def test_gather_sources_are_interior(which):
+    """Every source of the ghost-fill maps is an interior cell or face (no
+    source is written by the same fill), also beyond non-periodic
+    boundaries, so the device fill can run every entry at once."""
+    H = workloads.tov_hierarchy(8) if which == "tov" else workloads.torus_hierarchy(8)
+    for key, m in H.gather_maps().items():
+        used = np.arange(8)[:, None] < m["cnt"][None, :]
+        assert not np.any(np.isin(m["src"][used], m["dst"])), key

@@ -235,3 +235,25 @@ def test_tuned_default_ranges_fill_every_cell(name):
     assert e.max() < STEP_TOL, e
     m, mo = gs[0][:, 7:], os_[0][:, 7:]
     assert np.max(np.abs(m - mo)) <= 1e-15 * np.max(np.abs(mo))
+
+
+@pytest.mark.parametrize("aux", [6, 7, 8])
+def test_deferred_backup_aux_pass_matches_oracle(aux):
+    """The aux pass with the entropy backups deferred to a second kernel
+    (tuned aux candidates 6..8) on the curved-metric blob with
+    beta_fallback raised to 1e3, so that nearly every cell distrusts its
+    Kastaun result and takes the backup: one RK3 step against the oracle,
+    C2P_ERR bit for bit (ERR_ENT_BACKUP on most cells)."""
+    from curved import curved_setup
+    P, su, f = curved_setup(emf=abi.EMF_GS, fofc=1)
+    P.beta_fallback = 1e3
+    dt = 0.25 / su.idx()[0, 0]
+    gs, ga, g = _gpu(P, su, f, dt, 1, abi.MODE_TUNED, tuning=(1, 1, 1, aux))
+    assert g.tuning()["aux"]["min_ctas_per_sm"] == [201, 204, 205][aux - 6]
+    os_, oa, counts = _oracle_run(P, su, f, dt, 1)
+    _check_state(gs, os_, su.ngz)
+    sel = (slice(None), tuned_aux_mask(su))
+    _check_aux(ga, oa, sel)
+    backup = (ga[:, abi.C2P_ERR][sel].astype(np.uint64) >> 19) & 1
+    assert backup.mean() > 0.5
+    assert g.status().device_flags == 0
