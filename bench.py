@@ -82,6 +82,10 @@ def parse():
                          "Fishbone-Moncrief torus on their FMR hierarchies (16^3 blocks, refluxing, gather-map "
                          "ghost fill)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
+    ap.add_argument("--e2e-runs", type=int, default=8,
+                    help="end-to-end leg: runs of blocks the host step pipelines over (1: no pipeline)")
+    ap.add_argument("--ref-blocks", type=int, default=8,
+                    help="reference arm: blocks per axis of the CPU sample (the central ones; --nb for the whole grid)")
     ap.add_argument("--profile-step", action="store_true",
                     help="after the warm-up, run one eager RK3 step between cudaProfilerStart/Stop and exit "
                          "(for ncu --profile-from-start off)")
@@ -198,12 +202,13 @@ def cpu_reference_run(nb_side, n, cfl, min_s=10.0):
 
 def reference_arm(args, rank):
     """The CPU reference on the host cores, rank 0 only: W warm-up and K
-    timed steps, each one RK3 step of the bounded sample (the central 8^3 of
-    the 16^3 blocks: an eighth of the workload, ~3 s per step on 16
-    threads), so that the whole run takes a couple of minutes."""
+    timed steps, each one RK3 step of the bounded sample (by default the
+    central 8^3 of the 16^3 blocks: an eighth of the workload, ~3 s per step
+    on 16 threads, so that the whole run takes a couple of minutes;
+    --ref-blocks 16 steps the whole grid)."""
     if rank != 0:
         return
-    R = CpuReference(8 if args.nb >= 8 else args.nb, args.n, args.cfl)
+    R = CpuReference(min(args.ref_blocks, args.nb), args.n, args.cfl)
     for _ in range(args.warmup):
         R.step()
     t0 = time.perf_counter()
@@ -242,6 +247,15 @@ def build_blast_on_device(blocks, su, nb, n, dev, torch, fields_cls, chunk=256):
     return st, aux
 
 
+def _brick_pipeline(g, su, nruns):
+    """(runs, fill_run, deps) of rk3_step_host for the brick: runs of whole
+    z-slabs of blocks, each filled by the block-range brick fill."""
+    from grace_b200.host import brick_runs
+    runs, deps = brick_runs(su.nb, su.periodic, nruns)
+    fill_run = lambda f, s, stream: g.fill_ghosts_brick(f, su.nb, su.periodic, stream=stream, blocks=runs[s])
+    return runs, fill_run, deps
+
+
 def make_workload(args, dev):
     """The timed workload: blocks, parameters, a device-field builder, the
     ghost fill between stages, the bench line's config and data strings and
@@ -256,6 +270,7 @@ def make_workload(args, dev):
         return {"blocks": blocks, "params": params.blast(), "idx": su.idx(),
                 "fields": lambda g: build_blast_on_device(blocks, su, nb, n, dev, torch, Fields),
                 "bc": lambda g: (lambda f: g.fill_ghosts_brick(f, su.nb, su.periodic)),
+                "runs": lambda g, nruns: _brick_pipeline(g, su, nruns),
                 "config": _workload_config(nb, n), "data": "synthetic (seeded blast-wave initial data)",
                 "cpu": lambda: cpu_reference_run(8 if nb >= 8 else nb, n, args.cfl, min_s=10.0)}
     if args.config == "tov":
@@ -271,7 +286,7 @@ def make_workload(args, dev):
         desc = (f"Fishbone-Moncrief torus (a=0.9375, r_in=6, r_pmax=12, Gamma=4/3, beta=100) in fixed Kerr-Schild, "
                 f"+-40, {H.nq} blocks of {n}^3 on 4 FMR levels ({'/'.join(str(c) for c in H.level_counts())}), "
                 "WENO-Z+HLLE+GS CT+FOFC, refluxing, SSP-RK3")
-        data = "synthetic (Fishbone-Moncrief equilibrium with seeded 2% pressure noise)"
+        data = "synthetic (Fishbone-Moncrief equilibrium with seeded 2% pressure and 0.1% density noise)"
     st, bx, by, bz, aux = f
     H.fill_ghosts(st, bx, by, bz)
     maps, R = H.gather_maps(), H.reflux_lists()
@@ -472,7 +487,13 @@ def ours(args, rank, world, local_rank):
             side.wait_stream(main)
             g.copy_evolved_packed(host, state, to_device=False, stream=side, arrays=faces_only)
 
+        pipe = W["runs"](g, args.e2e_runs) if ("runs" in W and args.e2e_runs > 1) else None
+        io = (torch.cuda.Stream(), torch.cuda.Stream())
         for _ in range(ksteps):
+            if pipe is not None:
+                runs, fill_run, deps = pipe
+                g.rk3_step_host(dt, host, state, sp, spp, aux, bc, runs, fill_run, deps, streams=io)
+                continue
             main.wait_stream(side)
             g.copy_evolved_packed(host, state, to_device=True)
             bc(state)
@@ -494,9 +515,15 @@ def ours(args, rank, world, local_rank):
                "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes, "steps": ksteps,
                "note": "interior of the evolved variables (7 HRSC + face B) copied between packed pinned host "
                        "arrays and the device every step (grb_copy_evolved_packed: one DMA copy per array "
-                       "through a device staging buffer; face B downloaded on a second stream once the last "
-                       "substep has made it final); each step refills the ghost zones and recomputes the "
+                       "through a device staging buffer); each step refills the ghost zones and recomputes the "
                        "primitives of the uploaded state first"}
+        if pipe is not None:
+            e2e["pipeline"] = (f"GRMHDEquationsSystem.rk3_step_host over {len(pipe[0])} runs of z-slabs of blocks: "
+                               "each run's upload overlaps the first substep of the runs before it, its download "
+                               "the last substep of the runs after it (upload, kernels, download on three streams)")
+        else:
+            e2e["pipeline"] = ("none: upload, refill, primitives, rk3_step, download in sequence (face B downloaded "
+                               "on a second stream once the last substep has made it final)")
 
     # --- FMR restriction into coarse buffers (a separate measurement, not
     # part of the step): every block restricted into a buffer, the 7 HRSC

@@ -189,6 +189,9 @@ PROTOTYPES = {
     "grb_fill_ghosts_brick": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields),
                                         C.c_int32, C.c_int32, C.c_int32,
                                         C.POINTER(C.c_int32), C.c_void_p]),
+    "grb_fill_ghosts_brick_range": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields),
+                                              C.c_int32, C.c_int32, C.c_int32,
+                                              C.POINTER(C.c_int32), C.c_int64, C.c_int64, C.c_void_p]),
     "grb_restrict_to_coarse": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Fields),
                                          C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int32),
                                          C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_void_p]),

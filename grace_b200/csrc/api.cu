@@ -226,11 +226,12 @@ PFN_cuTensorMapEncodeTiled_v12000 tma_encoder() {
   }
   return fn;
 }
-// Tile of direction dir for the face box b (one block's face ranges).
-FluxTile flux_tile(int dir, const Geo& G, const Box& b) {
+// Tile of direction dir for the face box b (one block's face ranges), for
+// CTAs of nt threads.
+FluxTile flux_tile(int dir, const Geo& G, const Box& b, int nt) {
   FluxTile T;
   for (int a = 0; a < 3; ++a) { T.lo[a] = b.lo[a]; T.n[a] = b.n[a]; }
-  T.R = 128 / T.n[0];
+  T.R = nt / T.n[0];
   T.BY = dir == 0 ? T.R : dir == 1 ? T.R + 5 : 1;
   T.BZ = dir == 2 ? T.R + 5 : 1;
   (void)G;
@@ -254,11 +255,11 @@ bool make_tmap(CUtensorMap* tm, const double* base, const Geo& G, int nv, int64_
              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
-template <int dir, int MINB>
+template <int dir, int MINB, int NT = 128>
 bool launch_flux_tma(cudaStream_t s, const DevParams& P, const Geo& G, const Box& b, const double* st,
                      const double* aux, const double* bf, const StageBufs& B) {
-  const FluxTile T = flux_tile(dir, G, b);
-  if (T.n[0] > 128 || b.nq > 65535) return false;
+  const FluxTile T = flux_tile(dir, G, b, NT);
+  if (T.n[0] > NT || b.nq > 65535) return false;
   CUtensorMap ta, tm;
   if (!make_tmap(&ta, aux, G, GRB_N_AUX_VARS, b.nq, T) || !make_tmap(&tm, st, G, GRB_N_EVOL_VARS, b.nq, T))
     return false;
@@ -268,7 +269,7 @@ bool launch_flux_tma(cudaStream_t s, const DevParams& P, const Geo& G, const Box
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
   if (smem > attr[dev]) {
-    if (cudaFuncSetAttribute(k_flux_tma<dir, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+    if (cudaFuncSetAttribute(k_flux_tma<dir, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
       return false;
     attr[dev] = smem;
@@ -276,21 +277,24 @@ bool launch_flux_tma(cudaStream_t s, const DevParams& P, const Geo& G, const Box
   const int nrow = dir == 2 ? T.n[2] : T.n[1];
   const int nother = dir == 2 ? T.n[1] : T.n[2];
   const dim3 grid((unsigned)((nrow + T.R - 1) / T.R), (unsigned)nother, (unsigned)b.nq);
-  k_flux_tma<dir, MINB><<<grid, 128, smem, s>>>(P, G, T, ta, tm, bf, B);
+  k_flux_tma<dir, MINB, NT><<<grid, NT, smem, s>>>(P, G, T, ta, tm, bf, B);
   return true;
 }
 
-// Flux candidates of the tuned mode: the global-load kernel capped at 4
-// CTAs/SM, and the TMA-staged kernel capped at 4 or 5.  Reported by
-// grb_get_tuning as min CTAs/SM, plus 100 for the TMA-staged kernel.
-constexpr int kFluxMinB[3] = {4, 4, 5};
+// Flux candidates of the tuned mode (tile shapes and register caps): the
+// global-load kernel at 4 CTAs/SM of 128 threads, the TMA-staged kernel
+// with 128-thread tiles at 4 CTAs/SM, and with 256-thread tiles (twice the
+// rows per tile, less halo re-read along y and z) at 2 CTAs/SM (the same
+// register budget).  Reported by grb_get_tuning as min CTAs/SM, plus 100
+// for the TMA-staged kernel.
+constexpr int kFluxMinB[3] = {4, 4, 2};
 constexpr bool kFluxTma[3] = {false, true, true};
 
 template <int dir>
 void launch_flux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                        const double* st, const double* aux, const double* bf, const StageBufs& B) {
   if (v == 1 && launch_flux_tma<dir, 4>(s, P, G, b, st, aux, bf, B)) return;
-  if (v == 2 && launch_flux_tma<dir, 5>(s, P, G, b, st, aux, bf, B)) return;
+  if (v == 2 && launch_flux_tma<dir, 2, 256>(s, P, G, b, st, aux, bf, B)) return;
   k_flux<dir, true, 4><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
 }
 void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
@@ -459,11 +463,18 @@ inline bool trimmed(const grb_handle* h) {
 }
 
 // The static-metric cache when it was built for this geometry and these
-// spacings and covers these blocks, else null.
+// spacings and covers these blocks, else null.  A grid whose idx points
+// into the cached spacings at block q0 (a run of blocks of the cached grid,
+// with its field pointers offset alike) gets the cache from block q0 on.
 const double* static_metric(const grb_handle* h, const Geo& G, const double* idx) {
-  if (!h->d_metder || idx != h->metder_idx || G.nq > h->metder_nq) return nullptr;
+  if (!h->d_metder || !idx || !h->metder_idx) return nullptr;
   const int key[4] = {G.nx, G.ny, G.nz, G.g};
-  return std::equal(key, key + 4, h->metder_key) ? h->d_metder : nullptr;
+  if (!std::equal(key, key + 4, h->metder_key)) return nullptr;
+  const uintptr_t a = (uintptr_t)idx, b = (uintptr_t)h->metder_idx;
+  if (a < b || (a - b) % (3 * sizeof(double))) return nullptr;
+  const int64_t q0 = (int64_t)((a - b) / (3 * sizeof(double)));
+  if (q0 + G.nq > h->metder_nq) return nullptr;
+  return h->d_metder + q0 * (int64_t)kMetDer * G.nx * G.ny * G.nz;
 }
 
 // Refluxing of the stage (grb_set_reflux): the fluxes after FOFC, the edge
@@ -1453,13 +1464,26 @@ static bool ghost_runs(grb_handle* h, const Geo& G, cudaStream_t s) {
 int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
                           int32_t nby, int32_t nbz, const int32_t* periodic, void* stream) {
   if (!h) return GRB_ERR_INVALID;
+  if (!g) return fail(h, GRB_ERR_INVALID);
+  return grb_fill_ghosts_brick_range(h, g, f, nbx, nby, nbz, periodic, 0, g->nq, stream);
+}
+
+int grb_fill_ghosts_brick_range(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
+                                int32_t nby, int32_t nbz, const int32_t* periodic, int64_t q_begin,
+                                int64_t q_end, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
   if (!g || !f || !f->state || !f->bx || !f->by || !f->bz || !periodic || g->ngz < 1 ||
-      nbx < 1 || nby < 1 || nbz < 1 || (int64_t)nbx * nby * nbz != g->nq || g->nq > 65535)
+      nbx < 1 || nby < 1 || nbz < 1 || (int64_t)nbx * nby * nbz != g->nq || g->nq > 65535 ||
+      q_begin < 0 || q_end > g->nq || q_begin >= q_end)
     return fail(h, GRB_ERR_INVALID);
-  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   Brick br;
   br.nbx = nbx; br.nby = nby; br.nbz = nbz;
+  br.q0 = (int)q_begin;
   for (int a = 0; a < 3; ++a) br.periodic[a] = periodic[a] != 0;
+  // the launches cover blocks [q_begin, q_end) (blockIdx.y from br.q0); the
+  // geometry keeps the whole brick's nq
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  const unsigned nfill = (unsigned)(q_end - q_begin);
   cudaStream_t s = (cudaStream_t)stream;
   double* bf[3] = {f->bx, f->by, f->bz};
   KScope ks(h, s, GRB_KIND_GHOST);
@@ -1479,14 +1503,14 @@ int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f,
     const int* o = h->ghost_off;
     const int* c = h->ghost_cnt;
     const int mx = std::max({c[0], c[1], c[2]});
-    const dim3 gr((unsigned)((mx + 127) / 128), (unsigned)G.nq, 3u);
+    const dim3 gr((unsigned)((mx + 127) / 128), nfill, 3u);
     k_ghost_runs<<<gr, 128, 0, s>>>(G, br, h->d_ghostruns, make_int3(o[0], o[1], o[2]), make_int3(c[0], c[1], c[2]),
                                     f->state, bf[1], bf[2]);
-    const dim3 gx((unsigned)((G.NY * G.NZ + 127) / 128), (unsigned)G.nq, 1u);
+    const dim3 gx((unsigned)((G.NY * G.NZ + 127) / 128), nfill, 1u);
     k_ghost_xfaces<<<gx, 128, 0, s>>>(G, br, make_fastdiv((uint32_t)G.NY), bf[0]);
     h->launches += 2;
   } else {
-    const dim3 grid((unsigned)((total + 255) / 256), (unsigned)G.nq, 4u);
+    const dim3 grid((unsigned)((total + 255) / 256), nfill, 4u);
     k_ghost<<<grid, 256, 0, s>>>(G, br, D, f->state, bf[0], bf[1], bf[2]);
     ++h->launches;
   }

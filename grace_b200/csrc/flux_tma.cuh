@@ -125,12 +125,14 @@ __host__ __device__ inline size_t flux_tile_smem(const Geo& G, const FluxTile& T
   return 2 * sizeof(double) * (size_t)flux_tile_doubles(G, T) + 16;
 }
 
-// grid: (ceil(n_row / R), n_other, nq); 128 threads; W = n[0] <= 128.
+// grid: (ceil(n_row / R), n_other, nq); NT threads (128 or 256); W = n[0]
+// <= NT; R = NT / W rows (a 256-thread tile re-reads the 5-row stencil halo
+// of the y and z directions over twice as many rows).
 //   dir 0: lanes i (faces), rows j, other k; box rows j (BY = R, BZ = 1)
 //   dir 1: lanes i, rows j (faces), other k; box rows j - 3 .. (BY = R + 5)
 //   dir 2: lanes i, rows k (faces), other j; box rows k - 3 .. (BZ = R + 5)
-template <int dir, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_flux_tma(DevParams P, Geo G, FluxTile T,
+template <int dir, int MINB, int NT = 128>
+__global__ void __launch_bounds__(NT, MINB) k_flux_tma(DevParams P, Geo G, FluxTile T,
                                                       const __grid_constant__ CUtensorMap tm_aux,
                                                       const __grid_constant__ CUtensorMap tm_met,
                                                       const double* __restrict__ bface, StageBufs B) {

@@ -1064,6 +1064,7 @@ __global__ void k_linop(int64_t n, double* __restrict__ a, const double* __restr
 struct Brick {
   int nbx, nby, nbz;
   int periodic[3];
+  int q0;  // first block filled: the launch's blockIdx.y counts from it
 };
 // One coordinate along one axis: true when x is a ghost index; then (sx,
 // off) is the source index and the block offset (-1, 0, +1) along the axis.
@@ -1091,13 +1092,13 @@ struct GhostDivs {
 };
 // One launch for the four arrays: blockIdx.z = 0 the cell-centred HRSC
 // variables, 1..3 the face array staggered along blockIdx.z - 1.  One
-// thread per cell of one block (blockIdx.y = q), x fastest; 32-bit index
+// thread per cell of one block (blockIdx.y = q - br.q0), x fastest; 32-bit index
 // arithmetic (q < 65536, a block's cells < 2^31).
 __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, GhostDivs D, double* __restrict__ cells,
                                               double* __restrict__ fx, double* __restrict__ fy,
                                               double* __restrict__ fz) {
   const int fd = (int)blockIdx.z - 1;
-  const int q = blockIdx.y;
+  const int q = br.q0 + (int)blockIdx.y;
   int n[3] = {G.NX, G.NY, G.NZ};
   if (fd >= 0) n[fd] += 1;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1138,7 +1139,7 @@ __global__ void __launch_bounds__(256) k_ghost(Geo G, Brick br, GhostDivs D, dou
 }
 
 // The x face array (rows of NX + 1 faces, staggered along x), one thread
-// per row of one block (blockIdx.y = q): a row whose y and z are interior
+// per row of one block (blockIdx.y = q - br.q0): a row whose y and z are interior
 // has 2 ngz ghost faces (x < ngz and x > nx + ngz), any other row is ghost
 // throughout.  Each thread loads up to 8 of its row's sources before it
 // stores them, so the copies of a row overlap; the source of every face is
@@ -1147,7 +1148,7 @@ __global__ void __launch_bounds__(128) k_ghost_xfaces(Geo G, Brick br, FastDiv d
   const int N0 = G.NX + 1, N1 = G.NY;
   const int row = blockIdx.x * blockDim.x + threadIdx.x;
   if (row >= N1 * G.NZ) return;
-  const int q = blockIdx.y;
+  const int q = br.q0 + (int)blockIdx.y;
   const int k = (int)fast_div((uint32_t)row, dny), j = row - k * N1;
   const int nb[3] = {br.nbx, br.nby, br.nbz};
   const int qyz = q / br.nbx;
@@ -1204,7 +1205,7 @@ __global__ void __launch_bounds__(128) k_ghost_runs(Geo G, Brick br, const uint3
   int n[3] = {G.NX, G.NY, G.NZ};
   if (fd > 0) n[fd] += 1;
   double* a = arr == 0 ? cells : arr == 1 ? fy : fz;
-  const int q = blockIdx.y;
+  const int q = br.q0 + (int)blockIdx.y;
   const int nin[3] = {G.nx, G.ny, G.nz};
   const int nb[3] = {br.nbx, br.nby, br.nbz};
   const int qyz = q / br.nbx;

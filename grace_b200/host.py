@@ -14,6 +14,7 @@ Every call goes through the C ABI of libgrace_b200.so on torch CUDA tensors
 Errors surface as RuntimeError with the library's status code, as GRACE's
 ERROR() macro would abort the run.
 """
+import contextlib
 import ctypes
 from dataclasses import dataclass
 
@@ -64,6 +65,10 @@ class Fields:
         return Fields(self.state.to(device), self.bx.to(device), self.by.to(device),
                       self.bz.to(device))
 
+    def view(self, q0, q1):
+        """Blocks [q0, q1) of the four arrays (views, no copy)."""
+        return Fields(self.state[q0:q1], self.bx[q0:q1], self.by[q0:q1], self.bz[q0:q1])
+
 
 class Blocks:
     """Block geometry: nq blocks of nx*ny*nz interior cells with ngz ghosts."""
@@ -80,6 +85,19 @@ class Blocks:
         return abi.Grid(self.nx, self.ny, self.nz, self.ngz, self.nq, self.idx.data_ptr(),
                         self.coords.data_ptr() if self.coords is not None else None)
 
+    def view(self, q0, q1):
+        """The run of blocks [q0, q1): the same geometry, nq = q1 - q0, the
+        spacings and coordinates as views of this object's (no copy)."""
+        if not 0 <= q0 < q1 <= self.nq:
+            raise ValueError(f"block run [{q0}, {q1}) outside [0, {self.nq})")
+        v = object.__new__(Blocks)
+        v.__dict__.update(self.__dict__)
+        v.nq = q1 - q0
+        v.idx = self.idx[q0:q1]
+        v.coords = None if self.coords is None else self.coords[q0:q1]
+        v.q0 = q0
+        return v
+
     def new_fields(self):
         z = lambda *s: torch.zeros(*s, dtype=torch.float64, device=self.device)
         return Fields(z(self.nq, abi.N_EVOL_VARS, self.NZ, self.NY, self.NX),
@@ -90,6 +108,36 @@ class Blocks:
     def new_aux(self):
         return torch.zeros(self.nq, abi.N_AUX_VARS, self.NZ, self.NY, self.NX,
                            dtype=torch.float64, device=self.device)
+
+
+def brick_runs(nb, periodic, nruns):
+    """Runs of blocks for rk3_step_host on a brick of nb = (nbx, nby, nbz)
+    blocks (block q = bx + nbx (by + nby bz)): nruns consecutive runs of
+    whole z-slabs, as even as the slabs allow, and for each run the set of
+    runs whose blocks its ghost fill reads (the face, edge and corner
+    neighbours, wrapping along periodic axes; a non-periodic outer face
+    copies from the block itself)."""
+    nbx, nby, nbz = nb
+    nruns = max(1, min(int(nruns), nbz))
+    cuts = [round(r * nbz / nruns) for r in range(nruns + 1)]
+    slab = nbx * nby
+    runs = [(cuts[r] * slab, cuts[r + 1] * slab) for r in range(nruns)]
+    run_of_z = np.zeros(nbz, dtype=np.int64)
+    for r in range(nruns):
+        run_of_z[cuts[r]:cuts[r + 1]] = r
+    deps = []
+    for r in range(nruns):
+        d = set()
+        for z in range(cuts[r], cuts[r + 1]):
+            for o in (-1, 0, 1):
+                zz = z + o
+                if periodic[2]:
+                    zz %= nbz
+                elif not 0 <= zz < nbz:
+                    continue
+                d.add(int(run_of_z[zz]))
+        deps.append(d)
+    return runs, deps
 
 
 class GRMHDEquationsSystem:
@@ -166,12 +214,34 @@ class GRMHDEquationsSystem:
                                             ctypes.byref(fc) if fc is not None else None, b, c,
                                             _stream_ptr(stream)), "grb_linop_apply")
 
-    def fill_ghosts_brick(self, fields, nb, periodic, stream=None):
+    def fill_ghosts_brick(self, fields, nb, periodic, stream=None, blocks=None):
+        """Ghost fill of a brick of same-level blocks (grb_fill_ghosts_brick);
+        blocks = (q0, q1): only the ghost zones of those blocks
+        (grb_fill_ghosts_brick_range)."""
         g = self.blocks.c()
         f = fields.c()
         per = (ctypes.c_int32 * 3)(*[int(bool(x)) for x in periodic])
-        _lib.check(self.lib.grb_fill_ghosts_brick(self.h, ctypes.byref(g), ctypes.byref(f), nb[0], nb[1],
-                                                  nb[2], per, _stream_ptr(stream)), "grb_fill_ghosts_brick")
+        if blocks is None:
+            _lib.check(self.lib.grb_fill_ghosts_brick(self.h, ctypes.byref(g), ctypes.byref(f), nb[0], nb[1],
+                                                      nb[2], per, _stream_ptr(stream)), "grb_fill_ghosts_brick")
+        else:
+            _lib.check(self.lib.grb_fill_ghosts_brick_range(self.h, ctypes.byref(g), ctypes.byref(f), nb[0],
+                                                            nb[1], nb[2], per, int(blocks[0]), int(blocks[1]),
+                                                            _stream_ptr(stream)), "grb_fill_ghosts_brick_range")
+
+    @contextlib.contextmanager
+    def block_range(self, q0, q1):
+        """Within the context every call of this object runs on the blocks
+        [q0, q1) of the reserved grid only (pass Fields.view(q0, q1) and
+        aux[q0:q1] as its arrays).  Stages are block-local once the ghost
+        zones are filled, so a run of blocks gives the same bits as the
+        whole grid there; the static-metric cache is found at block q0."""
+        full = self.blocks
+        self.blocks = full.view(q0, q1)
+        try:
+            yield self
+        finally:
+            self.blocks = full
 
     def restrict_to_coarse(self, fine, cbuf, src_q, dst_q, child_id=None, vars_lo=(), vars_ho=(),
                            faces=True, stream=None):
@@ -475,6 +545,106 @@ class GRMHDEquationsSystem:
             if next_dt is not None:
                 self.find_stable_timestep(state, aux, *next_dt, stream=stream)
         self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
+
+    def rk3_step_host(self, dt, host, state, state_p, state_pp, aux, bc, runs, fill_run, deps, t=0.0,
+                      streams=None):
+        """One SSP-RK3 step of a state held in packed pinned host arrays
+        (packed_host_fields): upload, boundary fill and primitives of the
+        uploaded state, the step, download — the same kernels in the same
+        per-block order as
+
+            copy_evolved_packed(host, state, True); bc(state);
+            compute_auxiliary_quantities(state, aux); rk3_step(...);
+            copy_evolved_packed(host, state, False)
+
+        (with state_p set to state first), so the same bits, but pipelined
+        over runs of blocks on three streams: the upload of each run overlaps
+        the first substep of the runs before it, the download of each run
+        the last substep of the runs after it.
+
+        runs: [(q0, q1)] consecutive runs covering [0, nq).
+        fill_run(fields, s, stream): the boundary fill of the ghost zones of
+        run s alone; deps[s]: the runs whose interiors it reads (brick_runs
+        gives both for a brick).
+        bc(fields): the fill of every block (the middle substep).
+        streams: (upload, download) CUDA streams, new ones by default; the
+        caller's current stream runs the kernels.  On return (stream order)
+        host holds the new interior and state, state_p, aux on the device
+        are as after rk3_step."""
+        main = torch.cuda.current_stream()
+        up, down = streams if streams is not None else (torch.cuda.Stream(), torch.cuda.Stream())
+        S = len(runs)
+        deps = [set(d) | {s} for s, d in enumerate(deps)]
+        # readers[r]: the runs whose ghost fill reads run r's interior.  A
+        # run's primitives pass may write corrected conserved variables
+        # back into its interior, so it waits until those fills are done
+        # (as the whole-grid order fills every block before any primitives).
+        readers = [{t for t in range(S) if r in deps[t]} for r in range(S)]
+        # the uploads read host arrays the previous step's downloads wrote
+        up.wait_stream(main)
+        up.wait_stream(down)
+        ev_up = []
+        for q0, q1 in runs:
+            with self.block_range(q0, q1):
+                self.copy_evolved_packed(host.view(q0, q1), state.view(q0, q1), True, stream=up)
+            e = torch.cuda.Event()
+            e.record(up)
+            ev_up.append(e)
+        # first substep, run by run as the runs they read arrive
+        filled, ready = set(), set()
+        for s in range(S):
+            for d in sorted(deps[s]):
+                main.wait_event(ev_up[d])
+            fill_run(state, s, main)
+            filled.add(s)
+            for r, (q0, q1) in enumerate(runs):
+                if r in ready or not readers[r] <= filled:
+                    continue
+                with self.block_range(q0, q1):
+                    sv, pv, a = state.view(q0, q1), state_p.view(q0, q1), aux[q0:q1]
+                    self.compute_auxiliary_quantities(sv, a, main)
+                    self.reset_c2p_diagnostics(a, main)
+                    self.linop_apply(pv, sv, None, 1.0, 0.0, main)
+                    self.advance_substep(t, dt, 1.0, pv, sv, a, main)
+                ready.add(r)
+        # middle substep on the whole grid
+        bc(state_p)
+        self.compute_auxiliary_quantities(state_p, aux, main)
+        self.linop_apply(state_pp, state, state_p, 0.75, 0.25, main)
+        self.advance_substep(t, dt, 0.25, state_pp, state_p, aux, main)
+        bc(state_pp)
+        self.compute_auxiliary_quantities(state_pp, aux, main)
+        self.linop_apply(state, state, state_pp, 1.0 / 3, 2.0 / 3.0, main)
+        # last substep run by run; a run is filled once the runs it reads
+        # are updated, and finished (primitives, state_p) and downloaded
+        # once the runs reading it are filled
+        updated, filled, finished = set(), set(), set()
+        for s, (q0, q1) in enumerate(runs):
+            with self.block_range(q0, q1):
+                self.advance_substep(t, dt, 2.0 / 3.0, state.view(q0, q1), state_pp.view(q0, q1), aux[q0:q1],
+                                     main)
+            updated.add(s)
+            for r in range(S):
+                if r not in filled and deps[r] <= updated:
+                    fill_run(state, r, main)
+                    filled.add(r)
+            for r, (r0, r1) in enumerate(runs):
+                if r in finished or r not in filled or not readers[r] <= filled:
+                    continue
+                with self.block_range(r0, r1):
+                    sv = state.view(r0, r1)
+                    self.compute_auxiliary_quantities(sv, aux[r0:r1], main)
+                    self.linop_apply(state_p.view(r0, r1), sv, None, 1.0, 0.0, main)
+                e = torch.cuda.Event()
+                e.record(main)
+                down.wait_event(e)
+                with self.block_range(r0, r1):
+                    self.copy_evolved_packed(host.view(r0, r1), state.view(r0, r1), False, stream=down)
+                finished.add(r)
+        if len(ready) != S or len(finished) != S:
+            raise ValueError("runs / deps do not cover every run")
+        main.wait_stream(down)
+        main.wait_stream(up)
 
     def capture_rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, next_dt=None, fused_dt=False):
         """Capture one rk3_step (same arguments) into a CUDA graph.  The

@@ -594,7 +594,7 @@ def kerr_schild_curvature(x, y, z, a, h=1e-5):
 
 
 def fm_torus(hier, a=0.9375, r_in=6.0, r_pmax=12.0, gamma=4.0 / 3.0, kappa=1e-3, rho_atm=1e-8,
-             beta_p=100.0, a_cut=0.2, noise=2e-2, seed=SEED):
+             beta_p=100.0, a_cut=0.2, noise=2e-2, rho_noise=1e-3, seed=SEED):
     """Fishbone-Moncrief torus in the fixed Kerr-Schild metric on the leaves
     of a static FMR hierarchy, written from the configuration text (the
     reference's own torus initial data is not part of its sources): the
@@ -605,7 +605,11 @@ def fm_torus(hier, a=0.9375, r_in=6.0, r_pmax=12.0, gamma=4.0 / 3.0, kappa=1e-3,
     frame, pressure of the same polytrope); a poloidal field from
     A = A_b max(rho/rho_max - a_cut, 0) (-y, x, 0) as the discrete curl on
     each block's edges, scaled so that max P / max(b^2/2) = beta_p; seeded
-    relative pressure noise.  Returns (state, bx, by, bz, aux)."""
+    relative pressure noise, and seeded relative density noise in
+    (-rho_noise, 0] everywhere (atmosphere included: without it the data are
+    mirror symmetric about z = 0, the mass flux through the equatorial faces
+    is a rounding residue and the sign that upwinds the Gardiner-Stone EMF
+    there is arbitrary).  Returns (state, bx, by, bz, aux)."""
     def lnh_bl(r, th, l):
         sth, cth = np.sin(th), np.cos(th)
         DD = r * r - 2 * r + a * a
@@ -669,14 +673,17 @@ def fm_torus(hier, a=0.9375, r_in=6.0, r_pmax=12.0, gamma=4.0 / 3.0, kappa=1e-3,
     x, y, zc = X[:, 0], X[:, 1], X[:, 2]
     g6, beta, alp, r, rho, zv = fluid(x, y, zc)
     Kc = kerr_schild_curvature(x, y, zc, a)
-    press = kappa * (rho * rho_max) ** gamma / rho_max  # normalised units: P / rho_max
     key = np.zeros((nq, 3, NN, NN, NN), dtype=np.int64)
     rr_ = np.arange(NN)
     for q, (lv, b) in enumerate(hier.leaves):
         key[q, 0] = b[0] * hier.n + rr_[None, None, :] + (lv << 20)
         key[q, 1] = b[1] * hier.n + rr_[:, None] * 0 + rr_[None, :, None]
         key[q, 2] = b[2] * hier.n + rr_[:, None, None]
-    u = _counter_uniform(np.moveaxis(key, 1, -1).reshape(-1, 3) + 64, seed, np.array([1 << 22, 1 << 22])).reshape(rho.shape)
+    gid = np.moveaxis(key, 1, -1).reshape(-1, 3) + 64
+    u = _counter_uniform(gid, seed, np.array([1 << 22, 1 << 22])).reshape(rho.shape)
+    u_rho = _counter_uniform(gid, seed + 1, np.array([1 << 22, 1 << 22])).reshape(rho.shape)
+    rho = rho * (1.0 + 0.5 * rho_noise * (u_rho - 1.0))
+    press = kappa * (rho * rho_max) ** gamma / rho_max  # normalised units: P / rho_max
     press = press * (1.0 + noise * u)
     eps = press / ((gamma - 1.0) * rho)
     s = np.log(eps) / (gamma - 1.0) - np.log(rho)

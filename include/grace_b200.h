@@ -220,7 +220,9 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt,
  * the same arithmetic as the stage's.  GRB_MODE_TUNED stages on a grid of
  * the same block geometry, the same idx pointer and at most these nq blocks
  * then read them instead of differentiating the metric (identical
- * results); the plain mode ignores them.  Call again after changing the
+ * results); so do stages on a run of these blocks, a grid whose idx points
+ * at block q0 of the cached spacings (and whose field pointers start at
+ * block q0 alike).  The plain mode ignores them.  Call again after changing the
  * metric or the spacings; st = NULL frees them.  GRB_ERR_NOMEM when the
  * cache cannot be allocated. */
 int grb_set_static_metric(grb_handle* h, const grb_grid* g, const grb_fields* st,
@@ -403,8 +405,10 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* new_state,
  * ms[12] (or NULL): timed milliseconds of the 3 candidates per family. */
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms);
 /* Choose the tuned-mode candidates without timing: variant[4] = candidate
- * index 0..2 of flux, flag, update, aux (flux: 0 global-load kernel, 1 and 2
- * TMA-staged kernel at 4 and 5 CTAs/SM; others: 1, 4, 5 CTAs/SM; aux also
+ * index 0..2 of flux, flag, update, aux (flux: 0 global-load kernel, 1 the
+ * TMA-staged kernel with 128-thread tiles at 4 CTAs/SM, 2 with 256-thread
+ * tiles (twice the face rows per tile) at 2 CTAs/SM; others: 1, 4, 5
+ * CTAs/SM; aux also
  * 3..5: the work-queue form — one wave of CTAs pulling chunks of 128-cell
  * tiles from a device counter — at 1, 4, 5 CTAs/SM, and 6..8: the
  * deferred-backup form — the cells whose Kastaun result is distrusted
@@ -453,6 +457,14 @@ int grb_kernel_times(grb_handle* h, double* ms, int64_t* counts, int32_t nkinds)
  * 7 evolved HRSC variables and the three face-B arrays. */
 int grb_fill_ghosts_brick(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
                           int32_t nby, int32_t nbz, const int32_t* periodic, void* stream);
+/* No counterpart in the reference: grb_fill_ghosts_brick restricted to the
+ * ghost zones of blocks [q_begin, q_end) of the brick (g and f still
+ * describe the whole brick; the sources, interior cells and faces of the
+ * neighbouring blocks, may lie anywhere in it).  For pipelines that fill a
+ * run of blocks as soon as the blocks it reads from are final. */
+int grb_fill_ghosts_brick_range(grb_handle* h, const grb_grid* g, const grb_fields* f, int32_t nbx,
+                                int32_t nby, int32_t nbz, const int32_t* periodic, int64_t q_begin,
+                                int64_t q_end, void* stream);
 /* No counterpart in the reference (its state stays on the device): copies
  * the interior of the evolved variables, i.e. the 7 HRSC variables on the
  * interior cells and the three face-B arrays on the interior faces

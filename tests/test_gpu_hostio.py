@@ -1,6 +1,8 @@
 """Interior copies between pinned host memory and the device
-(grb_copy_evolved_interior): exact round trips, ghost zones untouched, and
-upload + ghost fill equal to copying whole arrays."""
+(grb_copy_evolved_interior, grb_copy_evolved_packed): exact round trips,
+ghost zones untouched, upload + ghost fill equal to copying whole arrays;
+the block-range brick fill and the host step pipelined over runs of blocks
+(rk3_step_host) equal to their whole-grid, sequential forms bit for bit."""
 import numpy as np
 import pytest
 import torch
@@ -158,3 +160,72 @@ def test_packed_copy_by_array_on_two_streams():
     torch.cuda.synchronize()
     for a, b in zip((split.state, split.bx, split.by, split.bz), (ref.state, ref.bx, ref.by, ref.bz)):
         assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_block_range_fill_equals_whole_fill(periodic):
+    """grb_fill_ghosts_brick_range over consecutive runs of blocks fills
+    every ghost exactly as one whole-brick fill."""
+    su, f = workloads.blast(nb=(2, 3, 4), n=(8, 8, 8))
+    g, dev = _system(su, params.blast())
+    rng = np.random.default_rng(11)
+    d = Fields(*[torch.from_numpy(rng.standard_normal(x.shape)).to(dev) for x in f[:4]])
+    ref = d.clone()
+    per = (periodic,) * 3
+    g.fill_ghosts_brick(ref, su.nb, per)
+    for q0, q1 in ((0, 5), (5, 6), (6, 17), (17, su.nq)):
+        g.fill_ghosts_brick(d, su.nb, per, blocks=(q0, q1))
+    torch.cuda.synchronize()
+    for a, b in zip((d.state, d.bx, d.by, d.bz), (ref.state, ref.bx, ref.by, ref.bz)):
+        assert torch.equal(a, b)
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_pipelined_host_step_matches_sequential(mode):
+    """GRMHDEquationsSystem.rk3_step_host (upload, fill, primitives, step and
+    download pipelined over runs of z-slabs on three streams) gives the bits
+    of the sequential host round trip, two steps in a row, in the host
+    arrays and in every device array; tuned: the static-metric cache found
+    at each run's first block, ranges trimmed to the next stage."""
+    from grace_b200.host import brick_runs
+    su, f = workloads.blast(nb=(2, 2, 5), n=(8, 8, 8))
+    P = params.blast()
+    if mode == abi.MODE_TUNED:
+        P.ranges = abi.RANGES_NEXT_STAGE
+    g, dev = _system(su, P)
+    g.set_mode(mode)
+    bc = lambda fl: g.fill_ghosts_brick(fl, su.nb, su.periodic)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    st0 = Fields(*[T(x) for x in f[:4]])
+    bc(st0)
+    aux0 = T(f[4])
+    g.compute_auxiliary_quantities(st0, aux0)
+    if mode == abi.MODE_TUNED:
+        g.set_static_metric(st0)
+        g.set_tuning(1, 1, 1, 1)
+    dt = 0.25 / su.idx()[0, 0]
+    runs, deps = brick_runs(su.nb, su.periodic, 3)
+    assert len(runs) == 3
+    fill_run = lambda fl, s, stream: g.fill_ghosts_brick(fl, su.nb, su.periodic, stream=stream, blocks=runs[s])
+    out = []
+    for piped in (False, True):
+        state, aux = st0.clone(), aux0.clone()
+        sp, spp = state.clone(), state.clone()
+        host = g.packed_host_fields()
+        g.copy_evolved_packed(host, state, to_device=False)
+        for _ in range(2):
+            if piped:
+                g.rk3_step_host(dt, host, state, sp, spp, aux, bc, runs, fill_run, deps)
+            else:
+                g.copy_evolved_packed(host, state, to_device=True)
+                bc(state)
+                g.compute_auxiliary_quantities(state, aux)
+                g.rk3_step(dt, state, sp, spp, aux, bc)
+                g.copy_evolved_packed(host, state, to_device=False)
+        torch.cuda.synchronize()
+        out.append([x.clone() for x in (host.state, host.bx, host.by, host.bz, state.state, state.bx, state.by,
+                                         state.bz, sp.state, sp.bx, sp.by, sp.bz, aux)])
+    assert not torch.equal(out[0][0], torch.from_numpy(f[0][:, :abi.N_HRSC, 4:12, 4:12, 4:12].copy()))
+    for k, (a, b) in enumerate(zip(*out)):
+        assert torch.equal(a, b), k
+    assert g.status().device_flags == 0

@@ -125,7 +125,7 @@ def test_benchmark_configuration_matches_oracle(tuning):
     assert st.device_flags == 0
     if tuning is None:
         # the autotuner picked one of the TMA-staged or global-load flux kernels
-        assert g.tuning()["flux"]["min_ctas_per_sm"] in (4, 104, 105)
+        assert g.tuning()["flux"]["min_ctas_per_sm"] in (4, 104, 102)
 
 
 @pytest.mark.parametrize("cap", [0, 7])

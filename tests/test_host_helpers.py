@@ -22,3 +22,32 @@ def test_outer_faces_of_a_brick():
             assert ix == 0
         if f == 1:
             assert ix == 2
+
+
+def test_brick_runs_cover_the_brick_and_name_every_neighbour():
+    """brick_runs: consecutive runs of whole z-slabs covering every block
+    once, and deps[r] holding the run of every face, edge and corner
+    neighbour of each of run r's blocks (wrapping along periodic axes)."""
+    from grace_b200.host import brick_runs
+    for nb, per, nruns in (((4, 3, 7), (False, False, False), 3), ((2, 2, 6), (True, True, True), 4),
+                           ((3, 1, 2), (False, True, False), 5), ((1, 1, 1), (True, True, True), 2)):
+        runs, deps = brick_runs(nb, per, nruns)
+        nq = nb[0] * nb[1] * nb[2]
+        assert runs[0][0] == 0 and runs[-1][1] == nq
+        assert all(a[1] == b[0] for a, b in zip(runs, runs[1:]))
+        assert all((q1 - q0) % (nb[0] * nb[1]) == 0 and q1 > q0 for q0, q1 in runs)
+        run_of = np.zeros(nq, dtype=int)
+        for r, (q0, q1) in enumerate(runs):
+            run_of[q0:q1] = r
+        for q in range(nq):
+            c = (q % nb[0], (q // nb[0]) % nb[1], q // (nb[0] * nb[1]))
+            for o in np.ndindex(3, 3, 3):
+                cc = []
+                for a in range(3):
+                    x = c[a] + o[a] - 1
+                    if per[a]:
+                        x %= nb[a]
+                    x = min(max(x, 0), nb[a] - 1)
+                    cc.append(x)
+                src = cc[0] + nb[0] * (cc[1] + nb[1] * cc[2])
+                assert run_of[src] in deps[run_of[q]], (nb, per, q, o)
