@@ -53,7 +53,7 @@ struct grb_handle {
   // learned c2p bracket: FP32 parameter block on the device
   float* d_mlp = nullptr;
   MlpSmem* d_mlp_pack = nullptr;  // shared-memory image of the network
-  unsigned long long* d_queue = nullptr;  // work-queue counter of the aux pass
+  unsigned long long* d_queue = nullptr;  // work-queue counters: [0] aux pass, [1] FOFC flag
   double* d_metder = nullptr;             // static-metric cache (grb_set_static_metric)
   size_t metder_bytes = 0;
   int metder_key[4] = {0, 0, 0, 0};       // nx, ny, nz, ngz it was built for
@@ -69,6 +69,7 @@ struct grb_handle {
   int auxlist_key[4] = {0, 0, 0, 0};      // nx, ny, nz, ngz it was built for
   float tune_aux_queue_ms = 0.f;
   float tune_aux_defer_ms = 0.f;
+  float tune_flag_queue_ms = 0.f;
   bool mlp_ready = false;
   uint32_t fcap_alloc = 0;  // entries allocated for the compacted FOFC face list
   // the tuned batch c2p's deferred entropy backups: records and their count
@@ -297,10 +298,40 @@ void launch_flux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, c
   if (v == 2 && launch_flux_tma<dir, 2, 256>(s, P, G, b, st, aux, bf, B)) return;
   k_flux<dir, true, 4><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
 }
+// One wave of the persistent FOFC flag kernel (per device ordinal), after
+// zeroing its queue counter.
+template <int MINB>
+void launch_flag_queue(cudaStream_t s, const DevParams& P, const Geo& G, const Box& b, double dt, double dtfact,
+                       const double* ns, const double* os, const double* bx, const double* by, const double* bz,
+                       const double* idx, const double* crd, const StageBufs& B, unsigned long long* queue) {
+  static int grids[kMaxDevices] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int grid = 0;
+  if (dev >= 0 && dev < kMaxDevices) grid = grids[dev];
+  if (grid == 0) {
+    int sms = 0, occ = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_fofc_flag_queue<MINB, true>, 128, 0);
+    grid = (sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+    if (dev >= 0 && dev < kMaxDevices) grids[dev] = grid;
+  }
+  cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+  k_fofc_flag_queue<MINB, true><<<grid, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
+}
+// Flag candidates: 0..2 one thread per cell at 1, 4, 5 CTAs/SM; 3..5 the
+// persistent work-queue form at the same caps (given the queue counter).
 void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                        double dt, double dtfact, const double* ns, const double* os, const double* bx,
                        const double* by, const double* bz, const double* idx, const double* crd,
-                       const StageBufs& B) {
+                       const StageBufs& B, unsigned long long* queue = nullptr) {
+  if (v >= 3 && queue) {
+    if (v == 4) launch_flag_queue<4>(s, P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
+    else if (v == 5) launch_flag_queue<5>(s, P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
+    else launch_flag_queue<1>(s, P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
+    return;
+  }
+  if (v >= 3) v -= 3;
   if (v == 1) k_fofc_flag<4, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
   else if (v == 2) k_fofc_flag<5, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
   else k_fofc_flag<1, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
@@ -566,7 +597,7 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
     {
       KScope ks(h, s, GRB_KIND_FOFC_FLAG);
       launch_flag_tuned(h->var_flag, nblk(fb.count(), T), s, P, G, fb, dt, dtfact, nw->state, old->state,
-                        old->bx, old->by, old->bz, g->idx, g->coords, B);
+                        old->bx, old->by, old->bz, g->idx, g->coords, B, h->d_queue + 1);
       ++launches;
     }
     {
@@ -670,7 +701,7 @@ int grb_create(grb_handle** out, const grb_params* p) {
   h->dp = to_dev(*p);
   if (cudaMalloc(&h->d_flags, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&h->d_counters, 2 * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&h->d_queue, sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMalloc(&h->d_queue, 2 * sizeof(unsigned long long)) != cudaSuccess) {
     cudaFree(h->d_flags);
     cudaFree(h->d_counters);
     delete h;
@@ -2003,7 +2034,12 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
       if (t < bt) { bt = t; best[fam] = v; }
     }
   }
-  // the work-queue form of the chosen aux register cap
+  // the work-queue forms of the chosen flag and aux register caps
+  h->tune_flag_queue_ms = time_it([&] {
+    launch_flag_tuned(best[1] + 3, nblk(fb.count(), 128), s, P, G, fb, 1e-3, 1.0, ns, os, fo.bx, fo.by, fo.bz,
+                      gs.idx, gs.coords, B, h->d_queue + 1);
+  });
+  if (h->tune_flag_queue_ms < h->tune_ms[1][best[1]]) best[1] += 3;
   h->tune_aux_queue_ms = time_it([&] {
     launch_aux_tuned(best[3] + 3, nblk(ab.count(), 128), s, P, G, ab, ns, fn.bx, fn.by, fn.bz, ax, gs.idx,
                      gs.coords, B, nullptr, h->d_queue);
@@ -2041,7 +2077,7 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   if (!h || !variant) return GRB_ERR_INVALID;
   variant[0] = kFluxMinB[h->var_flux] + (kFluxTma[h->var_flux] ? 100 : 0);
-  variant[1] = kMinB[h->var_flag];
+  variant[1] = kMinB[h->var_flag % 3] + 100 * (h->var_flag / 3);
   variant[2] = h->d_metder ? kMinBCached[h->var_update] : kMinB[h->var_update];
   variant[3] = kMinB[h->var_aux % 3] + 100 * (h->var_aux / 3);
   if (ms)
@@ -2050,10 +2086,19 @@ int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   return GRB_OK;
 }
 
+int grb_get_tuning_forms(grb_handle* h, float* ms) {
+  if (!h || !ms) return GRB_ERR_INVALID;
+  ms[0] = h->tune_flag_queue_ms;
+  ms[1] = h->tune_aux_queue_ms;
+  ms[2] = h->tune_aux_defer_ms;
+  return GRB_OK;
+}
+
 int grb_set_tuning(grb_handle* h, const int32_t* variant) {
   if (!h || !variant) return GRB_ERR_INVALID;
   for (int f = 0; f < 4; ++f)
-    if (variant[f] < 0 || variant[f] >= (f == 3 ? 3 * kNumVar : kNumVar)) return fail(h, GRB_ERR_INVALID);
+    if (variant[f] < 0 || variant[f] >= (f == 3 ? 3 * kNumVar : f == 1 ? 2 * kNumVar : kNumVar))
+      return fail(h, GRB_ERR_INVALID);
   if (variant[3] >= 2 * kNumVar) {
     // the deferred-backup aux pass: its list, for the reserved grid
     if (!h->reserved) return fail(h, GRB_ERR_NOT_RESERVED);

@@ -401,19 +401,17 @@ __device__ __forceinline__ double cell_r(const Geo& G, const double* coords, con
   return sqrt(x * x + y * y + z * z);
 }
 
-// flag_fofc_cells (evolve.cpp:456-635) over cells [g-1, n+g]^3
-template <int MINB = 1, bool kFast = false>
-__global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box box, double dt,
-                                                    double dtfact, const double* __restrict__ ns,
-                                                    const double* __restrict__ os,
-                                                    const double* __restrict__ obx,
-                                                    const double* __restrict__ oby,
-                                                    const double* __restrict__ obz,
-                                                    const double* __restrict__ idx,
-                                                    const double* __restrict__ coords, StageBufs B) {
-  int i, j, k;
-  int64_t q;
-  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+// Cells per work-queue item of the persistent launches: 8 tiles of 128.
+constexpr int kAuxChunk = 8;
+
+// flag_fofc_cells (evolve.cpp:456-635) for one cell of [g-1, n+g]^3
+template <bool kFast>
+__device__ __forceinline__ void fofc_flag_cell(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
+                                               double dt, double dtfact, const double* __restrict__ ns,
+                                               const double* __restrict__ os, const double* __restrict__ obx,
+                                               const double* __restrict__ oby, const double* __restrict__ obz,
+                                               const double* __restrict__ idx,
+                                               const double* __restrict__ coords, const StageBufs& B) {
   const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
   double c[10];
   const double* F = B.flux;
@@ -460,6 +458,54 @@ __global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box
     E[emi(G, i, j, k, 0, q)] = 1; E[emi(G, i, j + 1, k, 0, q)] = 1; E[emi(G, i, j, k + 1, 0, q)] = 1; E[emi(G, i, j + 1, k + 1, 0, q)] = 1;
     E[emi(G, i, j, k, 1, q)] = 1; E[emi(G, i + 1, j, k, 1, q)] = 1; E[emi(G, i, j, k + 1, 1, q)] = 1; E[emi(G, i + 1, j, k + 1, 1, q)] = 1;
     E[emi(G, i, j, k, 2, q)] = 1; E[emi(G, i + 1, j, k, 2, q)] = 1; E[emi(G, i, j + 1, k, 2, q)] = 1; E[emi(G, i + 1, j + 1, k, 2, q)] = 1;
+  }
+}
+
+// over cells [g-1, n+g]^3, one thread per cell
+template <int MINB = 1, bool kFast = false>
+__global__ void __launch_bounds__(128, MINB) k_fofc_flag(DevParams P, Geo G, Box box, double dt,
+                                                    double dtfact, const double* __restrict__ ns,
+                                                    const double* __restrict__ os,
+                                                    const double* __restrict__ obx,
+                                                    const double* __restrict__ oby,
+                                                    const double* __restrict__ obz,
+                                                    const double* __restrict__ idx,
+                                                    const double* __restrict__ coords, StageBufs B) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  fofc_flag_cell<kFast>(P, G, i, j, k, q, dt, dtfact, ns, os, obx, oby, obz, idx, coords, B);
+}
+
+// The same as a persistent launch (tuned candidate): one wave of CTAs
+// pulling chunks of kAuxChunk tiles of 128 cells, numbered block by block,
+// from the device work queue *queue (zeroed before the launch) until the
+// box is exhausted; per-cell work unchanged.  For uneven per-block cost
+// (the c2p dry run's iterations vary with the state).
+template <int MINB = 1, bool kFast = false>
+__global__ void __launch_bounds__(128, MINB) k_fofc_flag_queue(DevParams P, Geo G, Box box, double dt,
+                                                          double dtfact, const double* __restrict__ ns,
+                                                          const double* __restrict__ os,
+                                                          const double* __restrict__ obx,
+                                                          const double* __restrict__ oby,
+                                                          const double* __restrict__ obz,
+                                                          const double* __restrict__ idx,
+                                                          const double* __restrict__ coords, StageBufs B,
+                                                          unsigned long long* __restrict__ queue) {
+  __shared__ unsigned long long item;
+  const int64_t ntiles = (box.count() + 127) / 128;
+  for (;;) {
+    if (threadIdx.x == 0) item = atomicAdd(queue, (unsigned long long)kAuxChunk);
+    __syncthreads();
+    const int64_t first = (int64_t)item;
+    __syncthreads();
+    if (first >= ntiles) break;
+    for (int c = 0; c < kAuxChunk; ++c) {
+      int i, j, k;
+      int64_t q;
+      if (first + c < ntiles && decode(box, (first + c) * 128 + threadIdx.x, i, j, k, q))
+        fofc_flag_cell<kFast>(P, G, i, j, k, q, dt, dtfact, ns, os, obx, oby, obz, idx, coords, B);
+    }
   }
 }
 
@@ -922,7 +968,6 @@ __global__ void __launch_bounds__(128, MINB) k_aux(DevParams P, Geo G, Box box, 
 // 128 cells (tiles numbered block by block, so a chunk stays inside one or
 // two blocks) from the device work queue *queue (zeroed before the launch)
 // until the box is exhausted.  Per-cell work is the same function.
-constexpr int kAuxChunk = 8;
 template <int MINB = 1, bool kDt = false, bool kFast = false>
 __global__ void __launch_bounds__(128, MINB) k_aux_queue(DevParams P, Geo G, Box box, double* __restrict__ st,
                                                     const double* __restrict__ bx,

@@ -444,11 +444,20 @@ class GRMHDEquationsSystem:
         ms = (ctypes.c_float * 12)()
         _lib.check(self.lib.grb_get_tuning(self.h, v, ms), "grb_get_tuning")
         fam = ["flux", "fofc_flag", "update", "aux"]
-        return {f: {"min_ctas_per_sm": v[i], "ms": [round(ms[3 * i + k], 4) for k in range(3)]}
-                for i, f in enumerate(fam)}
+        out = {f: {"min_ctas_per_sm": v[i], "ms": [round(ms[3 * i + k], 4) for k in range(3)]}
+               for i, f in enumerate(fam)}
+        forms = (ctypes.c_float * 3)()
+        _lib.check(self.lib.grb_get_tuning_forms(self.h, forms), "grb_get_tuning_forms")
+        r = lambda x: round(x, 4) if x < 1e29 else None
+        out["fofc_flag"]["queue_ms"] = r(forms[0])
+        out["aux"]["queue_ms"] = r(forms[1])
+        out["aux"]["deferred_ms"] = r(forms[2])
+        return out
 
     def set_tuning(self, flux=0, flag=0, update=0, aux=0):
-        """Pick tuned-mode candidates (indices 0..2) without timing."""
+        """Pick tuned-mode candidates without timing (grb_set_tuning: indices
+        0..2; flag and aux 3..5 the work-queue forms; aux 6..8 the
+        deferred-backup form)."""
         v = (ctypes.c_int32 * 4)(flux, flag, update, aux)
         _lib.check(self.lib.grb_set_tuning(self.h, v), "grb_set_tuning")
 
@@ -554,10 +563,12 @@ class GRMHDEquationsSystem:
         per-block order as
 
             copy_evolved_packed(host, state, True); bc(state);
-            compute_auxiliary_quantities(state, aux); rk3_step(...);
+            compute_auxiliary_quantities(state, aux);
+            linop_apply(state_p, state, None, 1.0); rk3_step(...);
             copy_evolved_packed(host, state, False)
 
-        (with state_p set to state first), so the same bits, but pipelined
+        (state_p is set to the state whose primitives were just computed:
+        rk3_step's entry condition), so the same bits, but pipelined
         over runs of blocks on three streams: the upload of each run overlaps
         the first substep of the runs before it, the download of each run
         the last substep of the runs after it.

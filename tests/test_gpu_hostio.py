@@ -220,6 +220,9 @@ def test_pipelined_host_step_matches_sequential(mode):
                 g.copy_evolved_packed(host, state, to_device=True)
                 bc(state)
                 g.compute_auxiliary_quantities(state, aux)
+                # rk3_step's entry condition: state_p equals state (whose
+                # conserved variables the primitives pass may have rewritten)
+                g.linop_apply(sp, state, None, 1.0, 0.0)
                 g.rk3_step(dt, state, sp, spp, aux, bc)
                 g.copy_evolved_packed(host, state, to_device=False)
         torch.cuda.synchronize()

@@ -106,8 +106,10 @@ def _check_aux(ga, oa, sel):
 
 
 # tuned candidates: the autotuner's pick; global-load flux at 4 CTAs/SM with
-# the others at 4; TMA-staged flux at 5 CTAs/SM with the work-queue aux pass
-@pytest.mark.parametrize("tuning", [None, (0, 1, 1, 1), (2, 2, 2, 4)])
+# the others at 4; 256-thread TMA flux tiles with the work-queue aux pass;
+# the work-queue FOFC flag with the deferred-backup aux pass, and with the
+# work-queue aux pass
+@pytest.mark.parametrize("tuning", [None, (0, 1, 1, 1), (2, 2, 2, 4), (1, 4, 1, 7), (1, 3, 1, 3)])
 def test_benchmark_configuration_matches_oracle(tuning):
     """One SSP-RK3 step of the benchmark's exact code path (16^3 blocks,
     tuned, static-metric cache, next-stage ranges, FOFC list) against the
@@ -126,6 +128,10 @@ def test_benchmark_configuration_matches_oracle(tuning):
     if tuning is None:
         # the autotuner picked one of the TMA-staged or global-load flux kernels
         assert g.tuning()["flux"]["min_ctas_per_sm"] in (4, 104, 102)
+    else:
+        t = g.tuning()
+        assert t["fofc_flag"]["min_ctas_per_sm"] == [1, 4, 5, 101, 104, 105][tuning[1]]
+        assert t["aux"]["min_ctas_per_sm"] == [1, 4, 5, 101, 104, 105, 201, 204, 205][tuning[3]]
 
 
 @pytest.mark.parametrize("cap", [0, 7])
