@@ -489,10 +489,12 @@ def ours(args, rank, world, local_rank):
 
         pipe = W["runs"](g, args.e2e_runs) if ("runs" in W and args.e2e_runs > 1) else None
         io = (torch.cuda.Stream(), torch.cuda.Stream())
+        prev = None
         for _ in range(ksteps):
             if pipe is not None:
                 runs, fill_run, deps = pipe
-                g.rk3_step_host(dt, host, state, sp, spp, aux, bc, runs, fill_run, deps, streams=io)
+                prev = g.rk3_step_host(dt, host, state, sp, spp, aux, bc, runs, fill_run, deps, streams=io,
+                                       after=prev, wait=False)
                 continue
             main.wait_stream(side)
             g.copy_evolved_packed(host, state, to_device=True)
@@ -502,6 +504,7 @@ def ours(args, rank, world, local_rank):
             g.rk3_step(dt, state, sp, spp, aux, bc, after_update=download_faces)
             g.copy_evolved_packed(host, state, to_device=False, arrays=cells_only)
         main.wait_stream(side)
+        main.wait_stream(io[1])
         f1.record()
         torch.cuda.synchronize()
         ems = f0.elapsed_time(f1)
@@ -521,7 +524,10 @@ def ours(args, rank, world, local_rank):
         if pipe is not None:
             e2e["pipeline"] = (f"GRMHDEquationsSystem.rk3_step_host over {len(pipe[0])} runs of z-slabs of blocks: "
                                "each run's upload overlaps the first substep of the runs before it, its download "
-                               "the last substep of the runs after it (upload, kernels, download on three streams)")
+                               "the last substep of the runs after it (upload, kernels, download on three streams); "
+                               "a step's upload of a run waits only for the previous step's download of that run, so "
+                               "it overlaps the previous step's last substep; the timed region ends after the last "
+                               "step's downloads")
         else:
             e2e["pipeline"] = ("none: upload, refill, primitives, rk3_step, download in sequence (face B downloaded "
                                "on a second stream once the last substep has made it final)")

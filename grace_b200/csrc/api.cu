@@ -70,6 +70,7 @@ struct grb_handle {
   float tune_aux_queue_ms = 0.f;
   float tune_aux_defer_ms = 0.f;
   float tune_flag_queue_ms = 0.f;
+  const double* res_idx = nullptr;        // spacings of the grid passed to grb_reserve
   bool mlp_ready = false;
   uint32_t fcap_alloc = 0;  // entries allocated for the compacted FOFC face list
   // the tuned batch c2p's deferred entropy backups: records and their count
@@ -493,6 +494,28 @@ inline bool trimmed(const grb_handle* h) {
   return h->mode == GRB_MODE_TUNED && h->p.ranges == GRB_RANGES_NEXT_STAGE;
 }
 
+// A grid that is a run of blocks of the reserved grid — the same block
+// geometry, idx pointing into the reserved grid's spacings at block q0 (its
+// field pointers offset alike) — has block offset q0; any other grid 0.
+int64_t run_offset(const grb_handle* h, const grb_grid* g) {
+  if (!h->reserved || !h->res_idx || !g->idx || h->geo.nx != g->nx || h->geo.ny != g->ny ||
+      h->geo.nz != g->nz || h->geo.g != g->ngz)
+    return 0;
+  const uintptr_t a = (uintptr_t)g->idx, b = (uintptr_t)h->res_idx;
+  if (a < b || (a - b) % (3 * sizeof(double))) return 0;
+  const int64_t q0 = (int64_t)((a - b) / (3 * sizeof(double)));
+  return q0 + g->nq <= h->geo.nq ? q0 : 0;
+}
+// The handle's scratch for a call on grid g: the scratch that outlives a
+// call (the Gardiner-Stone cell-centred E, written by the aux pass and read
+// by the next substep) is addressed from the run's first block, so that
+// calls on runs of blocks of the reserved grid see their own blocks'.
+StageBufs run_bufs(const grb_handle* h, const grb_grid* g) {
+  StageBufs B = h->B;
+  if (B.ecenter) B.ecenter += run_offset(h, g) * 3 * h->geo.cells;
+  return B;
+}
+
 // The static-metric cache when it was built for this geometry and these
 // spacings and covers these blocks, else null.  A grid whose idx points
 // into the cached spacings at block q0 (a run of blocks of the cached grid,
@@ -751,6 +774,7 @@ int grb_destroy(grb_handle* h) {
 int grb_reserve(grb_handle* h, const grb_grid* g) {
   if (!h || !g || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->nq < 1 || g->ngz < 4) return fail(h, GRB_ERR_INVALID);
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  h->res_idx = g->idx;
   if (h->reserved && same_geo(h->geo, g)) return GRB_OK;
   free_scratch(h);
   const int64_t nf = G.fcells * G.nq, nc = G.cells * G.nq;
@@ -824,7 +848,9 @@ int grb_advance_substep(grb_handle* h, const grb_grid* g, double t, double dt, d
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   const DevParams& P = h->dp;
   const int gz = G.g, T = 128;
-  StageBufs B = h->B;
+  // refluxing descriptors name blocks of the reserved grid
+  if (h->reflux && (run_offset(h, g) != 0 || g->nq != h->geo.nq)) return fail(h, GRB_ERR_INVALID);
+  StageBufs B = run_bufs(h, g);
   if (h->mode == GRB_MODE_TUNED) {
     const int nl = stage_tuned(h, G, g, dt, dtfact, nw, old, aux, s, B, true);
     if (nl < 0) return fail(h, GRB_ERR_CUDA);
@@ -967,16 +993,17 @@ int grb_compute_auxiliary_quantities_dt(grb_handle* h, const grb_grid* g, const 
     k_dt_init<<<1, 1, 0, s>>>(dta.out);
     ++h->launches;
   }
+  const StageBufs B = run_bufs(h, g);
   if (h->mode == GRB_MODE_TUNED) {
     const Box tb = trimmed(h) ? tuned_aux_box(h, G, s) : b;
     launch_aux_tuned(h->var_aux, nblk(tb.count(), 128), s, h->dp, G, tb, st->state, st->bx, st->by, st->bz, aux,
-                     g->idx, g->coords, h->B, dt_out ? &dta : nullptr, h->d_queue);
+                     g->idx, g->coords, B, dt_out ? &dta : nullptr, h->d_queue);
   } else if (dt_out) {
     k_aux<1, true><<<nblk(b.count(), 128), 128, 0, s>>>(h->dp, G, b, st->state, st->bx, st->by, st->bz, aux,
-                                                        g->idx, g->coords, h->B, dta);
+                                                        g->idx, g->coords, B, dta);
   } else {
     k_aux<1><<<nblk(b.count(), 128), 128, 0, s>>>(h->dp, G, b, st->state, st->bx, st->by, st->bz, aux, g->idx,
-                                                  g->coords, h->B);
+                                                  g->coords, B);
   }
   ++h->launches;
   CK(cudaGetLastError());
@@ -1646,19 +1673,28 @@ int grb_copy_evolved_packed(grb_handle* h, const grb_grid* g, const grb_fields* 
   const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
   if ((int64_t)GRB_N_HRSC * G.nq >= (1ll << 32) - 1) return fail(h, GRB_ERR_INVALID);
   cudaStream_t s = (cudaStream_t)stream;
-  // packed sizes (doubles) and offsets of the four arrays in the staging
-  // (each array has its own region, so calls on different streams that
-  // move different arrays do not share staging)
+  // packed sizes (doubles) and offsets of the four arrays in the staging:
+  // each array and each direction has its own region, laid out for the
+  // larger of this call's blocks and the reserved grid's (so calls on runs
+  // of blocks find the same regions as whole-grid calls), and calls on
+  // different streams that move different arrays, or the same array in
+  // opposite directions, do not share staging
+  const bool same_blocks = h->reserved && h->geo.nx == g->nx && h->geo.ny == g->ny && h->geo.nz == g->nz &&
+                           h->geo.g == g->ngz;
+  const int64_t nq_lay = same_blocks ? std::max(G.nq, h->geo.nq) : G.nq;
   int64_t cnt[4], off[4], tot = 0;
   for (int a = 0; a < 4; ++a) {
     int n[3] = {G.nx, G.ny, G.nz};
     if (a > 0) n[a - 1] += 1;
-    cnt[a] = (int64_t)n[0] * n[1] * n[2] * (a == 0 ? GRB_N_HRSC : 1) * G.nq;
+    const int64_t per_q = (int64_t)n[0] * n[1] * n[2] * (a == 0 ? GRB_N_HRSC : 1);
+    cnt[a] = per_q * G.nq;
     off[a] = tot;
-    tot += (cnt[a] + 31) / 32 * 32;  // 256-byte aligned starts
+    tot += (per_q * nq_lay + 31) / 32 * 32;  // 256-byte aligned starts
   }
   if (cnt[0] >= (1ll << 32)) return fail(h, GRB_ERR_INVALID);
-  const size_t bytes = sizeof(double) * (size_t)tot;
+  if (to_device)
+    for (int a = 0; a < 4; ++a) off[a] += tot;
+  const size_t bytes = sizeof(double) * (size_t)(2 * tot);
   if (bytes > h->stage_io_bytes) {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)

@@ -556,7 +556,7 @@ class GRMHDEquationsSystem:
         self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
 
     def rk3_step_host(self, dt, host, state, state_p, state_pp, aux, bc, runs, fill_run, deps, t=0.0,
-                      streams=None):
+                      streams=None, after=None, wait=True):
         """One SSP-RK3 step of a state held in packed pinned host arrays
         (packed_host_fields): upload, boundary fill and primitives of the
         uploaded state, the step, download — the same kernels in the same
@@ -581,21 +581,36 @@ class GRMHDEquationsSystem:
         streams: (upload, download) CUDA streams, new ones by default; the
         caller's current stream runs the kernels.  On return (stream order)
         host holds the new interior and state, state_p, aux on the device
-        are as after rk3_step."""
+        are as after rk3_step.
+
+        Consecutive steps: wait=False leaves the downloads pending (the
+        caller's stream does not wait for them) and returns one event per
+        run, recorded when its download is done; passed as `after` to the
+        next call (same arrays and streams, nothing else touching them in
+        between), each run's upload waits for that run's download only, so
+        the uploads of a step overlap the last substep of the step before.
+        The caller's stream waits for the download stream before it reads
+        host."""
         main = torch.cuda.current_stream()
         up, down = streams if streams is not None else (torch.cuda.Stream(), torch.cuda.Stream())
         S = len(runs)
+        if after is not None and len(after) != S:
+            raise ValueError("after: one event per run of the previous step")
         deps = [set(d) | {s} for s, d in enumerate(deps)]
         # readers[r]: the runs whose ghost fill reads run r's interior.  A
         # run's primitives pass may write corrected conserved variables
         # back into its interior, so it waits until those fills are done
         # (as the whole-grid order fills every block before any primitives).
         readers = [{t for t in range(S) if r in deps[t]} for r in range(S)]
-        # the uploads read host arrays the previous step's downloads wrote
-        up.wait_stream(main)
-        up.wait_stream(down)
+        # the uploads read host arrays the previous step's downloads wrote,
+        # into device blocks the previous step has finished with
+        if after is None:
+            up.wait_stream(main)
+            up.wait_stream(down)
         ev_up = []
-        for q0, q1 in runs:
+        for r, (q0, q1) in enumerate(runs):
+            if after is not None:
+                up.wait_event(after[r])
             with self.block_range(q0, q1):
                 self.copy_evolved_packed(host.view(q0, q1), state.view(q0, q1), True, stream=up)
             e = torch.cuda.Event()
@@ -630,6 +645,7 @@ class GRMHDEquationsSystem:
         # are updated, and finished (primitives, state_p) and downloaded
         # once the runs reading it are filled
         updated, filled, finished = set(), set(), set()
+        ev_down = [None] * S
         for s, (q0, q1) in enumerate(runs):
             with self.block_range(q0, q1):
                 self.advance_substep(t, dt, 2.0 / 3.0, state.view(q0, q1), state_pp.view(q0, q1), aux[q0:q1],
@@ -651,11 +667,15 @@ class GRMHDEquationsSystem:
                 down.wait_event(e)
                 with self.block_range(r0, r1):
                     self.copy_evolved_packed(host.view(r0, r1), state.view(r0, r1), False, stream=down)
+                ev_down[r] = torch.cuda.Event()
+                ev_down[r].record(down)
                 finished.add(r)
         if len(ready) != S or len(finished) != S:
             raise ValueError("runs / deps do not cover every run")
-        main.wait_stream(down)
         main.wait_stream(up)
+        if wait:
+            main.wait_stream(down)
+        return ev_down
 
     def capture_rk3_step(self, dt, state, state_p, state_pp, aux, bc, t=0.0, next_dt=None, fused_dt=False):
         """Capture one rk3_step (same arguments) into a CUDA graph.  The

@@ -198,7 +198,16 @@ int grb_eos_setup_pwpoly(grb_eos_params* e, int32_t n_pieces, double kappa_0,
 int grb_create(grb_handle** out, const grb_params* p);
 int grb_destroy(grb_handle* h);
 /* Size library-owned scratch (fluxes, face/edge EMFs, FOFC tags) for grid g;
- * mirrors resize_aux_staging_and_flux_buffers (variables.cpp:227-). */
+ * mirrors resize_aux_staging_and_flux_buffers (variables.cpp:227-).
+ * Calls on smaller grids use a prefix of the scratch.  A run of blocks
+ * [q0, q1) of the reserved grid — the same block geometry, idx = the
+ * reserved idx + 3 q0, every field pointer at block q0, nq = q1 - q0 — is
+ * a grid of its own for every stage call; the scratch that outlives a call
+ * (the Gardiner-Stone cell-centred E that the aux pass leaves for the next
+ * substep) is then addressed from block q0, so runs of blocks may be
+ * stepped one after another (each run's ghost zones filled).  With
+ * refluxing descriptors set (grb_set_reflux), substeps take the whole
+ * reserved grid only (GRB_ERR_INVALID otherwise). */
 int grb_reserve(grb_handle* h, const grb_grid* g);
 int grb_get_status(grb_handle* h, grb_status* st);
 int grb_clear_status(grb_handle* h);

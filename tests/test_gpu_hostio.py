@@ -183,7 +183,8 @@ def test_block_range_fill_equals_whole_fill(periodic):
 @pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
 def test_pipelined_host_step_matches_sequential(mode):
     """GRMHDEquationsSystem.rk3_step_host (upload, fill, primitives, step and
-    download pipelined over runs of z-slabs on three streams) gives the bits
+    download pipelined over runs of z-slabs on three streams; also chained,
+    each step's uploads overlapping the previous step's tail) gives the bits
     of the sequential host round trip, two steps in a row, in the host
     arrays and in every device array; tuned: the static-metric cache found
     at each run's first block, ranges trimmed to the next stage."""
@@ -208,13 +209,20 @@ def test_pipelined_host_step_matches_sequential(mode):
     assert len(runs) == 3
     fill_run = lambda fl, s, stream: g.fill_ghosts_brick(fl, su.nb, su.periodic, stream=stream, blocks=runs[s])
     out = []
-    for piped in (False, True):
+    io = (torch.cuda.Stream(), torch.cuda.Stream())
+    for piped in (False, True, "chained"):
         state, aux = st0.clone(), aux0.clone()
         sp, spp = state.clone(), state.clone()
         host = g.packed_host_fields()
         g.copy_evolved_packed(host, state, to_device=False)
+        prev = None
         for _ in range(2):
-            if piped:
+            if piped == "chained":
+                # each step's uploads wait only for the previous step's
+                # download of the same run
+                prev = g.rk3_step_host(dt, host, state, sp, spp, aux, bc, runs, fill_run, deps, streams=io,
+                                       after=prev, wait=False)
+            elif piped:
                 g.rk3_step_host(dt, host, state, sp, spp, aux, bc, runs, fill_run, deps)
             else:
                 g.copy_evolved_packed(host, state, to_device=True)
@@ -225,10 +233,12 @@ def test_pipelined_host_step_matches_sequential(mode):
                 g.linop_apply(sp, state, None, 1.0, 0.0)
                 g.rk3_step(dt, state, sp, spp, aux, bc)
                 g.copy_evolved_packed(host, state, to_device=False)
+        torch.cuda.current_stream().wait_stream(io[1])
         torch.cuda.synchronize()
         out.append([x.clone() for x in (host.state, host.bx, host.by, host.bz, state.state, state.bx, state.by,
                                          state.bz, sp.state, sp.bx, sp.by, sp.bz, aux)])
     assert not torch.equal(out[0][0], torch.from_numpy(f[0][:, :abi.N_HRSC, 4:12, 4:12, 4:12].copy()))
-    for k, (a, b) in enumerate(zip(*out)):
-        assert torch.equal(a, b), k
+    for other in out[1:]:
+        for k, (a, b) in enumerate(zip(out[0], other)):
+            assert torch.equal(a, b), k
     assert g.status().device_flags == 0
