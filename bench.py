@@ -681,8 +681,15 @@ def ours(args, rank, world, local_rank):
     # --- c2p micro-benchmark (2^24 states): plain, then with the learned
     # bracket trained on the GPU from 2^20 other seeded states
     c2p = None
-    if not args.no_c2p and rank == 0 and args.config == "blast":
-        c2p = c2p_bench(dev, learned=not args.no_learned)
+    if not args.no_c2p and rank == 0:
+        if args.config == "blast":
+            c2p = c2p_bench(dev, learned=not args.no_learned)
+        else:
+            # the configuration's own cells after the timed steps: the c2p
+            # with and without the learned bracket on the states it meets
+            c2p = c2p_bench(dev, learned=not args.no_learned, states=_cell_states(torch, abi, state, blocks),
+                            P=P)
+            c2p["states_from"] = "every interior cell of the configuration after the timed steps"
 
     cpu = None
     if rank == 0 and not args.no_cpu and world == 1:
@@ -712,6 +719,25 @@ def ours(args, rank, world, local_rank):
     g.close()
 
 
+def _cell_states(torch, abi, f, blocks):
+    """(cons (10, n), metric (10, n)) of every interior cell of device
+    Fields f: the 7 HRSC variables, the cell-centred B (means of the face
+    pairs), the 3-metric, shift and lapse."""
+    g, n = blocks.ngz, blocks.nx
+    i = slice(g, g + n)
+    st = f.state
+    cons = torch.empty(10, blocks.nq, n, n, n, dtype=torch.float64, device=st.device)
+    cons[:abi.N_HRSC] = st[:, :abi.N_HRSC, i, i, i].permute(1, 0, 2, 3, 4)
+    cons[7] = 0.5 * (f.bx[:, i, i, g:g + n] + f.bx[:, i, i, g + 1:g + n + 1])
+    cons[8] = 0.5 * (f.by[:, i, g:g + n, i] + f.by[:, i, g + 1:g + n + 1, i])
+    cons[9] = 0.5 * (f.bz[:, g:g + n, i, i] + f.bz[:, g + 1:g + n + 1, i, i])
+    met = torch.empty(10, blocks.nq, n, n, n, dtype=torch.float64, device=st.device)
+    met[:6] = st[:, abi.GXX:abi.GXX + 6, i, i, i].permute(1, 0, 2, 3, 4)
+    met[6:9] = st[:, abi.BETAX:abi.BETAX + 3, i, i, i].permute(1, 0, 2, 3, 4)
+    met[9] = st[:, abi.ALP, i, i, i]
+    return cons.reshape(10, -1).contiguous(), met.reshape(10, -1).contiguous()
+
+
 def _c2p_agreement(torch, pr_a, pr_p):
     """State-normalised residual of primitives against the plain c2p's: the
     largest, its ratio to the bound 1e-12 max(1, W^2) (Brent's absolute
@@ -728,24 +754,35 @@ def _c2p_agreement(torch, pr_a, pr_p):
             "frac_within_1e-12": float((d[ok] <= 1e-12).double().mean())}
 
 
-def c2p_bench(dev, learned=True, n=1 << 24, reps=5):
+def c2p_bench(dev, learned=True, n=1 << 24, reps=5, states=None, P=None):
+    """c2p solves/s, plain / tuned / learned bracket / learned + tuned, with
+    the agreement of each with the plain solve.  Default: the 2^24 seeded
+    states of the c2p workload (flat metric), the network trained on 2^20
+    other seeded states.  states = (cons (10, n), metric (10, n)) device
+    tensors and P their parameters: those states (a configuration's own
+    cells), the network trained on 2^20 of them picked at random."""
     import torch
     from grace_b200 import abi, params, workloads
     from grace_b200.host import GRMHDEquationsSystem
-    cons, _ = workloads.c2p_states(n, seed=5)
-    gc = GRMHDEquationsSystem(params.c2p_bench())
-    c_d = torch.from_numpy(cons).to(dev)
-    del cons
+    if states is None:
+        cons, _ = workloads.c2p_states(n, seed=5)
+        gc = GRMHDEquationsSystem(params.c2p_bench())
+        c_d, m_d = torch.from_numpy(cons).to(dev), None
+        del cons
+    else:
+        c_d, m_d = states
+        n = c_d.shape[1]
+        gc = GRMHDEquationsSystem(P)
 
     def timed(use_learned):
         for _ in range(2):
-            gc.conservs_to_prims(c_d, use_learned=use_learned)
+            gc.conservs_to_prims(c_d, m_d, use_learned=use_learned)
         torch.cuda.synchronize()
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
         a0.record()
         for _ in range(reps):
-            gc.conservs_to_prims(c_d, use_learned=use_learned)
+            gc.conservs_to_prims(c_d, m_d, use_learned=use_learned)
         a1.record()
         torch.cuda.synchronize()
         return n * reps / (a0.elapsed_time(a1) * 1e-3)
@@ -753,7 +790,7 @@ def c2p_bench(dev, learned=True, n=1 << 24, reps=5):
     def iters(use_learned):
         it = torch.zeros(n, dtype=torch.int32, device=dev)
         gu = torch.zeros(n, dtype=torch.int8, device=dev)
-        pr = gc.conservs_to_prims(c_d, use_learned=use_learned, diag={"iters": it, "guess_used": gu})
+        pr = gc.conservs_to_prims(c_d, m_d, use_learned=use_learned, diag={"iters": it, "guess_used": gu})
         m = (n // 32) * 32
         st = {"mean_brent_iters": float(it.double().mean()), "max_brent_iters": int(it.max()),
               "warp_max_brent_iters": float(it[:m].view(-1, 32).max(1).values.double().mean())}
@@ -771,9 +808,13 @@ def c2p_bench(dev, learned=True, n=1 << 24, reps=5):
     out["tuned_vs_plain"] = _c2p_agreement(torch, pr_t, pr_p)
     gc.set_mode(abi.MODE_PLAIN)
     if learned:
-        tr, _ = workloads.c2p_states(1 << 20, seed=6)
-        rep = gc.train_c2p_model(torch.from_numpy(tr).to(dev))
-        del tr
+        if states is None:
+            tr, _ = workloads.c2p_states(1 << 20, seed=6)
+            rep = gc.train_c2p_model(torch.from_numpy(tr).to(dev))
+            del tr
+        else:
+            pick = torch.randperm(n, generator=torch.Generator().manual_seed(6))[:min(n, 1 << 20)].to(dev)
+            rep = gc.train_c2p_model(c_d[:, pick].contiguous(), m_d[:, pick].contiguous())
         out["learned_solves_per_s"] = timed(True)
         pr_l, out["learned"] = iters(True)
         out["learned_vs_plain"] = _c2p_agreement(torch, pr_l, pr_p)
