@@ -209,6 +209,9 @@ struct KScope {
 // compiler; 1 leaves the register count free, 4 caps it at 128, 5 at 102.
 constexpr int kMaxDevices = 64;  // device ordinals tracked by per-device launch set-up
 constexpr int kMinB[3] = {1, 4, 5};
+// The c2p-bearing kernels (FOFC flag, aux pass) in their tuned forms: 3, 4,
+// 5 (uncapped they need 180-250 registers, two CTAs per SM at most).
+constexpr int kMinBC2p[3] = {3, 4, 5};
 // The update kernel that reads the static-metric cache: 1, 3, 4.
 constexpr int kMinBCached[3] = {1, 3, 4};
 constexpr int kNumVar = 3;
@@ -320,7 +323,7 @@ void launch_flag_queue(cudaStream_t s, const DevParams& P, const Geo& G, const B
   cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
   k_fofc_flag_queue<MINB, true><<<grid, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
 }
-// Flag candidates: 0..2 one thread per cell at 1, 4, 5 CTAs/SM; 3..5 the
+// Flag candidates: 0..2 one thread per cell at 3, 4, 5 CTAs/SM; 3..5 the
 // persistent work-queue form at the same caps (given the queue counter).
 void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                        double dt, double dtfact, const double* ns, const double* os, const double* bx,
@@ -329,13 +332,13 @@ void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, c
   if (v >= 3 && queue) {
     if (v == 4) launch_flag_queue<4>(s, P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
     else if (v == 5) launch_flag_queue<5>(s, P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
-    else launch_flag_queue<1>(s, P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
+    else launch_flag_queue<3>(s, P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B, queue);
     return;
   }
   if (v >= 3) v -= 3;
   if (v == 1) k_fofc_flag<4, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
   else if (v == 2) k_fofc_flag<5, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
-  else k_fofc_flag<1, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
+  else k_fofc_flag<3, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, bx, by, bz, idx, crd, B);
 }
 // Update candidates: 0..2 at 1, 4, 5 CTAs/SM; with the static-metric
 // cache md the kernel that reads it (capped at 1, 3, 4 CTAs/SM).
@@ -387,9 +390,9 @@ void launch_aux_deferred(unsigned nb, cudaStream_t s, const DevParams& P, const 
                                                                        dta);
 }
 
-// Aux candidates: 0..2 one thread per cell at kMinB[v] CTAs/SM; 3..5 the
-// work-queue form at kMinB[v - 3]; 6..8 the deferred-backup form at
-// kMinB[v - 6].
+// Aux candidates: 0..2 one thread per cell at kMinBC2p[v] CTAs/SM; 3..5
+// the work-queue form at kMinBC2p[v - 3]; 6..8 the deferred-backup form at
+// kMinBC2p[v - 6].
 void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                       double* st, const double* bx, const double* by, const double* bz, double* aux,
                       const double* idx, const double* crd, const StageBufs& B,
@@ -400,11 +403,11 @@ void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, co
     if (dta) {
       if (m == 1) launch_aux_deferred<4, true>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
       else if (m == 2) launch_aux_deferred<5, true>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
-      else launch_aux_deferred<1, true>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+      else launch_aux_deferred<3, true>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
     } else {
       if (m == 1) launch_aux_deferred<4, false>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, d0);
       else if (m == 2) launch_aux_deferred<5, false>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, d0);
-      else launch_aux_deferred<1, false>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, d0);
+      else launch_aux_deferred<3, false>(nb, s, P, G, b, st, bx, by, bz, aux, idx, crd, B, d0);
     }
     return;
   }
@@ -415,11 +418,11 @@ void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, co
     if (dta) {
       if (m == 1) launch_aux_queue<4, true>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, *dta);
       else if (m == 2) launch_aux_queue<5, true>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, *dta);
-      else launch_aux_queue<1, true>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, *dta);
+      else launch_aux_queue<3, true>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, *dta);
     } else {
       if (m == 1) launch_aux_queue<4, false>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, d0);
       else if (m == 2) launch_aux_queue<5, false>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, d0);
-      else launch_aux_queue<1, false>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, d0);
+      else launch_aux_queue<3, false>(s, P, G, b, st, bx, by, bz, aux, idx, crd, B, queue, d0);
     }
     return;
   }
@@ -427,12 +430,12 @@ void launch_aux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, co
   if (dta) {
     if (v == 1) k_aux<4, true, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
     else if (v == 2) k_aux<5, true, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
-    else k_aux<1, true, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
+    else k_aux<3, true, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B, *dta);
     return;
   }
   if (v == 1) k_aux<4, false, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
   else if (v == 2) k_aux<5, false, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
-  else k_aux<1, false, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
+  else k_aux<3, false, true><<<nb, 128, 0, s>>>(P, G, b, st, bx, by, bz, aux, idx, crd, B);
 }
 
 // A = b X (+ c Y) on the planes z in [zlo, zlo + nz) and rows y in [ylo,
@@ -2113,9 +2116,9 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   if (!h || !variant) return GRB_ERR_INVALID;
   variant[0] = kFluxMinB[h->var_flux] + (kFluxTma[h->var_flux] ? 100 : 0);
-  variant[1] = kMinB[h->var_flag % 3] + 100 * (h->var_flag / 3);
+  variant[1] = kMinBC2p[h->var_flag % 3] + 100 * (h->var_flag / 3);
   variant[2] = h->d_metder ? kMinBCached[h->var_update] : kMinB[h->var_update];
-  variant[3] = kMinB[h->var_aux % 3] + 100 * (h->var_aux / 3);
+  variant[3] = kMinBC2p[h->var_aux % 3] + 100 * (h->var_aux / 3);
   if (ms)
     for (int f = 0; f < 4; ++f)
       for (int v = 0; v < kNumVar; ++v) ms[f * kNumVar + v] = h->tune_ms[f][v];

@@ -422,8 +422,9 @@ int grb_get_tuning_forms(grb_handle* h, float* ms);
 /* Choose the tuned-mode candidates without timing: variant[4] = candidate
  * index 0..2 of flux, flag, update, aux (flux: 0 global-load kernel, 1 the
  * TMA-staged kernel with 128-thread tiles at 4 CTAs/SM, 2 with 256-thread
- * tiles (twice the face rows per tile) at 2 CTAs/SM; others: 1, 4, 5
- * CTAs/SM; flag and aux also
+ * tiles (twice the face rows per tile) at 2 CTAs/SM; update: 1, 4, 5
+ * CTAs/SM (1, 3, 4 for the kernel that reads the static-metric cache);
+ * flag and aux: 3, 4, 5 CTAs/SM; flag and aux also
  * 3..5: the work-queue form — one wave of CTAs pulling chunks of 128-cell
  * tiles from a device counter — at 1, 4, 5 CTAs/SM; aux also 6..8: the
  * deferred-backup form — the cells whose Kastaun result is distrusted

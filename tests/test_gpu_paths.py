@@ -130,8 +130,8 @@ def test_benchmark_configuration_matches_oracle(tuning):
         assert g.tuning()["flux"]["min_ctas_per_sm"] in (4, 104, 102)
     else:
         t = g.tuning()
-        assert t["fofc_flag"]["min_ctas_per_sm"] == [1, 4, 5, 101, 104, 105][tuning[1]]
-        assert t["aux"]["min_ctas_per_sm"] == [1, 4, 5, 101, 104, 105, 201, 204, 205][tuning[3]]
+        assert t["fofc_flag"]["min_ctas_per_sm"] == [3, 4, 5, 103, 104, 105][tuning[1]]
+        assert t["aux"]["min_ctas_per_sm"] == [3, 4, 5, 103, 104, 105, 203, 204, 205][tuning[3]]
 
 
 @pytest.mark.parametrize("cap", [0, 7])
@@ -255,7 +255,7 @@ def test_deferred_backup_aux_pass_matches_oracle(aux):
     P.beta_fallback = 1e3
     dt = 0.25 / su.idx()[0, 0]
     gs, ga, g = _gpu(P, su, f, dt, 1, abi.MODE_TUNED, tuning=(1, 1, 1, aux))
-    assert g.tuning()["aux"]["min_ctas_per_sm"] == [201, 204, 205][aux - 6]
+    assert g.tuning()["aux"]["min_ctas_per_sm"] == [203, 204, 205][aux - 6]
     os_, oa, counts = _oracle_run(P, su, f, dt, 1)
     _check_state(gs, os_, su.ngz)
     sel = (slice(None), tuned_aux_mask(su))
