@@ -82,7 +82,7 @@ def parse():
                          "Fishbone-Moncrief torus on their FMR hierarchies (16^3 blocks, refluxing, gather-map "
                          "ghost fill)")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-form comparison run")
-    ap.add_argument("--e2e-runs", type=int, default=16,
+    ap.add_argument("--e2e-runs", type=int, default=8,
                     help="end-to-end leg: runs of blocks the host step pipelines over (1: no pipeline)")
     ap.add_argument("--ref-blocks", type=int, default=8,
                     help="reference arm: blocks per axis of the CPU sample (the central ones; --nb for the whole grid)")
