@@ -458,3 +458,70 @@ def test_two_level_blocks_in_one_launch_match_oracle(mode):
     dto = S.find_stable_timestep(ost, ax_, np.ascontiguousarray(1.0 / idx), 0.25)
     assert abs(dtd.item() - dto) <= 1e-12 * dto, (dtd.item(), dto)
     assert g.status().device_flags == 0
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_curved_radius_excision_matches_oracle(mode):
+    """Excision by radius (excision_criterion: radius) on the curved setup:
+    the c2p excises the cells whose centre, from the block coordinates
+    (grb_grid.coords: the centre of cell (0, 0, 0) of each block), lies
+    within r_ex = 3.6 of the origin (the brick spans r = 3 .. 5.2); one
+    SSP-RK3 step against the oracle given the same coordinates."""
+    from curved import curved_setup
+    P, su, f = curved_setup(emf=abi.EMF_GS, fofc=1)
+    P.excise_by_radius = 1
+    P.r_ex = 3.6
+    crd = su.coords()
+    X = su.cell_centres()
+    r = np.sqrt(np.sum(X ** 2, axis=1))
+    assert r.min() < P.r_ex < r.max()
+    dt = 0.25 / su.idx()[0, 0]
+    idx = su.idx()
+    # oracle, coordinates passed to every substep and aux pass
+    st, bx, by, bz, aux = [x.copy() for x in f]
+    S = _oracle.Stage(P, su.n[0], su.n[1], su.n[2], su.ngz, su.nq)
+    state = [st, bx, by, bz]
+    bc_o = lambda fl: _oracle.fill_ghosts("orc", su, fl)
+    bc_o(state)
+    S.compute_aux(idx.copy(), state, aux, crd)
+    sp = [x.copy() for x in state]
+    spp = [x.copy() for x in state]
+    S.reset_diag(aux)
+    S.advance_substep(idx.copy(), dt, 1.0, sp, state, aux, crd)
+    bc_o(sp)
+    S.compute_aux(idx.copy(), sp, aux, crd)
+    S.linop(spp, state, sp, 0.75, 0.25)
+    S.advance_substep(idx.copy(), dt, 0.25, spp, sp, aux, crd)
+    bc_o(spp)
+    S.compute_aux(idx.copy(), spp, aux, crd)
+    S.linop(state, state, spp, 1.0 / 3, 2.0 / 3.0)
+    S.advance_substep(idx.copy(), dt, 2.0 / 3.0, state, spp, aux, crd)
+    bc_o(state)
+    S.compute_aux(idx.copy(), state, aux, crd)
+    # GPU, the same coordinates in the grid
+    dev = torch.device("cuda:0")
+    blocks = Blocks(su.n[0], su.n[1], su.n[2], su.ngz, su.nq, idx, coords=crd, device=dev)
+    g = GRMHDEquationsSystem(P)
+    g.reserve(blocks)
+    g.set_mode(mode)
+    if mode == abi.MODE_TUNED:
+        g.set_tuning(1, 1, 1, 1)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    gst = Fields(*[T(x) for x in f[:4]])
+    gaux = T(f[4])
+    bc = lambda fl: g.fill_ghosts_brick(fl, su.nb, su.periodic)
+    bc(gst)
+    g.compute_auxiliary_quantities(gst, gaux)
+    gsp, gspp = gst.clone(), gst.clone()
+    g.rk3_step(dt, gst, gsp, gspp, gaux, bc)
+    torch.cuda.synchronize()
+    gs = [x.cpu().numpy() for x in (gst.state, gst.bx, gst.by, gst.bz)]
+    ga = gaux.cpu().numpy()
+    e = cons_rel_err(interior(gs[0][:, :7], su.ngz), interior(state[0][:, :7], su.ngz))
+    assert e.max() < STEP_TOL, e
+    for a, b in zip(gs[1:], state[1:]):
+        assert np.max(np.abs(a - b)) < STEP_TOL * np.max(np.abs(b))
+    # the excised cells carry the excision flag in both, the same cells
+    sel = (slice(None),) + tuple(slice(su.ngz, -su.ngz) for _ in range(3))
+    np.testing.assert_array_equal(ga[:, abi.C2P_ERR][sel], aux[:, abi.C2P_ERR][sel])
+    assert g.status().device_flags == 0
