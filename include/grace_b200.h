@@ -426,10 +426,10 @@ int grb_get_tuning_forms(grb_handle* h, float* ms);
  * CTAs/SM (1, 3, 4 for the kernel that reads the static-metric cache);
  * flag and aux: 3, 4, 5 CTAs/SM; flag and aux also
  * 3..5: the work-queue form — one wave of CTAs pulling chunks of 128-cell
- * tiles from a device counter — at 1, 4, 5 CTAs/SM; aux also 6..8: the
+ * tiles from a device counter — at 3, 4, 5 CTAs/SM; aux also 6..8: the
  * deferred-backup form — the cells whose Kastaun result is distrusted
  * listed and finished by a second kernel running their entropy backups
- * together — at 1, 4, 5 CTAs/SM, its list allocated here for the reserved
+ * together — at 3, 4, 5 CTAs/SM, its list allocated here for the reserved
  * grid: call before any stream capture). */
 int grb_set_tuning(grb_handle* h, const int32_t* variant);
 
