@@ -174,7 +174,7 @@ PROTOTYPES = {
     "grb_autotune": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields), C.POINTER(Fields),
                                C.c_void_p, C.c_void_p]),
     "grb_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32), C.POINTER(C.c_float)]),
-    "grb_get_tuning_forms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "grb_get_tuning_forms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float), C.c_int32]),
     "grb_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(C.c_int32)]),
     "grb_set_fofc_list_capacity": (C.c_int, [C.c_void_p, C.c_int64]),
     "grb_set_reflux": (C.c_int, [C.c_void_p, C.POINTER(Reflux)]),

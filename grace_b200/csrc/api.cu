@@ -14,6 +14,8 @@
 #include <cstdio>
 #include <cstring>
 #include <random>
+#include <tuple>
+#include <utility>
 #include <new>
 #include <vector>
 
@@ -53,7 +55,7 @@ struct grb_handle {
   // learned c2p bracket: FP32 parameter block on the device
   float* d_mlp = nullptr;
   MlpSmem* d_mlp_pack = nullptr;  // shared-memory image of the network
-  unsigned long long* d_queue = nullptr;  // work-queue counters: [0] aux pass, [1] FOFC flag
+  unsigned long long* d_queue = nullptr;  // work-queue counters: [0] aux pass, [1] FOFC flag, [2] flux, [3] update
   double* d_metder = nullptr;             // static-metric cache (grb_set_static_metric)
   size_t metder_bytes = 0;
   int metder_key[4] = {0, 0, 0, 0};       // nx, ny, nz, ngz it was built for
@@ -70,6 +72,8 @@ struct grb_handle {
   float tune_aux_queue_ms = 0.f;
   float tune_aux_defer_ms = 0.f;
   float tune_flag_queue_ms = 0.f;
+  float tune_flux_queue_ms = 0.f;
+  float tune_update_queue_ms = 0.f;
   const double* res_idx = nullptr;        // spacings of the grid passed to grb_reserve
   bool mlp_ready = false;
   uint32_t fcap_alloc = 0;  // entries allocated for the compacted FOFC face list
@@ -286,6 +290,69 @@ bool launch_flux_tma(cudaStream_t s, const DevParams& P, const Geo& G, const Box
   return true;
 }
 
+// One wave of a persistent one-thread-per-item kernel (occupancy x SMs CTAs
+// of 128 threads, per device ordinal and kernel), after zeroing its queue
+// counter on the stream; the kernel's last argument is the counter.
+template <class... KArgs, class... Args>
+void launch_item_queue(cudaStream_t s, void (*kernel)(KArgs...), Args&&... args) {
+  static int grids[kMaxDevices] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int grid = dev >= 0 && dev < kMaxDevices ? grids[dev] : 0;
+  if (grid == 0) {
+    int sms = 0, occ = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, 128, 0);
+    grid = (sms > 0 ? sms : 1) * (occ > 0 ? occ : 1);
+    if (dev >= 0 && dev < kMaxDevices) grids[dev] = grid;
+  }
+  unsigned long long* queue = std::get<sizeof...(Args) - 1>(std::forward_as_tuple(args...));
+  cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s);
+  kernel<<<grid, 128, 0, s>>>(std::forward<Args>(args)...);
+}
+
+// The TMA-staged flux as one wave of persistent CTAs pulling tiles from the
+// queue counter (zeroed first on the stream); false when the tile does not
+// fit (the caller then launches another form).
+template <int dir, int MINB, int NT = 128>
+bool launch_flux_tma_queue(cudaStream_t s, const DevParams& P, const Geo& G, const Box& b, const double* st,
+                           const double* aux, const double* bf, const StageBufs& B, unsigned long long* queue) {
+  const FluxTile T = flux_tile(dir, G, b, NT);
+  if (T.n[0] > NT || !queue) return false;
+  CUtensorMap ta, tm;
+  if (!make_tmap(&ta, aux, G, GRB_N_AUX_VARS, b.nq, T) || !make_tmap(&tm, st, G, GRB_N_EVOL_VARS, b.nq, T))
+    return false;
+  const size_t smem = flux_tile_smem(G, T);
+  static size_t attr[kMaxDevices] = {};
+  static int occ_for[kMaxDevices] = {};
+  static size_t occ_smem[kMaxDevices] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return false;
+  if (smem > attr[dev]) {
+    if (cudaFuncSetAttribute(k_flux_tma_queue<dir, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return false;
+    attr[dev] = smem;
+  }
+  if (occ_smem[dev] != smem) {
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_flux_tma_queue<dir, MINB, NT>, NT, smem) !=
+            cudaSuccess || occ < 1)
+      return false;
+    occ_for[dev] = occ;
+    occ_smem[dev] = smem;
+  }
+  int sms = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int nrow = dir == 2 ? T.n[2] : T.n[1];
+  const int nother = dir == 2 ? T.n[1] : T.n[2];
+  const int ntx = (nrow + T.R - 1) / T.R;
+  if (cudaMemsetAsync(queue, 0, sizeof(unsigned long long), s) != cudaSuccess) return false;
+  k_flux_tma_queue<dir, MINB, NT><<<(unsigned)(std::max(sms, 1) * occ_for[dev]), NT, smem, s>>>(
+      P, G, T, ta, tm, bf, B, queue, ntx, nother);
+  return true;
+}
+
 // Flux candidates of the tuned mode (tile shapes and register caps): the
 // global-load kernel at 4 CTAs/SM of 128 threads, the TMA-staged kernel
 // with 128-thread tiles at 4 CTAs/SM, and with 256-thread tiles (twice the
@@ -295,9 +362,20 @@ bool launch_flux_tma(cudaStream_t s, const DevParams& P, const Geo& G, const Box
 constexpr int kFluxMinB[3] = {4, 4, 2};
 constexpr bool kFluxTma[3] = {false, true, true};
 
+// Candidates 3..5: the same three as persistent launches pulling work from
+// the queue counter (given): the global-load kernel's 128-face tiles, or
+// the TMA-staged kernel's tiles.
 template <int dir>
 void launch_flux_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
-                       const double* st, const double* aux, const double* bf, const StageBufs& B) {
+                       const double* st, const double* aux, const double* bf, const StageBufs& B,
+                       unsigned long long* queue = nullptr) {
+  if (v >= 3 && queue) {
+    if (v == 4 && launch_flux_tma_queue<dir, 4>(s, P, G, b, st, aux, bf, B, queue)) return;
+    if (v == 5 && launch_flux_tma_queue<dir, 2, 256>(s, P, G, b, st, aux, bf, B, queue)) return;
+    launch_item_queue(s, k_flux_queue<dir, true, 4>, P, G, b, st, aux, bf, B, queue);
+    return;
+  }
+  if (v >= 3) v -= 3;
   if (v == 1 && launch_flux_tma<dir, 4>(s, P, G, b, st, aux, bf, B)) return;
   if (v == 2 && launch_flux_tma<dir, 2, 256>(s, P, G, b, st, aux, bf, B)) return;
   k_flux<dir, true, 4><<<nb, 128, 0, s>>>(P, G, b, st, aux, bf, B);
@@ -342,9 +420,27 @@ void launch_flag_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, c
 }
 // Update candidates: 0..2 at 1, 4, 5 CTAs/SM; with the static-metric
 // cache md the kernel that reads it (capped at 1, 3, 4 CTAs/SM).
+// 3..5: the same caps as persistent launches pulling 128-cell tiles from the
+// queue counter (given).
 void launch_update_tuned(int v, unsigned nb, cudaStream_t s, const DevParams& P, const Geo& G, const Box& b,
                          double dt, double dtfact, double* ns, const double* os, const double* aux,
-                         const double* idx, const StageBufs& B, const double* md = nullptr) {
+                         const double* idx, const StageBufs& B, const double* md = nullptr,
+                         unsigned long long* queue = nullptr) {
+  if (v >= 3 && queue) {
+    const int m = v - 3;
+    if (md) {
+      if (m == 1) launch_item_queue(s, k_update_queue<3, true>, P, G, b, dt, dtfact, ns, os, aux, idx, B, md, queue);
+      else if (m == 2) launch_item_queue(s, k_update_queue<4, true>, P, G, b, dt, dtfact, ns, os, aux, idx, B, md, queue);
+      else launch_item_queue(s, k_update_queue<1, true>, P, G, b, dt, dtfact, ns, os, aux, idx, B, md, queue);
+    } else {
+      const double* none = nullptr;
+      if (m == 1) launch_item_queue(s, k_update_queue<4, false>, P, G, b, dt, dtfact, ns, os, aux, idx, B, none, queue);
+      else if (m == 2) launch_item_queue(s, k_update_queue<5, false>, P, G, b, dt, dtfact, ns, os, aux, idx, B, none, queue);
+      else launch_item_queue(s, k_update_queue<1, false>, P, G, b, dt, dtfact, ns, os, aux, idx, B, none, queue);
+    }
+    return;
+  }
+  if (v >= 3) v -= 3;
   if (md) {
     static_assert(kMinBCached[1] == 3 && kMinBCached[2] == 4, "update candidates");
     if (v == 1) k_update<3, true><<<nb, 128, 0, s>>>(P, G, b, dt, dtfact, ns, os, aux, idx, B, md);
@@ -599,9 +695,9 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
     }
     const Box b = box(lo[0], lo[1], lo[2], n[0], n[1], n[2], G.nq);
     const unsigned nb = nblk(b.count(), T);
-    if (dir == 0) launch_flux_tuned<0>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[0], B);
-    if (dir == 1) launch_flux_tuned<1>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[1], B);
-    if (dir == 2) launch_flux_tuned<2>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[2], B);
+    if (dir == 0) launch_flux_tuned<0>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[0], B, h->d_queue + 2);
+    if (dir == 1) launch_flux_tuned<1>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[1], B, h->d_queue + 2);
+    if (dir == 2) launch_flux_tuned<2>(h->var_flux, nb, s, P, G, b, old->state, aux, bf[2], B, h->d_queue + 2);
     ++launches;
   }
   const Box eb = box(gz, gz, gz, G.nx + 1, G.ny + 1, G.nz + 1, G.nq);
@@ -651,7 +747,7 @@ int stage_tuned(grb_handle* h, const Geo& G, const grb_grid* g, double dt, doubl
   {
     KScope ks(h, s, GRB_KIND_UPDATE);
     launch_update_tuned(h->var_update, nblk(ub.count(), T), s, P, G, ub, dt, dtfact, nw->state, old->state,
-                        aux, g->idx, B, static_metric(h, G, g->idx));
+                        aux, g->idx, B, static_metric(h, G, g->idx), h->d_queue + 3);
     ++launches;
   }
   if (h->reflux) {
@@ -727,7 +823,7 @@ int grb_create(grb_handle** out, const grb_params* p) {
   h->dp = to_dev(*p);
   if (cudaMalloc(&h->d_flags, sizeof(uint32_t)) != cudaSuccess ||
       cudaMalloc(&h->d_counters, 2 * sizeof(unsigned long long)) != cudaSuccess ||
-      cudaMalloc(&h->d_queue, 2 * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaMalloc(&h->d_queue, 4 * sizeof(unsigned long long)) != cudaSuccess) {
     cudaFree(h->d_flags);
     cudaFree(h->d_counters);
     delete h;
@@ -2073,7 +2169,16 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
       if (t < bt) { bt = t; best[fam] = v; }
     }
   }
-  // the work-queue forms of the chosen flag and aux register caps
+  // the work-queue forms of the chosen candidates of every family
+  h->tune_flux_queue_ms = time_it([&] {
+    launch_flux_tuned<0>(best[0] + 3, nblk(fbx.count(), 128), s, P, G, fbx, os, ax, fo.bx, B, h->d_queue + 2);
+  });
+  if (h->tune_flux_queue_ms < h->tune_ms[0][best[0]]) best[0] += 3;
+  h->tune_update_queue_ms = time_it([&] {
+    launch_update_tuned(best[2] + 3, nblk(ub.count(), 128), s, P, G, ub, 1e-12, 1.0, ns, os, ax, gs.idx, B, md,
+                        h->d_queue + 3);
+  });
+  if (h->tune_update_queue_ms < h->tune_ms[2][best[2]]) best[2] += 3;
   h->tune_flag_queue_ms = time_it([&] {
     launch_flag_tuned(best[1] + 3, nblk(fb.count(), 128), s, P, G, fb, 1e-3, 1.0, ns, os, fo.bx, fo.by, fo.bz,
                       gs.idx, gs.coords, B, h->d_queue + 1);
@@ -2115,9 +2220,9 @@ int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* nw, const g
 
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   if (!h || !variant) return GRB_ERR_INVALID;
-  variant[0] = kFluxMinB[h->var_flux] + (kFluxTma[h->var_flux] ? 100 : 0);
+  variant[0] = kFluxMinB[h->var_flux % 3] + (kFluxTma[h->var_flux % 3] ? 100 : 0) + 1000 * (h->var_flux / 3);
   variant[1] = kMinBC2p[h->var_flag % 3] + 100 * (h->var_flag / 3);
-  variant[2] = h->d_metder ? kMinBCached[h->var_update] : kMinB[h->var_update];
+  variant[2] = (h->d_metder ? kMinBCached[h->var_update % 3] : kMinB[h->var_update % 3]) + 100 * (h->var_update / 3);
   variant[3] = kMinBC2p[h->var_aux % 3] + 100 * (h->var_aux / 3);
   if (ms)
     for (int f = 0; f < 4; ++f)
@@ -2125,18 +2230,18 @@ int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms) {
   return GRB_OK;
 }
 
-int grb_get_tuning_forms(grb_handle* h, float* ms) {
-  if (!h || !ms) return GRB_ERR_INVALID;
-  ms[0] = h->tune_flag_queue_ms;
-  ms[1] = h->tune_aux_queue_ms;
-  ms[2] = h->tune_aux_defer_ms;
+int grb_get_tuning_forms(grb_handle* h, float* ms, int32_t n) {
+  if (!h || !ms || n < 0) return GRB_ERR_INVALID;
+  const float v[5] = {h->tune_flag_queue_ms, h->tune_aux_queue_ms, h->tune_aux_defer_ms, h->tune_flux_queue_ms,
+                      h->tune_update_queue_ms};
+  for (int i = 0; i < n && i < 5; ++i) ms[i] = v[i];
   return GRB_OK;
 }
 
 int grb_set_tuning(grb_handle* h, const int32_t* variant) {
   if (!h || !variant) return GRB_ERR_INVALID;
   for (int f = 0; f < 4; ++f)
-    if (variant[f] < 0 || variant[f] >= (f == 3 ? 3 * kNumVar : f == 1 ? 2 * kNumVar : kNumVar))
+    if (variant[f] < 0 || variant[f] >= (f == 3 ? 3 * kNumVar : 2 * kNumVar))
       return fail(h, GRB_ERR_INVALID);
   if (variant[3] >= 2 * kNumVar) {
     // the deferred-backup aux pass: its list, for the reserved grid

@@ -117,12 +117,44 @@ constexpr int kTmaWaitLimit = 1 << 22;
 
 // Shared memory of one CTA: aux tile and metric tile, each
 // [10 vars][BZ][BY][NX] doubles, the metric tile starting on a 128-byte
-// boundary, then the mbarrier.
+// boundary, then the mbarrier and one more word (the persistent form's
+// current tile).
 __host__ __device__ inline int flux_tile_doubles(const Geo& G, const FluxTile& T) {
   return (10 * T.BY * T.BZ * G.NX + 15) / 16 * 16;
 }
 __host__ __device__ inline size_t flux_tile_smem(const Geo& G, const FluxTile& T) {
   return 2 * sizeof(double) * (size_t)flux_tile_doubles(G, T) + 16;
+}
+
+// The face of this thread in a staged tile (box origin oy, oz of block q):
+// lanes along x, rows along the tile's row axis; threads past the tile's
+// faces do nothing.
+template <int dir>
+__device__ __forceinline__ void flux_tile_face(const DevParams& P, const Geo& G, const FluxTile& T,
+                                               const double* sa, const double* sm, int vs, int oy, int oz,
+                                               int64_t q, const double* __restrict__ bface, const StageBufs& B) {
+  const int W = T.n[0];
+  const int w = threadIdx.x % W, r = threadIdx.x / W;
+  if (r >= T.R) return;
+  const int i = T.lo[0] + w;
+  int j, k, base, st;
+  if (dir == 0) {
+    j = oy + r; k = oz;
+    if (j >= T.lo[1] + T.n[1]) return;
+    base = r * G.NX + i - 3; st = 1;
+  } else if (dir == 1) {
+    j = oy + 3 + r; k = oz;
+    if (j >= T.lo[1] + T.n[1]) return;
+    base = r * G.NX + i; st = G.NX;
+  } else {
+    j = oy; k = oz + 3 + r;
+    if (k >= T.lo[2] + T.n[2]) return;
+    base = r * G.NX + i; st = G.NX;
+  }
+  const int64_t bi = dir == 0 ? bxi(G, i, j, k, q) : dir == 1 ? byi(G, i, j, k, q) : bzi(G, i, j, k, q);
+  double f[7], vb[4];
+  getflux_tile<dir>(P, P.recon, P.riemann == GRB_RIEMANN_LLF, sa + base, sm + base, vs, st, __ldg(bface + bi), f, vb);
+  store_face(G, B, P.emf, dir, i, j, k, q, f, vb);
 }
 
 // grid: (ceil(n_row / R), n_other, nq); NT threads (128 or 256); W = n[0]
@@ -173,28 +205,76 @@ __global__ void __launch_bounds__(NT, MINB) k_flux_tma(DevParams P, Geo G, FluxT
     if (threadIdx.x == 0) atomicOr(B.flags, GRB_FLAG_WAIT_TIMEOUT);
     return;
   }
-  const int W = T.n[0];
-  const int w = threadIdx.x % W, r = threadIdx.x / W;
-  if (r >= T.R) return;
-  const int i = T.lo[0] + w;
-  int j, k, base, st;
-  if (dir == 0) {
-    j = oy + r; k = oz;
-    if (j >= T.lo[1] + T.n[1]) return;
-    base = r * G.NX + i - 3; st = 1;
-  } else if (dir == 1) {
-    j = oy + 3 + r; k = oz;
-    if (j >= T.lo[1] + T.n[1]) return;
-    base = r * G.NX + i; st = G.NX;
-  } else {
-    j = oy; k = oz + 3 + r;
-    if (k >= T.lo[2] + T.n[2]) return;
-    base = r * G.NX + i; st = G.NX;
+  flux_tile_face<dir>(P, G, T, sa, sm, vs, oy, oz, q, bface, B);
+}
+
+// The same as a persistent launch (tuned candidate): one wave of CTAs, each
+// taking tiles, numbered tile row fastest, then the other index, then the
+// block, from the device work queue *queue (zeroed before the launch) until
+// they run out; per tile the same two TMA loads into the same shared
+// memory, the mbarrier's phase alternating from tile to tile.  Every thread
+// reaches every barrier; a wait that gives up sets the flag and ends the
+// CTA.  ntx, nother: tiles along the row axis, indices along the third.
+template <int dir, int MINB, int NT = 128>
+__global__ void __launch_bounds__(NT, MINB) k_flux_tma_queue(DevParams P, Geo G, FluxTile T,
+                                                            const __grid_constant__ CUtensorMap tm_aux,
+                                                            const __grid_constant__ CUtensorMap tm_met,
+                                                            const double* __restrict__ bface, StageBufs B,
+                                                            unsigned long long* __restrict__ queue, int ntx,
+                                                            int nother) {
+  extern __shared__ __align__(128) unsigned char sm_raw[];
+  const int vs = T.BY * T.BZ * G.NX;
+  const int td = flux_tile_doubles(G, T);
+  double* sa = reinterpret_cast<double*>(sm_raw);
+  double* sm = sa + td;
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(sm + td);
+  // the tile taken from the queue, in the second word after the mbarrier
+  unsigned long long& item = *reinterpret_cast<unsigned long long*>(mbar + 1);
+  const uint32_t mb = smem_u32(mbar);
+  // both destinations start on 128-byte boundaries (the same for every
+  // thread, so the CTA leaves as a whole otherwise)
+  if (((smem_u32(sa) | smem_u32(sm)) & 127u) != 0) {
+    if (threadIdx.x == 0) atomicOr(B.flags, GRB_FLAG_WAIT_TIMEOUT);
+    return;
   }
-  const int64_t bi = dir == 0 ? bxi(G, i, j, k, q) : dir == 1 ? byi(G, i, j, k, q) : bzi(G, i, j, k, q);
-  double f[7], vb[4];
-  getflux_tile<dir>(P, P.recon, P.riemann == GRB_RIEMANN_LLF, sa + base, sm + base, vs, st, __ldg(bface + bi), f, vb);
-  store_face(G, B, P.emf, dir, i, j, k, q, f, vb);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  const unsigned long long ntiles = (unsigned long long)ntx * (unsigned long long)nother * (unsigned long long)G.nq;
+  const uint32_t bytes = (uint32_t)(2 * 10 * vs * sizeof(double));
+  uint32_t parity = 0;
+  for (;;) {
+    // every thread is done with the previous tile's shared memory here
+    __syncthreads();
+    if (threadIdx.x == 0) item = atomicAdd(queue, 1ull);
+    __syncthreads();
+    const unsigned long long t = item;
+    if (t >= ntiles) break;
+    const int tile = (int)(t % (unsigned long long)ntx);
+    const unsigned long long rest = t / (unsigned long long)ntx;
+    const int other = (int)(rest % (unsigned long long)nother);
+    const int64_t q = (int64_t)(rest / (unsigned long long)nother);
+    int oy, oz;
+    if (dir == 0) { oy = T.lo[1] + tile * T.R; oz = T.lo[2] + other; }
+    else if (dir == 1) { oy = T.lo[1] + tile * T.R - 3; oz = T.lo[2] + other; }
+    else { oy = T.lo[1] + other; oz = T.lo[2] + tile * T.R - 3; }
+    if (threadIdx.x == 0) {
+      // the async proxy overwrites what the generic proxy just read
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(bytes) : "memory");
+      tma_load5(smem_u32(sa), &tm_aux, 0, oy, oz, 0, (int)q, mb);
+      tma_load5(smem_u32(sm), &tm_met, 0, oy, oz, GRB_GXX, (int)q, mb);
+    }
+    const bool ok = mbar_wait(mb, parity, kTmaWaitLimit);
+    parity ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) atomicOr(B.flags, GRB_FLAG_WAIT_TIMEOUT);
+      return;
+    }
+    flux_tile_face<dir>(P, G, T, sa, sm, vs, oy, oz, q, bface, B);
+  }
 }
 
 }  // namespace grb

@@ -404,6 +404,43 @@ __device__ __forceinline__ double cell_r(const Geo& G, const double* coords, con
 // Cells per work-queue item of the persistent launches: 8 tiles of 128.
 constexpr int kAuxChunk = 8;
 
+// The persistent loop of a one-thread-per-item kernel: the CTA takes chunks
+// of kAuxChunk 128-item tiles of the box from the device work queue *queue
+// (zeroed before the launch) until the box is exhausted, and calls
+// item(i, j, k, q) for each of its items.  Every thread reaches every
+// barrier.
+template <class Item>
+__device__ __forceinline__ void for_queue_items(const Box& box, unsigned long long* queue, Item&& item) {
+  __shared__ unsigned long long chunk;
+  const int64_t ntiles = (box.count() + 127) / 128;
+  for (;;) {
+    if (threadIdx.x == 0) chunk = atomicAdd(queue, (unsigned long long)kAuxChunk);
+    __syncthreads();
+    const int64_t first = (int64_t)chunk;
+    __syncthreads();
+    if (first >= ntiles) break;
+    for (int c = 0; c < kAuxChunk; ++c) {
+      int i, j, k;
+      int64_t q;
+      if (first + c < ntiles && decode(box, (first + c) * 128 + threadIdx.x, i, j, k, q)) item(i, j, k, q);
+    }
+  }
+}
+
+// k_flux as a persistent launch (tuned candidate); per face the same work.
+template <int dir, bool FAST = false, int MINB = 1>
+__global__ void __launch_bounds__(128, MINB) k_flux_queue(DevParams P, Geo G, Box box,
+                                                     const double* __restrict__ st,
+                                                     const double* __restrict__ aux,
+                                                     const double* __restrict__ bface, StageBufs B,
+                                                     unsigned long long* __restrict__ queue) {
+  for_queue_items(box, queue, [&](int i, int j, int k, int64_t q) {
+    double f[7], vb[4];
+    getflux<dir, FAST>(P, G, i, j, k, q, P.recon, P.riemann == GRB_RIEMANN_LLF, st, aux, bface, f, vb);
+    store_face(G, B, P.emf, dir, i, j, k, q, f, vb);
+  });
+}
+
 // flag_fofc_cells (evolve.cpp:456-635) for one cell of [g-1, n+g]^3
 template <bool kFast>
 __device__ __forceinline__ void fofc_flag_cell(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
@@ -688,18 +725,15 @@ __global__ void __launch_bounds__(128) k_metric_derivs(Geo G, Box box, const dou
   for (int c = 0; c < kMetDer; ++c) md[mdi(G, i, j, k, c, q)] = d[c];
 }
 
-// add_fluxes_and_source_terms.  kCached: read the metric derivatives from
-// the static-metric cache md (tuned mode, Cowling) instead of
-// differentiating the metric here.
-template <int MINB = 1, bool kCached = false>
-__global__ void __launch_bounds__(128, MINB) k_update(DevParams P, Geo G, Box box, double dt, double dtfact,
-                                                 double* __restrict__ ns, const double* __restrict__ os,
-                                                 const double* __restrict__ aux,
-                                                 const double* __restrict__ idx, StageBufs B,
-                                                 const double* __restrict__ md = nullptr) {
-  int i, j, k;
-  int64_t q;
-  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+// add_fluxes_and_source_terms for one interior cell.  kCached: the metric
+// derivatives from the static-metric cache md (tuned mode, Cowling) instead
+// of differentiating the metric here.
+template <bool kCached>
+__device__ __forceinline__ void update_cell(const DevParams& P, const Geo& G, int i, int j, int k, int64_t q,
+                                            double dt, double dtfact, double* __restrict__ ns,
+                                            const double* __restrict__ os, const double* __restrict__ aux,
+                                            const double* __restrict__ idx, const StageBufs& B,
+                                            const double* __restrict__ md) {
   const double ix[3] = {idx[3 * q], idx[3 * q + 1], idx[3 * q + 2]};
   const Met m = cell_met(G, os, i, j, k, q);
   const int64_t a0 = cvar(G, i, j, k, 0, GRB_N_AUX_VARS, q);
@@ -734,6 +768,32 @@ __global__ void __launch_bounds__(128, MINB) k_update(DevParams P, Geo G, Box bo
     const double dFz = (F[flx(G, i, j, k, v, 2, q)] - F[flx(G, i, j, k + 1, v, 2, q)]) * ix[2];
     *p = u + dt * dtfact * ((dFx + dFy) + dFz);
   }
+}
+
+template <int MINB = 1, bool kCached = false>
+__global__ void __launch_bounds__(128, MINB) k_update(DevParams P, Geo G, Box box, double dt, double dtfact,
+                                                 double* __restrict__ ns, const double* __restrict__ os,
+                                                 const double* __restrict__ aux,
+                                                 const double* __restrict__ idx, StageBufs B,
+                                                 const double* __restrict__ md = nullptr) {
+  int i, j, k;
+  int64_t q;
+  if (!decode(box, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, i, j, k, q)) return;
+  update_cell<kCached>(P, G, i, j, k, q, dt, dtfact, ns, os, aux, idx, B, md);
+}
+
+// k_update as a persistent launch (tuned candidate); per cell the same work.
+template <int MINB = 1, bool kCached = false>
+__global__ void __launch_bounds__(128, MINB) k_update_queue(DevParams P, Geo G, Box box, double dt,
+                                                       double dtfact, double* __restrict__ ns,
+                                                       const double* __restrict__ os,
+                                                       const double* __restrict__ aux,
+                                                       const double* __restrict__ idx, StageBufs B,
+                                                       const double* __restrict__ md,
+                                                       unsigned long long* __restrict__ queue) {
+  for_queue_items(box, queue, [&](int i, int j, int k, int64_t q) {
+    update_cell<kCached>(P, G, i, j, k, q, dt, dtfact, ns, os, aux, idx, B, md);
+  });
 }
 
 // update_CT on faces [g, n+g] (+1 on the face's own axis)

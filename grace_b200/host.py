@@ -446,17 +446,19 @@ class GRMHDEquationsSystem:
         fam = ["flux", "fofc_flag", "update", "aux"]
         out = {f: {"min_ctas_per_sm": v[i], "ms": [round(ms[3 * i + k], 4) for k in range(3)]}
                for i, f in enumerate(fam)}
-        forms = (ctypes.c_float * 3)()
-        _lib.check(self.lib.grb_get_tuning_forms(self.h, forms), "grb_get_tuning_forms")
+        forms = (ctypes.c_float * 5)()
+        _lib.check(self.lib.grb_get_tuning_forms(self.h, forms, 5), "grb_get_tuning_forms")
         r = lambda x: round(x, 4) if x < 1e29 else None
         out["fofc_flag"]["queue_ms"] = r(forms[0])
         out["aux"]["queue_ms"] = r(forms[1])
         out["aux"]["deferred_ms"] = r(forms[2])
+        out["flux"]["queue_ms"] = r(forms[3])
+        out["update"]["queue_ms"] = r(forms[4])
         return out
 
     def set_tuning(self, flux=0, flag=0, update=0, aux=0):
         """Pick tuned-mode candidates without timing (grb_set_tuning: indices
-        0..2; flag and aux 3..5 the work-queue forms; aux 6..8 the
+        0..2 grid launches, 3..5 their work-queue forms; aux 6..8 the
         deferred-backup form)."""
         v = (ctypes.c_int32 * 4)(flux, flag, update, aux)
         _lib.check(self.lib.grb_set_tuning(self.h, v), "grb_set_tuning")

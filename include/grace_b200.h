@@ -408,25 +408,27 @@ int grb_set_mode(grb_handle* h, int32_t mode);
 int grb_autotune(grb_handle* h, const grb_grid* g, const grb_fields* new_state,
                  const grb_fields* old_state, const double* aux, void* stream);
 /* variant[4]: chosen minimum-CTAs-per-SM of flux, flag, update, aux (flux:
- * plus 100 when the TMA-staged shared-memory kernel was chosen; update: of
- * the kernel that reads the static-metric cache when one is set; flag and
- * aux: plus 100 for the work-queue form; aux: plus 200 for the
- * deferred-backup form); ms[12] (or NULL): timed milliseconds of the 3
- * one-thread-per-item candidates per family. */
+ * plus 100 when the TMA-staged shared-memory kernel was chosen, plus 1000
+ * for its work-queue form; update: of the kernel that reads the
+ * static-metric cache when one is set; flag, update and aux: plus 100 for
+ * the work-queue form; aux: plus 200 for the deferred-backup form); ms[12]
+ * (or NULL): timed milliseconds of the 3 grid-launched candidates per
+ * family. */
 int grb_get_tuning(grb_handle* h, int32_t* variant, float* ms);
-/* ms[3]: milliseconds grb_autotune timed for the other launch forms at the
- * register cap it chose: the work-queue FOFC flag, the work-queue aux pass,
- * the deferred-backup aux pass (0 before autotuning; 1e30 for a form that
- * could not be set up). */
-int grb_get_tuning_forms(grb_handle* h, float* ms);
+/* ms[n] (n <= 5 written): milliseconds grb_autotune timed for the other
+ * launch forms of the candidate it chose in each family: the work-queue
+ * FOFC flag, the work-queue aux pass, the deferred-backup aux pass, the
+ * work-queue flux (x faces), the work-queue update (0 before autotuning;
+ * 1e30 for a form that could not be set up). */
+int grb_get_tuning_forms(grb_handle* h, float* ms, int32_t n);
 /* Choose the tuned-mode candidates without timing: variant[4] = candidate
- * index 0..2 of flux, flag, update, aux (flux: 0 global-load kernel, 1 the
+ * index of flux, flag, update, aux: 0..2 grid launches (flux: 0 global-load kernel, 1 the
  * TMA-staged kernel with 128-thread tiles at 4 CTAs/SM, 2 with 256-thread
  * tiles (twice the face rows per tile) at 2 CTAs/SM; update: 1, 4, 5
  * CTAs/SM (1, 3, 4 for the kernel that reads the static-metric cache);
- * flag and aux: 3, 4, 5 CTAs/SM; flag and aux also
- * 3..5: the work-queue form — one wave of CTAs pulling chunks of 128-cell
- * tiles from a device counter — at 3, 4, 5 CTAs/SM; aux also 6..8: the
+ * flag and aux: 3, 4, 5 CTAs/SM); 3..5 the work-queue form of candidate
+ * 0..2 — one wave of persistent CTAs pulling tiles (128 items, or the TMA
+ * flux kernel's tiles) from a device counter; aux also 6..8: the
  * deferred-backup form — the cells whose Kastaun result is distrusted
  * listed and finished by a second kernel running their entropy backups
  * together — at 3, 4, 5 CTAs/SM, its list allocated here for the reserved

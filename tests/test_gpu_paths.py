@@ -108,8 +108,10 @@ def _check_aux(ga, oa, sel):
 # tuned candidates: the autotuner's pick; global-load flux at 4 CTAs/SM with
 # the others at 4; 256-thread TMA flux tiles with the work-queue aux pass;
 # the work-queue FOFC flag with the deferred-backup aux pass, and with the
-# work-queue aux pass
-@pytest.mark.parametrize("tuning", [None, (0, 1, 1, 1), (2, 2, 2, 4), (1, 4, 1, 7), (1, 3, 1, 3)])
+# work-queue aux pass; the work-queue forms of the flux (TMA 128 and 256,
+# global loads) and of the update
+@pytest.mark.parametrize("tuning", [None, (0, 1, 1, 1), (2, 2, 2, 4), (1, 4, 1, 7), (1, 3, 1, 3), (4, 1, 4, 1),
+                                    (5, 4, 3, 4), (3, 1, 5, 1)])
 def test_benchmark_configuration_matches_oracle(tuning):
     """One SSP-RK3 step of the benchmark's exact code path (16^3 blocks,
     tuned, static-metric cache, next-stage ranges, FOFC list) against the
@@ -126,10 +128,12 @@ def test_benchmark_configuration_matches_oracle(tuning):
     assert (st.fofc_faces, st.fofc_edges) == counts
     assert st.device_flags == 0
     if tuning is None:
-        # the autotuner picked one of the TMA-staged or global-load flux kernels
-        assert g.tuning()["flux"]["min_ctas_per_sm"] in (4, 104, 102)
+        # the autotuner picked one of the flux candidates
+        assert g.tuning()["flux"]["min_ctas_per_sm"] in (4, 104, 102, 1004, 1104, 1102)
     else:
         t = g.tuning()
+        assert t["flux"]["min_ctas_per_sm"] == [4, 104, 102, 1004, 1104, 1102][tuning[0]]
+        assert t["update"]["min_ctas_per_sm"] == [1, 3, 4, 101, 103, 104][tuning[2]]
         assert t["fofc_flag"]["min_ctas_per_sm"] == [3, 4, 5, 103, 104, 105][tuning[1]]
         assert t["aux"]["min_ctas_per_sm"] == [3, 4, 5, 103, 104, 105, 203, 204, 205][tuning[3]]
 
