@@ -470,7 +470,7 @@ def ours(args, rank, world, local_rank):
     if not args.no_e2e:
         host = g.packed_host_fields()
         g.copy_evolved_packed(host, state, to_device=False)
-        ksteps = max(1, min(args.steps, 10))
+        ksteps = max(1, min(args.steps, 20))
         torch.cuda.synchronize()
         barrier()
         f0 = torch.cuda.Event(enable_timing=True)
