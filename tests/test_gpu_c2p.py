@@ -45,6 +45,27 @@ def test_c2p_batch_matches_oracle(preset, mode):
     assert np.mean(rho_rel < PRIM_TOL) > 0.95
 
 
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_c2p_without_entropy_backup_matches_oracle(mode):
+    """use_ent_backup = 0 (grmhd.c2p.use_entropy_backup off): the states whose
+    Kastaun result is distrusted keep it instead of the entropy-based solve
+    (the tuned mode's deferred second pass then has nothing to do), against
+    the oracle with the same switch."""
+    P = params.c2p_bench()
+    P.use_ent_backup = 0
+    cons, _ = workloads.c2p_states(50000, seed=12)
+    pr_g, co_g, err_g, pr_o, co_o, err_o = _compare(P, cons, mode=mode)
+    assert (err_g == err_o).mean() > 0.999
+    same = err_g == err_o
+    res = state_residual(pr_g[:, same], pr_o[:, same])
+    assert np.all(res < prim_tol(pr_o)[same]), res.max()
+    # the switch matters on this workload: with the backup on, a fifth of the
+    # states (the magnetically dominated ones) come out of the other solve,
+    # different beyond 1e-12
+    pr_b = _oracle.c2p_batch(params.c2p_bench(), cons)[0]
+    assert np.mean(state_residual(pr_b, pr_o) > 1e-12) > 0.1
+
+
 def test_c2p_curved_metric_matches_oracle():
     """Schwarzschild in Cartesian Kerr-Schild at R=4 (the curved-metric sweep
     of test/test_c2p.cpp:359-455): primitives -> cons on that metric -> c2p."""
