@@ -66,6 +66,28 @@ def test_c2p_without_entropy_backup_matches_oracle(mode):
     assert np.mean(state_residual(pr_b, pr_o) > 1e-12) > 0.1
 
 
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_c2p_velocity_limit_matches_oracle(mode):
+    """max_w = 10 (grmhd.c2p.max_lorentz_factor): limit_primitives rescales
+    the velocity of the 80 % of the workload's states that would move
+    faster (c2p.cpp:63-115), flagged in the error bits; against the oracle
+    with the same limit."""
+    P = params.c2p_bench()
+    P.max_w = 10.0
+    cons, _ = workloads.c2p_states(50000, seed=13)
+    pr_g, co_g, err_g, pr_o, co_o, err_o = _compare(P, cons, mode=mode)
+    assert (err_g == err_o).mean() > 0.999
+    same = err_g == err_o
+    # the limiter rescales the solved state, so the solver's window is that
+    # of the unlimited state: the W^2-aware bound of the unlimited solve
+    pr_u, _, err_u, _, _, _ = _oracle.c2p_batch(params.c2p_bench(), cons)
+    res = state_residual(pr_g[:, same], pr_o[:, same])
+    assert np.all(res < prim_tol(pr_u)[same]), res.max()
+    W = np.sqrt(1.0 + np.sum(pr_g[abi.P_ZX:abi.P_ZZ + 1] ** 2, axis=0))
+    assert W.max() < 10.0
+    assert np.mean(err_o != err_u) > 0.5
+
+
 def test_c2p_curved_metric_matches_oracle():
     """Schwarzschild in Cartesian Kerr-Schild at R=4 (the curved-metric sweep
     of test/test_c2p.cpp:359-455): primitives -> cons on that metric -> c2p."""
