@@ -88,6 +88,31 @@ def test_c2p_velocity_limit_matches_oracle(mode):
     assert np.mean(err_o != err_u) > 0.5
 
 
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+@pytest.mark.parametrize("knob", ["temp_fl", "eps_max"])
+def test_c2p_floors_and_ceilings_match_oracle(knob, mode):
+    """The temperature floor (grmhd.atmosphere.temp_fl: the floored states'
+    temperature reset and pressure recomputed, c2p.cpp:356-370) and the eps
+    ceiling (eos.eps_maximum: the Kastaun result distrusted above it,
+    c2p.cpp:303, and the upper eps bound of the EOS range) set where they act
+    on about 30 % of the workload's states, against the oracle with the same
+    setting."""
+    cons, _ = workloads.c2p_states(50000, seed=14)
+    base = _oracle.c2p_batch(params.c2p_bench(), cons)
+    P = params.c2p_bench()
+    if knob == "temp_fl":
+        P.temp_fl = float(np.quantile(base[0][abi.P_TEMP], 0.3))
+    else:
+        P.eos.eps_max = float(np.quantile(base[0][abi.P_EPS], 0.7))
+    pr_g, co_g, err_g, pr_o, co_o, err_o = _compare(P, cons, mode=mode)
+    assert np.mean(err_o != base[2]) > 0.2  # the knob acts
+    assert (err_g == err_o).mean() > 0.999
+    same = err_g == err_o
+    res = state_residual(pr_g[:, same], pr_o[:, same])
+    assert np.all(res < prim_tol(base[0])[same]), res.max()
+    assert np.all(np.isfinite(pr_g[:12]))
+
+
 def test_c2p_curved_metric_matches_oracle():
     """Schwarzschild in Cartesian Kerr-Schild at R=4 (the curved-metric sweep
     of test/test_c2p.cpp:359-455): primitives -> cons on that metric -> c2p."""
