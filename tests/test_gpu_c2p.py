@@ -93,8 +93,9 @@ def test_c2p_velocity_limit_matches_oracle(mode):
 def test_c2p_floors_and_ceilings_match_oracle(knob, mode):
     """The temperature floor (grmhd.atmosphere.temp_fl: the floored states'
     temperature reset and pressure recomputed, c2p.cpp:356-370) and the eps
-    ceiling (eos.eps_maximum: the Kastaun result distrusted above it,
-    c2p.cpp:303, and the upper eps bound of the EOS range) set where they act
+    ceiling (eos.eps_maximum: the upper eps bound of the EOS range that
+    limit_conservatives and the solves use, and the entropy backup's result
+    accepted only below it, c2p.cpp:303) set where they act
     on about 30 % of the workload's states, against the oracle with the same
     setting."""
     cons, _ = workloads.c2p_states(50000, seed=14)
