@@ -174,6 +174,25 @@ def test_llf_stage_matches_oracle(c_limit, mode):
 
 
 @pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+@pytest.mark.parametrize("recon", [abi.RECON_WENOZ, abi.RECON_MC2])
+def test_llf_with_uct_matches_oracle(recon, mode):
+    """The LLF solver under the UCT EMF, whose edge EMFs take the Riemann
+    speeds of the faces around each edge (evolve.cpp:1131-1340): Balsara-1
+    on a 4x1x1 brick of 8^3 blocks, WENO-Z and MC2, one SSP-RK3 step
+    against the oracle."""
+    P = params.balsara1()
+    P.riemann = abi.RIEMANN_LLF
+    P.recon = recon
+    su, f = workloads.balsara1(nb=(4, 1, 1), n=(8, 8, 8))
+    dt = 0.4 / su.idx()[0, 0]
+    gs, ga, g = _gpu(P, su, f, dt, 1, mode, tuning=(1, 1, 1, 1))
+    os_, oa, counts = _oracle_run(P, su, f, dt, 1)
+    _check_state(gs, os_, su.ngz)
+    _check_aux(ga, oa, (slice(None),))
+    assert g.status().device_flags == 0
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
 def test_pwpoly_three_pieces_c2p_matches_oracle(mode):
     """c2p with a three-piece cold polytrope (non-integer indices: pow) on
     states whose densities span all three pieces."""
