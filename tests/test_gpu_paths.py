@@ -6,7 +6,8 @@ the CPU oracle through the C ABI:
   the next stage's cells, the static-metric cache, the TMA-staged flux
   tiles, the per-block aux cell list and the compacted FOFC face list;
 * the LLF (Rusanov) Riemann solver of the stage, with and without the
-  light-cone floor rusanov_use_c_limit (grmhd.hh:855-883);
+  light-cone floor rusanov_use_c_limit (grmhd.hh:855-883), and under the
+  UCT EMF;
 * the compacted FOFC list's overflow path (more tagged faces than the list
   holds: the whole-box recompute);
 * a three-piece piecewise-polytropic cold EOS through the c2p and the stage;
