@@ -154,6 +154,9 @@ PROTOTYPES = {
     "grb_linop_apply": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields),
                                   C.POINTER(Fields), C.POINTER(Fields), C.c_double,
                                   C.c_double, C.c_void_p]),
+    "grb_linop_apply3": (C.c_int, [C.c_void_p, C.POINTER(Grid), C.POINTER(Fields),
+                                   C.POINTER(Fields), C.POINTER(Fields), C.POINTER(Fields),
+                                   C.c_double, C.c_double, C.c_double, C.c_void_p]),
     "grb_c2p_batch": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
                                 C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]),
     "grb_c2p_batch_diag": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,

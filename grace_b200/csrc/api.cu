@@ -1183,6 +1183,30 @@ int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A, const
   return GRB_OK;
 }
 
+int grb_linop_apply3(grb_handle* h, const grb_grid* g, const grb_fields* A, const grb_fields* Bf,
+                     const grb_fields* Cf, const grb_fields* Df, double b, double c, double d, void* stream) {
+  if (!h) return GRB_ERR_INVALID;
+  if (!g || g->nq < 1 || g->nx < 1 || g->ny < 1 || g->nz < 1 || g->ngz < 0) return fail(h, GRB_ERR_INVALID);
+  const grb_fields* f[4] = {A, Bf, Cf, Df};
+  for (const grb_fields* x : f)
+    if (!x || !x->state || !x->bx || !x->by || !x->bz) return fail(h, GRB_ERR_INVALID);
+  const Geo G = make_geo(g->nx, g->ny, g->nz, g->ngz, g->nq);
+  cudaStream_t s = (cudaStream_t)stream;
+  const int64_t n[4] = {G.cells * GRB_N_EVOL_VARS * G.nq, (int64_t)(G.NX + 1) * G.NY * G.NZ * G.nq,
+                        (int64_t)G.NX * (G.NY + 1) * G.NZ * G.nq, (int64_t)G.NX * G.NY * (G.NZ + 1) * G.nq};
+  double* a[4] = {A->state, A->bx, A->by, A->bz};
+  const double* x[4] = {Bf->state, Bf->bx, Bf->by, Bf->bz};
+  const double* y[4] = {Cf->state, Cf->bx, Cf->by, Cf->bz};
+  const double* z[4] = {Df->state, Df->bx, Df->by, Df->bz};
+  KScope ks(h, s, GRB_KIND_LINOP);
+  for (int v = 0; v < 4; ++v) {
+    k_linop3<<<148 * 16, 256, 0, s>>>(n[v], a[v], x[v], y[v], z[v], b, c, d);
+    ++h->launches;
+  }
+  CK(cudaGetLastError());
+  return GRB_OK;
+}
+
 }  // extern "C"
 
 namespace {

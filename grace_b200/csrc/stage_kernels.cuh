@@ -1156,6 +1156,14 @@ __global__ void k_linop(int64_t n, double* __restrict__ a, const double* __restr
   for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
     a[t] = y ? b * x[t] + c * y[t] : b * x[t];
 }
+// the three-term linop_apply: a = b*x + c*y + d*z elementwise, the sums
+// left to right.  a may be any of x, y, z (each element is read before it
+// is written by the same thread).
+__global__ void k_linop3(int64_t n, double* a, const double* x, const double* y, const double* z, double b,
+                         double c, double d) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x)
+    a[t] = b * x[t] + c * y[t] + d * z[t];
+}
 
 
 // ---- ghost fill for a brick of same-level blocks ---------------------------

@@ -214,6 +214,14 @@ class GRMHDEquationsSystem:
                                             ctypes.byref(fc) if fc is not None else None, b, c,
                                             _stream_ptr(stream)), "grb_linop_apply")
 
+    def linop_apply3(self, A, B, C, D, b, c, d, stream=None):
+        """The three-term linop_apply (tstep_utils.hh:231-311): A = b B + c C +
+        d D on every cell and face (grb_linop_apply3)."""
+        g = self.blocks.c()
+        f = [x.c() for x in (A, B, C, D)]
+        _lib.check(self.lib.grb_linop_apply3(self.h, ctypes.byref(g), *[ctypes.byref(x) for x in f], b, c, d,
+                                             _stream_ptr(stream)), "grb_linop_apply3")
+
     def fill_ghosts_brick(self, fields, nb, periodic, stream=None, blocks=None):
         """Ghost fill of a brick of same-level blocks (grb_fill_ghosts_brick);
         blocks = (q0, q1): only the ghost zones of those blocks

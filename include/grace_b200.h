@@ -284,6 +284,14 @@ int grb_reset_c2p_diagnostics(grb_handle* h, const grb_grid* g, double* aux,
 int grb_linop_apply(grb_handle* h, const grb_grid* g, const grb_fields* A,
                     const grb_fields* B, const grb_fields* C, double b,
                     double c, void* stream);
+/* = the three-term grace::linop_apply (include/grace/utils/tstep_utils.hh:
+ *   231-311), which the reference's other time integrators use:
+ *   A = b*B + c*C + d*D on every cell of all 23 variables and every face,
+ *   whatever the mode and params.ranges.  A may be the same arrays as B, C
+ *   or D. */
+int grb_linop_apply3(grb_handle* h, const grb_grid* g, const grb_fields* A, const grb_fields* B,
+                     const grb_fields* C, const grb_fields* D, double b, double c, double d,
+                     void* stream);
 /* Batched c2p on n independent states (the unit of the c2p micro-benchmark):
  *   cons   [GRB_NUM_CONS][n] densitized conserved incl. cell-centred B*sqrtg
  *   metric [10][n] gxx,gxy,gxz,gyy,gyz,gzz,betax,betay,betaz,alp, or NULL
