@@ -565,6 +565,71 @@ class GRMHDEquationsSystem:
                 self.find_stable_timestep(state, aux, *next_dt, stream=stream)
         self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
 
+    # --- the other explicit branches of evolve_impl (evolve.cpp:173-332) ---
+    # Same entry condition as rk3_step (aux holds the primitives of state,
+    # state_p equals state: GRACE copies it at the start of every step,
+    # evolve.cpp:147) and the same exit (state_p set to the new state).
+
+    def euler_step(self, dt, state, state_p, aux, bc, t=0.0, stream=None):
+        """Forward Euler (evolve.cpp:173-178): state += dt L(state_p)."""
+        self.reset_c2p_diagnostics(aux, stream)
+        self.advance_substep(t, dt, 1.0, state, state_p, aux, stream)
+        bc(state)
+        self.compute_auxiliary_quantities(state, aux, stream)
+        self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
+
+    def rk2_step(self, dt, state, state_p, aux, bc, t=0.0, stream=None):
+        """Midpoint RK2 (evolve.cpp:179-189): state_p += dt/2 L(state), then
+        state += dt L(state_p)."""
+        self.reset_c2p_diagnostics(aux, stream)
+        self.advance_substep(t, dt, 0.5, state_p, state, aux, stream)
+        bc(state_p)
+        self.compute_auxiliary_quantities(state_p, aux, stream)
+        self.advance_substep(t, dt, 1.0, state, state_p, aux, stream)
+        bc(state)
+        self.compute_auxiliary_quantities(state, aux, stream)
+        self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
+
+    # four-stage low-storage coefficients (delta, gamma1, gamma2, beta) of the
+    # reference's rk4 branch, stage by stage (evolve.cpp:226-332)
+    RK4_COEFFS = ((1.0, 0.0, 1.0, 1.193743905974738),
+                  (0.217683334308543, 0.121098479554482, 0.721781678111411, 0.099279895495783),
+                  (1.065841341361089, -3.843833699660025, 2.121209265338722, 1.131678018054042),
+                  (0.0, 0.546370891121863, 0.198653035682705, 0.310665766509336))
+
+    def rk4_step(self, dt, state, state_p, stage, aux, bc, t=0.0, stream=None):
+        """The rk4 branch of evolve_impl (evolve.cpp:226-332): four stages of
+        a low-storage scheme over state (s1), state_p (s2) and a staging
+        buffer `stage` (s3, any Fields of the same shape holding the static
+        metric), each a two-term linop_apply or two, advance_substep with
+        dtfact = beta, the boundary fill and the primitives pass."""
+        s1, s2, s3 = state, state_p, stage
+        (d1, g11, g21, b1), (d2, g12, g22, b2), (d3, g13, g23, b3), (d4, g14, g24, b4) = self.RK4_COEFFS
+        self.reset_c2p_diagnostics(aux, stream)
+        # stage 1: s3 = gamma1 s1 + gamma2 s2; s3 += beta dt F(s1)
+        self.linop_apply(s3, s1, s2, g11, g21, stream)
+        self.advance_substep(t, dt, b1, s3, s1, aux, stream)
+        bc(s3)
+        self.compute_auxiliary_quantities(s3, aux, stream)
+        # stage 2: s2 += delta s3; s1 = gamma1 s3 + gamma2 s2; s1 += beta dt F(s3)
+        self.linop_apply(s2, s2, s3, 1.0, d2, stream)
+        self.linop_apply(s1, s3, s2, g12, g22, stream)
+        self.advance_substep(t, dt, b2, s1, s3, aux, stream)
+        bc(s1)
+        self.compute_auxiliary_quantities(s1, aux, stream)
+        # stage 3: s2 += delta s1; s3 = gamma1 s1 + gamma2 s2; s3 += beta dt F(s1)
+        self.linop_apply(s2, s2, s1, 1.0, d3, stream)
+        self.linop_apply(s3, s1, s2, g13, g23, stream)
+        self.advance_substep(t, dt, b3, s3, s1, aux, stream)
+        bc(s3)
+        self.compute_auxiliary_quantities(s3, aux, stream)
+        # stage 4 (delta = 0: no s2 update): s1 = gamma1 s3 + gamma2 s2; s1 += beta dt F(s3)
+        self.linop_apply(s1, s3, s2, g14, g24, stream)
+        self.advance_substep(t, dt, b4, s1, s3, aux, stream)
+        bc(s1)
+        self.compute_auxiliary_quantities(s1, aux, stream)
+        self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
+
     def rk3_step_host(self, dt, host, state, state_p, state_pp, aux, bc, runs, fill_run, deps, t=0.0,
                       streams=None, after=None, wait=True):
         """One SSP-RK3 step of a state held in packed pinned host arrays
