@@ -51,3 +51,28 @@ def test_brick_runs_cover_the_brick_and_name_every_neighbour():
                     cc.append(x)
                 src = cc[0] + nb[0] * (cc[1] + nb[1] * cc[2])
                 assert run_of[src] in deps[run_of[q]], (nb, per, q, o)
+
+
+def test_rk4_coefficients_are_fourth_order():
+    """The rk4 branch's low-storage coefficients (as rk4_step applies them)
+    integrate y' = -y with a local error shrinking as h^5: halving the step
+    divides it by ~32."""
+    from grace_b200.host import GRMHDEquationsSystem as G
+
+    def step(y, h, lam=-1.0):
+        (_, g11, g21, b1), (d2, g12, g22, b2), (d3, g13, g23, b3), (_, g14, g24, b4) = G.RK4_COEFFS
+        s1 = s2 = y
+        s3 = g11 * s1 + g21 * s2
+        s3 = s3 + b1 * h * lam * s1
+        s2 = s2 + d2 * s3
+        s1 = g12 * s3 + g22 * s2
+        s1 = s1 + b2 * h * lam * s3
+        s2 = s2 + d3 * s1
+        s3 = g13 * s1 + g23 * s2
+        s3 = s3 + b3 * h * lam * s1
+        s1 = g14 * s3 + g24 * s2
+        return s1 + b4 * h * lam * s3
+
+    e1 = abs(step(1.0, 0.1) - np.exp(-0.1))
+    e2 = abs(step(1.0, 0.05) - np.exp(-0.05))
+    assert 25.0 < e1 / e2 < 40.0, (e1, e2)
