@@ -823,7 +823,7 @@ def c2p_bench(dev, learned=True, n=1 << 24, reps=5, states=None, P=None):
         gc.set_mode(abi.MODE_PLAIN)
         out["training"] = {k: rep[k] for k in ("states", "labelled", "loss_first", "loss_last", "err_q50",
                                                "err_q90", "err_q99",
-                                               "err_q999", "err_max", "delta", "delta_cand", "calib_ms",
+                                               "err_q999", "err_max", "delta", "delta_cand", "calib_ms", "calib_cost",
                                                "train_ms")}
         out["learned_speedup"] = out["learned_solves_per_s"] / out["plain_solves_per_s"]
         out["learned_tuned_speedup"] = out["learned_tuned_solves_per_s"] / out["plain_solves_per_s"]

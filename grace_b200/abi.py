@@ -124,7 +124,7 @@ class TrainReport(C.Structure):
                 ("loss_last", C.c_float), ("err_q50", C.c_float), ("err_q90", C.c_float),
                 ("err_q99", C.c_float), ("err_q999", C.c_float),
                 ("err_max", C.c_float), ("delta", C.c_float), ("delta_cand", C.c_float * 4),
-                ("calib_ms", C.c_float * 4), ("train_ms", C.c_double)]
+                ("calib_ms", C.c_float * 4), ("train_ms", C.c_double), ("calib_cost", C.c_float * 4)]
 
 
 # Every extern "C" symbol declared in include/grace_b200.h, with its

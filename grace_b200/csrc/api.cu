@@ -1541,15 +1541,35 @@ int grb_c2p_train(grb_handle* h, int64_t n, const double* cons, const double* me
   const float q9999 = quant(0.9999);
   R.err_max = *std::max_element(err.begin(), err.end());
   const float cand[4] = {1.2f * R.err_q90, 1.2f * R.err_q99, 1.2f * R.err_q999, 1.2f * q9999};
-  // 5. autotune delta: time the learned c2p on the calibration states
+  // 5. choose delta on the calibration states by the learned c2p's cost in
+  // Brent iterations as warps see it (deterministic), and time each choice
   h->mlp_ready = true;
   const int64_t nc = std::min<int64_t>(n, C.calib_states > 0 ? C.calib_states : n);
+  DevBuf its, used;
+  CK(cudaMalloc(&its.p, sizeof(int32_t) * (size_t)nc));
+  CK(cudaMalloc(&used.p, sizeof(int8_t) * (size_t)nc));
+  std::vector<int32_t> hits((size_t)nc);
+  std::vector<int8_t> hused((size_t)nc);
   int best = 0;
   for (int ci = 0; ci < 4; ++ci) {
     const float dlt = std::max(cand[ci], 1e-6f);
     R.delta_cand[ci] = dlt;
     CK(cudaMemcpyAsync(h->d_mlp + kMlpOffNorm + 2 * kMlpIn + 2, &dlt, sizeof(float), cudaMemcpyHostToDevice, s));
     if (int rc = pack_mlp(h, s)) return rc;
+    grb_c2p_diag cd{its.as<int32_t>(), used.as<int8_t>(), nullptr, nullptr};
+    if (int rc = launch_c2p(h, nc, cons, metric, prims.as<double>(), nullptr, nullptr, true, &cd, s)) return rc;
+    CK(cudaMemcpyAsync(hits.data(), its.p, sizeof(int32_t) * (size_t)nc, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hused.data(), used.p, sizeof(int8_t) * (size_t)nc, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    double cost = 0.0;
+    int64_t warps = 0;
+    for (int64_t w0 = 0; w0 < nc; w0 += 32, ++warps) {
+      int32_t m = 0;
+      for (int64_t t = w0; t < std::min<int64_t>(nc, w0 + 32); ++t)
+        m = std::max<int32_t>(m, hits[(size_t)t] + (hused[(size_t)t] ? 0 : 1));
+      cost += m;
+    }
+    R.calib_cost[ci] = (float)(cost / (double)std::max<int64_t>(warps, 1));
     float bestms = 1e30f;
     for (int rep_i = 0; rep_i < 3; ++rep_i) {
       CK(cudaEventRecord(e0, s));
@@ -1561,7 +1581,7 @@ int grb_c2p_train(grb_handle* h, int64_t n, const double* cons, const double* me
       bestms = std::min(bestms, ms);
     }
     R.calib_ms[ci] = bestms;
-    if (bestms < R.calib_ms[best] || ci == 0) best = ci;
+    if (R.calib_cost[ci] < R.calib_cost[best]) best = ci;
   }
   R.delta = R.delta_cand[best];
   CK(cudaMemcpyAsync(h->d_mlp + kMlpOffNorm + 2 * kMlpIn + 2, &R.delta, sizeof(float), cudaMemcpyHostToDevice, s));

@@ -397,6 +397,7 @@ class GRMHDEquationsSystem:
         out = {k: getattr(r, k) for k, _ in abi.TrainReport._fields_}
         out["delta_cand"] = list(r.delta_cand)
         out["calib_ms"] = list(r.calib_ms)
+        out["calib_cost"] = list(r.calib_cost)
         return out
 
     def c2p_model(self):

@@ -364,13 +364,18 @@ typedef struct grb_train_report {
   float delta_cand[4];  /* candidates: 1.2 x the q90, q99, q999, q9999 errors */
   float calib_ms[4];    /* learned c2p time on the calibration states */
   double train_ms;      /* device time: labels + statistics + Adam steps */
+  float calib_cost[4];  /* the choice's cost: mean over warps of the largest
+                           per-state Brent iterations (+1 where the learned
+                           bracket missed the root) */
 } grb_train_report;
 void grb_train_config_defaults(grb_train_config* c);
 /* Train the bracket network on the GPU from n states (cons/metric as for
  * grb_c2p_batch): labels are the roots of the plain FP64 c2p of the same
  * states; the tensor-core forward, the FP32 backward and Adam run as this
  * library's kernels; delta is then chosen among four quantiles of the
- * prediction error by timing the learned c2p.  Synchronises the stream. */
+ * prediction error by the learned c2p's warp-level Brent cost on the
+ * calibration states (a count, so the same training gives the same model
+ * every run; the times are reported beside it).  Synchronises the stream. */
 int grb_c2p_train(grb_handle* h, int64_t n, const double* cons,
                   const double* metric, const grb_train_config* cfg,
                   grb_train_report* report, void* stream);

@@ -153,3 +153,20 @@ def test_model_roundtrip(trained):
     bad[abi.MLP_NUM_WEIGHTS] = np.nan
     with pytest.raises(RuntimeError):
         s2.set_c2p_model(bad)
+
+
+def test_training_is_reproducible():
+    """Two trainings on the same states with the same settings give the
+    same model bit for bit, delta included: the gradients are summed in a
+    fixed order and delta is chosen by a Brent-iteration count, not by
+    timing (the calibration times are reported beside the counts)."""
+    cons, _ = workloads.c2p_states(1 << 16, seed=9)
+    models = []
+    for _ in range(2):
+        s = GRMHDEquationsSystem(params.c2p_bench())
+        rep = s.train_c2p_model(dev(cons), steps=500, calib_states=1 << 14)
+        models.append((s.c2p_model(), rep["delta"], rep["calib_cost"]))
+        s.close()
+    np.testing.assert_array_equal(models[0][0], models[1][0])
+    assert models[0][1] == models[1][1]
+    assert models[0][2] == models[1][2] and min(models[0][2]) > 0
