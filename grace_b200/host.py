@@ -140,6 +140,36 @@ def brick_runs(nb, periodic, nruns):
     return runs, deps
 
 
+def gather_runs(maps, blocks, nruns):
+    """Runs of blocks for rk3_step_host on a hierarchy filled by gather maps
+    (grace_b200.fmr.Hierarchy.gather_maps): nruns consecutive runs of about
+    nq / nruns blocks; for each run the part of the maps whose destinations
+    lie in its blocks, and the runs whose blocks those entries read (the
+    run itself included).  Returns (runs, run_maps, deps)."""
+    nq = blocks.nq
+    nruns = max(1, min(int(nruns), nq))
+    cuts = [round(r * nq / nruns) for r in range(nruns + 1)]
+    runs = [(cuts[r], cuts[r + 1]) for r in range(nruns)]
+    run_of = np.zeros(nq, dtype=np.int64)
+    for r, (q0, q1) in enumerate(runs):
+        run_of[q0:q1] = r
+    NX, NY, NZ = blocks.NX, blocks.NY, blocks.NZ
+    qstride = {"cells": abi.N_EVOL_VARS * NX * NY * NZ, 0: (NX + 1) * NY * NZ, 1: NX * (NY + 1) * NZ,
+               2: NX * NY * (NZ + 1)}
+    run_maps = [dict() for _ in runs]
+    deps = [{r} for r in range(nruns)]
+    for key, m in maps.items():
+        dst_run = run_of[m["dst"] // qstride[key]]
+        used = np.arange(m["src"].shape[0])[:, None] < m["cnt"][None, :]
+        src_run = run_of[np.where(used, m["src"], 0) // qstride[key]]
+        for r in range(nruns):
+            sel = dst_run == r
+            run_maps[r][key] = {"cnt": np.ascontiguousarray(m["cnt"][sel]), "dst": np.ascontiguousarray(m["dst"][sel]),
+                                "src": np.ascontiguousarray(m["src"][:, sel]), "w": np.ascontiguousarray(m["w"][:, sel])}
+            deps[r] |= {int(x) for x in np.unique(src_run[:, sel][used[:, sel]])}
+    return runs, run_maps, deps
+
+
 class GRMHDEquationsSystem:
     """grmhd_equations_system_t<eos_t> + the evolve.cpp drivers, on the GPU."""
 
@@ -474,15 +504,16 @@ class GRMHDEquationsSystem:
 
     def fill_ghosts_gather(self, fields, maps, nvars=abi.N_HRSC, stream=None):
         """Ghost fill by gather maps (grb_fill_ghosts_gather).  maps: the dict
-        of grace_b200.fmr.Hierarchy.gather_maps (numpy), uploaded on first use
-        and kept by this object."""
+        of grace_b200.fmr.Hierarchy.gather_maps (numpy), or one run's part of
+        it (gather_runs), uploaded on first use and kept by this object."""
+        cache = self.__dict__.setdefault("_gmaps", {})
         key = id(maps)
-        if getattr(self, "_gmaps_key", None) != key:
+        if key not in cache:
             dev = self.blocks.device
             up = lambda m: {k: torch.from_numpy(np.ascontiguousarray(m[k])).to(dev) for k in ("cnt", "dst", "src", "w")}
-            self._gmaps = {k: up(v) for k, v in maps.items()}
-            self._gmaps_key = key
-        G = self._gmaps
+            # the maps object is kept with its upload, so its id stays its own
+            cache[key] = (maps, {k: up(v) for k, v in maps.items()})
+        G = cache[key][1]
         mk = lambda t: abi.Gather(t["dst"].numel(), t["cnt"].data_ptr(), t["dst"].data_ptr(), t["src"].data_ptr(),
                                   t["w"].data_ptr())
         cells = mk(G["cells"])
@@ -632,7 +663,7 @@ class GRMHDEquationsSystem:
         self.linop_apply(state_p, state, None, 1.0, 0.0, stream)
 
     def rk3_step_host(self, dt, host, state, state_p, state_pp, aux, bc, runs, fill_run, deps, t=0.0,
-                      streams=None, after=None, wait=True):
+                      streams=None, after=None, wait=True, whole_grid_substeps=False):
         """One SSP-RK3 step of a state held in packed pinned host arrays
         (packed_host_fields): upload, boundary fill and primitives of the
         uploaded state, the step, download — the same kernels in the same
@@ -666,7 +697,14 @@ class GRMHDEquationsSystem:
         between), each run's upload waits for that run's download only, so
         the uploads of a step overlap the last substep of the step before.
         The caller's stream waits for the download stream before it reads
-        host."""
+        host.
+
+        whole_grid_substeps=True (refluxing: its corrections couple blocks of
+        different runs): the first and last substeps run on the whole grid
+        too; the uploads then overlap the fills and primitives passes of the
+        runs before them, the downloads the primitives passes of the runs
+        after them (gather_runs gives runs, fill maps and deps for an FMR
+        hierarchy)."""
         main = torch.cuda.current_stream()
         up, down = streams if streams is not None else (torch.cuda.Stream(), torch.cuda.Stream())
         S = len(runs)
@@ -707,8 +745,11 @@ class GRMHDEquationsSystem:
                     self.compute_auxiliary_quantities(sv, a, main)
                     self.reset_c2p_diagnostics(a, main)
                     self.linop_apply(pv, sv, None, 1.0, 0.0, main)
-                    self.advance_substep(t, dt, 1.0, pv, sv, a, main)
+                    if not whole_grid_substeps:
+                        self.advance_substep(t, dt, 1.0, pv, sv, a, main)
                 ready.add(r)
+        if whole_grid_substeps:
+            self.advance_substep(t, dt, 1.0, state_p, state, aux, main)
         # middle substep on the whole grid
         bc(state_p)
         self.compute_auxiliary_quantities(state_p, aux, main)
@@ -722,10 +763,14 @@ class GRMHDEquationsSystem:
         # once the runs reading it are filled
         updated, filled, finished = set(), set(), set()
         ev_down = [None] * S
+        if whole_grid_substeps:
+            self.advance_substep(t, dt, 2.0 / 3.0, state, state_pp, aux, main)
+            updated = set(range(S))
         for s, (q0, q1) in enumerate(runs):
-            with self.block_range(q0, q1):
-                self.advance_substep(t, dt, 2.0 / 3.0, state.view(q0, q1), state_pp.view(q0, q1), aux[q0:q1],
-                                     main)
+            if not whole_grid_substeps:
+                with self.block_range(q0, q1):
+                    self.advance_substep(t, dt, 2.0 / 3.0, state.view(q0, q1), state_pp.view(q0, q1), aux[q0:q1],
+                                         main)
             updated.add(s)
             for r in range(S):
                 if r not in filled and deps[r] <= updated:

@@ -101,3 +101,29 @@ def test_gather_sources_are_interior(which):
     for key, m in H.gather_maps().items():
         used = np.arange(8)[:, None] < m["cnt"][None, :]
         assert not np.any(np.isin(m["src"][used], m["dst"])), key
+
+
+def test_gather_runs_partition_the_maps_and_name_their_sources():
+    """gather_runs: the runs' maps split every entry of the hierarchy's maps
+    by the run of its destination, and deps[r] holds the run of every
+    source block those entries read."""
+    from grace_b200.host import Blocks, gather_runs
+    H = workloads.tov_hierarchy(8)
+    maps = H.gather_maps()
+    blocks = Blocks(H.n, H.n, H.n, H.ngz, H.nq, H.idx(), device="cpu")
+    runs, run_maps, deps = gather_runs(maps, blocks, 6)
+    assert runs[0][0] == 0 and runs[-1][1] == H.nq and len(runs) == 6
+    NN = H.n + 2 * H.ngz
+    qs = {"cells": abi.N_EVOL_VARS * NN ** 3, 0: (NN + 1) * NN * NN, 1: (NN + 1) * NN * NN, 2: (NN + 1) * NN * NN}
+    for key, m in maps.items():
+        assert sum(rm[key]["dst"].size for rm in run_maps) == m["dst"].size
+        got = np.sort(np.concatenate([rm[key]["dst"] for rm in run_maps]))
+        np.testing.assert_array_equal(got, np.sort(m["dst"]))
+        for r, ((q0, q1), rm) in enumerate(zip(runs, run_maps)):
+            d = rm[key]["dst"] // qs[key]
+            assert np.all((d >= q0) & (d < q1))
+            used = np.arange(8)[:, None] < rm[key]["cnt"][None, :]
+            src_q = rm[key]["src"][used] // qs[key]
+            src_runs = {int(np.searchsorted([b for _, b in runs], q, side="right")) for q in np.unique(src_q)}
+            assert src_runs <= deps[r], (key, r)
+    assert any(len(d) > 1 for d in deps)

@@ -142,3 +142,61 @@ def test_gather_fill_matches_host_fill():
     H.fill_ghosts(st, bx, by, bz)
     for a, b in zip((f.state, f.bx, f.by, f.bz), (st, bx, by, bz)):
         assert np.array_equal(a.cpu().numpy(), b)
+
+
+@pytest.mark.parametrize("mode", [abi.MODE_PLAIN, abi.MODE_TUNED])
+def test_fmr_host_step_pipeline_matches_sequential(mode):
+    """rk3_step_host on the TOV hierarchy (refluxing, gather fill): runs of
+    blocks filled by their part of the gather maps, the substeps on the
+    whole grid, two chained steps; the same bits as the sequential host
+    round trip in the host arrays and every device array."""
+    from grace_b200.host import gather_runs
+    H, P, (st, bx, by, bz, aux) = _case("tov")
+    H.fill_ghosts(st, bx, by, bz)
+    R, maps, idx = H.reflux_lists(), H.gather_maps(), H.idx()
+    dt = 0.25 / idx[:, 0].max()
+    dev = torch.device("cuda:0")
+    Pg = abi.Params.from_buffer_copy(P)
+    if mode == abi.MODE_TUNED:
+        Pg.ranges = abi.RANGES_NEXT_STAGE
+    g = GRMHDEquationsSystem(Pg)
+    blocks = Blocks(H.n, H.n, H.n, H.ngz, H.nq, idx, device=dev)
+    g.reserve(blocks)
+    g.set_mode(mode)
+    g.set_reflux(R)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    st0 = Fields(T(st), T(bx), T(by), T(bz))
+    aux0 = T(aux)
+    g.compute_auxiliary_quantities(st0, aux0)
+    if mode == abi.MODE_TUNED:
+        g.set_static_metric(st0)
+        g.set_tuning(1, 1, 1, 1)
+    bc = lambda fl: g.fill_ghosts_gather(fl, maps)
+    runs, run_maps, deps = gather_runs(maps, blocks, 5)
+    fill_run = lambda fl, s, stream: g.fill_ghosts_gather(fl, run_maps[s], stream=stream)
+    io = (torch.cuda.Stream(), torch.cuda.Stream())
+    out = []
+    for piped in (False, True):
+        state, a = st0.clone(), aux0.clone()
+        sp, spp = state.clone(), state.clone()
+        host = g.packed_host_fields()
+        g.copy_evolved_packed(host, state, to_device=False)
+        prev = None
+        for _ in range(2):
+            if piped:
+                prev = g.rk3_step_host(dt, host, state, sp, spp, a, bc, runs, fill_run, deps, streams=io, after=prev,
+                                       wait=False, whole_grid_substeps=True)
+            else:
+                g.copy_evolved_packed(host, state, to_device=True)
+                bc(state)
+                g.compute_auxiliary_quantities(state, a)
+                g.linop_apply(sp, state, None, 1.0, 0.0)
+                g.rk3_step(dt, state, sp, spp, a, bc)
+                g.copy_evolved_packed(host, state, to_device=False)
+        torch.cuda.current_stream().wait_stream(io[1])
+        torch.cuda.synchronize()
+        out.append([x.clone() for x in (host.state, host.bx, host.by, host.bz, state.state, state.bx, state.by,
+                                         state.bz, sp.state, a)])
+    for k, (x, y) in enumerate(zip(*out)):
+        assert torch.equal(x, y), k
+    assert g.status().device_flags == 0
